@@ -1,0 +1,355 @@
+"""Benchmark of the packed strand generator on B200.
+
+Workload (per GPU): the single large description -- displaced sphere with
+200,000 triangles, 4,096 guides of 32 CVs, 8-guide stencils, 1,000,000
+strands x 32 points, taper 0.02 -> 0.002, noise 0.2 at frequency 12 --
+written as float4(position, radius) plus point counts, roots and root UVs,
+the outputs of the reference's generate_packed_cpu (asset.cpp:412-449).
+
+A step is one generation of that workload with inputs resident in HBM.
+The L2 is flushed (a 256 MiB write) between timed steps.  With N GPUs each
+rank generates its own 1,000,000-strand range of an N x 1,000,000-strand
+description (weak scaling; strands are independent, so there is no
+collective on the data path).
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+STRANDS_PER_GPU = 1_000_000
+FALLBACK_HBM_GBS = 6650.0
+KERNELS_PER_STEP = 4  # strand_keys, exclusive_scan, scatter_order, generate
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["nxg", "reference"], default="nxg")
+    ap.add_argument("--strands", type=int, default=STRANDS_PER_GPU, help="strands per GPU")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU-baseline budget")
+    return ap.parse_args()
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except (OSError, ValueError, KeyError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def profile_traffic_per_point():
+    """DRAM bytes per generated point of the generate kernel, from the ncu
+    summary committed under profiles/ (None until one exists)."""
+    path = os.path.join(ROOT, "profiles", "generate_kernel_large_sphere.md")
+    try:
+        with open(path) as fh:
+            m = re.search(r"traffic_bytes_per_point:\s*([0-9.eE+-]+)", fh.read())
+            return float(m.group(1)) if m else None
+    except OSError:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=10)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def workload(strands_total: int):
+    from nanoxgen_b200 import fixtures
+    w = fixtures.large_sphere(strands=strands_total)
+    return w
+
+
+def cpu_baseline(asset, params, seconds: float):
+    """The reference's generate_packed_cpu (oracle/_ref) on all host cores over
+    a bounded prefix sample of the workload's strands; the C restatement of
+    the oracle when the reference library is absent."""
+    cores = os.cpu_count() or 1
+    try:
+        from oracle.checker import Reference, reference_available
+        if not reference_available():
+            raise FileNotFoundError
+        ref = Reference()
+        handle = ref.handle(asset.buffer)
+        kind = "reference"
+
+        def run(n):
+            p = params.copy(strand_count=n)
+            t0 = time.perf_counter()
+            ref.generate(handle, p, 1.0, workers=cores, want_output=False)
+            return time.perf_counter() - t0
+    except (FileNotFoundError, OSError):
+        from oracle.checker import Oracle
+        orc = Oracle()
+        kind = "port"
+
+        def run(n):
+            t0 = time.perf_counter()
+            orc.generate(asset.buffer, params.copy(strand_count=n), 1.0, count=n, threads=cores)
+            return time.perf_counter() - t0
+    P = int(params.cvs_per_strand)
+    probe = 20_000
+    t = run(probe)
+    per_strand = t / probe
+    reps = 3
+    n = int(min(params.strand_count, max(probe, seconds / reps / max(per_strand, 1e-9))))
+    times = [run(n) for _ in range(reps)]
+    med = statistics.median(times)
+    return {"value": n * P / med, "unit": "points/s", "cores": cores, "kind": kind,
+            "sample": "first %d strands x %d CVs of the workload (median of %d calls, %.2f s each; "
+                      "includes the reference's per-call asset validation)" % (n, P, reps, med)}
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from nanoxgen_b200.asset import build_asset
+    w = workload(args.strands)
+    asset = build_asset(w.build_input, w.stencil_slots)
+    cores = os.cpu_count() or 1
+    P = int(w.params.cvs_per_strand)
+    from oracle.checker import Oracle, Reference, reference_available
+    if reference_available():
+        ref = Reference()
+        handle = ref.handle(asset.buffer)
+        kind = "reference"
+
+        def run(n):
+            t0 = time.perf_counter()
+            ref.generate(handle, w.params.copy(strand_count=n), 1.0, workers=cores, want_output=False)
+            return time.perf_counter() - t0
+    else:
+        orc = Oracle()
+        kind = "port"
+
+        def run(n):
+            t0 = time.perf_counter()
+            orc.generate(asset.buffer, w.params.copy(strand_count=n), 1.0, count=n, threads=cores)
+            return time.perf_counter() - t0
+    per = run(20_000) / 20_000
+    budget = 90.0 / max(1, args.steps + args.warmup)
+    n = int(min(w.params.strand_count, max(20_000, min(2.0, budget) / max(per, 1e-9))))
+    for _ in range(args.warmup):
+        run(n)
+    times = [run(n) for _ in range(args.steps)]
+    total = sum(times)
+    value = args.steps * n * P / total
+    line = {"metric": "points/sec", "value": value, "unit": "points/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": w.name, "strands_per_step": n, "cvs_per_strand": P,
+                       "note": "generate_packed_cpu on the host cores over a prefix sample of the workload"},
+            "cpu_baseline": {"value": value, "unit": "points/s", "cores": cores, "kind": kind,
+                             "sample": "first %d strands x %d CVs per step" % (n, P)},
+            "e2e": {"value": value, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_gpu_arm(args):
+    import torch
+    import torch.distributed as dist
+
+    from nanoxgen_b200.asset import build_asset
+    from nanoxgen_b200.generator import (DeviceAsset, HostPipeline, allocate_outputs, generate_packed_ordered,
+                                         prepare_strand_order)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=device)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    S = args.strands
+    w = workload(S * world)
+    params = w.params
+    first = rank * S
+    P = int(params.cvs_per_strand)
+    asset = build_asset(w.build_input, w.stencil_slots)
+    dasset = DeviceAsset(asset, device)
+    points, roots, uvs, counts = allocate_outputs(S, P, device)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=device)
+    stream = torch.cuda.current_stream(device)
+
+    def step(ev=None):
+        ws = prepare_strand_order(dasset, params, first, S, stream=stream)
+        if ev is not None:
+            ev.record(stream)
+        generate_packed_ordered(dasset, params, points, roots, uvs, counts, 1.0, None, first, S, ws, stream=stream)
+
+    for _ in range(args.warmup):
+        flush.fill_(1)
+        step()
+    torch.cuda.synchronize(device)
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    barrier()
+    torch.cuda.synchronize(device)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+           torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for k in range(args.steps):
+        flush.fill_(k & 0xFF)
+        ev[k][0].record(stream)
+        step(ev[k][1])
+        ev[k][2].record(stream)
+    torch.cuda.synchronize(device)
+    barrier()
+    step_ms = [a.elapsed_time(c) for a, b, c in ev]
+    kern_ms = [b.elapsed_time(c) for a, b, c in ev]
+    total_ms = max_over_ranks(sum(step_ms))
+    kernel_ms = max_over_ranks(statistics.mean(kern_ms))
+
+    e2e = None
+    if not args.no_e2e:
+        pipe = HostPipeline(asset, params, 1.0, chunks=8, device=device, first_strand=first, count=S)
+        for _ in range(max(1, min(args.warmup, 3))):
+            pipe.run()
+        torch.cuda.synchronize(device)
+        barrier()
+        torch.cuda.synchronize(device)
+        e_start, e_stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e_start.record(pipe.compute)
+        for _ in range(args.steps):
+            pipe.run()
+        pipe.compute.wait_stream(pipe.copy)
+        e_stop.record(pipe.compute)
+        torch.cuda.synchronize(device)
+        barrier()
+        e2e_ms = max_over_ranks(e_start.elapsed_time(e_stop))
+        pts = pipe.host_points.numpy()
+        assert pts.shape[0] == S * P and float(abs(pts[:, 3]).max()) > 0.0
+        e2e = {"value": world * S * P * args.steps / (e2e_ms / 1e3), "unit": "points/s",
+               "h2d_bytes_per_step": pipe.h2d_bytes, "d2h_bytes_per_step": pipe.d2h_bytes,
+               "ms_per_step": e2e_ms / args.steps,
+               "path": "HostPipeline: pinned asset upload, nxg_generate_packed_range in 8 ranges, "
+                       "overlapped D2H of points/roots/root_uvs/point_counts to pinned host arrays"}
+    clocks = sampler.stop()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(asset, params.copy(strand_count=S), args.cpu_seconds)
+
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+
+    ms_per_step = total_ms / args.steps
+    points_total = world * S * P
+    out_bytes = S * P * 16 + S * (48 + 8 + 4)
+    alg_bytes = out_bytes + asset.nbytes
+    peak, peak_kind = measured_peak()
+    achieved = alg_bytes / (kernel_ms / 1e3) / 1e9
+    tpp = profile_traffic_per_point()
+    line = {
+        "metric": "points/sec", "value": points_total / (ms_per_step / 1e3), "unit": "points/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": w.name, "triangles": int(asset.header.triangle_count),
+                   "guides": int(asset.header.guide_count), "stencil_slots": w.stencil_slots,
+                   "strands_per_gpu": S, "cvs_per_strand": P, "noise_amplitude": params.noise_amplitude,
+                   "noise_frequency": params.noise_frequency, "outputs": "points,roots,root_uvs,point_counts",
+                   "l2": "flushed between timed steps (256 MiB write); outputs 572 MB > L2",
+                   "parallelism": "strand ranges per GPU (no collective)"},
+        "hbm_gbs": world * alg_bytes / (ms_per_step / 1e3) / 1e9,
+        "roofline": {"bound": "hbm", "kernel": "generate_kernel<32,1,noise>", "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                     "traffic": (tpp * S * P) if tpp else None,
+                     "algorithmic_bytes": alg_bytes, "kernel_ms": kernel_ms,
+                     "note": "algorithmic bytes = 16 B/point + 60 B/strand (roots, root UVs, counts) + asset"},
+        "clocks": clocks, "gpu_launches": KERNELS_PER_STEP * args.steps,
+    }
+    if e2e:
+        line["e2e"] = e2e
+    if cpu:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_gpu_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,187 @@
+"""Seeded synthetic workloads with the shapes of the benchmark configurations.
+
+No production grooming assets are available, so these generators stand in
+for them: UV spheres (optionally displaced), guides rooted at seeded
+area-weighted surface points with CVs along the surface normal, and the
+generation parameters each configuration names.  Everything is derived from
+fixed seeds with numpy's PCG64, so a workload is reproducible on any host.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+from typing import Callable, Optional
+
+import numpy as np
+
+from ._abi import INVALID_INDEX, GenerationParams
+from .asset import AssetBuildInput, GuideSet
+
+
+def sphere_mesh(n_lon: int, n_rings: int,
+                radius: Optional[Callable[[np.ndarray, np.ndarray], np.ndarray]] = None):
+    """UV sphere: `n_rings` vertex rings pole to pole (n_rings-1 bands), `n_lon`
+    segments, a duplicated seam column for continuous UVs, 2*n_lon*(n_rings-1)
+    triangles wound outward.  Returns (positions, texcoords, triangles)."""
+    j = np.arange(n_rings, dtype=np.float64)
+    i = np.arange(n_lon + 1, dtype=np.float64)
+    theta = (math.pi * j / (n_rings - 1))[:, None] * np.ones((1, n_lon + 1))
+    phi = np.ones((n_rings, 1)) * (2.0 * math.pi * i / n_lon)[None, :]
+    r = np.ones_like(theta) if radius is None else radius(theta, phi)
+    pos = np.stack([r * np.sin(theta) * np.cos(phi), r * np.cos(theta), r * np.sin(theta) * np.sin(phi)], -1)
+    uv = np.stack([np.broadcast_to(i[None, :] / n_lon, theta.shape), np.broadcast_to(j[:, None] / (n_rings - 1), theta.shape)], -1)
+    cols = n_lon + 1
+    jj, ii = np.meshgrid(np.arange(n_rings - 1), np.arange(n_lon), indexing="ij")
+    v00 = jj * cols + ii
+    v01 = v00 + 1
+    v10 = v00 + cols
+    v11 = v10 + 1
+    tris = np.stack([np.stack([v00, v01, v11], -1), np.stack([v00, v11, v10], -1)], axis=2).reshape(-1, 3)
+    return (pos.reshape(-1, 3).astype(np.float32), uv.reshape(-1, 2).astype(np.float32),
+            tris.astype(np.uint32))
+
+
+def vertex_normals(positions: np.ndarray, triangles: np.ndarray) -> np.ndarray:
+    p = positions.astype(np.float64)
+    t = triangles.astype(np.int64)
+    n = np.cross(p[t[:, 1]] - p[t[:, 0]], p[t[:, 2]] - p[t[:, 0]])
+    acc = np.zeros_like(p)
+    for k in range(3):
+        np.add.at(acc, t[:, k], n)
+    length = np.linalg.norm(acc, axis=1, keepdims=True)
+    acc = np.where(length > 1e-30, acc / np.maximum(length, 1e-30), np.array([0.0, 1.0, 0.0]))
+    return acc.astype(np.float32)
+
+
+def triangle_areas(positions: np.ndarray, triangles: np.ndarray) -> np.ndarray:
+    p = positions.astype(np.float64)
+    t = triangles.astype(np.int64)
+    return 0.5 * np.linalg.norm(np.cross(p[t[:, 1]] - p[t[:, 0]], p[t[:, 2]] - p[t[:, 0]]), axis=1)
+
+
+def surface_guides(positions, triangles, count, cvs, rng, length=(0.3, 0.6), jitter=0.02,
+                   texcoords=None) -> GuideSet:
+    """`count` guides rooted at area-weighted random surface points, each with
+    `cvs` CVs running along the interpolated vertex normal for a length drawn
+    from U(length), plus N(0, jitter) per-component jitter on CVs 1.."""
+    areas = triangle_areas(positions, triangles)
+    tri = rng.choice(triangles.shape[0], size=count, p=areas / areas.sum()).astype(np.int64)
+    r1 = rng.random(count)
+    r2 = rng.random(count)
+    s = np.sqrt(r1)
+    b = np.stack([1.0 - s, s * (1.0 - r2), s * r2], 1)
+    t = triangles[tri].astype(np.int64)
+    p = positions.astype(np.float64)
+    root = (p[t[:, 0]] * b[:, :1] + p[t[:, 1]] * b[:, 1:2] + p[t[:, 2]] * b[:, 2:3])
+    vn = vertex_normals(positions, triangles).astype(np.float64)
+    nrm = vn[t[:, 0]] * b[:, :1] + vn[t[:, 1]] * b[:, 1:2] + vn[t[:, 2]] * b[:, 2:3]
+    nrm /= np.maximum(np.linalg.norm(nrm, axis=1, keepdims=True), 1e-30)
+    lengths = rng.uniform(length[0], length[1], size=count)
+    steps = np.linspace(0.0, 1.0, cvs)
+    curve = root[:, None, :] + nrm[:, None, :] * (lengths[:, None, None] * steps[None, :, None])
+    noise = rng.normal(0.0, jitter, size=curve.shape)
+    noise[:, 0, :] = 0.0
+    curve = (curve + noise).astype(np.float32)
+    curve[:, 0, :] = root.astype(np.float32)
+    uv = np.zeros((count, 2), np.float32)
+    if texcoords is not None:
+        tc = texcoords.astype(np.float64)
+        uv = (tc[t[:, 0]] * b[:, :1] + tc[t[:, 1]] * b[:, 1:2] + tc[t[:, 2]] * b[:, 2:3]).astype(np.float32)
+    return GuideSet(cv_counts=np.full(count, cvs, np.uint32), cvs=curve.reshape(-1, 3),
+                    root_normals=nrm.astype(np.float32), root_uvs=uv, triangles=tri.astype(np.uint32),
+                    barycentrics=b[:, 1:].astype(np.float32), support_radii=np.zeros(count, np.float32))
+
+
+@dataclasses.dataclass
+class Workload:
+    name: str
+    build_input: AssetBuildInput
+    stencil_slots: int
+    params: GenerationParams
+    radius_scale: float = 1.0
+    note: str = ""
+
+    @property
+    def points(self) -> int:
+        return int(self.params.strand_count) * int(self.params.cvs_per_strand)
+
+
+def plain_sphere(strands: int = 10_000, cvs: int = 16, seed: int = 2024) -> Workload:
+    """Plain method, CPU-runnable size: unit UV sphere with 2,048 triangles
+    (32 segments x 33 rings), 64 guides of 16 CVs, 4-guide stencils,
+    10,000 strands x 16 points, taper 0.01 -> 0.001, noise 0.1 at frequency 8."""
+    rng = np.random.default_rng(seed)
+    pos, uv, tris = sphere_mesh(32, 33)
+    guides = surface_guides(pos, tris, 64, 16, rng, texcoords=uv)
+    params = GenerationParams(strand_count=strands, cvs_per_strand=cvs, seed=7, root_width=0.01,
+                              tip_width=0.001, noise_amplitude=0.1, noise_frequency=8.0)
+    return Workload("uv-sphere-2k-tris/64-guides/k4/10k-strands-x16", AssetBuildInput(pos, tris, guides, None, uv),
+                    4, params)
+
+
+def displaced_sphere_radius(theta, phi):
+    return 1.0 + 0.05 * np.sin(7.0 * theta) * np.sin(5.0 * phi)
+
+
+def large_sphere(strands: int = 1_000_000, cvs: int = 32, guides: int = 4096, seed: int = 2025,
+                 n_lon: int = 400, n_rings: int = 251) -> Workload:
+    """Single large description: displaced sphere (200,000 triangles, radial
+    displacement 0.05 sin(7 theta) sin(5 phi)), 4,096 guides of 32 CVs,
+    8-guide stencils, 1,000,000 strands x 32 points, taper 0.02 -> 0.002,
+    noise 0.2 at frequency 12 (output 32M float4 = 512 MiB)."""
+    rng = np.random.default_rng(seed)
+    pos, uv, tris = sphere_mesh(n_lon, n_rings, displaced_sphere_radius)
+    gs = surface_guides(pos, tris, guides, 32, rng, texcoords=uv)
+    params = GenerationParams(strand_count=strands, cvs_per_strand=cvs, seed=11, root_width=0.02,
+                              tip_width=0.002, noise_amplitude=0.2, noise_frequency=12.0)
+    name = "displaced-sphere-%dk-tris/%d-guides/k8/%d-strands-x%d" % (tris.shape[0] // 1000, guides, strands, cvs)
+    return Workload(name, AssetBuildInput(pos, tris, gs, None, uv), 8, params)
+
+
+def reference_unit_fixture() -> AssetBuildInput:
+    """The one-triangle, one-guide asset the reference's unit tests use
+    (tests/test_main.cpp:39-53)."""
+    pos = np.array([[0, 0, 0], [1, 0, 0], [0, 0, 1]], np.float32)
+    nrm = np.array([[0, 1, 0]] * 3, np.float32)
+    uv = np.array([[0, 0], [1, 0], [0, 1]], np.float32)
+    tris = np.array([[0, 1, 2]], np.uint32)
+    guides = GuideSet(cv_counts=np.array([3], np.uint32),
+                      cvs=np.array([[0.25, 0.0, 0.25], [0.25, 0.5, 0.25], [0.5, 1.0, 0.25]], np.float32),
+                      root_normals=np.array([[0, 1, 0]], np.float32), root_uvs=np.zeros((1, 2), np.float32),
+                      triangles=np.array([0], np.uint32), barycentrics=np.array([[0.25, 0.25]], np.float32),
+                      support_radii=np.array([10.0], np.float32))
+    return AssetBuildInput(pos, tris, guides, nrm, uv)
+
+
+def reference_area_fixture() -> AssetBuildInput:
+    """Two triangles with areas 1.0 and 0.5 and one guide
+    (tests/test_main.cpp:309-321)."""
+    pos = np.array([[0, 0, 0], [2, 0, 0], [0, 0, 1], [10, 0, 0], [11, 0, 0], [10, 0, 1]], np.float32)
+    nrm = np.array([[0, 1, 0]] * 6, np.float32)
+    tris = np.array([[0, 1, 2], [3, 4, 5]], np.uint32)
+    guides = GuideSet(cv_counts=np.array([2], np.uint32), cvs=np.array([[0, 0, 0], [0, 1, 0]], np.float32),
+                      root_normals=np.array([[0, 1, 0]], np.float32), root_uvs=np.zeros((1, 2), np.float32),
+                      triangles=np.array([INVALID_INDEX], np.uint32), barycentrics=np.zeros((1, 2), np.float32),
+                      support_radii=np.array([100.0], np.float32))
+    return AssetBuildInput(pos, tris, guides, nrm, None)
+
+
+def reference_benchmark_fixture() -> AssetBuildInput:
+    """The reference benchmark's 10x10 quad with four 8-CV guides
+    (tools/benchmark.cpp:22-41)."""
+    pos = np.array([[-5, 0, -5], [5, 0, -5], [5, 0, 5], [-5, 0, 5]], np.float32)
+    nrm = np.array([[0, 1, 0]] * 4, np.float32)
+    uv = np.array([[0, 0], [1, 0], [1, 1], [0, 1]], np.float32)
+    tris = np.array([[0, 1, 2], [0, 2, 3]], np.uint32)
+    roots = np.array([[-4, 0, -4], [4, 0, -4], [4, 0, 4], [-4, 0, 4]], np.float32)
+    t = (np.arange(8, dtype=np.float32) / np.float32(7.0)).astype(np.float32)
+    cvs = []
+    for root in roots:
+        for tv in t:
+            cvs.append(root + np.array([np.float32(0.15) * tv * tv, np.float32(1.0) * tv,
+                                        np.float32(0.08) * tv * tv], np.float32))
+    guides = GuideSet(cv_counts=np.full(4, 8, np.uint32), cvs=np.array(cvs, np.float32),
+                      root_normals=np.array([[0, 1, 0]] * 4, np.float32), root_uvs=np.zeros((4, 2), np.float32),
+                      triangles=np.full(4, INVALID_INDEX, np.uint32), barycentrics=np.zeros((4, 2), np.float32),
+                      support_radii=np.full(4, 12.0, np.float32))
+    return AssetBuildInput(pos, tris, guides, nrm, uv)

@@ -1,0 +1,251 @@
+"""Python access to the test-only checkers.
+
+TEST INFRASTRUCTURE ONLY.  Loads oracle/liboracle.so (the C restatement in
+nxg_oracle.c) and, where it was built, oracle/_ref/libnxg_ref.so (the
+reference's own src/asset.cpp behind ref_shim.cpp).  Only tests/,
+__graft_entry__.smoke() and bench.py's CPU legs may import this module.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_PATH = os.path.join(HERE, "liboracle.so")
+REF_PATH = os.path.join(HERE, "_ref", "libnxg_ref.so")
+
+ROOT_DTYPE = np.dtype([("position", "<f4", 3), ("normal", "<f4", 3), ("uv", "<f4", 2),
+                       ("triangle_index", "<u4"), ("barycentric", "<f4", 2), ("surface_face_id", "<u4")])
+# StrandState of nxg_oracle.c / RefStrandState of ref_shim.cpp (156 bytes).
+STATE_DTYPE = np.dtype([("root", ROOT_DTYPE), ("indices", "<u4", 8), ("weights", "<f4", 8),
+                        ("weight_sum", "<f4"), ("nearest", "<u4"), ("surface_u", "<f4", 3),
+                        ("noise_domain", "<f4", 3), ("original_length", "<f4"),
+                        ("effective_noise_frequency", "<f4"), ("preserve_scale", "<f4")])
+assert ROOT_DTYPE.itemsize == 48 and STATE_DTYPE.itemsize == 156
+
+_P = ctypes.c_void_p
+
+
+def _ensure_built(path: str, target: str) -> None:
+    if not os.path.exists(path):
+        subprocess.check_call(["make", "-s", "-C", HERE, target])
+
+
+def _aligned(nbytes: int) -> np.ndarray:
+    raw = np.empty(nbytes + 64, np.uint8)
+    off = (-raw.ctypes.data) % 64
+    return raw[off:off + nbytes]
+
+
+def as_aligned_blob(data) -> np.ndarray:
+    src = np.frombuffer(bytes(data), np.uint8) if not isinstance(data, np.ndarray) else data.view(np.uint8)
+    if src.ctypes.data % 64 == 0:
+        return src
+    buf = _aligned(src.size)
+    buf[:] = src
+    return buf
+
+
+def _vec_ptr(a: Optional[np.ndarray]):
+    return None if a is None else np.ascontiguousarray(a, np.float32).ctypes.data
+
+
+class Oracle:
+    """The C restatement of generate.h / asset.cpp (nxg_oracle.c)."""
+
+    def __init__(self):
+        _ensure_built(ORACLE_PATH, "oracle")
+        lib = ctypes.CDLL(ORACLE_PATH)
+        lib.orc_random01.restype = ctypes.c_float
+        lib.orc_random01.argtypes = [ctypes.c_uint32] * 3
+        lib.orc_gradient_noise.restype = ctypes.c_float
+        lib.orc_gradient_noise.argtypes = [_P, ctypes.c_float, ctypes.c_float, ctypes.c_float]
+        lib.orc_noise_hash.restype = ctypes.c_uint32
+        lib.orc_noise_hash.argtypes = [ctypes.c_int32] * 3
+        lib.orc_strand_state.restype = None
+        lib.orc_strand_state.argtypes = [_P, _P, _P, _P, _P, ctypes.c_uint32, _P]
+        lib.orc_fnv1a.restype = ctypes.c_uint64
+        lib.orc_fnv1a.argtypes = [_P, ctypes.c_uint64]
+        lib.orc_validate_asset.restype = ctypes.c_int
+        lib.orc_validate_asset.argtypes = [_P, ctypes.c_uint64, ctypes.c_char_p, ctypes.c_uint64]
+        lib.orc_generate_packed.restype = ctypes.c_int
+        lib.orc_generate_packed.argtypes = [_P, _P, ctypes.c_float, _P, _P, _P, _P, ctypes.c_uint32,
+                                            ctypes.c_uint32, _P, _P, _P, _P, ctypes.c_int]
+        self.lib = lib
+
+    def generate(self, blob, params, radius_scale: float = 1.0, positions=None, normals=None, guide_cvs=None,
+                 strands=None, first: int = 0, count: Optional[int] = None, threads: int = 1):
+        """Packed generation of the listed strands (or first..first+count-1)."""
+        blob = as_aligned_blob(blob)
+        P = int(params.cvs_per_strand)
+        if strands is not None:
+            ids = np.ascontiguousarray(strands, np.uint32)
+            n = ids.size
+        else:
+            ids = None
+            n = int(params.strand_count) - first if count is None else int(count)
+        points = np.zeros((n * P, 4), np.float32)
+        roots = np.zeros(n, ROOT_DTYPE)
+        uvs = np.zeros((n, 2), np.float32)
+        counts = np.zeros(n, np.uint32)
+        keep = [np.ascontiguousarray(a, np.float32) if a is not None else None for a in (positions, normals, guide_cvs)]
+        rc = self.lib.orc_generate_packed(
+            blob.ctypes.data, ctypes.byref(params), radius_scale,
+            *(k.ctypes.data if k is not None else None for k in keep),
+            ids.ctypes.data if ids is not None else None, first, n,
+            points.ctypes.data, roots.ctypes.data, uvs.ctypes.data, counts.ctypes.data, threads)
+        assert rc == 0
+        return points, roots, uvs, counts
+
+    def strand_state(self, blob, params, strand: int, positions=None, normals=None, guide_cvs=None) -> np.ndarray:
+        blob = as_aligned_blob(blob)
+        out = np.zeros(1, STATE_DTYPE)
+        keep = [np.ascontiguousarray(a, np.float32) if a is not None else None for a in (positions, normals, guide_cvs)]
+        self.lib.orc_strand_state(blob.ctypes.data, *(k.ctypes.data if k is not None else None for k in keep),
+                                  ctypes.byref(params), strand, out.ctypes.data)
+        return out[0]
+
+    def gradient_noise(self, blob, x: float, y: float, z: float) -> float:
+        blob = as_aligned_blob(blob)
+        return float(self.lib.orc_gradient_noise(blob.ctypes.data, x, y, z))
+
+    def noise_hash(self, x: int, y: int, z: int) -> int:
+        return int(self.lib.orc_noise_hash(x, y, z))
+
+    def random01(self, seed: int, strand: int, dim: int) -> float:
+        return float(self.lib.orc_random01(seed, strand, dim))
+
+    def validate_asset(self, blob) -> str:
+        blob = as_aligned_blob(blob)
+        msg = ctypes.create_string_buffer(256)
+        self.lib.orc_validate_asset(blob.ctypes.data, blob.size, msg, 256)
+        return msg.value.decode()
+
+
+def reference_available() -> bool:
+    if os.path.exists(REF_PATH):
+        return True
+    ref = os.environ.get("NXG_REFERENCE_ROOT", "/root/reference")
+    if os.path.isfile(os.path.join(ref, "src", "asset.cpp")):
+        subprocess.check_call(["make", "-s", "-C", HERE, "ref", "REF=" + ref])
+        return os.path.exists(REF_PATH)
+    return False
+
+
+class Reference:
+    """The reference's own CPU implementation (oracle/_ref/libnxg_ref.so)."""
+
+    def __init__(self):
+        if not reference_available():
+            raise FileNotFoundError("oracle/_ref/libnxg_ref.so is not built and the reference checkout is absent")
+        lib = ctypes.CDLL(REF_PATH)
+        lib.ref_build_asset.restype = ctypes.c_int
+        lib.ref_build_asset.argtypes = [_P, ctypes.c_uint32, _P, _P, _P, ctypes.c_uint32, ctypes.c_uint32,
+                                        _P, _P, _P, _P, _P, _P, _P, ctypes.POINTER(ctypes.c_void_p),
+                                        ctypes.POINTER(ctypes.c_uint64), ctypes.c_char_p, ctypes.c_uint64]
+        lib.ref_free.argtypes = [_P]
+        lib.ref_validate_asset.restype = ctypes.c_int
+        lib.ref_validate_asset.argtypes = [_P, ctypes.c_uint64, ctypes.c_char_p, ctypes.c_uint64]
+        lib.ref_asset_create.restype = _P
+        lib.ref_asset_create.argtypes = [_P, ctypes.c_uint64]
+        lib.ref_asset_destroy.argtypes = [_P]
+        lib.ref_generate_packed.restype = ctypes.c_int
+        lib.ref_generate_packed.argtypes = [_P, _P, ctypes.c_float, ctypes.c_uint32, ctypes.c_uint32,
+                                            _P, ctypes.c_uint64, _P, ctypes.c_uint64, _P, ctypes.c_uint64,
+                                            _P, _P, _P, _P, ctypes.POINTER(ctypes.c_double), ctypes.c_char_p,
+                                            ctypes.c_uint64]
+        lib.ref_strand_state.argtypes = [_P, _P, _P, _P, _P, ctypes.c_uint32, _P]
+        lib.ref_gradient_noise.restype = ctypes.c_float
+        lib.ref_gradient_noise.argtypes = [_P, ctypes.c_float, ctypes.c_float, ctypes.c_float]
+        lib.ref_validate_packed_request.restype = ctypes.c_uint32
+        lib.ref_validate_packed_request.argtypes = [_P, _P, ctypes.c_uint64, _P, ctypes.c_uint64, _P,
+                                                    ctypes.c_uint64, _P, ctypes.c_uint64, _P, _P, _P, _P,
+                                                    ctypes.c_float, _P, ctypes.c_uint64, ctypes.c_uint64,
+                                                    ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32]
+        lib.ref_validate_motion_request.restype = ctypes.c_uint32
+        lib.ref_validate_motion_request.argtypes = [_P, _P, ctypes.c_uint64, _P, ctypes.c_uint32, _P, _P,
+                                                    ctypes.c_uint64, ctypes.c_uint32]
+        lib.ref_error_message.restype = ctypes.c_char_p
+        lib.ref_error_message.argtypes = [ctypes.c_uint32]
+        self.lib = lib
+
+    def build_asset(self, src) -> np.ndarray:
+        """asset.h:119 build_asset on an nanoxgen_b200.asset.AssetBuildInput."""
+        g = src.guides
+        arrs = dict(
+            positions=np.ascontiguousarray(src.positions, np.float32),
+            normals=None if src.normals is None else np.ascontiguousarray(src.normals, np.float32),
+            texcoords=None if src.texcoords is None else np.ascontiguousarray(src.texcoords, np.float32),
+            triangles=np.ascontiguousarray(src.triangles, np.uint32),
+            counts=np.ascontiguousarray(g.cv_counts, np.uint32), cvs=np.ascontiguousarray(g.cvs, np.float32),
+            rn=np.ascontiguousarray(g.root_normals, np.float32), ruv=np.ascontiguousarray(g.root_uvs, np.float32),
+            gt=np.ascontiguousarray(g.triangles, np.uint32), gb=np.ascontiguousarray(g.barycentrics, np.float32),
+            gr=np.ascontiguousarray(g.support_radii, np.float32))
+        out = ctypes.c_void_p()
+        size = ctypes.c_uint64()
+        msg = ctypes.create_string_buffer(256)
+        p = lambda a: None if a is None else a.ctypes.data
+        rc = self.lib.ref_build_asset(p(arrs["positions"]), arrs["positions"].shape[0], p(arrs["normals"]),
+                                      p(arrs["texcoords"]), p(arrs["triangles"]), arrs["triangles"].shape[0],
+                                      arrs["counts"].size, p(arrs["counts"]), p(arrs["cvs"]), p(arrs["rn"]),
+                                      p(arrs["ruv"]), p(arrs["gt"]), p(arrs["gb"]), p(arrs["gr"]),
+                                      ctypes.byref(out), ctypes.byref(size), msg, 256)
+        if rc != 0:
+            raise ValueError(msg.value.decode())
+        data = ctypes.string_at(out, size.value)
+        self.lib.ref_free(out)
+        return as_aligned_blob(data)
+
+    def validate_asset(self, blob) -> str:
+        blob = as_aligned_blob(blob)
+        msg = ctypes.create_string_buffer(256)
+        self.lib.ref_validate_asset(blob.ctypes.data, blob.size, msg, 256)
+        return msg.value.decode()
+
+    class Handle:
+        def __init__(self, ref, blob):
+            self.ref = ref
+            blob = as_aligned_blob(blob)
+            self.ptr = ref.lib.ref_asset_create(blob.ctypes.data, blob.size)
+
+        def __del__(self):
+            if getattr(self, "ptr", None):
+                self.ref.lib.ref_asset_destroy(self.ptr)
+                self.ptr = None
+
+    def handle(self, blob) -> "Reference.Handle":
+        return Reference.Handle(self, blob)
+
+    def generate(self, handle, params, radius_scale: float = 1.0, workers: int = 1, tile: int = 128,
+                 positions=None, normals=None, guide_cvs=None, want_output: bool = True):
+        """generate_packed_deformed_cpu; returns (points, roots, uvs, counts, ms)."""
+        S, P = int(params.strand_count), int(params.cvs_per_strand)
+        points = np.zeros((S * P, 4), np.float32) if want_output else None
+        roots = np.zeros(S, ROOT_DTYPE) if want_output else None
+        uvs = np.zeros((S, 2), np.float32) if want_output else None
+        counts = np.zeros(S, np.uint32) if want_output else None
+        keep = [np.ascontiguousarray(a, np.float32) if a is not None else None for a in (positions, normals, guide_cvs)]
+        n = [0 if k is None else k.size // 3 for k in keep]
+        ms = ctypes.c_double()
+        msg = ctypes.create_string_buffer(256)
+        p = lambda a: None if a is None else a.ctypes.data
+        rc = self.lib.ref_generate_packed(handle.ptr, ctypes.byref(params), radius_scale, workers, tile,
+                                          p(keep[0]), n[0], p(keep[1]), n[1], p(keep[2]), n[2],
+                                          p(points), p(roots), p(uvs), p(counts), ctypes.byref(ms), msg, 256)
+        if rc != 0:
+            raise ValueError(msg.value.decode())
+        return points, roots, uvs, counts, ms.value
+
+    def strand_state(self, handle, params, strand: int, positions=None, normals=None, guide_cvs=None):
+        out = np.zeros(1, STATE_DTYPE)
+        keep = [np.ascontiguousarray(a, np.float32) if a is not None else None for a in (positions, normals, guide_cvs)]
+        self.lib.ref_strand_state(handle.ptr, *(k.ctypes.data if k is not None else None for k in keep),
+                                  ctypes.byref(params), strand, out.ctypes.data)
+        return out[0]
+
+    def gradient_noise(self, handle, x, y, z) -> float:
+        return float(self.lib.ref_gradient_noise(handle.ptr, x, y, z))

@@ -1,0 +1,245 @@
+"""Parity of the CUDA generator (nxg_generate_packed through the C ABI)
+against the oracle and the reference's golden outputs.
+
+Bars (stated per assertion): root triangle indices, stencil indices, nearest
+guides and point counts bit-exact; positions and radii within 1e-5 of the
+mesh bounding-box diagonal.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from helpers import max_position_error, patch_stencil
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+TOL = 1e-5  # x mesh bounding-box diagonal
+
+
+@pytest.fixture(scope="module")
+def torch_cuda(cuda, nxg_lib):
+    import torch
+    return torch
+
+
+def _gen(torch_cuda, asset, params, radius_scale=1.0, deformed=None, **kw):
+    from nanoxgen_b200.generator import DeviceAsset, generate_packed
+    d = asset if isinstance(asset, DeviceAsset) else DeviceAsset(asset)
+    out = generate_packed(d, params, radius_scale, deformed, **kw)
+    torch_cuda.cuda.synchronize()
+    roots = out.roots_numpy() if out.roots is not None else None
+    return (out.points.cpu().numpy(), roots,
+            out.root_uvs.cpu().numpy() if out.root_uvs is not None else None,
+            out.point_counts.cpu().numpy().view(np.uint32) if out.point_counts is not None else None)
+
+
+def _compare(asset, params, mine, theirs, tol=TOL, radius_scale=1.0):
+    diag = asset.bbox_diagonal()
+    pts, roots, uvs, counts = mine
+    rpts, rroots, ruvs, rcounts = theirs[:4]
+    assert np.array_equal(roots["triangle_index"], rroots["triangle_index"])       # bit-exact
+    assert np.array_equal(roots.view(np.uint8), rroots.view(np.uint8))              # whole RootSample bit-exact
+    assert np.array_equal(counts, rcounts) and np.all(counts == params.cvs_per_strand)
+    assert np.array_equal(uvs, ruvs)
+    err = max_position_error(pts, rpts)
+    assert err <= tol * diag, "max position error %.3g > %.3g" % (err, tol * diag)
+    rerr = float(np.abs(pts[:, 3] - rpts[:, 3]).max())
+    assert rerr <= tol * diag
+    return err / diag
+
+
+@pytest.fixture(scope="module")
+def sphere(nxg_lib):
+    from nanoxgen_b200 import fixtures
+    from nanoxgen_b200.asset import build_asset
+    w = fixtures.plain_sphere()
+    return w, build_asset(w.build_input, w.stencil_slots)
+
+
+def test_plain_sphere_full_parity(torch_cuda, oracle, sphere):
+    w, asset = sphere
+    for params in (w.params, w.params.copy(noise_amplitude=0.0),
+                   w.params.copy(noise_mask=0.83, noise_correlation=0.35, noise_preserve_length=0.4),
+                   w.params.copy(noise_preserve_length=1.0, seed=99)):
+        mine = _gen(torch_cuda, asset, params, 1.5)
+        theirs = oracle.generate(asset.buffer, params, 1.5, threads=8)
+        rel = _compare(asset, params, mine, theirs)
+        print("plain sphere max rel error %.3g" % rel)
+
+
+def test_stencil_indices_bit_exact(torch_cuda, oracle, sphere):
+    from nanoxgen_b200.generator import DeviceAsset, query_strand_states
+    w, asset = sphere
+    d = DeviceAsset(asset)
+    ids = np.arange(0, w.params.strand_count, 7, dtype=np.uint32)
+    for params in (w.params, w.params.copy(normal_rejection_cos=0.5, guide_support_scale=0.4)):
+        states = query_strand_states(d, params, ids)
+        for s, st in zip(ids, states):
+            ref = oracle.strand_state(asset.buffer, params, int(s))
+            assert np.array_equal(st["indices"], ref["indices"]), s
+            assert st["nearest"] == ref["nearest"], s
+            assert st["root"].tobytes() == ref["root"].tobytes(), s
+            assert st["weight_sum"] == pytest.approx(ref["weight_sum"], rel=1e-5)
+            np.testing.assert_allclose(st["weights"], ref["weights"], rtol=1e-5, atol=1e-7)
+
+
+@pytest.mark.parametrize("name", ["unit_fixture.npz", "plain_sphere.npz"])
+def test_golden_outputs(torch_cuda, name):
+    """Against the reference's own outputs committed under tests/golden."""
+    from nanoxgen_b200._abi import GenerationParams
+    from nanoxgen_b200.asset import Asset
+    g = np.load(os.path.join(GOLDEN, name))
+    asset = Asset(g["asset"])
+    rs = float(g["radius_scale"])
+    k = 0
+    while "params%d" % k in g:
+        params = GenerationParams.from_buffer_copy(g["params%d" % k].tobytes())
+        pts, roots, uvs, counts = _gen(torch_cuda, asset, params, rs)
+        ids = g["strands"]
+        ids = ids[ids < params.strand_count]
+        P = int(params.cvs_per_strand)
+        idx = (ids[:, None] * P + np.arange(P)[None, :]).reshape(-1)
+        n = ids.size
+        theirs = (g["points%d" % k][: n * P], g["roots%d" % k].view(roots.dtype)[:n], g["uvs%d" % k][:n],
+                  g["counts%d" % k][:n])
+        _compare(asset, params, (pts[idx], roots[ids], uvs[ids], counts[ids]), theirs)
+        k += 1
+
+
+def test_unit_fixture_known_answers(torch_cuda, nxg_lib):
+    """tests/test_main.cpp:66-100 on the device path."""
+    from nanoxgen_b200 import fixtures
+    from nanoxgen_b200._abi import GenerationParams
+    from nanoxgen_b200.asset import build_asset
+    asset = build_asset(fixtures.reference_unit_fixture())
+    pts, roots, _, _ = _gen(torch_cuda, asset, GenerationParams(strand_count=1, cvs_per_strand=3, seed=7))
+    assert abs(pts[1, 1] - 0.5) < 1e-6 and abs(pts[2, 1] - 1.0) < 1e-6
+    assert abs((pts[2, 0] - roots["position"][0, 0]) - 0.25) < 1e-6
+    params = GenerationParams(strand_count=128, cvs_per_strand=7, seed=42)
+    a = _gen(torch_cuda, asset, params)
+    b = _gen(torch_cuda, asset, params)
+    assert all(np.array_equal(x, y) for x, y in zip(a, b))            # bitwise deterministic
+    assert np.array_equal(a[0][::7, :3], a[1]["position"])             # CV 0 is the root
+
+
+@pytest.mark.parametrize("cvs", [2, 3, 8, 12, 17, 24, 32, 33, 48, 64, 65, 100, 128, 129, 200])
+def test_cv_counts_and_tile_shapes(torch_cuda, oracle, sphere, cvs):
+    w, asset = sphere
+    params = w.params.copy(strand_count=777, cvs_per_strand=cvs,
+                           noise_preserve_length=0.3 if cvs % 2 else 0.0)
+    _compare(asset, params, _gen(torch_cuda, asset, params), oracle.generate(asset.buffer, params, threads=8))
+
+
+def test_fallbacks_and_degenerate_stencils(torch_cuda, oracle, sphere):
+    """Zero blend weight -> nearest guide; every guide rejected -> normal * t
+    (generate.h:261-266)."""
+    w, asset = sphere
+    for params in (w.params.copy(guide_support_scale=0.0, strand_count=3000),
+                   w.params.copy(guide_support_scale=0.05, strand_count=3000),
+                   w.params.copy(normal_rejection_cos=1.0, strand_count=3000),
+                   w.params.copy(guide_weight_power=0.0, length_scale=1.7, strand_count=3000)):
+        _compare(asset, params, _gen(torch_cuda, asset, params), oracle.generate(asset.buffer, params, threads=8))
+
+
+def test_asset_without_texcoords_and_single_guide(torch_cuda, oracle, nxg_lib):
+    from nanoxgen_b200 import fixtures
+    from nanoxgen_b200._abi import GenerationParams
+    from nanoxgen_b200.asset import build_asset
+    for src in (fixtures.reference_area_fixture(), fixtures.reference_benchmark_fixture()):
+        asset = build_asset(src)
+        for params in (GenerationParams(strand_count=2000, cvs_per_strand=12, seed=23),
+                       GenerationParams(strand_count=2000, cvs_per_strand=12, seed=23, noise_amplitude=0.043,
+                                        noise_frequency=3.17, noise_mask=0.83, noise_correlation=0.35,
+                                        noise_preserve_length=0.4)):
+            _compare(asset, params, _gen(torch_cuda, asset, params), oracle.generate(asset.buffer, params))
+
+
+def test_deformed_geometry(torch_cuda, oracle, sphere):
+    import torch
+    from nanoxgen_b200.generator import DeformedGeometry
+    w, asset = sphere
+    rng = np.random.default_rng(11)
+    pos = (asset.positions() + rng.normal(0, 0.02, asset.positions().shape)).astype(np.float32)
+    nrm = asset.normals()
+    gcv = (asset.guide_cvs() + rng.normal(0, 0.01, asset.guide_cvs().shape)).astype(np.float32)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    for kw in ({"positions": pos}, {"positions": pos, "normals": nrm}, {"normals": nrm},
+               {"positions": pos, "normals": nrm, "guide_cvs": gcv}, {"guide_cvs": gcv}):
+        deformed = DeformedGeometry(**{k: dev(v) for k, v in kw.items()})
+        mine = _gen(torch_cuda, asset, w.params, 1.0, deformed)
+        theirs = oracle.generate(asset.buffer, w.params, 1.0, threads=8, **kw)
+        _compare(asset, w.params, mine, theirs)
+
+
+def test_range_generation_matches_full(torch_cuda, sphere):
+    w, asset = sphere
+    full = _gen(torch_cuda, asset, w.params)
+    P = w.params.cvs_per_strand
+    for first, count in ((0, 1), (1234, 4321), (9999, 1), (5000, 5000)):
+        part = _gen(torch_cuda, asset, w.params, first_strand=first, count=count)
+        assert np.array_equal(part[0], full[0][first * P:(first + count) * P])
+        assert np.array_equal(part[1].view(np.uint8), full[1][first:first + count].view(np.uint8))
+
+
+def test_optional_outputs_and_errors(torch_cuda, sphere):
+    import torch
+    from nanoxgen_b200._abi import ERRORS, NxgError
+    from nanoxgen_b200.generator import DeviceAsset, generate_packed
+    w, asset = sphere
+    d = DeviceAsset(asset)
+    pts_only = generate_packed(d, w.params, want_roots=False)
+    torch.cuda.synchronize()
+    full = _gen(torch_cuda, d, w.params)
+    assert np.array_equal(pts_only.points.cpu().numpy(), full[0])
+    small = torch.empty((w.params.strand_count * w.params.cvs_per_strand - 1, 4), device="cuda")
+    with pytest.raises(NxgError) as e:
+        generate_packed(d, w.params, points=small)
+    assert e.value.code == ERRORS["PointCapacityTooSmall"]
+    with pytest.raises(NxgError) as e:
+        generate_packed(d, w.params, radius_scale=float("nan"))
+    assert e.value.code == ERRORS["InvalidRadiusScale"]
+    with pytest.raises(NxgError) as e:
+        generate_packed(d, w.params.copy(cvs_per_strand=1))
+    assert e.value.code == ERRORS["InvalidGenerationParameters"]
+    base = torch.empty((w.params.strand_count * w.params.cvs_per_strand + 1, 4), device="cuda")
+    shifted = base.view(-1)[1:1 + w.params.strand_count * w.params.cvs_per_strand * 4].view(-1, 4)
+    with pytest.raises(NxgError) as e:
+        generate_packed(d, w.params, points=shifted)
+    assert e.value.code == ERRORS["MisalignedOutput"]
+
+
+def test_graph_capture_replays_identically(torch_cuda, sphere):
+    import torch
+    from nanoxgen_b200.generator import DeviceAsset, allocate_outputs, generate_packed
+    w, asset = sphere
+    d = DeviceAsset(asset)
+    P = w.params.cvs_per_strand
+    pts, roots, uvs, pc = allocate_outputs(w.params.strand_count, P, "cuda")
+    eager = generate_packed(d, w.params).points.clone()
+    s = torch.cuda.Stream()
+    g = torch.cuda.CUDAGraph()
+    d.workspace(w.params.strand_count)
+    torch.cuda.synchronize()
+    with torch.cuda.graph(g, stream=s):
+        generate_packed(d, w.params, points=pts, roots=roots, root_uvs=uvs, point_counts=pc, stream=s)
+    pts.zero_()
+    g.replay()
+    torch.cuda.synchronize()
+    assert torch.equal(pts, eager)
+
+
+def test_large_sphere_full_size_parity(torch_cuda, oracle, nxg_lib):
+    """The 1,000,000 x 32 single-description workload: every strand against
+    the oracle (multi-threaded), plus the size-independent properties."""
+    from nanoxgen_b200 import fixtures
+    from nanoxgen_b200.asset import build_asset
+    w = fixtures.large_sphere()
+    asset = build_asset(w.build_input, w.stencil_slots)
+    mine = _gen(torch_cuda, asset, w.params)
+    assert np.all(mine[3] == 32)
+    assert np.array_equal(mine[0][::32, :3], mine[1]["position"])     # CV 0 == root, bitwise
+    theirs = oracle.generate(asset.buffer, w.params, threads=os.cpu_count() or 8)
+    rel = _compare(asset, w.params, mine, theirs)
+    print("large sphere max rel error %.3g" % rel)
