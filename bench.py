@@ -43,6 +43,8 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU-baseline budget")
+    ap.add_argument("--noise-amplitude", type=float, default=None,
+                    help="override the workload's noise magnitude (0 = the noise-free path)")
     return ap.parse_args()
 
 
@@ -237,6 +239,8 @@ def run_gpu_arm(args):
 
     S = args.strands
     w = workload(S * world)
+    if args.noise_amplitude is not None:
+        w.params = w.params.copy(noise_amplitude=args.noise_amplitude)
     params = w.params
     first = rank * S
     P = int(params.cvs_per_strand)

@@ -322,9 +322,12 @@ uint32_t nxg_validate_motion_request(const nxg_device_asset_desc *asset,
 /* --------------------------------------------------------------------- */
 
 /* Bytes of device workspace nxg_generate_packed needs for `strand_count`
- * strands of this asset (the strand-locality sort: keys, permutation and
- * per-guide bins).  The workspace must be 256-byte aligned. */
-uint64_t nxg_packed_workspace_size(const nxg_device_asset_desc *asset, uint32_t strand_count);
+ * strands of this asset at params->cvs_per_strand CVs: the strand-locality
+ * sort (keys, permutation, per-guide bins) and the per-frame guide-offset
+ * table (guide_count x cvs_per_strand float4).  The workspace must be
+ * 256-byte aligned; its contents need no initialisation. */
+uint64_t nxg_packed_workspace_size(const nxg_device_asset_desc *asset, const nxg_generation_params *params,
+                                   uint32_t strand_count);
 
 /* The device form of asset.cpp:412-449 generate_packed_cpu /
  * generate_packed_deformed_cpu over generate.h:612-642
@@ -359,16 +362,16 @@ uint32_t nxg_prepare_strand_order(const nxg_device_asset_desc *asset, const nxg_
                                   uint32_t first_strand, uint32_t strand_count, void *workspace,
                                   uint64_t workspace_bytes, void *stream);
 
-/* Phase 2: the generator over the order nxg_prepare_strand_order left in
- * `workspace` (same asset, seed and range), or over strand order when
- * `workspace` is NULL.  Output is identical either way; the order only
- * changes which strands share a CTA and hence the cache locality. */
+/* Phase 2: rebuilds the frame's guide-offset table in `workspace` and runs
+ * the generator over the order nxg_prepare_strand_order left there (same
+ * asset, seed and range).  The order only decides which strands share a CTA
+ * (cache locality); the output does not depend on it. */
 uint32_t nxg_generate_packed_ordered(const nxg_device_asset_desc *asset,
                                      const nxg_deformed_desc *deformed,
                                      const nxg_generation_params *params,
                                      const nxg_packed_output_desc *output,
                                      const nxg_launch_config *config, uint32_t first_strand,
-                                     uint32_t strand_count, const void *workspace,
+                                     uint32_t strand_count, void *workspace,
                                      uint64_t workspace_bytes, void *stream);
 
 /* Per-strand blend state: the RootSample of generate.h:101-135, the

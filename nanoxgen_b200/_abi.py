@@ -212,7 +212,8 @@ _SIGNATURES = {
                                                       ctypes.POINTER(GenerationParams),
                                                       ctypes.POINTER(MotionOutputDesc),
                                                       ctypes.POINTER(LaunchConfig)]),
-    "nxg_packed_workspace_size": (ctypes.c_uint64, [ctypes.POINTER(DeviceAssetDesc), ctypes.c_uint32]),
+    "nxg_packed_workspace_size": (ctypes.c_uint64, [ctypes.POINTER(DeviceAssetDesc),
+                                                    ctypes.POINTER(GenerationParams), ctypes.c_uint32]),
     "nxg_generate_packed": (ctypes.c_uint32, [ctypes.POINTER(DeviceAssetDesc), ctypes.POINTER(DeformedDesc),
                                               ctypes.POINTER(GenerationParams),
                                               ctypes.POINTER(PackedOutputDesc),

@@ -71,250 +71,547 @@ __device__ __forceinline__ float strand_radius(const ParamArgs &p, float t) {
     return 0.5f * width * p.radius_scale;
 }
 
-// One strand on an L-lane group; see the file comment for the layout.
-template <int L, int PPT, bool NOISE>
-__device__ __forceinline__ void process_strand(const LaunchArgs &g, uint32_t local, bool active, int gl,
-                                               Slot *slots, const float4 *table) {
+// ---------------------------------------------------------------------------
+// Per-strand records a warp stages in shared memory between its two phases
+// (one column per strand of the warp's 32-strand batch).
+// ---------------------------------------------------------------------------
+enum RecordField : int {
+    kRecPx = 0, kRecPy, kRecPz,        // root position
+    kRecNx, kRecNy, kRecNz,            // root normal
+    kRecMode,                          // blended-slot count | mode << 8
+    kRecInvW,                          // 1 / weight_sum (mode 0)
+    kRecGuide0,                        // 8 blended guides, in slot order
+    kRecWeight0 = kRecGuide0 + 8,      // their weights
+    kRecNearest = kRecWeight0 + 8,     // nearest eligible guide (mode 1)
+    kRecSUx, kRecSUy, kRecSUz,         // surface_u (noise)
+    kRecDx, kRecDy, kRecDz,            // noise domain (noise)
+    kRecLocal,                         // output record | invalid << 31
+    kRecFields
+};
+enum : uint32_t { kModeBlend = 0u, kModeNearest = 1u, kModeNormal = 2u };
+
+struct Records {
+    uint32_t *base;  // kRecFields x 32 words
+    __device__ __forceinline__ uint32_t &u(int field, int strand) const { return base[field * 32 + strand]; }
+    __device__ __forceinline__ float f(int field, int strand) const { return __uint_as_float(base[field * 32 + strand]); }
+    __device__ __forceinline__ void setf(int field, int strand, float v) const { base[field * 32 + strand] = __float_as_uint(v); }
+    __device__ __forceinline__ F3 f3(int field, int strand) const { return {f(field, strand), f(field + 1, strand), f(field + 2, strand)}; }
+};
+
+// Phase A: lane i sets up strand i of the batch -- root sample, the eight
+// stencil slots, the blend mode and (with noise) the surface frame inputs.
+template <bool NOISE>
+__device__ __forceinline__ void setup_strand(const LaunchArgs &g, const Records &rec, int lane, uint32_t pick,
+                                             bool valid) {
     const AssetArgs &a = g.a;
     const FrameArgs &f = g.f;
     const ParamArgs &p = g.p;
-    const uint32_t P = p.cvs_per_strand;
-    const uint32_t strand = g.first_strand + local;
-
-    const Root root = sample_root(a, f, p.seed, strand);
-    if (gl < static_cast<int>(kSlots)) { slots[gl] = eval_slot(a, f, p, root, static_cast<uint32_t>(gl)); }
-    __syncwarp();
-
-    // Blend state (generate.h:214-244): weight sum in slot order, nearest
-    // eligible guide by strict first minimum.
+    uint32_t local = __ldg(g.order + pick);
+    if (local >= g.count) {
+        local = 0u;
+        valid = false;
+    }
+    const Root root = sample_root(a, f, p.seed, g.first_strand + local);
     float wsum = 0.0f;
     float nearest_d2 = FLT_MAX;
-    int nearest = -1;
+    uint32_t nearest = kInvalid;
     uint32_t blended = 0u;
-#pragma unroll
+#pragma unroll 1
     for (uint32_t j = 0; j < kSlots; ++j) {
-        const uint32_t flags = slots[j].flags;
-        const float d2 = slots[j].d2;
-        if (flags & kSlotEligible) {
-            if (d2 < nearest_d2) {
-                nearest_d2 = d2;
-                nearest = static_cast<int>(j);
-            }
+        const Slot s = eval_slot(a, f, p, root, j);
+        if ((s.flags & kSlotEligible) && s.d2 < nearest_d2) {  // strict first minimum (generate.h:234)
+            nearest_d2 = s.d2;
+            nearest = s.guide;
         }
-        if (flags & kSlotBlended) {
-            wsum = __fadd_rn(wsum, slots[j].w);
-            blended |= 1u << j;
+        if (s.flags & kSlotBlended) {
+            rec.u(kRecGuide0 + blended, lane) = s.guide;
+            rec.setf(kRecWeight0 + blended, lane, s.w);
+            ++blended;
+            wsum = __fadd_rn(wsum, s.w);
         }
     }
+    const uint32_t mode = wsum > 1.0e-12f ? kModeBlend : (nearest != kInvalid ? kModeNearest : kModeNormal);
+    rec.u(kRecMode, lane) = blended | (mode << 8);
+    rec.setf(kRecInvW, lane, mode == kModeBlend ? 1.0f / wsum : 0.0f);
+    rec.u(kRecNearest, lane) = nearest;
+    rec.setf(kRecPx, lane, root.position.x);
+    rec.setf(kRecPy, lane, root.position.y);
+    rec.setf(kRecPz, lane, root.position.z);
+    rec.setf(kRecNx, lane, root.normal.x);
+    rec.setf(kRecNy, lane, root.normal.y);
+    rec.setf(kRecNz, lane, root.normal.z);
+    rec.u(kRecLocal, lane) = local | (valid ? 0u : 0x80000000u);
+    if constexpr (NOISE) {
+        const F3 su = root_surface_u(a, f, root);
+        const float decorrelation = 1.0f - p.noise_correlation;
+        const float domain_scale = 100.0f * decorrelation * decorrelation;
+        const F3 dom = (rest_root_position(a, root) + F3{0.419276f, 0.184247f, 0.805721f}) * domain_scale;
+        rec.setf(kRecSUx, lane, su.x);
+        rec.setf(kRecSUy, lane, su.y);
+        rec.setf(kRecSUz, lane, su.z);
+        rec.setf(kRecDx, lane, dom.x);
+        rec.setf(kRecDy, lane, dom.y);
+        rec.setf(kRecDz, lane, dom.z);
+    }
+}
 
-    // Base curve (generate.h:246-267, :300-310).
+// generate.h:404-418 rotate_by for angle = acos(c), with cos(angle) = c and
+// sin(angle) = sqrt(1 - c^2) evaluated as sqrt(fma(-c, c, 1)) (one rounding,
+// accurate near |c| = 1).
+__device__ __forceinline__ M3 rotation_cs(F3 axis, float c, float s) {
+    const float omc = 1.0f - c;
+    M3 r;
+    r.m[0] = axis.x * axis.x * omc + c;
+    r.m[1] = axis.x * axis.y * omc - axis.z * s;
+    r.m[2] = axis.x * axis.z * omc + axis.y * s;
+    r.m[3] = axis.x * axis.y * omc + axis.z * s;
+    r.m[4] = axis.y * axis.y * omc + c;
+    r.m[5] = axis.y * axis.z * omc - axis.x * s;
+    r.m[6] = axis.x * axis.z * omc - axis.y * s;
+    r.m[7] = axis.y * axis.z * omc + axis.x * s;
+    r.m[8] = axis.z * axis.z * omc + c;
+    return r;
+}
+
+__device__ __forceinline__ float component(F3 v, int axis) { return axis == 0 ? v.x : (axis == 1 ? v.y : v.z); }
+__device__ __forceinline__ float component4(float4 v, int axis) { return axis == 0 ? v.x : (axis == 1 ? v.y : v.z); }
+
+// Gradient noise along one axis of a strand (generate.h:370-402 evaluated at
+// domain + distance * e_axis).  Only the `axis` coordinate moves along the
+// strand, so the fade weights of the two fixed axes are constants and the
+// eight-corner trilinear blend folds, per lattice column X of the moving
+// axis, into A(X) = sum_corners w_b w_c g_axis and
+// B(X) = sum_corners w_b w_c (g_b (f_b - o_b) + g_c (f_c - o_c)):
+//   noise = 0.5 * ((1 - s(f)) (A(X) f + B(X)) + s(f) (A(X+1) (f - 1) + B(X+1))) + 0.5
+// with X = floor(x), f = x - X.  The columns of a strand are filled once;
+// each CV then needs two table entries instead of eight hashed corners.
+struct Lattice {
+    float2 *col[3];   // per axis: (A, B) for X = lo[axis] + k
+    int lo[3];
+    int n[3];
+};
+
+__device__ __forceinline__ float lattice_noise(const Lattice &lat, int axis, float x) {
+    const float fx = floorf(x);
+    const float w = x - fx;
+    int k = static_cast<int>(fx) - lat.lo[axis];
+    k = max(0, min(k, lat.n[axis] - 2));
+    const float2 c0 = lat.col[axis][k];
+    const float2 c1 = lat.col[axis][k + 1];
+    const float s = s_curve(w);
+    const float v0 = c0.x * w + c0.y;
+    const float v1 = c1.x * (w - 1.0f) + c1.y;
+    return 0.5f * ((1.0f - s) * v0 + s * v1) + 0.5f;
+}
+
+// Fill column k of `axis`: the four corners (o_b, o_c) of lattice column X.
+__device__ __forceinline__ float2 lattice_column(const float4 *table, int axis, int X, F3 dom) {
+    const int ib = axis == 0 ? 1 : 0;           // the fixed axes, ascending
+    const int ic = axis == 2 ? 1 : 2;
+    const float db = component(dom, ib), dc = component(dom, ic);
+    const float fb = floorf(db), fc = floorf(dc);
+    const float wb = db - fb, wc = dc - fc;
+    const float sb = s_curve(wb), sc = s_curve(wc);
+    const int Yb = static_cast<int>(fb), Zc = static_cast<int>(fc);
+    float A = 0.0f, B = 0.0f;
+#pragma unroll
+    for (int corner = 0; corner < 4; ++corner) {
+        const int ob = corner & 1, oc = corner >> 1;
+        const int cx = axis == 0 ? X : Yb + ob;
+        const int cy = axis == 1 ? X : (axis == 0 ? Yb + ob : Zc + oc);
+        const int cz = axis == 2 ? X : Zc + oc;
+        const uint32_t seed = static_cast<uint32_t>(cx) * kLcgA2 + static_cast<uint32_t>(cy) * kLcgA +
+                              static_cast<uint32_t>(cz) + kLcgK;
+        const float4 gr = table[temper_index(seed)];
+        const float wgt = (ob ? sb : 1.0f - sb) * (oc ? sc : 1.0f - sc);
+        A += wgt * component4(gr, axis);
+        B += wgt * (component4(gr, ib) * (wb - static_cast<float>(ob)) + component4(gr, ic) * (wc - static_cast<float>(oc)));
+    }
+    return make_float2(A, B);
+}
+
+// Phase B: strand b of the batch on an L-lane group; lane gl owns the
+// consecutive CVs gl*PPT .. gl*PPT+PPT-1.
+template <int L, int PPT, bool NOISE>
+__device__ __forceinline__ void emit_strand(const LaunchArgs &g, const Records &rec, int b, int gl,
+                                            const float4 *table, const float4 *offsets, const float *tvals,
+                                            float4 *stage, float2 *lattice_area, int lattice_max) {
+    const ParamArgs &p = g.p;
+    const int P = static_cast<int>(p.cvs_per_strand);
+    const uint32_t local_word = rec.u(kRecLocal, b);
+    const bool active = (local_word >> 31) == 0u;
+    const uint32_t local = local_word & 0x7fffffffu;
+    const F3 root = rec.f3(kRecPx, b);
+    const F3 rnormal = rec.f3(kRecNx, b);
+    const uint32_t mode_word = rec.u(kRecMode, b);
+    const uint32_t nb = mode_word & 0xffu;
+    const uint32_t mode = mode_word >> 8;
+    const int cv0 = gl * PPT;
+
+    // Base curve (generate.h:246-267, :300-310) from the guide-offset table:
+    // offsets[g*P + cv] = sample_guide(g, cv/(P-1)) - guide_root(g).
     float tcv[PPT];
     F3 base[PPT];
 #pragma unroll
-    for (int c = 0; c < PPT; ++c) {
-        const uint32_t cv = static_cast<uint32_t>(c * L + gl);
-        tcv[c] = cv < P ? __fdiv_rn(static_cast<float>(cv), static_cast<float>(P - 1u)) : 1.0f;
-        base[c] = F3{0.0f, 0.0f, 0.0f};
+    for (int j = 0; j < PPT; ++j) {
+        tcv[j] = tvals[min(cv0 + j, P - 1)];
+        base[j] = F3{0.0f, 0.0f, 0.0f};
     }
-    if (wsum > 1.0e-12f) {
+    if (mode == kModeBlend) {
 #pragma unroll
-        for (uint32_t j = 0; j < kSlots; ++j) {
-            if (blended & (1u << j)) {
-                const Slot s = slots[j];
+        for (uint32_t k = 0; k < kSlots; ++k) {
+            if (k < nb) {
+                const float4 *row = offsets + static_cast<uint64_t>(rec.u(kRecGuide0 + k, b)) * P;
+                const float w = rec.f(kRecWeight0 + k, b);
 #pragma unroll
-                for (int c = 0; c < PPT; ++c) { base[c] = base[c] + guide_offset(f.guide_cvs, s, tcv[c]) * s.w; }
+                for (int j = 0; j < PPT; ++j) {
+                    const float4 d = __ldg(row + min(cv0 + j, P - 1));
+                    base[j] = base[j] + F3{d.x, d.y, d.z} * w;
+                }
             }
         }
-        const float inv = 1.0f / wsum;
+        const float inv = rec.f(kRecInvW, b);
 #pragma unroll
-        for (int c = 0; c < PPT; ++c) { base[c] = base[c] * inv; }
-    } else if (nearest >= 0) {
-        const Slot s = slots[nearest];
+        for (int j = 0; j < PPT; ++j) { base[j] = base[j] * inv; }
+    } else if (mode == kModeNearest) {
+        const float4 *row = offsets + static_cast<uint64_t>(rec.u(kRecNearest, b)) * P;
 #pragma unroll
-        for (int c = 0; c < PPT; ++c) { base[c] = guide_offset(f.guide_cvs, s, tcv[c]); }
+        for (int j = 0; j < PPT; ++j) {
+            const float4 d = __ldg(row + min(cv0 + j, P - 1));
+            base[j] = F3{d.x, d.y, d.z};
+        }
     } else {
 #pragma unroll
-        for (int c = 0; c < PPT; ++c) { base[c] = root.normal * tcv[c]; }
+        for (int j = 0; j < PPT; ++j) { base[j] = rnormal * tcv[j]; }
     }
 #pragma unroll
-    for (int c = 0; c < PPT; ++c) { base[c] = root.position + base[c] * p.length_scale; }
+    for (int j = 0; j < PPT; ++j) { base[j] = root + base[j] * p.length_scale; }
 
-    float4 *out = g.points + static_cast<uint64_t>(local) * P;
-
+    F3 point[PPT];
     if constexpr (!NOISE) {
 #pragma unroll
-        for (int c = 0; c < PPT; ++c) {
-            const uint32_t cv = static_cast<uint32_t>(c * L + gl);
-            if (active && cv < P) {
-                __stcs(out + cv, make_float4(base[c].x, base[c].y, base[c].z, strand_radius(p, tcv[c])));
-            }
-        }
+        for (int j = 0; j < PPT; ++j) { point[j] = base[j]; }
     } else {
-        const F3 surface_u = root_surface_u(a, f, root);
-        // Arc length: inclusive prefix of segment lengths (generate.h:420-433, :465-468).
+        const F3 surface_u = rec.f3(kRecSUx, b);
+        const F3 domain = rec.f3(kRecDx, b);
+        const F3 prev_lane_base = group_shfl_up<L>(base[PPT - 1], 1);
+        const F3 next_lane_base = group_shfl_down<L>(base[0], 1);
+
+        // Arc length: prefix of segment lengths (generate.h:420-433, :465-468).
         float arc[PPT];
-        float carry = 0.0f;
+        float run = 0.0f;
 #pragma unroll
-        for (int c = 0; c < PPT; ++c) {
-            const uint32_t cv = static_cast<uint32_t>(c * L + gl);
-            const F3 up = group_shfl_up<L>(base[c], 1);
-            const F3 prev_chunk = c > 0 ? group_shfl<L>(base[c > 0 ? c - 1 : 0], L - 1) : base[c];
-            const F3 pb = gl > 0 ? up : prev_chunk;
-            const F3 d = base[c] - pb;
-            const float seg = (cv >= 1u && cv < P) ? sqrtf(dot(d, d)) : 0.0f;
-            const float inc = group_scan_add<L>(seg, gl) + carry;
-            arc[c] = inc;
-            carry = group_shfl<L>(inc, L - 1);
+        for (int j = 0; j < PPT; ++j) {
+            const int cv = cv0 + j;
+            const F3 prev = j > 0 ? base[j > 0 ? j - 1 : 0] : prev_lane_base;
+            const F3 d = base[j] - prev;
+            run += (cv >= 1 && cv < P) ? sqrtf(dot(d, d)) : 0.0f;
+            arc[j] = run;
         }
-        const float original_length = carry;
+        const float lane_incl = group_scan_add<L>(run, gl);
+        const float lane_excl = __shfl_up_sync(kFull, lane_incl, 1, L);
+        const float offset_arc = gl > 0 ? lane_excl : 0.0f;
+#pragma unroll
+        for (int j = 0; j < PPT; ++j) { arc[j] += offset_arc; }
+        const float original_length = __shfl_sync(kFull, lane_incl, L - 1, L);
         const float f_eff = original_length > 0.0f ? fmaxf(0.5f / original_length, p.noise_frequency)
                                                    : p.noise_frequency;
-        const float decorrelation = 1.0f - p.noise_correlation;
-        const float domain_scale = 100.0f * decorrelation * decorrelation;
-        const F3 domain = (rest_root_position(a, root) + F3{0.419276f, 0.184247f, 0.805721f}) * domain_scale;
 
         // Tangent after CV k: the next segment's direction, carried forward over
         // zero-length segments and at the tip (generate.h:470-474).
         F3 cand[PPT];
-        F3 tan[PPT];
-        int last_valid = -1;
+        bool valid[PPT];
+        int lane_last = -1;
+        F3 lane_last_cand = {0.0f, 0.0f, 0.0f};
 #pragma unroll
-        for (int c = 0; c < PPT; ++c) {
-            const uint32_t cv = static_cast<uint32_t>(c * L + gl);
-            const F3 dn = group_shfl_down<L>(base[c], 1);
-            const F3 next_chunk = c + 1 < PPT ? group_shfl<L>(base[c + 1 < PPT ? c + 1 : c], 0) : base[c];
-            const F3 nb = gl < L - 1 ? dn : next_chunk;
-            const F3 e = xsub(nb, base[c]);
-            const bool valid = (cv + 1u < P) && xdot(e, e) > 0.0f;
-            cand[c] = valid ? xnormalize(e) : F3{0.0f, 0.0f, 0.0f};
-            const int jv = valid ? static_cast<int>(cv) : -1;
-            const int jm = max(group_scan_max<L>(jv, gl), last_valid);
-            last_valid = __shfl_sync(kFull, jm, L - 1, L);
-            F3 sel = root.normal;
-#pragma unroll
-            for (int c2 = 0; c2 <= c; ++c2) {
-                const F3 v = group_shfl<L>(cand[c2], jm & (L - 1));
-                if (jm >= 0 && jm / L == c2) { sel = v; }
+        for (int j = 0; j < PPT; ++j) {
+            const int cv = cv0 + j;
+            const F3 next = j + 1 < PPT ? base[j + 1 < PPT ? j + 1 : j] : next_lane_base;
+            const F3 e = xsub(next, base[j]);
+            valid[j] = (cv + 1 < P) && xdot(e, e) > 0.0f;
+            cand[j] = valid[j] ? xnormalize(e) : F3{0.0f, 0.0f, 0.0f};
+            if (valid[j]) {
+                lane_last = cv;
+                lane_last_cand = cand[j];
             }
-            tan[c] = sel;
+        }
+        const int incl_last = group_scan_max<L>(lane_last, gl);
+        const int up_last = __shfl_up_sync(kFull, incl_last, 1, L);  // every lane shuffles
+        const int excl_last = gl > 0 ? up_last : -1;
+        const F3 from_lanes = group_shfl<L>(lane_last_cand, max(excl_last, 0) / PPT);
+        F3 carry_t = excl_last >= 0 ? from_lanes : rnormal;
+        F3 tan[PPT];
+#pragma unroll
+        for (int j = 0; j < PPT; ++j) {
+            if (valid[j]) { carry_t = cand[j]; }
+            tan[j] = carry_t;
         }
 
-        // Transported normal: N_k = normalize(M_k ... M_0 surface_u), with M_k the
-        // reference's rotate_by matrix (generate.h:475-481); the product of the
-        // per-CV matrices is an inclusive scan across lanes and chunks.
-        F3 normal[PPT];
-        M3 carry_m = identity3();
+        // Transported normal N_k = normalize(M_k ... M_0 surface_u) with M_k the
+        // reference's rotate_by matrix (generate.h:475-481): a lane multiplies
+        // its own matrices, an exclusive scan across lanes supplies the product
+        // of all earlier CVs, and the lane then walks its CVs.
+        M3 mats[PPT];
+        M3 lane_prod = identity3();
+        const F3 prev_lane_tan = group_shfl_up<L>(tan[PPT - 1], 1);
 #pragma unroll
-        for (int c = 0; c < PPT; ++c) {
-            const uint32_t cv = static_cast<uint32_t>(c * L + gl);
-            const F3 up = group_shfl_up<L>(tan[c], 1);
-            const F3 prev_chunk = c > 0 ? group_shfl<L>(tan[c > 0 ? c - 1 : 0], L - 1) : root.normal;
-            const F3 tp = gl > 0 ? up : prev_chunk;
-            const F3 axis = xcross(tp, tan[c]);
-            M3 m = identity3();
+        for (int j = 0; j < PPT; ++j) {
+            const int cv = cv0 + j;
+            const F3 tp = j > 0 ? tan[j > 0 ? j - 1 : 0] : (gl > 0 ? prev_lane_tan : rnormal);
+            const F3 axis = xcross(tp, tan[j]);
+            mats[j] = identity3();
             if (cv < P && xdot(axis, axis) > 0.0f) {
-                const float angle = acosf(fminf(fmaxf(dot(tp, tan[c]), -1.0f), 1.0f));
-                m = rotation3(axis, angle);
+                const float cs = fminf(fmaxf(dot(tp, tan[j]), -1.0f), 1.0f);
+                mats[j] = rotation_cs(axis, cs, sqrtf(fmaf(-cs, cs, 1.0f)));
             }
-            M3 q = group_scan_mat<L>(m, gl);
-            q = mul3(q, carry_m);
-            carry_m = group_shfl<L>(q, L - 1);
-            normal[c] = normalize(apply3(q, surface_u));
+            lane_prod = j == 0 ? mats[0] : mul3(mats[j], lane_prod);
         }
+        const M3 incl_prod = group_scan_mat<L>(lane_prod, gl);
+        M3 earlier;
+#pragma unroll
+        for (int i = 0; i < 9; ++i) { earlier.m[i] = __shfl_up_sync(kFull, incl_prod.m[i], 1, L); }
+        F3 v = gl > 0 ? apply3(earlier, surface_u) : surface_u;
+        F3 normal[PPT];
+#pragma unroll
+        for (int j = 0; j < PPT; ++j) {
+            v = normalize(apply3(mats[j], v));
+            normal[j] = v;
+        }
+
+        // Lattice columns of the three noise axes for this strand.
+        Lattice lat;
+        const float span = original_length * f_eff;
+        bool fits = true;
+#pragma unroll
+        for (int ax = 0; ax < 3; ++ax) {
+            const float d0 = component(domain, ax);
+            lat.lo[ax] = static_cast<int>(floorf(d0));
+            // columns lo .. floor(d0 + span) + 2: every CV's X and X + 1, with one
+            // column of margin for rounding in the arc-length prefix
+            lat.n[ax] = static_cast<int>(floorf(d0 + span)) + 3 - lat.lo[ax];
+            fits = fits && lat.n[ax] >= 2 && lat.n[ax] <= lattice_max;
+            lat.col[ax] = lattice_area + ax * lattice_max;
+        }
+        const int total = fits ? lat.n[0] + lat.n[1] + lat.n[2] : 0;
+        int rounds = (total + L - 1) / L;
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) { rounds = max(rounds, __shfl_xor_sync(kFull, rounds, d)); }
+        rounds = min(rounds, (3 * lattice_max + L - 1) / L);  // a group never has more columns
+        for (int r = 0; r < rounds; ++r) {
+            const int item = r * L + gl;
+            if (item < total) {
+                const int ax = item < lat.n[0] ? 0 : (item < lat.n[0] + lat.n[1] ? 1 : 2);
+                const int k = item - (ax > 0 ? lat.n[0] : 0) - (ax > 1 ? lat.n[1] : 0);
+                lat.col[ax][k] = lattice_column(table, ax, lat.lo[ax] + k, domain);
+            }
+        }
+        __syncwarp();
 
         // Displacement in the transported frame (generate.h:482-502).
         const float magnitude_scale = p.noise_mask * p.noise_amplitude;
-        F3 point[PPT];
 #pragma unroll
-        for (int c = 0; c < PPT; ++c) {
-            const uint32_t cv = static_cast<uint32_t>(c * L + gl);
-            F3 q = base[c];
-            if (cv > 0u && cv < P) {
-                const F3 n = normal[c];
-                const F3 b = cross(n, tan[c]);
-                const F3 t = cross(b, n);
-                const float distance = arc[c] * f_eff;
-                const float magnitude = magnitude_scale * tcv[c];
-                const float lx = (gradient_noise(table, domain.x + distance, domain.y, domain.z) - 0.5f) * magnitude;
-                const float ly = (gradient_noise(table, domain.x, domain.y + distance, domain.z) - 0.5f) * magnitude;
-                const float lz = (gradient_noise(table, domain.x, domain.y, domain.z + distance) - 0.5f) * magnitude;
-                q = q + n * lx + b * ly + t * lz;
+        for (int j = 0; j < PPT; ++j) {
+            const int cv = cv0 + j;
+            F3 q = base[j];
+            if (cv > 0 && cv < P) {
+                const F3 n = normal[j];
+                const F3 bn = cross(n, tan[j]);
+                const F3 t = cross(bn, n);
+                const float distance = arc[j] * f_eff;
+                const float magnitude = magnitude_scale * tcv[j];
+                float gx, gy, gz;
+                if (fits) {
+                    gx = lattice_noise(lat, 0, domain.x + distance);
+                    gy = lattice_noise(lat, 1, domain.y + distance);
+                    gz = lattice_noise(lat, 2, domain.z + distance);
+                } else {
+                    gx = gradient_noise(table, domain.x + distance, domain.y, domain.z);
+                    gy = gradient_noise(table, domain.x, domain.y + distance, domain.z);
+                    gz = gradient_noise(table, domain.x, domain.y, domain.z + distance);
+                }
+                q = q + n * ((gx - 0.5f) * magnitude) + bn * ((gy - 0.5f) * magnitude) + t * ((gz - 0.5f) * magnitude);
             }
-            point[c] = q;
+            point[j] = q;
         }
 
         // preserveLength (generate.h:553-563), from the noisy points already in
         // registers instead of a second cursor pass.
-        float scale = 1.0f;
         if (p.noise_preserve_length > 0.001f) {
+            const F3 prev_lane_point = group_shfl_up<L>(point[PPT - 1], 1);
             float partial = 0.0f;
 #pragma unroll
-            for (int c = 0; c < PPT; ++c) {
-                const uint32_t cv = static_cast<uint32_t>(c * L + gl);
-                const F3 up = group_shfl_up<L>(point[c], 1);
-                const F3 prev_chunk = c > 0 ? group_shfl<L>(point[c > 0 ? c - 1 : 0], L - 1) : point[c];
-                const F3 pb = gl > 0 ? up : prev_chunk;
-                const F3 d = point[c] - pb;
-                partial += (cv >= 1u && cv < P) ? sqrtf(dot(d, d)) : 0.0f;
+            for (int j = 0; j < PPT; ++j) {
+                const int cv = cv0 + j;
+                const F3 prev = j > 0 ? point[j > 0 ? j - 1 : 0] : prev_lane_point;
+                const F3 d = point[j] - prev;
+                partial += (cv >= 1 && cv < P) ? sqrtf(dot(d, d)) : 0.0f;
             }
             const float noisy = group_sum<L>(partial);
+            float scale = 1.0f;
             if (noisy > 0.0f) {
                 const float target = original_length * p.noise_preserve_length +
                                      noisy * (1.0f - p.noise_preserve_length);
                 if (fabsf(noisy - target) >= 0.0001f) { scale = target / noisy; }
             }
-        }
+            if (scale != 1.0f) {
 #pragma unroll
-        for (int c = 0; c < PPT; ++c) {
-            const uint32_t cv = static_cast<uint32_t>(c * L + gl);
-            F3 q = point[c];
-            if (scale != 1.0f) { q = root.position + (q - root.position) * scale; }
-            if (active && cv < P) { __stcs(out + cv, make_float4(q.x, q.y, q.z, strand_radius(p, tcv[c]))); }
+                for (int j = 0; j < PPT; ++j) { point[j] = root + (point[j] - root) * scale; }
+            }
         }
     }
 
-    if (active) {
-        if (g.roots && gl < 12) { g.roots[static_cast<uint64_t>(local) * 12u + gl] = root_word(root, gl); }
-        if (gl == 0) {
-            if (g.root_uvs) { g.root_uvs[local] = make_float2(root.u, root.v); }
-            if (g.point_counts) { g.point_counts[local] = P; }
-        }
+    // Stage the strand's float4s in shared memory, then write them with
+    // consecutive lanes on consecutive CVs (coalesced streaming stores).
+#pragma unroll
+    for (int j = 0; j < PPT; ++j) {
+        const int cv = cv0 + j;
+        if (cv < P) { stage[cv] = make_float4(point[j].x, point[j].y, point[j].z, strand_radius(p, tcv[j])); }
     }
+    __syncwarp();
+    if (active) {
+        float4 *out = g.points + static_cast<uint64_t>(local) * static_cast<uint32_t>(P);
+        for (int cv = gl; cv < P; cv += L) { __stcs(out + cv, stage[cv]); }
+    }
+    __syncwarp();
 }
 
+// Persistent CTAs over contiguous ranges of the strand order.  Each warp
+// takes 32 strands at a time: phase A sets them up one lane per strand,
+// phase B emits them one L-lane group per strand.
 template <int L, int PPT, bool NOISE>
-__global__ void generate_kernel(LaunchArgs g) {
+__global__ void generate_kernel(LaunchArgs g, const float4 *offsets) {
     extern __shared__ float4 smem[];
+    constexpr int kGroups = 32 / L;
+    constexpr int kLatticePerWarp = 384;                 // float2 columns per warp (3 axes)
+    constexpr int kLatticeMax = kLatticePerWarp / 3 / kGroups;
+    const int P = static_cast<int>(g.p.cvs_per_strand);
+    const int warps = blockDim.x >> 5;
+    // Layout: gradient table | t values | per warp: records, stage, lattice.
     float4 *table = smem;
-    Slot *all_slots = reinterpret_cast<Slot *>(smem + kTableFloat4);
+    float *tvals = reinterpret_cast<float *>(smem + kTableFloat4);
+    unsigned char *warp_base = reinterpret_cast<unsigned char *>(tvals + ((P + 3) & ~3));
+    const size_t rec_bytes = sizeof(uint32_t) * kRecFields * 32;
+    const size_t stage_bytes = sizeof(float4) * kGroups * L * PPT;
+    const size_t lattice_bytes = NOISE ? sizeof(float2) * kLatticePerWarp : 0;
+    const size_t per_warp = rec_bytes + stage_bytes + lattice_bytes;
     if constexpr (NOISE) {
         for (int i = threadIdx.x; i < kTableFloat4; i += blockDim.x) {
             table[i] = make_float4(__ldg(g.a.gradients + 3 * i), __ldg(g.a.gradients + 3 * i + 1),
                                    __ldg(g.a.gradients + 3 * i + 2), 0.0f);
         }
-        __syncthreads();
     }
-    constexpr int kGroups = 32 / L;
+    for (int i = threadIdx.x; i < P; i += blockDim.x) {  // t = cv / (P - 1) (generate.h:295-298)
+        tvals[i] = __fdiv_rn(static_cast<float>(i), static_cast<float>(P - 1));
+    }
+    __syncthreads();
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    const int warps = blockDim.x >> 5;
     const int group = lane / L;
     const int gl = lane % L;
-    Slot *slots = all_slots + (warp * kGroups + group) * kSlots;
+    unsigned char *mine = warp_base + per_warp * warp;
+    const Records rec{reinterpret_cast<uint32_t *>(mine)};
+    float4 *stage = reinterpret_cast<float4 *>(mine + rec_bytes) + group * (L * PPT);
+    float2 *lattice = reinterpret_cast<float2 *>(mine + rec_bytes + stage_bytes) + group * (kLatticePerWarp / kGroups);
     const uint32_t begin = static_cast<uint32_t>(static_cast<uint64_t>(blockIdx.x) * g.count / gridDim.x);
     const uint32_t end = static_cast<uint32_t>(static_cast<uint64_t>(blockIdx.x + 1u) * g.count / gridDim.x);
-    for (uint32_t base = begin + static_cast<uint32_t>(warp * kGroups); base < end;
-         base += static_cast<uint32_t>(warps * kGroups)) {
-        const uint32_t item = base + static_cast<uint32_t>(group);
-        bool active = item < end;
-        const uint32_t pick = active ? item : begin;
-        uint32_t local = g.order ? __ldg(g.order + pick) : pick;
-        if (local >= g.count) {
-            local = 0u;
-            active = false;
-        }
-        process_strand<L, PPT, NOISE>(g, local, active, gl, slots, table);
+    for (uint32_t batch = begin + static_cast<uint32_t>(warp) * 32u; batch < end;
+         batch += static_cast<uint32_t>(warps) * 32u) {
+        const uint32_t item = batch + static_cast<uint32_t>(lane);
+        const bool valid = item < end;
+        setup_strand<NOISE>(g, rec, lane, valid ? item : batch, valid);
         __syncwarp();
+        const uint32_t in_batch = min(32u, end - batch);
+#pragma unroll 1
+        for (uint32_t r = 0; r < in_batch; r += kGroups) {
+            emit_strand<L, PPT, NOISE>(g, rec, static_cast<int>(r) + group, gl, table, offsets, tvals, stage,
+                                       lattice, kLatticeMax);
+        }
+        __syncwarp();
+    }
+}
+
+// RootSample, root UV and point count of every strand of the range, in
+// output order (coalesced), for the frame (generate.h:101-135, :621-623).
+__global__ void strand_roots_kernel(LaunchArgs g) {
+    __shared__ uint32_t staged[8][32 * 12];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const uint32_t P = g.p.cvs_per_strand;
+    for (uint32_t base = (blockIdx.x * (blockDim.x >> 5) + warp) * 32u; base < g.count;
+         base += gridDim.x * (blockDim.x >> 5) * 32u) {
+        const uint32_t i = base + lane;
+        const bool valid = i < g.count;
+        const Root r = sample_root(g.a, g.f, g.p.seed, g.first_strand + (valid ? i : base));
+        uint32_t *rec = staged[warp] + lane * 12;
+        rec[0] = __float_as_uint(r.position.x);
+        rec[1] = __float_as_uint(r.position.y);
+        rec[2] = __float_as_uint(r.position.z);
+        rec[3] = __float_as_uint(r.normal.x);
+        rec[4] = __float_as_uint(r.normal.y);
+        rec[5] = __float_as_uint(r.normal.z);
+        rec[6] = __float_as_uint(r.u);
+        rec[7] = __float_as_uint(r.v);
+        rec[8] = r.triangle;
+        rec[9] = __float_as_uint(r.b1);
+        rec[10] = __float_as_uint(r.b2);
+        rec[11] = r.triangle;  // surface_face_id == triangle_index (generate.h:134)
+        __syncwarp();
+        const uint32_t n = min(32u, g.count - base);
+        if (g.roots) {
+            uint32_t *dst = g.roots + static_cast<uint64_t>(base) * 12u;
+            for (uint32_t w = lane; w < n * 12u; w += 32u) { dst[w] = staged[warp][w]; }
+        }
+        if (valid) {
+            if (g.root_uvs) { g.root_uvs[i] = make_float2(r.u, r.v); }
+            if (g.point_counts) { g.point_counts[i] = P; }
+        }
+        __syncwarp();
+    }
+}
+
+// offsets[g*P + cv] = sample_guide(g, cv/(P-1)) - guide_root(g) for the frame,
+// in the reference's exact (uncontracted) arithmetic (generate.h:137-205).
+__global__ void guide_offsets_kernel(AssetArgs a, FrameArgs f, uint32_t P, float4 *offsets) {
+    const uint64_t n = static_cast<uint64_t>(a.guide_count) * P;
+    for (uint64_t idx = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; idx < n;
+         idx += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint32_t gi = static_cast<uint32_t>(idx / P);
+        const uint32_t cv = static_cast<uint32_t>(idx % P);
+        const uint32_t *rec = a.guides + 14u * static_cast<uint64_t>(gi);
+        const uint32_t first = __ldg(rec + 0);
+        if (first >= a.guide_cv_count) {
+            offsets[idx] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            continue;
+        }
+        const uint32_t count = min(__ldg(rec + 1) & 0xffffu, a.guide_cv_count - first);
+        const uint32_t gtri = __ldg(rec + 2);
+        const float gb1 = __uint_as_float(__ldg(rec + 4));
+        const float gb2 = __uint_as_float(__ldg(rec + 5));
+        const F3 rest_root = {__uint_as_float(__ldg(rec + 8)), __uint_as_float(__ldg(rec + 9)),
+                              __uint_as_float(__ldg(rec + 10))};
+        const bool bound = gtri < a.triangle_count;
+        F3 groot = rest_root;
+        if (f.deformed_guide_cvs) {
+            groot = ld3(f.guide_cvs, first);
+        } else if (f.deformed_positions && bound) {
+            const uint3 t = load_triangle(a, gtri);
+            const float gb0 = __fsub_rn(__fsub_rn(1.0f, gb1), gb2);
+            groot = xbary(ld3(f.positions, t.x), ld3(f.positions, t.y), ld3(f.positions, t.z), gb0, gb1, gb2);
+        }
+        F3 v;
+        if (count <= 1u) {
+            v = ld3(f.guide_cvs, first);
+        } else {
+            const float t = __fdiv_rn(static_cast<float>(cv), static_cast<float>(P - 1u));
+            const float x = __fmul_rn(fminf(fmaxf(t, 0.0f), 1.0f), static_cast<float>(count - 1u));
+            uint32_t i = static_cast<uint32_t>(x);
+            if (i >= count - 1u) { i = count - 2u; }
+            const float fr = __fsub_rn(x, static_cast<float>(i));
+            v = xadd(xmul(ld3(f.guide_cvs, first + i), __fsub_rn(1.0f, fr)), xmul(ld3(f.guide_cvs, first + i + 1u), fr));
+        }
+        if (!f.deformed_guide_cvs && f.deformed_positions && bound) { v = xsub(xadd(v, groot), rest_root); }
+        const F3 d = xsub(v, groot);
+        offsets[idx] = make_float4(d.x, d.y, d.z, 0.0f);
     }
 }
 
@@ -602,15 +899,27 @@ constexpr uint64_t kWorkspaceAlign = 256u;
 inline uint64_t align_up(uint64_t v, uint64_t a) { return (v + a - 1u) / a * a; }
 
 struct WorkspaceLayout {
-    uint64_t keys, order, hist, total;
+    uint64_t keys, order, hist, offsets, offset_bytes, total;
 };
 
-WorkspaceLayout workspace_layout(uint32_t guide_count, uint32_t count) {
+// Largest guide-offset table the warp-parallel generator stages; beyond it
+// (or beyond 128 CVs) strands take the serial per-thread kernel.
+constexpr uint64_t kMaxOffsetTableBytes = uint64_t{1} << 30;
+constexpr uint32_t kMaxParallelCvs = 128u;
+
+bool parallel_path(uint32_t guide_count, uint32_t P) {
+    return P <= kMaxParallelCvs && uint64_t{guide_count} * P * 16u <= kMaxOffsetTableBytes;
+}
+
+// keys[count] | order[count] | bins[guides + 1] | offsets[guides * P] (float4)
+WorkspaceLayout workspace_layout(uint32_t guide_count, uint32_t count, uint32_t P) {
     WorkspaceLayout w{};
     w.keys = 0u;
     w.order = align_up(uint64_t{count} * 4u, kWorkspaceAlign);
     w.hist = w.order + align_up(uint64_t{count} * 4u, kWorkspaceAlign);
-    w.total = w.hist + align_up((uint64_t{guide_count} + 1u) * 4u, kWorkspaceAlign);
+    w.offsets = w.hist + align_up((uint64_t{guide_count} + 1u) * 4u, kWorkspaceAlign);
+    w.offset_bytes = parallel_path(guide_count, P) ? uint64_t{guide_count} * P * 16u : 0u;
+    w.total = w.offsets + align_up(w.offset_bytes, kWorkspaceAlign);
     return w;
 }
 
@@ -678,24 +987,45 @@ dev::ParamArgs resolve_params(const nxg_generation_params &p, float radius_scale
     return r;
 }
 
-using KernelFn = void (*)(LaunchArgs);
+using KernelFn = void (*)(LaunchArgs, const float4 *);
 
 template <int L, int PPT>
 KernelFn pick_noise(bool noise) {
     return noise ? dev::generate_kernel<L, PPT, true> : dev::generate_kernel<L, PPT, false>;
 }
 
-// Tile shape for P CVs: the narrowest power-of-two lane group that holds the
-// strand in one chunk, else 32 lanes with up to 4 CVs per lane.
-KernelFn pick_kernel(uint32_t P, bool noise, int *lanes) {
-    if (P <= 8u) { *lanes = 8; return pick_noise<8, 1>(noise); }
-    if (P <= 16u) { *lanes = 16; return pick_noise<16, 1>(noise); }
-    *lanes = 32;
-    if (P <= 32u) { return pick_noise<32, 1>(noise); }
-    if (P <= 64u) { return pick_noise<32, 2>(noise); }
-    if (P <= 96u) { return pick_noise<32, 3>(noise); }
-    if (P <= 128u) { return pick_noise<32, 4>(noise); }
-    return nullptr;
+template <int PPT>
+KernelFn pick_lanes(int lanes, bool noise) {
+    switch (lanes) {
+        case 2: return pick_noise<2, PPT>(noise);
+        case 4: return pick_noise<4, PPT>(noise);
+        case 8: return pick_noise<8, PPT>(noise);
+        case 16: return pick_noise<16, PPT>(noise);
+        default: return pick_noise<32, PPT>(noise);
+    }
+}
+
+// Tile shape (lanes per strand x CVs per lane) for P CVs: four CVs per lane
+// on the narrowest power-of-two group that holds the strand.
+void default_tile(uint32_t P, int *lanes, int *ppt) {
+    *ppt = 4;
+    int l = 2;
+    while (l < 32 && static_cast<uint32_t>(l * 4) < P) { l *= 2; }
+    *lanes = l;
+}
+
+KernelFn pick_kernel(int lanes, int ppt, bool noise) {
+    switch (ppt) {
+        case 1: return pick_lanes<1>(lanes, noise);
+        case 2: return pick_lanes<2>(lanes, noise);
+        default: return pick_lanes<4>(lanes, noise);
+    }
+}
+
+size_t generate_smem_bytes(uint32_t P, int lanes, int ppt, bool noise, uint32_t warps) {
+    const size_t per_warp = sizeof(uint32_t) * dev::kRecFields * 32u + sizeof(float4) * 32u / lanes * lanes * ppt +
+                            (noise ? sizeof(float2) * 384u : 0u);
+    return sizeof(float4) * dev::kTableFloat4 + sizeof(float) * ((P + 3u) & ~3u) + per_warp * warps;
 }
 
 uint32_t record_cuda(cudaError_t e) {
@@ -715,9 +1045,9 @@ uint32_t check_launch_inputs(const nxg_device_asset_desc &asset, const nxg_packe
     return NXG_ERROR_NONE;
 }
 
-uint32_t check_workspace(const nxg_device_asset_desc &asset, uint32_t count, const void *workspace,
+uint32_t check_workspace(const nxg_device_asset_desc &asset, uint32_t count, uint32_t P, const void *workspace,
                          uint64_t workspace_bytes) {
-    const WorkspaceLayout ws = workspace_layout(asset.header.guide_count, count);
+    const WorkspaceLayout ws = workspace_layout(asset.header.guide_count, count, P);
     if (!workspace || workspace_bytes < ws.total) { return NXG_ERROR_WORKSPACE_TOO_SMALL; }
     if (reinterpret_cast<std::uintptr_t>(workspace) % kWorkspaceAlign != 0u) { return NXG_ERROR_MISALIGNED_OUTPUT; }
     return NXG_ERROR_NONE;
@@ -726,8 +1056,8 @@ uint32_t check_workspace(const nxg_device_asset_desc &asset, uint32_t count, con
 // Counting sort of strands [first, first + count) by their triangle's first
 // stencil guide; leaves the permutation in the workspace's order section.
 uint32_t launch_order(const nxg_device_asset_desc &asset, uint32_t seed, uint32_t first, uint32_t count,
-                      void *workspace, cudaStream_t stream) {
-    const WorkspaceLayout ws = workspace_layout(asset.header.guide_count, count);
+                      uint32_t P, void *workspace, cudaStream_t stream) {
+    const WorkspaceLayout ws = workspace_layout(asset.header.guide_count, count, P);
     auto *wbase = static_cast<unsigned char *>(workspace);
     auto *keys = reinterpret_cast<uint32_t *>(wbase + ws.keys);
     auto *order = reinterpret_cast<uint32_t *>(wbase + ws.order);
@@ -749,13 +1079,16 @@ uint32_t launch_order(const nxg_device_asset_desc &asset, uint32_t seed, uint32_
     return record_cuda(cudaGetLastError());
 }
 
-// The generator over a strand order (the workspace's, or identity when
-// `workspace` is null).
+// The generator over the strand order prepared in `workspace`: the
+// guide-offset table for this frame, then the persistent generate kernel.
 uint32_t launch_generate(const nxg_device_asset_desc &asset, const nxg_deformed_desc &deformed,
                          const nxg_generation_params &params, const nxg_packed_output_desc &output,
-                         const nxg_launch_config &config, uint32_t first, uint32_t count, const void *workspace,
+                         const nxg_launch_config &config, uint32_t first, uint32_t count, void *workspace,
                          cudaStream_t stream) {
     set_last_cuda_error(0);
+    const uint32_t P = params.cvs_per_strand;
+    const WorkspaceLayout ws = workspace_layout(asset.header.guide_count, count, P);
+    auto *wbase = static_cast<unsigned char *>(workspace);
     LaunchArgs g{};
     g.a = resolve_asset(asset);
     g.f = resolve_frame(g.a, deformed);
@@ -766,24 +1099,52 @@ uint32_t launch_generate(const nxg_device_asset_desc &asset, const nxg_deformed_
     g.roots = reinterpret_cast<uint32_t *>(output.roots);
     g.root_uvs = reinterpret_cast<float2 *>(output.root_uvs);
     g.point_counts = output.point_counts;
-    g.order = workspace ? reinterpret_cast<const uint32_t *>(static_cast<const unsigned char *>(workspace) +
-                                                             workspace_layout(asset.header.guide_count, count).order)
-                        : nullptr;
+    g.order = reinterpret_cast<const uint32_t *>(wbase + ws.order);
     const int sms = device_sm_count();
     uint32_t status = NXG_ERROR_NONE;
-    const uint32_t block = std::max<uint32_t>(32u, (config.block_size + 31u) / 32u * 32u);
-    int lanes = 32;
-    KernelFn fn = pick_kernel(params.cvs_per_strand, g.p.noise != 0u, &lanes);
-    if (!fn) {
+    if (!parallel_path(asset.header.guide_count, P)) {
         const uint32_t threads = 128u;
         const uint32_t blocks = static_cast<uint32_t>(std::min<uint64_t>((count + threads - 1u) / threads,
                                                                           static_cast<uint64_t>(sms) * 8u));
         dev::generate_serial_kernel<<<blocks, threads, 0, stream>>>(g);
         return record_cuda(cudaGetLastError());
     }
+    auto *offsets = reinterpret_cast<float4 *>(wbase + ws.offsets);
+    {
+        const uint64_t n = uint64_t{asset.header.guide_count} * P;
+        const uint32_t threads = 256u;
+        const uint32_t blocks = static_cast<uint32_t>(std::min<uint64_t>((n + threads - 1u) / threads,
+                                                                          static_cast<uint64_t>(sms) * 16u));
+        dev::guide_offsets_kernel<<<blocks, threads, 0, stream>>>(g.a, g.f, P, offsets);
+        if ((status = record_cuda(cudaGetLastError()))) { return status; }
+    }
+    if (g.roots || g.root_uvs || g.point_counts) {
+        const uint32_t threads = 256u;
+        const uint32_t per_block = threads;  // one strand per thread
+        const uint32_t blocks = static_cast<uint32_t>(std::min<uint64_t>((count + per_block - 1u) / per_block,
+                                                                          static_cast<uint64_t>(sms) * 8u));
+        dev::strand_roots_kernel<<<blocks, threads, 0, stream>>>(g);
+        if ((status = record_cuda(cudaGetLastError()))) { return status; }
+    }
+    int lanes = 32, ppt = 4;
+    default_tile(P, &lanes, &ppt);
+    const bool noise = g.p.noise != 0u;
+    KernelFn fn = pick_kernel(lanes, ppt, noise);
+    // block_size in [1, 1024] is a request: rounded up to whole warps, then
+    // capped at what this kernel's register footprint can launch.
+    cudaFuncAttributes attr{};
+    if ((status = record_cuda(cudaFuncGetAttributes(&attr, reinterpret_cast<const void *>(fn))))) { return status; }
+    const uint32_t launchable = std::max<uint32_t>(32u, static_cast<uint32_t>(attr.maxThreadsPerBlock) / 32u * 32u);
+    uint32_t block = std::min(launchable, std::max<uint32_t>(32u, (config.block_size + 31u) / 32u * 32u));
+    int device = 0, smem_optin = 48 * 1024;
+    if (cudaGetDevice(&device) == cudaSuccess) {
+        cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    }
+    while (block > 32u && generate_smem_bytes(P, lanes, ppt, noise, block / 32u) > static_cast<size_t>(smem_optin)) {
+        block -= 32u;
+    }
     const uint32_t warps = block / 32u;
-    const uint32_t groups = warps * static_cast<uint32_t>(32 / lanes);
-    const size_t shm = sizeof(float4) * dev::kTableFloat4 + sizeof(dev::Slot) * dev::kSlots * groups;
+    const size_t shm = generate_smem_bytes(P, lanes, ppt, noise, warps);
     if (shm > 48u * 1024u) {
         if ((status = record_cuda(cudaFuncSetAttribute(reinterpret_cast<const void *>(fn),
                                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -797,9 +1158,9 @@ uint32_t launch_generate(const nxg_device_asset_desc &asset, const nxg_deformed_
         return status;
     }
     per_sm = std::max(per_sm, 1);
-    const uint64_t needed = (uint64_t{count} + groups - 1u) / groups;
+    const uint64_t needed = (uint64_t{count} + 32u * warps - 1u) / (32u * warps);
     const uint32_t grid = static_cast<uint32_t>(std::min<uint64_t>(needed, static_cast<uint64_t>(sms) * per_sm));
-    fn<<<grid, block, shm, stream>>>(g);
+    fn<<<grid, block, shm, stream>>>(g, offsets);
     return record_cuda(cudaGetLastError());
 }
 
@@ -837,9 +1198,10 @@ uint32_t validate_range_request(const nxg_device_asset_desc *asset, const nxg_de
 
 extern "C" {
 
-uint64_t nxg_packed_workspace_size(const nxg_device_asset_desc *asset, uint32_t strand_count) {
-    if (!asset || strand_count == 0u) { return 0u; }
-    return nxg::workspace_layout(asset->header.guide_count, strand_count).total;
+uint64_t nxg_packed_workspace_size(const nxg_device_asset_desc *asset, const nxg_generation_params *params,
+                                   uint32_t strand_count) {
+    if (!asset || !params || strand_count == 0u) { return 0u; }
+    return nxg::workspace_layout(asset->header.guide_count, strand_count, params->cvs_per_strand).total;
 }
 
 uint32_t nxg_generate_packed(const nxg_device_asset_desc *asset, const nxg_deformed_desc *deformed,
@@ -861,12 +1223,16 @@ uint32_t nxg_generate_packed_range(const nxg_device_asset_desc *asset, const nxg
     if (error != NXG_ERROR_NONE) { return error; }
     if ((error = nxg::check_launch_inputs(*asset, output)) != NXG_ERROR_NONE) { return error; }
     if (strand_count == 0u) { return NXG_ERROR_NONE; }
-    if ((error = nxg::check_workspace(*asset, strand_count, workspace, workspace_bytes)) != NXG_ERROR_NONE) {
+    if ((error = nxg::check_workspace(*asset, strand_count, params->cvs_per_strand, workspace, workspace_bytes)) !=
+        NXG_ERROR_NONE) {
         return error;
     }
     const auto s = static_cast<cudaStream_t>(stream);
     nxg::set_last_cuda_error(0);
-    if ((error = nxg::launch_order(*asset, params->seed, first_strand, strand_count, workspace, s))) { return error; }
+    if ((error = nxg::launch_order(*asset, params->seed, first_strand, strand_count, params->cvs_per_strand,
+                                   workspace, s))) {
+        return error;
+    }
     const nxg_deformed_desc none{};
     const nxg_launch_config default_config{128u};
     return nxg::launch_generate(*asset, deformed ? *deformed : none, *params, *output,
@@ -886,26 +1252,27 @@ uint32_t nxg_prepare_strand_order(const nxg_device_asset_desc *asset, const nxg_
     }
     if ((error = nxg::check_launch_inputs(*asset, nullptr)) != NXG_ERROR_NONE) { return error; }
     if (strand_count == 0u) { return NXG_ERROR_NONE; }
-    if ((error = nxg::check_workspace(*asset, strand_count, workspace, workspace_bytes)) != NXG_ERROR_NONE) {
+    if ((error = nxg::check_workspace(*asset, strand_count, params->cvs_per_strand, workspace, workspace_bytes)) !=
+        NXG_ERROR_NONE) {
         return error;
     }
     nxg::set_last_cuda_error(0);
-    return nxg::launch_order(*asset, params->seed, first_strand, strand_count, workspace,
+    return nxg::launch_order(*asset, params->seed, first_strand, strand_count, params->cvs_per_strand, workspace,
                              static_cast<cudaStream_t>(stream));
 }
 
 uint32_t nxg_generate_packed_ordered(const nxg_device_asset_desc *asset, const nxg_deformed_desc *deformed,
                                      const nxg_generation_params *params, const nxg_packed_output_desc *output,
                                      const nxg_launch_config *config, uint32_t first_strand,
-                                     uint32_t strand_count, const void *workspace, uint64_t workspace_bytes,
+                                     uint32_t strand_count, void *workspace, uint64_t workspace_bytes,
                                      void *stream) {
     uint32_t error =
         nxg::validate_range_request(asset, deformed, params, output, config, first_strand, strand_count);
     if (error != NXG_ERROR_NONE) { return error; }
     if ((error = nxg::check_launch_inputs(*asset, output)) != NXG_ERROR_NONE) { return error; }
     if (strand_count == 0u) { return NXG_ERROR_NONE; }
-    if (workspace &&
-        (error = nxg::check_workspace(*asset, strand_count, workspace, workspace_bytes)) != NXG_ERROR_NONE) {
+    if ((error = nxg::check_workspace(*asset, strand_count, params->cvs_per_strand, workspace, workspace_bytes)) !=
+        NXG_ERROR_NONE) {
         return error;
     }
     const nxg_deformed_desc none{};

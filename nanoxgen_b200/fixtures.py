@@ -119,6 +119,14 @@ def plain_sphere(strands: int = 10_000, cvs: int = 16, seed: int = 2024) -> Work
                     4, params)
 
 
+# Per-CV guide jitter of the 32-CV guides: a tenth of the mean CV spacing
+# (0.45 / 31).  Jitter comparable to the spacing folds guides back on
+# themselves (consecutive tangents turning by close to 180 degrees), where the
+# reference's transported frame (generate.h:475-481) is ill-conditioned: a
+# one-ulp change of a base CV then moves noisy points by up to 1e-3.
+GUIDE_JITTER_32 = 0.1 * 0.45 / 31
+
+
 def displaced_sphere_radius(theta, phi):
     return 1.0 + 0.05 * np.sin(7.0 * theta) * np.sin(5.0 * phi)
 
@@ -131,7 +139,7 @@ def large_sphere(strands: int = 1_000_000, cvs: int = 32, guides: int = 4096, se
     noise 0.2 at frequency 12 (output 32M float4 = 512 MiB)."""
     rng = np.random.default_rng(seed)
     pos, uv, tris = sphere_mesh(n_lon, n_rings, displaced_sphere_radius)
-    gs = surface_guides(pos, tris, guides, 32, rng, texcoords=uv)
+    gs = surface_guides(pos, tris, guides, 32, rng, texcoords=uv, jitter=GUIDE_JITTER_32)
     params = GenerationParams(strand_count=strands, cvs_per_strand=cvs, seed=11, root_width=0.02,
                               tip_width=0.002, noise_amplitude=0.2, noise_frequency=12.0)
     name = "displaced-sphere-%dk-tris/%d-guides/k8/%d-strands-x%d" % (tris.shape[0] // 1000, guides, strands, cvs)

@@ -50,20 +50,22 @@ class DeviceAsset:
                                                       ctypes.byref(self.desc), msg, 256)
         if code:
             raise _abi.NxgError(code, "make_device_asset_descriptor " + msg.value.decode())
-        self._workspaces: dict[int, torch.Tensor] = {}
+        self._workspaces: dict[tuple, torch.Tensor] = {}
 
     @property
     def header(self):
         return self.desc.header
 
-    def workspace(self, strand_count: int) -> torch.Tensor:
-        """A cached device workspace for `strand_count` strands (256-byte aligned)."""
-        need = int(lib().nxg_packed_workspace_size(ctypes.byref(self.desc), strand_count))
-        ws = self._workspaces.get(strand_count)
+    def workspace(self, params: GenerationParams, strand_count: int) -> torch.Tensor:
+        """A cached device workspace for `strand_count` strands of `params`
+        (256-byte aligned; reused by every call with the same sizes)."""
+        need = int(lib().nxg_packed_workspace_size(ctypes.byref(self.desc), ctypes.byref(params), strand_count))
+        key = (strand_count, int(params.cvs_per_strand))
+        ws = self._workspaces.get(key)
         if ws is None or ws.numel() < need:
             ws = torch.empty(max(need, 256), dtype=torch.uint8, device=self.device)
             assert ws.data_ptr() % 256 == 0
-            self._workspaces[strand_count] = ws
+            self._workspaces[key] = ws
         return ws
 
 
@@ -156,7 +158,7 @@ def generate_packed(dasset: DeviceAsset, params: GenerationParams, radius_scale:
     out = packed_output_descriptor(points, roots, root_uvs, point_counts, radius_scale)
     ddesc = deformed.descriptor() if deformed is not None else DeformedDesc()
     cfg = LaunchConfig(block_size)
-    ws = dasset.workspace(max(n, 1))
+    ws = dasset.workspace(params, max(n, 1))
     handle = _stream_handle(stream)
     if first_strand == 0 and n == int(params.strand_count):
         code = lib().nxg_generate_packed(ctypes.byref(dasset.desc), ctypes.byref(ddesc), ctypes.byref(params),
@@ -198,7 +200,7 @@ def prepare_strand_order(dasset: DeviceAsset, params: GenerationParams, first_st
     """Phase 1 (nxg_prepare_strand_order): sort the strand range into the
     asset's cached workspace, which is returned for phase 2."""
     n = int(params.strand_count) - first_strand if count is None else int(count)
-    ws = dasset.workspace(max(n, 1))
+    ws = dasset.workspace(params, max(n, 1))
     check(lib().nxg_prepare_strand_order(ctypes.byref(dasset.desc), ctypes.byref(params), first_strand, n,
                                          ws.data_ptr(), ws.numel(), _stream_handle(stream)),
           "nxg_prepare_strand_order")
@@ -210,16 +212,17 @@ def generate_packed_ordered(dasset: DeviceAsset, params: GenerationParams, point
                             deformed: Optional[DeformedGeometry] = None, first_strand: int = 0,
                             count: Optional[int] = None, workspace: Optional[torch.Tensor] = None,
                             block_size: int = 128, stream: Optional[torch.cuda.Stream] = None) -> None:
-    """Phase 2 (nxg_generate_packed_ordered) over a prepared workspace, or
-    strand order when `workspace` is None."""
+    """Phase 2 (nxg_generate_packed_ordered) over a workspace prepared by
+    prepare_strand_order for the same range."""
     n = int(params.strand_count) - first_strand if count is None else int(count)
+    if workspace is None:
+        workspace = dasset.workspace(params, max(n, 1))
     out = packed_output_descriptor(points, roots, root_uvs, point_counts, radius_scale)
     ddesc = deformed.descriptor() if deformed is not None else DeformedDesc()
     cfg = LaunchConfig(block_size)
     check(lib().nxg_generate_packed_ordered(
         ctypes.byref(dasset.desc), ctypes.byref(ddesc), ctypes.byref(params), ctypes.byref(out),
-        ctypes.byref(cfg), first_strand, n, workspace.data_ptr() if workspace is not None else None,
-        workspace.numel() if workspace is not None else 0, _stream_handle(stream)),
+        ctypes.byref(cfg), first_strand, n, workspace.data_ptr(), workspace.numel(), _stream_handle(stream)),
         "nxg_generate_packed_ordered")
 
 
@@ -251,7 +254,7 @@ class HostPipeline:
         self.ranges = [(int(a), int(b)) for a, b in zip(bounds[:-1], bounds[1:]) if b > a]
         self.events = [torch.cuda.Event() for _ in self.ranges]
         for a, b in self.ranges:
-            self.dasset.workspace(b - a)
+            self.dasset.workspace(params, b - a)
 
     @property
     def h2d_bytes(self) -> int:

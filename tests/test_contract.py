@@ -242,8 +242,8 @@ def test_launch_entry_points_reject_before_device_work(nxg_lib):
     assert L.nxg_generate_packed(ctypes.byref(c.desc), None, ctypes.byref(c.params), ctypes.byref(c.out), None,
                                  ws.ctypes.data, ws.size, None) == ERRORS["InvalidAssetMetadata"]
     c = Case()
-    need = L.nxg_packed_workspace_size(ctypes.byref(c.desc), 7)
-    assert need % 256 == 0 and need >= 3 * 256
+    need = L.nxg_packed_workspace_size(ctypes.byref(c.desc), ctypes.byref(c.params), 7)
+    assert need % 256 == 0 and need >= 4 * 256
     assert L.nxg_prepare_strand_order(ctypes.byref(c.desc), ctypes.byref(c.params), 0, 8, ws.ctypes.data, ws.size,
                                       None) == ERRORS["InvalidStrandRange"]
     # zero-length ranges succeed without touching the device

@@ -220,7 +220,7 @@ def test_graph_capture_replays_identically(torch_cuda, sphere):
     eager = generate_packed(d, w.params).points.clone()
     s = torch.cuda.Stream()
     g = torch.cuda.CUDAGraph()
-    d.workspace(w.params.strand_count)
+    d.workspace(w.params, w.params.strand_count)
     torch.cuda.synchronize()
     with torch.cuda.graph(g, stream=s):
         generate_packed(d, w.params, points=pts, roots=roots, root_uvs=uvs, point_counts=pc, stream=s)
@@ -243,3 +243,13 @@ def test_large_sphere_full_size_parity(torch_cuda, oracle, nxg_lib):
     theirs = oracle.generate(asset.buffer, w.params, threads=os.cpu_count() or 8)
     rel = _compare(asset, w.params, mine, theirs)
     print("large sphere max rel error %.3g" % rel)
+
+
+@pytest.mark.parametrize("block", [1, 32, 100, 256, 1024])
+def test_launch_block_sizes(torch_cuda, sphere, block):
+    """DeviceLaunchConfig::block_size anywhere in [1, 1024] (device_contract.h:54-56,
+    :165-167) launches and leaves the output unchanged."""
+    w, asset = sphere
+    ref = _gen(torch_cuda, asset, w.params)
+    out = _gen(torch_cuda, asset, w.params, block_size=block)
+    assert all(np.array_equal(x, y) for x, y in zip(ref, out))
