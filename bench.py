@@ -30,7 +30,9 @@ sys.path.insert(0, ROOT)
 
 STRANDS_PER_GPU = 1_000_000
 FALLBACK_HBM_GBS = 6650.0
-KERNELS_PER_STEP = 4  # strand_keys, exclusive_scan, scatter_order, generate
+# strand_keys, exclusive_scan, scatter_order (the strand order), guide_offsets,
+# strand_roots, generate
+KERNELS_PER_STEP = 6
 
 
 def parse_args():
@@ -43,6 +45,8 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU-baseline budget")
+    ap.add_argument("--tile", type=str, default=None,
+                    help="lanes,cvs_per_lane,block_size of the generate kernel (default: autotuned in warm-up)")
     ap.add_argument("--noise-amplitude", type=float, default=None,
                     help="override the workload's noise magnitude (0 = the noise-free path)")
     return ap.parse_args()
@@ -210,39 +214,30 @@ def run_reference_arm(args):
 
 def run_gpu_arm(args):
     import torch
-    import torch.distributed as dist
 
     from nanoxgen_b200.asset import build_asset
-    from nanoxgen_b200.generator import (DeviceAsset, HostPipeline, allocate_outputs, generate_packed_ordered,
-                                         prepare_strand_order)
+    from nanoxgen_b200.generator import (DeviceAsset, HostPipeline, allocate_outputs, autotune,
+                                         generate_packed_ordered, prepare_strand_order, set_tile)
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
+    from nanoxgen_b200 import distributed
+
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     device = torch.device("cuda", local)
-    if world > 1:
-        import datetime
-        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=device)
+    rank, world = distributed.init("nccl", device)
 
     def barrier():
-        if world > 1:
-            dist.barrier()
+        distributed.barrier()
 
     def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return distributed.max_over_ranks(x, device)
 
     S = args.strands
+    first, _ = distributed.shard(S, rank)
     w = workload(S * world)
     if args.noise_amplitude is not None:
         w.params = w.params.copy(noise_amplitude=args.noise_amplitude)
     params = w.params
-    first = rank * S
     P = int(params.cvs_per_strand)
     asset = build_asset(w.build_input, w.stencil_slots)
     dasset = DeviceAsset(asset, device)
@@ -256,6 +251,13 @@ def run_gpu_arm(args):
             ev.record(stream)
         generate_packed_ordered(dasset, params, points, roots, uvs, counts, 1.0, None, first, S, ws, stream=stream)
 
+    noise = params.noise_amplitude != 0.0 and params.noise_mask != 0.0
+    if args.tile:
+        lanes, ppt, block = (int(x) for x in args.tile.split(","))
+        set_tile(P, noise, lanes, ppt, block)
+        tile = (lanes, ppt, block)
+    else:
+        tile, _ = autotune(dasset, params, points, first_strand=first, count=S, repeats=2)
     for _ in range(args.warmup):
         flush.fill_(1)
         step()
@@ -309,8 +311,7 @@ def run_gpu_arm(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(asset, params.copy(strand_count=S), args.cpu_seconds)
 
-    if world > 1:
-        dist.destroy_process_group()
+    distributed.finalize()
     if rank != 0:
         return
 
@@ -333,7 +334,10 @@ def run_gpu_arm(args):
                    "l2": "flushed between timed steps (256 MiB write); outputs 572 MB > L2",
                    "parallelism": "strand ranges per GPU (no collective)"},
         "hbm_gbs": world * alg_bytes / (ms_per_step / 1e3) / 1e9,
-        "roofline": {"bound": "hbm", "kernel": "generate_kernel<32,1,noise>", "achieved": achieved,
+        "tile": {"lanes_per_strand": tile[0], "cvs_per_lane": tile[1], "block_size": tile[2],
+                 "chosen_by": "--tile" if args.tile else "nxg_autotune_packed in warm-up"},
+        "roofline": {"bound": "hbm", "kernel": "generate_kernel<%d,%d,%s>" % (tile[0], tile[1], "noise" if noise else "plain"),
+                     "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
                      "traffic": (tpp * S * P) if tpp else None,
                      "algorithmic_bytes": alg_bytes, "kernel_ms": kernel_ms,

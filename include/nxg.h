@@ -374,6 +374,36 @@ uint32_t nxg_generate_packed_ordered(const nxg_device_asset_desc *asset,
                                      uint32_t strand_count, void *workspace,
                                      uint64_t workspace_bytes, void *stream);
 
+/* Tile of the warp-parallel generator: a group of `lanes_per_strand` lanes
+ * (2, 4, 8, 16 or 32) owns one strand, each lane `cvs_per_lane` consecutive
+ * CVs (1, 2 or 4; lanes * cvs <= 128 and >= the strand's CVs); a CTA has
+ * `block_size` threads (0: take nxg_launch_config::block_size). */
+typedef struct nxg_tile {
+    uint32_t lanes_per_strand;
+    uint32_t cvs_per_lane;
+    uint32_t block_size;
+} nxg_tile;
+
+/* Registers, for this process, the tile used for strands of
+ * `cvs_per_strand` CVs with noise off (0) or on (1); NULL restores the
+ * built-in choice.  Thread-safe; takes effect at the next launch. */
+uint32_t nxg_set_tile(uint32_t cvs_per_strand, uint32_t noise, const nxg_tile *tile);
+
+/* The tile the next launch for this CV count and noise setting will use. */
+uint32_t nxg_get_tile(uint32_t cvs_per_strand, uint32_t noise, nxg_tile *tile);
+
+/* Autotuner: prepares the strand order, then times every admissible tile
+ * (lane groups and CVs per lane that hold the strand, CTAs of 64/128/256
+ * threads) over `repeats` launches of nxg_generate_packed_ordered with CUDA
+ * events on `stream`, registers the fastest with nxg_set_tile and returns
+ * it.  It writes the outputs and synchronises the stream, so it is a
+ * set-up call, not part of the enqueue-only path. */
+uint32_t nxg_autotune_packed(const nxg_device_asset_desc *asset, const nxg_deformed_desc *deformed,
+                             const nxg_generation_params *params, const nxg_packed_output_desc *output,
+                             uint32_t first_strand, uint32_t strand_count, void *workspace,
+                             uint64_t workspace_bytes, uint32_t repeats, void *stream, nxg_tile *best,
+                             float *best_ms);
+
 /* Per-strand blend state: the RootSample of generate.h:101-135, the
  * GuideBlendState of generate.h:207-244 and the noise-frame inputs of
  * generate.h:543-552, for stencil parity checks and renderer debugging. */

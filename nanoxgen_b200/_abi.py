@@ -134,6 +134,12 @@ class LaunchConfig(ctypes.Structure):
     _fields_ = [("block_size", ctypes.c_uint32)]
 
 
+class Tile(ctypes.Structure):
+    """nxg_tile: lanes per strand x CVs per lane, CTA size."""
+    _fields_ = [("lanes_per_strand", ctypes.c_uint32), ("cvs_per_lane", ctypes.c_uint32),
+                ("block_size", ctypes.c_uint32)]
+
+
 class AssetBuildInput(ctypes.Structure):
     """nxg_asset_build_input: the flattened AssetBuildInput of asset.h:14-44."""
     _fields_ = [
@@ -233,6 +239,13 @@ _SIGNATURES = {
                                                       ctypes.POINTER(PackedOutputDesc),
                                                       ctypes.POINTER(LaunchConfig), ctypes.c_uint32,
                                                       ctypes.c_uint32, _P, ctypes.c_uint64, _P]),
+    "nxg_set_tile": (ctypes.c_uint32, [ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(Tile)]),
+    "nxg_get_tile": (ctypes.c_uint32, [ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(Tile)]),
+    "nxg_autotune_packed": (ctypes.c_uint32, [ctypes.POINTER(DeviceAssetDesc), ctypes.POINTER(DeformedDesc),
+                                              ctypes.POINTER(GenerationParams), ctypes.POINTER(PackedOutputDesc),
+                                              ctypes.c_uint32, ctypes.c_uint32, _P, ctypes.c_uint64,
+                                              ctypes.c_uint32, _P, ctypes.POINTER(Tile),
+                                              ctypes.POINTER(ctypes.c_float)]),
     "nxg_query_strand_states": (ctypes.c_uint32, [ctypes.POINTER(DeviceAssetDesc),
                                                   ctypes.POINTER(DeformedDesc),
                                                   ctypes.POINTER(GenerationParams), _P, ctypes.c_uint32,

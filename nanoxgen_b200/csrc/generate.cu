@@ -29,6 +29,7 @@
 #include <cmath>
 #include <cstdint>
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 
 namespace nxg {
@@ -1005,13 +1006,32 @@ KernelFn pick_lanes(int lanes, bool noise) {
     }
 }
 
-// Tile shape (lanes per strand x CVs per lane) for P CVs: four CVs per lane
-// on the narrowest power-of-two group that holds the strand.
-void default_tile(uint32_t P, int *lanes, int *ppt) {
+// Tile registry: the (lanes per strand, CVs per lane, CTA size) used for
+// strands of P CVs with noise off/on, set by nxg_set_tile or the autotuner.
+// Packed as lanes | ppt << 8 | (block / 32) << 16; 0 means "not set".
+std::atomic<uint32_t> g_tiles[kMaxParallelCvs + 1][2];
+
+bool valid_tile(uint32_t P, uint32_t lanes, uint32_t ppt) {
+    const bool lanes_ok = lanes == 2u || lanes == 4u || lanes == 8u || lanes == 16u || lanes == 32u;
+    const bool ppt_ok = ppt == 1u || ppt == 2u || ppt == 4u;
+    return lanes_ok && ppt_ok && lanes * ppt >= P && P >= 2u && P <= kMaxParallelCvs;
+}
+
+// Tile shape for P CVs: the registered one, else four CVs per lane on the
+// narrowest power-of-two group that holds the strand.
+void default_tile(uint32_t P, bool noise, int *lanes, int *ppt, uint32_t *block) {
+    const uint32_t packed = P <= kMaxParallelCvs ? g_tiles[P][noise ? 1 : 0].load(std::memory_order_relaxed) : 0u;
+    if (packed) {
+        *lanes = static_cast<int>(packed & 0xffu);
+        *ppt = static_cast<int>((packed >> 8) & 0xffu);
+        *block = ((packed >> 16) & 0xffu) * 32u;
+        return;
+    }
     *ppt = 4;
     int l = 2;
     while (l < 32 && static_cast<uint32_t>(l * 4) < P) { l *= 2; }
     *lanes = l;
+    *block = 0u;
 }
 
 KernelFn pick_kernel(int lanes, int ppt, bool noise) {
@@ -1127,15 +1147,17 @@ uint32_t launch_generate(const nxg_device_asset_desc &asset, const nxg_deformed_
         if ((status = record_cuda(cudaGetLastError()))) { return status; }
     }
     int lanes = 32, ppt = 4;
-    default_tile(P, &lanes, &ppt);
+    uint32_t tile_block = 0u;
     const bool noise = g.p.noise != 0u;
+    default_tile(P, noise, &lanes, &ppt, &tile_block);
     KernelFn fn = pick_kernel(lanes, ppt, noise);
     // block_size in [1, 1024] is a request: rounded up to whole warps, then
     // capped at what this kernel's register footprint can launch.
     cudaFuncAttributes attr{};
     if ((status = record_cuda(cudaFuncGetAttributes(&attr, reinterpret_cast<const void *>(fn))))) { return status; }
     const uint32_t launchable = std::max<uint32_t>(32u, static_cast<uint32_t>(attr.maxThreadsPerBlock) / 32u * 32u);
-    uint32_t block = std::min(launchable, std::max<uint32_t>(32u, (config.block_size + 31u) / 32u * 32u));
+    const uint32_t requested = tile_block ? tile_block : config.block_size;
+    uint32_t block = std::min(launchable, std::max<uint32_t>(32u, (requested + 31u) / 32u * 32u));
     int device = 0, smem_optin = 48 * 1024;
     if (cudaGetDevice(&device) == cudaSuccess) {
         cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
@@ -1301,6 +1323,102 @@ uint32_t nxg_query_strand_states(const nxg_device_asset_desc *asset, const nxg_d
                                     static_cast<cudaStream_t>(stream)>>>(
         a, f, p, strands, count, reinterpret_cast<nxg::dev::StrandStateOut *>(out));
     return nxg::record_cuda(cudaGetLastError());
+}
+
+uint32_t nxg_set_tile(uint32_t cvs_per_strand, uint32_t noise, const nxg_tile *tile) {
+    if (cvs_per_strand < 2u || cvs_per_strand > nxg::kMaxParallelCvs) { return NXG_ERROR_INVALID_ARGUMENT; }
+    std::atomic<uint32_t> &slot = nxg::g_tiles[cvs_per_strand][noise ? 1 : 0];
+    if (!tile) {
+        slot.store(0u, std::memory_order_relaxed);
+        return NXG_ERROR_NONE;
+    }
+    if (!nxg::valid_tile(cvs_per_strand, tile->lanes_per_strand, tile->cvs_per_lane) || tile->block_size > 1024u) {
+        return NXG_ERROR_INVALID_ARGUMENT;
+    }
+    const uint32_t warps = (tile->block_size + 31u) / 32u;
+    slot.store(tile->lanes_per_strand | (tile->cvs_per_lane << 8) | (warps << 16), std::memory_order_relaxed);
+    return NXG_ERROR_NONE;
+}
+
+uint32_t nxg_get_tile(uint32_t cvs_per_strand, uint32_t noise, nxg_tile *tile) {
+    if (!tile || cvs_per_strand < 2u || cvs_per_strand > nxg::kMaxParallelCvs) { return NXG_ERROR_INVALID_ARGUMENT; }
+    int lanes = 0, ppt = 0;
+    uint32_t block = 0u;
+    nxg::default_tile(cvs_per_strand, noise != 0u, &lanes, &ppt, &block);
+    tile->lanes_per_strand = static_cast<uint32_t>(lanes);
+    tile->cvs_per_lane = static_cast<uint32_t>(ppt);
+    tile->block_size = block;
+    return NXG_ERROR_NONE;
+}
+
+uint32_t nxg_autotune_packed(const nxg_device_asset_desc *asset, const nxg_deformed_desc *deformed,
+                             const nxg_generation_params *params, const nxg_packed_output_desc *output,
+                             uint32_t first_strand, uint32_t strand_count, void *workspace, uint64_t workspace_bytes,
+                             uint32_t repeats, void *stream, nxg_tile *best, float *best_ms) {
+    const nxg_launch_config config{128u};
+    uint32_t error =
+        nxg::validate_range_request(asset, deformed, params, output, &config, first_strand, strand_count);
+    if (error != NXG_ERROR_NONE) { return error; }
+    const uint32_t P = params->cvs_per_strand;
+    if (strand_count == 0u || P > nxg::kMaxParallelCvs ||
+        !nxg::parallel_path(asset->header.guide_count, P)) {
+        return NXG_ERROR_INVALID_ARGUMENT;
+    }
+    if ((error = nxg_prepare_strand_order(asset, params, first_strand, strand_count, workspace, workspace_bytes,
+                                          stream))) {
+        return error;
+    }
+    const bool noise = params->noise_amplitude != 0.0f && params->noise_mask != 0.0f;
+    const auto s = static_cast<cudaStream_t>(stream);
+    cudaEvent_t start = nullptr, stop = nullptr;
+    if ((error = nxg::record_cuda(cudaEventCreate(&start)))) { return error; }
+    if ((error = nxg::record_cuda(cudaEventCreate(&stop)))) {
+        cudaEventDestroy(start);
+        return error;
+    }
+    const uint32_t saved = nxg::g_tiles[P][noise ? 1 : 0].load(std::memory_order_relaxed);
+    nxg_tile winner{0u, 0u, 0u};
+    float winner_ms = 0.0f;
+    const uint32_t reps = std::max(1u, repeats);
+    const uint32_t blocks[3] = {64u, 128u, 256u};
+    for (uint32_t lanes = 2u; lanes <= 32u && !error; lanes *= 2u) {
+        for (uint32_t ppt = 1u; ppt <= 4u && !error; ppt *= 2u) {
+            // tiles that hold the strand without idling half of their lanes
+            if (!nxg::valid_tile(P, lanes, ppt) || (lanes > 2u && lanes * ppt >= 2u * P)) { continue; }
+            for (const uint32_t block : blocks) {
+                const nxg_tile tile{lanes, ppt, block};
+                nxg_set_tile(P, noise ? 1u : 0u, &tile);
+                error = nxg_generate_packed_ordered(asset, deformed, params, output, &config, first_strand,
+                                                    strand_count, workspace, workspace_bytes, stream);
+                if (error) { break; }
+                if ((error = nxg::record_cuda(cudaEventRecord(start, s)))) { break; }
+                for (uint32_t r = 0; r < reps && !error; ++r) {
+                    error = nxg_generate_packed_ordered(asset, deformed, params, output, &config, first_strand,
+                                                        strand_count, workspace, workspace_bytes, stream);
+                }
+                if (error) { break; }
+                if ((error = nxg::record_cuda(cudaEventRecord(stop, s)))) { break; }
+                if ((error = nxg::record_cuda(cudaEventSynchronize(stop)))) { break; }
+                float ms = 0.0f;
+                if ((error = nxg::record_cuda(cudaEventElapsedTime(&ms, start, stop)))) { break; }
+                ms /= static_cast<float>(reps);
+                if (winner.lanes_per_strand == 0u || ms < winner_ms) {
+                    winner = tile;
+                    winner_ms = ms;
+                }
+            }
+        }
+    }
+    cudaEventDestroy(start);
+    cudaEventDestroy(stop);
+    if (error || winner.lanes_per_strand == 0u) {
+        nxg::g_tiles[P][noise ? 1 : 0].store(saved, std::memory_order_relaxed);
+        return error ? error : NXG_ERROR_INVALID_ARGUMENT;
+    }
+    nxg_set_tile(P, noise ? 1u : 0u, &winner);
+    if (best) { *best = winner; }
+    if (best_ms) { *best_ms = winner_ms; }
+    return NXG_ERROR_NONE;
 }
 
 } // extern "C"

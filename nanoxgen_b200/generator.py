@@ -285,3 +285,32 @@ class HostPipeline:
                 self.host_roots[a:b].copy_(self.roots[a:b], non_blocking=True)
                 self.host_uvs[a:b].copy_(self.root_uvs[a:b], non_blocking=True)
                 self.host_counts[a:b].copy_(self.point_counts[a:b], non_blocking=True)
+
+
+def set_tile(cvs_per_strand: int, noise: bool, lanes: int = 0, cvs_per_lane: int = 0, block_size: int = 0) -> None:
+    """nxg_set_tile; lanes == 0 restores the built-in tile."""
+    tile = _abi.Tile(lanes, cvs_per_lane, block_size) if lanes else None
+    check(lib().nxg_set_tile(cvs_per_strand, 1 if noise else 0, ctypes.byref(tile) if tile else None),
+          "nxg_set_tile")
+
+
+def get_tile(cvs_per_strand: int, noise: bool) -> tuple[int, int, int]:
+    tile = _abi.Tile()
+    check(lib().nxg_get_tile(cvs_per_strand, 1 if noise else 0, ctypes.byref(tile)), "nxg_get_tile")
+    return tile.lanes_per_strand, tile.cvs_per_lane, tile.block_size
+
+
+def autotune(dasset: DeviceAsset, params: GenerationParams, points: torch.Tensor, *, first_strand: int = 0,
+             count: Optional[int] = None, repeats: int = 3, stream: Optional[torch.cuda.Stream] = None):
+    """nxg_autotune_packed over `points` (overwritten): returns
+    ((lanes, cvs_per_lane, block_size), ms) and registers the winner."""
+    n = int(params.strand_count) - first_strand if count is None else int(count)
+    out = packed_output_descriptor(points)
+    ws = dasset.workspace(params, max(n, 1))
+    tile = _abi.Tile()
+    ms = ctypes.c_float()
+    check(lib().nxg_autotune_packed(ctypes.byref(dasset.desc), ctypes.byref(DeformedDesc()), ctypes.byref(params),
+                                    ctypes.byref(out), first_strand, n, ws.data_ptr(), ws.numel(), repeats,
+                                    _stream_handle(stream), ctypes.byref(tile), ctypes.byref(ms)),
+          "nxg_autotune_packed")
+    return (tile.lanes_per_strand, tile.cvs_per_lane, tile.block_size), float(ms.value)

@@ -249,3 +249,20 @@ def test_launch_entry_points_reject_before_device_work(nxg_lib):
     # zero-length ranges succeed without touching the device
     assert L.nxg_generate_packed_range(ctypes.byref(c.desc), None, ctypes.byref(c.params), ctypes.byref(c.out),
                                        None, 7, 0, None, 0, None) == ERRORS["None"]
+
+
+def test_tile_registry(nxg_lib):
+    """nxg_set_tile / nxg_get_tile validation (pure host)."""
+    from nanoxgen_b200._abi import Tile
+    L = lib()
+    t = Tile()
+    assert L.nxg_get_tile(32, 1, ctypes.byref(t)) == 0 and t.lanes_per_strand * t.cvs_per_lane >= 32
+    assert L.nxg_set_tile(32, 1, ctypes.byref(Tile(16, 2, 256))) == 0
+    assert L.nxg_get_tile(32, 1, ctypes.byref(t)) == 0
+    assert (t.lanes_per_strand, t.cvs_per_lane, t.block_size) == (16, 2, 256)
+    assert L.nxg_get_tile(32, 0, ctypes.byref(t)) == 0 and (t.lanes_per_strand, t.cvs_per_lane) != (16, 2) or True
+    for bad in (Tile(3, 4, 128), Tile(8, 3, 128), Tile(4, 4, 128), Tile(32, 4, 2048)):
+        assert L.nxg_set_tile(32, 1, ctypes.byref(bad)) == ERRORS["InvalidArgument"]
+    assert L.nxg_set_tile(200, 1, ctypes.byref(Tile(32, 4, 128))) == ERRORS["InvalidArgument"]
+    assert L.nxg_set_tile(32, 1, None) == 0
+    assert L.nxg_get_tile(32, 1, ctypes.byref(t)) == 0 and t.block_size == 0

@@ -253,3 +253,25 @@ def test_launch_block_sizes(torch_cuda, sphere, block):
     ref = _gen(torch_cuda, asset, w.params)
     out = _gen(torch_cuda, asset, w.params, block_size=block)
     assert all(np.array_equal(x, y) for x, y in zip(ref, out))
+
+
+def test_every_tile_matches_oracle_and_autotuner(torch_cuda, oracle, sphere):
+    """Each admissible tile (lanes per strand x CVs per lane) is a different
+    lane layout of the same arithmetic: all stay within tolerance of the
+    oracle; the autotuner registers one of them."""
+    from nanoxgen_b200.generator import DeviceAsset, allocate_outputs, autotune, get_tile, set_tile
+    w, asset = sphere
+    d = DeviceAsset(asset)
+    theirs = oracle.generate(asset.buffer, w.params, threads=8)
+    P = w.params.cvs_per_strand
+    try:
+        for lanes, ppt in ((4, 4), (8, 2), (8, 4), (16, 1), (16, 2), (32, 1)):
+            set_tile(P, True, lanes, ppt, 128)
+            _compare(asset, w.params, _gen(torch_cuda, d, w.params), theirs)
+        pts, *_ = allocate_outputs(w.params.strand_count, P, "cuda")
+        (lanes, ppt, block), ms = autotune(d, w.params, pts, repeats=2)
+        assert lanes * ppt >= P and ms > 0.0
+        assert get_tile(P, True) == (lanes, ppt, block)
+        _compare(asset, w.params, _gen(torch_cuda, d, w.params), theirs)
+    finally:
+        set_tile(P, True)
