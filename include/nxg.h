@@ -222,6 +222,7 @@ typedef enum nxg_error {
     NXG_ERROR_INVALID_STRAND_RANGE = 65,  /* first + count exceeds strand_count */
     NXG_ERROR_WORKSPACE_TOO_SMALL = 66,   /* workspace missing or below the queried size */
     NXG_ERROR_MISALIGNED_OUTPUT = 67,     /* points not 16-byte aligned, or workspace not 256-byte aligned */
+    NXG_ERROR_STATIC_SCRATCH_LIMIT = 68,  /* request needs more than NXG_STATIC_SCRATCH_BYTES of scratch */
     NXG_ERROR_CUDA = 96                   /* a CUDA runtime call failed; see nxg_last_cuda_error */
 } nxg_error;
 
@@ -403,6 +404,30 @@ uint32_t nxg_autotune_packed(const nxg_device_asset_desc *asset, const nxg_defor
                              uint32_t first_strand, uint32_t strand_count, void *workspace,
                              uint64_t workspace_bytes, uint32_t repeats, void *stream, nxg_tile *best,
                              float *best_ms);
+
+/* Size of the library-owned device scratch used by
+ * nxg_generate_packed_static_scratch (4 MiB, held on every device that
+ * loads the library until the process exits). */
+#define NXG_STATIC_SCRATCH_BYTES (4ull << 20)
+
+/* No counterpart in the reference.  nxg_generate_packed for callers that
+ * cannot allocate device memory -- a plugin whose host application owns all
+ * allocations and their budget, or a frame loop where cudaMalloc would
+ * synchronise the device -- using the library's own fixed scratch instead
+ * of a caller workspace.  Same validation and output as
+ * nxg_generate_packed; returns NXG_ERROR_STATIC_SCRATCH_LIMIT, before
+ * touching the device, when nxg_packed_workspace_size for the request
+ * exceeds NXG_STATIC_SCRATCH_BYTES (for a 4,096-guide description at 32
+ * CVs, about 260,000 strands fit and a million do not).  Allocates
+ * nothing.  The first call on each device looks up the scratch's device
+ * address (once per device), so make that first call before any stream
+ * capture.  Every call shares the one scratch: calls that can overlap on
+ * the GPU (different streams without ordering between them) race on it. */
+uint32_t nxg_generate_packed_static_scratch(const nxg_device_asset_desc *asset,
+                                            const nxg_deformed_desc *deformed,
+                                            const nxg_generation_params *params,
+                                            const nxg_packed_output_desc *output,
+                                            const nxg_launch_config *config, void *stream);
 
 /* Per-strand blend state: the RootSample of generate.h:101-135, the
  * GuideBlendState of generate.h:207-244 and the noise-frame inputs of

@@ -185,7 +185,8 @@ ERROR_NAMES = [
 ]
 ERRORS = {name: code for code, name in enumerate(ERROR_NAMES)}
 ERRORS.update(InvalidArgument=64, InvalidStrandRange=65, WorkspaceTooSmall=66,
-              MisalignedOutput=67, Cuda=96)
+              MisalignedOutput=67, StaticScratchLimit=68, Cuda=96)
+STATIC_SCRATCH_BYTES = 4 << 20  # NXG_STATIC_SCRATCH_BYTES
 ERROR_BY_CODE = {code: name for name, code in ERRORS.items()}
 
 # Every entry point include/nxg.h declares: name -> (restype, argtypes).
@@ -246,6 +247,11 @@ _SIGNATURES = {
                                               ctypes.c_uint32, ctypes.c_uint32, _P, ctypes.c_uint64,
                                               ctypes.c_uint32, _P, ctypes.POINTER(Tile),
                                               ctypes.POINTER(ctypes.c_float)]),
+    "nxg_generate_packed_static_scratch": (ctypes.c_uint32, [ctypes.POINTER(DeviceAssetDesc),
+                                                             ctypes.POINTER(DeformedDesc),
+                                                             ctypes.POINTER(GenerationParams),
+                                                             ctypes.POINTER(PackedOutputDesc),
+                                                             ctypes.POINTER(LaunchConfig), _P]),
     "nxg_query_strand_states": (ctypes.c_uint32, [ctypes.POINTER(DeviceAssetDesc),
                                                   ctypes.POINTER(DeformedDesc),
                                                   ctypes.POINTER(GenerationParams), _P, ctypes.c_uint32,

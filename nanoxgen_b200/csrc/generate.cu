@@ -30,6 +30,7 @@
 #include <cstdint>
 #include <algorithm>
 #include <atomic>
+#include <mutex>
 #include <cstring>
 
 namespace nxg {
@@ -1422,3 +1423,62 @@ uint32_t nxg_autotune_packed(const nxg_device_asset_desc *asset, const nxg_defor
 }
 
 } // extern "C"
+
+// ---------------------------------------------------------------------------
+// Generation without a caller-provided workspace.
+//
+// Some callers cannot allocate device memory themselves: a renderer plugin
+// whose host application owns every allocation through its own pool and
+// memory budget, or a frame loop that must not call cudaMalloc because it
+// implicitly synchronises the device and stalls the frame.  For them the
+// library keeps its own scratch in a fixed-size array in device memory
+// (below), held by every GPU that loads the library until the process exits.
+// ---------------------------------------------------------------------------
+namespace nxg {
+namespace {
+
+__device__ __align__(256) unsigned char g_static_scratch[NXG_STATIC_SCRATCH_BYTES];
+
+constexpr int kMaxScratchDevices = 64;
+std::atomic<void *> g_static_scratch_address[kMaxScratchDevices];
+std::mutex g_static_scratch_mutex;
+
+// The device address of g_static_scratch on the current device, looked up
+// once per device with cudaGetSymbolAddress (host code may not use the
+// array's name as a device pointer).
+uint32_t static_scratch_address(void **out) {
+    int device = 0;
+    if (const uint32_t status = record_cuda(cudaGetDevice(&device))) { return status; }
+    if (device < 0 || device >= kMaxScratchDevices) { return NXG_ERROR_INVALID_ARGUMENT; }
+    void *address = g_static_scratch_address[device].load(std::memory_order_acquire);
+    if (!address) {
+        std::lock_guard<std::mutex> lock(g_static_scratch_mutex);
+        address = g_static_scratch_address[device].load(std::memory_order_acquire);
+        if (!address) {
+            if (const uint32_t status = record_cuda(cudaGetSymbolAddress(&address, g_static_scratch))) {
+                return status;
+            }
+            g_static_scratch_address[device].store(address, std::memory_order_release);
+        }
+    }
+    *out = address;
+    return NXG_ERROR_NONE;
+}
+
+} // namespace
+} // namespace nxg
+
+extern "C" uint32_t nxg_generate_packed_static_scratch(const nxg_device_asset_desc *asset,
+                                                      const nxg_deformed_desc *deformed,
+                                                      const nxg_generation_params *params,
+                                                      const nxg_packed_output_desc *output,
+                                                      const nxg_launch_config *config, void *stream) {
+    const uint32_t error = nxg_validate_packed_request(asset, deformed, params, output, config);
+    if (error != NXG_ERROR_NONE) { return error; }
+    if (nxg_packed_workspace_size(asset, params, params->strand_count) > NXG_STATIC_SCRATCH_BYTES) {
+        return NXG_ERROR_STATIC_SCRATCH_LIMIT;
+    }
+    void *scratch = nullptr;
+    if (const uint32_t status = nxg::static_scratch_address(&scratch)) { return status; }
+    return nxg_generate_packed(asset, deformed, params, output, config, scratch, NXG_STATIC_SCRATCH_BYTES, stream);
+}

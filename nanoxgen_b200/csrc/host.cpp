@@ -423,6 +423,8 @@ const char *nxg_error_message(uint32_t code) {
         case NXG_ERROR_WORKSPACE_TOO_SMALL: return "device workspace is missing or too small";
         case NXG_ERROR_MISALIGNED_OUTPUT:
             return "device point output must be 16-byte aligned and workspace 256-byte aligned";
+        case NXG_ERROR_STATIC_SCRATCH_LIMIT:
+            return "request needs more scratch than the library's static scratch holds (NXG_STATIC_SCRATCH_BYTES)";
         case NXG_ERROR_CUDA: return "a CUDA runtime call failed";
         default: return "unknown device generation error";
     }
