@@ -405,6 +405,27 @@ uint32_t nxg_autotune_packed(const nxg_device_asset_desc *asset, const nxg_defor
                              uint64_t workspace_bytes, uint32_t repeats, void *stream, nxg_tile *best,
                              float *best_ms);
 
+/* Motion samples of one description in one enqueue (the device form of one
+ * generate_packed_deformed_cpu call per shutter sample, asset.cpp:421-449):
+ * sample i (strictly increasing finite times, each deformation validated as
+ * in device_contract.h:256-288) is written to outputs[i], a packed output
+ * with the same contract as nxg_generate_packed's.  The strand order is
+ * prepared once for all samples; strand identities are shared. */
+uint32_t nxg_generate_motion_packed(const nxg_device_asset_desc *asset,
+                                    const nxg_motion_sample_desc *samples, uint32_t sample_count,
+                                    const nxg_generation_params *params,
+                                    const nxg_packed_output_desc *outputs,
+                                    const nxg_launch_config *config, void *workspace,
+                                    uint64_t workspace_bytes, void *stream);
+
+/* The reference's motion contract (device_contract.h:42-53, :256-288):
+ * validated exactly as nxg_validate_motion_request, then writes sample-major
+ * absolute Vec3 positions, strand_count * cvs_per_strand per sample. */
+uint32_t nxg_generate_motion(const nxg_device_asset_desc *asset, const nxg_motion_sample_desc *samples,
+                             uint32_t sample_count, const nxg_generation_params *params,
+                             const nxg_motion_output_desc *output, const nxg_launch_config *config,
+                             void *workspace, uint64_t workspace_bytes, void *stream);
+
 /* Size of the library-owned device scratch used by
  * nxg_generate_packed_static_scratch (4 MiB, held on every device that
  * loads the library until the process exits). */

@@ -252,6 +252,14 @@ _SIGNATURES = {
                                                              ctypes.POINTER(GenerationParams),
                                                              ctypes.POINTER(PackedOutputDesc),
                                                              ctypes.POINTER(LaunchConfig), _P]),
+    "nxg_generate_motion_packed": (ctypes.c_uint32, [ctypes.POINTER(DeviceAssetDesc), ctypes.POINTER(MotionSampleDesc),
+                                                     ctypes.c_uint32, ctypes.POINTER(GenerationParams),
+                                                     ctypes.POINTER(PackedOutputDesc), ctypes.POINTER(LaunchConfig),
+                                                     _P, ctypes.c_uint64, _P]),
+    "nxg_generate_motion": (ctypes.c_uint32, [ctypes.POINTER(DeviceAssetDesc), ctypes.POINTER(MotionSampleDesc),
+                                              ctypes.c_uint32, ctypes.POINTER(GenerationParams),
+                                              ctypes.POINTER(MotionOutputDesc), ctypes.POINTER(LaunchConfig), _P,
+                                              ctypes.c_uint64, _P]),
     "nxg_query_strand_states": (ctypes.c_uint32, [ctypes.POINTER(DeviceAssetDesc),
                                                   ctypes.POINTER(DeformedDesc),
                                                   ctypes.POINTER(GenerationParams), _P, ctypes.c_uint32,

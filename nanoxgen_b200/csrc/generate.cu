@@ -43,6 +43,7 @@ struct LaunchArgs {
     uint32_t first_strand;   // global id of output record 0
     uint32_t count;          // strands in this launch
     float4 *points;
+    float *vec3_points;      // when set: sample-major Vec3 output instead of float4 (motion contract)
     uint32_t *roots;         // 12 words per strand, or nullptr
     float2 *root_uvs;
     uint32_t *point_counts;
@@ -471,8 +472,18 @@ __device__ __forceinline__ void emit_strand(const LaunchArgs &g, const Records &
     }
     __syncwarp();
     if (active) {
-        float4 *out = g.points + static_cast<uint64_t>(local) * static_cast<uint32_t>(P);
-        for (int cv = gl; cv < P; cv += L) { __stcs(out + cv, stage[cv]); }
+        if (g.vec3_points) {
+            // Vec3 positions, 3P consecutive floats per strand (device_contract.h:47-52)
+            float *out3 = g.vec3_points + static_cast<uint64_t>(local) * static_cast<uint32_t>(3 * P);
+            const float *st = reinterpret_cast<const float *>(stage);
+            for (int i = gl; i < 3 * P; i += L) {
+                const int cv = i / 3;
+                __stcs(out3 + i, st[4 * cv + (i - 3 * cv)]);
+            }
+        } else {
+            float4 *out = g.points + static_cast<uint64_t>(local) * static_cast<uint32_t>(P);
+            for (int cv = gl; cv < P; cv += L) { __stcs(out + cv, stage[cv]); }
+        }
     }
     __syncwarp();
 }
@@ -684,6 +695,17 @@ __device__ F3 serial_advance(const LaunchArgs &g, const Root &root, const Slot *
     return point;
 }
 
+__device__ __forceinline__ void serial_store(const LaunchArgs &g, uint32_t local, uint32_t cv, F3 q, float radius) {
+    const uint64_t index = static_cast<uint64_t>(local) * g.p.cvs_per_strand + cv;
+    if (g.vec3_points) {
+        g.vec3_points[3u * index] = q.x;
+        g.vec3_points[3u * index + 1u] = q.y;
+        g.vec3_points[3u * index + 2u] = q.z;
+    } else {
+        g.points[index] = make_float4(q.x, q.y, q.z, radius);
+    }
+}
+
 __global__ void generate_serial_kernel(LaunchArgs g) {
     __shared__ float4 table[kTableFloat4];
     for (int i = threadIdx.x; i < kTableFloat4; i += blockDim.x) {
@@ -707,7 +729,6 @@ __global__ void generate_serial_kernel(LaunchArgs g) {
             }
             if (slots[j].flags & kSlotBlended) { wsum = __fadd_rn(wsum, slots[j].w); }
         }
-        float4 *out = g.points + static_cast<uint64_t>(local) * P;
         float scale = 1.0f;
         F3 domain = {0.0f, 0.0f, 0.0f};
         float f_eff = 0.0f;
@@ -751,13 +772,13 @@ __global__ void generate_serial_kernel(LaunchArgs g) {
                 F3 q = serial_advance(g, root, slots, wsum, nearest, domain, f_eff, table, c);
                 if (scale != 1.0f) { q = root.position + (q - root.position) * scale; }
                 const float t = __fdiv_rn(static_cast<float>(cv), static_cast<float>(P - 1u));
-                out[cv] = make_float4(q.x, q.y, q.z, strand_radius(p, t));
+                serial_store(g, local, cv, q, strand_radius(p, t));
             }
         } else {
             for (uint32_t cv = 0u; cv < P; ++cv) {
                 const F3 q = serial_base_cv(g, root, slots, wsum, nearest, cv);
                 const float t = __fdiv_rn(static_cast<float>(cv), static_cast<float>(P - 1u));
-                out[cv] = make_float4(q.x, q.y, q.z, strand_radius(p, t));
+                serial_store(g, local, cv, q, strand_radius(p, t));
             }
         }
         if (g.roots) {
@@ -1105,7 +1126,7 @@ uint32_t launch_order(const nxg_device_asset_desc &asset, uint32_t seed, uint32_
 uint32_t launch_generate(const nxg_device_asset_desc &asset, const nxg_deformed_desc &deformed,
                          const nxg_generation_params &params, const nxg_packed_output_desc &output,
                          const nxg_launch_config &config, uint32_t first, uint32_t count, void *workspace,
-                         cudaStream_t stream) {
+                         cudaStream_t stream, float *vec3_points = nullptr) {
     set_last_cuda_error(0);
     const uint32_t P = params.cvs_per_strand;
     const WorkspaceLayout ws = workspace_layout(asset.header.guide_count, count, P);
@@ -1117,6 +1138,7 @@ uint32_t launch_generate(const nxg_device_asset_desc &asset, const nxg_deformed_
     g.first_strand = first;
     g.count = count;
     g.points = reinterpret_cast<float4 *>(output.points);
+    g.vec3_points = vec3_points;
     g.roots = reinterpret_cast<uint32_t *>(output.roots);
     g.root_uvs = reinterpret_cast<float2 *>(output.root_uvs);
     g.point_counts = output.point_counts;
@@ -1423,6 +1445,95 @@ uint32_t nxg_autotune_packed(const nxg_device_asset_desc *asset, const nxg_defor
 }
 
 } // extern "C"
+
+// ---------------------------------------------------------------------------
+// Motion samples (device_contract.h:42-53, :256-288): one description at
+// several deformed frames, strand identities shared.  The strand order depends
+// only on rest data and the seed, so it is prepared once; each sample then
+// rebuilds the offset table for its frame and runs the generator.
+// ---------------------------------------------------------------------------
+namespace nxg {
+namespace {
+
+uint32_t validate_motion_samples(const nxg_device_asset_desc &asset, const nxg_motion_sample_desc *samples,
+                                 uint32_t sample_count, const nxg_generation_params &params,
+                                 const nxg_launch_config &config) {
+    if (!samples || sample_count == 0u) { return NXG_ERROR_MISSING_MOTION_SAMPLES; }
+    float previous = -INFINITY;
+    for (uint32_t i = 0; i < sample_count; ++i) {
+        if (!std::isfinite(samples[i].time) || samples[i].time <= previous) { return NXG_ERROR_INVALID_MOTION_TIMES; }
+        previous = samples[i].time;
+        const uint32_t error = validate_common(asset, samples[i].deformation, params, config);
+        if (error != NXG_ERROR_NONE) { return error; }
+    }
+    return NXG_ERROR_NONE;
+}
+
+} // namespace
+} // namespace nxg
+
+extern "C" uint32_t nxg_generate_motion_packed(const nxg_device_asset_desc *asset,
+                                               const nxg_motion_sample_desc *samples, uint32_t sample_count,
+                                               const nxg_generation_params *params,
+                                               const nxg_packed_output_desc *outputs,
+                                               const nxg_launch_config *config, void *workspace,
+                                               uint64_t workspace_bytes, void *stream) {
+    if (!asset || !params || !outputs) { return NXG_ERROR_INVALID_ARGUMENT; }
+    const nxg_launch_config cfg = config ? *config : nxg_launch_config{128u};
+    uint32_t error = nxg::validate_motion_samples(*asset, samples, sample_count, *params, cfg);
+    if (error != NXG_ERROR_NONE) { return error; }
+    for (uint32_t i = 0; i < sample_count; ++i) {
+        error = nxg::validate_range_request(asset, &samples[i].deformation, params, &outputs[i], &cfg, 0u,
+                                            params->strand_count);
+        if (error == NXG_ERROR_NONE) { error = nxg::check_launch_inputs(*asset, &outputs[i]); }
+        if (error != NXG_ERROR_NONE) { return error; }
+    }
+    if ((error = nxg::check_workspace(*asset, params->strand_count, params->cvs_per_strand, workspace,
+                                      workspace_bytes)) != NXG_ERROR_NONE) {
+        return error;
+    }
+    const auto s = static_cast<cudaStream_t>(stream);
+    nxg::set_last_cuda_error(0);
+    if ((error = nxg::launch_order(*asset, params->seed, 0u, params->strand_count, params->cvs_per_strand,
+                                   workspace, s))) {
+        return error;
+    }
+    for (uint32_t i = 0; i < sample_count && !error; ++i) {
+        error = nxg::launch_generate(*asset, samples[i].deformation, *params, outputs[i], cfg, 0u,
+                                     params->strand_count, workspace, s);
+    }
+    return error;
+}
+
+extern "C" uint32_t nxg_generate_motion(const nxg_device_asset_desc *asset, const nxg_motion_sample_desc *samples,
+                                        uint32_t sample_count, const nxg_generation_params *params,
+                                        const nxg_motion_output_desc *output, const nxg_launch_config *config,
+                                        void *workspace, uint64_t workspace_bytes, void *stream) {
+    uint32_t error = nxg_validate_motion_request(asset, samples, sample_count, params, output, config);
+    if (error != NXG_ERROR_NONE) { return error; }
+    if ((error = nxg::check_launch_inputs(*asset, nullptr)) != NXG_ERROR_NONE) { return error; }
+    if (reinterpret_cast<std::uintptr_t>(output->points) % 4u != 0u) { return NXG_ERROR_MISALIGNED_OUTPUT; }
+    if ((error = nxg::check_workspace(*asset, params->strand_count, params->cvs_per_strand, workspace,
+                                      workspace_bytes)) != NXG_ERROR_NONE) {
+        return error;
+    }
+    const nxg_launch_config cfg = config ? *config : nxg_launch_config{128u};
+    const auto s = static_cast<cudaStream_t>(stream);
+    nxg::set_last_cuda_error(0);
+    if ((error = nxg::launch_order(*asset, params->seed, 0u, params->strand_count, params->cvs_per_strand,
+                                   workspace, s))) {
+        return error;
+    }
+    const uint64_t per_sample = uint64_t{params->strand_count} * params->cvs_per_strand * 3u;
+    nxg_packed_output_desc none{};
+    none.radius_scale = 1.0f;
+    for (uint32_t i = 0; i < sample_count && !error; ++i) {
+        float *dst = reinterpret_cast<float *>(output->points) + per_sample * i;
+        error = nxg::launch_generate(*asset, samples[i].deformation, *params, none, cfg, 0u, params->strand_count,
+                                     workspace, s, dst);
+    }
+    return error;
+}
 
 // ---------------------------------------------------------------------------
 // Generation without a caller-provided workspace.

@@ -193,3 +193,49 @@ def reference_benchmark_fixture() -> AssetBuildInput:
                       triangles=np.full(4, INVALID_INDEX, np.uint32), barycentrics=np.zeros((4, 2), np.float32),
                       support_radii=np.full(4, 12.0, np.float32))
     return AssetBuildInput(pos, tris, guides, nrm, uv)
+
+
+@dataclasses.dataclass
+class MotionFrames:
+    """Deformed geometry of one description at several shutter times."""
+    times: np.ndarray                 # (n,) float32, strictly increasing
+    positions: list                   # n x (V, 3) float32
+    normals: list                     # n x (V, 3) float32
+    guide_cvs: list                   # n x (GCV, 3) float32
+
+
+def motion_frames(build_input: AssetBuildInput, samples: int = 5, amplitude: float = 0.03,
+                  seed: int = 4242) -> MotionFrames:
+    """Seeded per-vertex sinusoidal displacement over `samples` shutter times:
+    v(t) = v + amplitude * sin(2 pi t + phase_v) * dir_v, normals recomputed
+    per sample, every guide translated with the displacement of its root's
+    triangle (the same transform as its patch), topology and root identities
+    shared."""
+    rng = np.random.default_rng(seed)
+    pos = build_input.positions.astype(np.float64)
+    tris = build_input.triangles.astype(np.int64)
+    V = pos.shape[0]
+    phase = rng.uniform(0.0, 2.0 * math.pi, V)
+    direction = rng.normal(size=(V, 3))
+    direction /= np.linalg.norm(direction, axis=1, keepdims=True)
+    g = build_input.guides
+    counts = np.asarray(g.cv_counts, np.int64)
+    owner = np.repeat(np.arange(counts.size), counts)
+    gtri = np.asarray(g.triangles, np.int64)
+    bound = gtri < tris.shape[0]
+    bary = np.asarray(g.barycentrics, np.float64)
+    b0 = 1.0 - bary[:, 0] - bary[:, 1]
+    times = np.linspace(0.0, 1.0, samples).astype(np.float32)
+    frames = MotionFrames(times, [], [], [])
+    cvs = np.asarray(g.cvs, np.float64)
+    for t in times:
+        disp = amplitude * np.sin(2.0 * math.pi * float(t) + phase)[:, None] * direction
+        moved = pos + disp
+        frames.positions.append(moved.astype(np.float32))
+        frames.normals.append(vertex_normals(moved.astype(np.float32), build_input.triangles))
+        gd = np.zeros((counts.size, 3))
+        t3 = tris[np.where(bound, gtri, 0)]
+        gd[bound] = (disp[t3[bound, 0]] * b0[bound, None] + disp[t3[bound, 1]] * bary[bound, 0:1] +
+                     disp[t3[bound, 2]] * bary[bound, 1:2])
+        frames.guide_cvs.append((cvs + gd[owner]).astype(np.float32))
+    return frames

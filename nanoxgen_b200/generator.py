@@ -314,3 +314,45 @@ def autotune(dasset: DeviceAsset, params: GenerationParams, points: torch.Tensor
                                     _stream_handle(stream), ctypes.byref(tile), ctypes.byref(ms)),
           "nxg_autotune_packed")
     return (tile.lanes_per_strand, tile.cvs_per_lane, tile.block_size), float(ms.value)
+
+
+def _motion_samples(frames, times) -> "ctypes.Array":
+    samples = (_abi.MotionSampleDesc * len(frames))()
+    for s, f, t in zip(samples, frames, times):
+        s.deformation = f.descriptor()
+        s.time = float(t)
+    return samples
+
+
+def generate_motion_packed(dasset: DeviceAsset, params: GenerationParams, frames: Sequence[DeformedGeometry],
+                           times: Sequence[float], radius_scale: float = 1.0, outputs=None,
+                           block_size: int = 128, stream: Optional[torch.cuda.Stream] = None) -> list:
+    """nxg_generate_motion_packed: one packed output per shutter sample."""
+    S, P = int(params.strand_count), int(params.cvs_per_strand)
+    if outputs is None:
+        outputs = [allocate_outputs(S, P, dasset.device) for _ in frames]
+    descs = (PackedOutputDesc * len(frames))(*[packed_output_descriptor(o[0], o[1], o[2], o[3], radius_scale)
+                                               for o in outputs])
+    samples = _motion_samples(frames, times)
+    ws = dasset.workspace(params, S)
+    check(lib().nxg_generate_motion_packed(ctypes.byref(dasset.desc), samples, len(frames), ctypes.byref(params),
+                                           descs, ctypes.byref(LaunchConfig(block_size)), ws.data_ptr(),
+                                           ws.numel(), _stream_handle(stream)), "nxg_generate_motion_packed")
+    return [PackedCurves(S, P, *o[:1], o[3], o[1], o[2]) for o in outputs]
+
+
+def generate_motion(dasset: DeviceAsset, params: GenerationParams, frames: Sequence[DeformedGeometry],
+                    times: Sequence[float], points: Optional[torch.Tensor] = None, block_size: int = 128,
+                    stream: Optional[torch.cuda.Stream] = None) -> torch.Tensor:
+    """nxg_generate_motion (device_contract.h:42-53): sample-major absolute
+    Vec3 positions, shape (samples, strands * cvs, 3)."""
+    S, P = int(params.strand_count), int(params.cvs_per_strand)
+    if points is None:
+        points = torch.empty((len(frames), S * P, 3), dtype=torch.float32, device=dasset.device)
+    out = _abi.MotionOutputDesc(points=points.data_ptr(), point_capacity=points.numel() // 3)
+    samples = _motion_samples(frames, times)
+    ws = dasset.workspace(params, S)
+    check(lib().nxg_generate_motion(ctypes.byref(dasset.desc), samples, len(frames), ctypes.byref(params),
+                                    ctypes.byref(out), ctypes.byref(LaunchConfig(block_size)), ws.data_ptr(),
+                                    ws.numel(), _stream_handle(stream)), "nxg_generate_motion")
+    return points
