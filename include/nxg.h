@@ -426,6 +426,26 @@ uint32_t nxg_generate_motion(const nxg_device_asset_desc *asset, const nxg_motio
                              const nxg_motion_output_desc *output, const nxg_launch_config *config,
                              void *workspace, uint64_t workspace_bytes, void *stream);
 
+/* Descriptions per nxg_generate_batched call. */
+#define NXG_MAX_BATCH 32u
+
+/* Workspace bytes of nxg_generate_batched for these descriptions. */
+uint64_t nxg_batched_workspace_size(const nxg_device_asset_desc *assets, const nxg_generation_params *params,
+                                    uint32_t count);
+
+/* Several descriptions -- each its own asset, strand count, CV count (<= 128),
+ * stencil and noise settings -- in one persistent generate launch: warps pull
+ * (description, 32-strand batch) work items from an atomic counter, costliest
+ * descriptions first, and run each with its description's registered tile
+ * (nxg_set_tile / nxg_autotune_packed).  Every description is validated as by
+ * nxg_validate_packed_request and written as by nxg_generate_packed;
+ * `deformed` is NULL or an array of `count`.  Seven launches per call, all
+ * enqueue-only (capturable as one graph). */
+uint32_t nxg_generate_batched(const nxg_device_asset_desc *assets, const nxg_deformed_desc *deformed,
+                              const nxg_generation_params *params, const nxg_packed_output_desc *outputs,
+                              uint32_t count, const nxg_launch_config *config, void *workspace,
+                              uint64_t workspace_bytes, void *stream);
+
 /* Size of the library-owned device scratch used by
  * nxg_generate_packed_static_scratch (4 MiB, held on every device that
  * loads the library until the process exits). */

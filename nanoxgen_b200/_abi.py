@@ -260,6 +260,9 @@ _SIGNATURES = {
                                               ctypes.c_uint32, ctypes.POINTER(GenerationParams),
                                               ctypes.POINTER(MotionOutputDesc), ctypes.POINTER(LaunchConfig), _P,
                                               ctypes.c_uint64, _P]),
+    "nxg_batched_workspace_size": (ctypes.c_uint64, [_P, _P, ctypes.c_uint32]),
+    "nxg_generate_batched": (ctypes.c_uint32, [_P, _P, _P, _P, ctypes.c_uint32, ctypes.POINTER(LaunchConfig), _P,
+                                               ctypes.c_uint64, _P]),
     "nxg_query_strand_states": (ctypes.c_uint32, [ctypes.POINTER(DeviceAssetDesc),
                                                   ctypes.POINTER(DeformedDesc),
                                                   ctypes.POINTER(GenerationParams), _P, ctypes.c_uint32,

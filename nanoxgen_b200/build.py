@@ -27,9 +27,9 @@ NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-
                      "-Xptxas", "-warn-spills"]
 CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-ffp-contract=off", "-Wall", "-Wextra", "-I" + INCLUDE]
 
-CUDA_SOURCES = ["generate.cu"]
+CUDA_SOURCES = ["generate.cu", "batched.cu"]
 HOST_SOURCES = ["host.cpp"]
-HEADERS = ["nxg_internal.h", "strand_math.cuh", "seexpr_gradients.inc"]
+HEADERS = ["nxg_internal.h", "strand_math.cuh", "generator_core.cuh", "seexpr_gradients.inc"]
 
 
 def _stale(target: str, deps: list[str]) -> bool:

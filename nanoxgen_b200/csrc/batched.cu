@@ -1,0 +1,472 @@
+// batched.cu -- many descriptions in one persistent generate launch.
+//
+// A frame of several descriptions (each its own .nxg asset, strand count,
+// CV count, stencil and noise settings) is generated by:
+//   batched_clear      zero the per-description bins and the work counter;
+//   batched_keys       alias-sample every strand's triangle, key it by its
+//                      first stencil guide (all descriptions, one grid);
+//   batched_scan       one CTA per description: bin offsets;
+//   batched_scatter    per-description strand-locality orders;
+//   batched_offsets    every description's guide-offset table;
+//   batched_roots      RootSample / root UV / point count, strand order;
+//   batched_generate   persistent warps pull (description, 32-strand batch)
+//                      items from an atomic counter -- items of the costliest
+//                      descriptions first -- and run each item with its
+//                      description's tile (lanes per strand x CVs per lane)
+//                      and noise setting.
+// Seven launches per frame whatever the description count, all enqueue-only
+// and capturable in one CUDA graph.
+#include "generator_core.cuh"
+#include "nxg_internal.h"
+#include "strand_math.cuh"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <numeric>
+#include <vector>
+
+namespace nxg {
+namespace dev {
+
+constexpr int kMaxBatch = NXG_MAX_BATCH;
+
+struct BatchDesc {
+    LaunchArgs g;              // asset, frame, params, count, outputs, order
+    const float4 *offsets;     // guide-offset table (G x P)
+    uint32_t *keys;            // count
+    uint32_t *bins;            // guide_count + 1
+    uint32_t lanes;            // tile: lanes per strand
+    uint32_t ppt;              // tile: CVs per lane (2 or 4)
+    uint32_t noise;
+    uint32_t want_roots;       // any of roots / root_uvs / point_counts
+    uint32_t strand_begin;     // prefix of strand counts (flat strand index)
+    uint32_t item_begin;       // first work item (32 strands each)
+    uint64_t offset_begin;     // prefix of guide_count * P (flat table index)
+};
+
+struct BatchArgs {
+    uint32_t count;
+    uint32_t total_strands;
+    uint32_t total_items;
+    uint32_t *item_counter;
+    uint64_t total_offsets;
+    BatchDesc d[kMaxBatch];
+};
+
+__device__ __forceinline__ int desc_of_strand(const BatchArgs &b, uint32_t i) {
+    int d = 0;
+    while (d + 1 < static_cast<int>(b.count) && b.d[d + 1].strand_begin <= i) { ++d; }
+    return d;
+}
+
+__global__ void batched_clear_kernel(const __grid_constant__ BatchArgs b) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) { *b.item_counter = 0u; }
+    for (uint32_t d = 0; d < b.count; ++d) {
+        const uint32_t bins = b.d[d].g.a.guide_count + 1u;
+        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < bins; i += gridDim.x * blockDim.x) {
+            b.d[d].bins[i] = 0u;
+        }
+    }
+}
+
+__global__ void batched_keys_kernel(const __grid_constant__ BatchArgs b) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < b.total_strands; i += gridDim.x * blockDim.x) {
+        const BatchDesc &d = b.d[desc_of_strand(b, i)];
+        const uint32_t local = i - d.strand_begin;
+        const uint32_t tri = sample_triangle(d.g.a, d.g.p.seed, d.g.first_strand + local);
+        const uint32_t gi = __ldg(d.g.a.stencil + static_cast<uint64_t>(tri) * kSlots);
+        const uint32_t key = gi < d.g.a.guide_count ? gi : d.g.a.guide_count;
+        d.keys[local] = key;
+        atomicAdd(&d.bins[key], 1u);
+    }
+}
+
+// One CTA (1024 threads) per description: exclusive scan of its bins.
+__global__ void __launch_bounds__(1024) batched_scan_kernel(const __grid_constant__ BatchArgs b) {
+    __shared__ uint32_t warp_sums[32];
+    const BatchDesc &d = b.d[blockIdx.x];
+    uint32_t *data = d.bins;
+    const uint32_t n = d.g.a.guide_count + 1u;
+    const uint32_t tid = threadIdx.x;
+    const uint32_t per = (n + blockDim.x - 1u) / blockDim.x;
+    const uint32_t lo = min(n, tid * per), hi = min(n, lo + per);
+    uint32_t sum = 0u;
+    for (uint32_t i = lo; i < hi; ++i) { sum += data[i]; }
+    uint32_t incl = sum;
+    const int lane = tid & 31;
+#pragma unroll
+    for (int k = 1; k < 32; k <<= 1) {
+        const uint32_t u = __shfl_up_sync(kFull, incl, k);
+        if (lane >= k) { incl += u; }
+    }
+    if (lane == 31) { warp_sums[tid >> 5] = incl; }
+    __syncthreads();
+    if (tid < 32) {
+        uint32_t w = tid < (blockDim.x >> 5) ? warp_sums[tid] : 0u;
+#pragma unroll
+        for (int k = 1; k < 32; k <<= 1) {
+            const uint32_t u = __shfl_up_sync(kFull, w, k);
+            if (lane >= k) { w += u; }
+        }
+        warp_sums[tid] = w;
+    }
+    __syncthreads();
+    uint32_t running = incl - sum + ((tid >> 5) ? warp_sums[(tid >> 5) - 1u] : 0u);
+    for (uint32_t i = lo; i < hi; ++i) {
+        const uint32_t v = data[i];
+        data[i] = running;
+        running += v;
+    }
+}
+
+__global__ void batched_scatter_kernel(const __grid_constant__ BatchArgs b) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < b.total_strands; i += gridDim.x * blockDim.x) {
+        const BatchDesc &d = b.d[desc_of_strand(b, i)];
+        const uint32_t local = i - d.strand_begin;
+        const uint32_t bins = d.g.a.guide_count + 1u;
+        const uint32_t pos = atomicAdd(&d.bins[min(d.keys[local], bins - 1u)], 1u);
+        if (pos < d.g.count) { const_cast<uint32_t *>(d.g.order)[pos] = local; }
+    }
+}
+
+__global__ void batched_offsets_kernel(const __grid_constant__ BatchArgs b) {
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < b.total_offsets;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        int di = 0;
+        while (di + 1 < static_cast<int>(b.count) && b.d[di + 1].offset_begin <= i) { ++di; }
+        const BatchDesc &d = b.d[di];
+        const uint64_t local = i - d.offset_begin;
+        const uint32_t P = d.g.p.cvs_per_strand;
+        const_cast<float4 *>(d.offsets)[local] = guide_offset_entry(d.g.a, d.g.f, P,
+                                                                    static_cast<uint32_t>(local / P),
+                                                                    static_cast<uint32_t>(local % P));
+    }
+}
+
+// RootSample / root UV / point count per strand, strand order.  A warp
+// stages its 32 records in shared memory and writes them as consecutive
+// words (a warp may straddle two descriptions; each word goes to its own).
+__global__ void batched_roots_kernel(const __grid_constant__ BatchArgs b) {
+    __shared__ uint32_t staged[8][32 * 12];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    for (uint32_t base = (blockIdx.x * (blockDim.x >> 5) + warp) * 32u; base < b.total_strands;
+         base += gridDim.x * (blockDim.x >> 5) * 32u) {
+        const uint32_t i = base + static_cast<uint32_t>(lane);
+        const bool valid = i < b.total_strands;
+        const int di = desc_of_strand(b, valid ? i : base);
+        const BatchDesc &d = b.d[di];
+        const uint32_t local = (valid ? i : base) - d.strand_begin;
+        const Root r = sample_root(d.g.a, d.g.f, d.g.p.seed, d.g.first_strand + local);
+        uint32_t *rec = staged[warp] + lane * 12;
+        for (int w = 0; w < 12; ++w) { rec[w] = root_word(r, w); }
+        __syncwarp();
+        for (int k = 0; k < 12; ++k) {
+            const int word = k * 32 + lane;           // word of the warp's staged records
+            const int slot = word / 12;               // which lane's strand
+            const int sdi = __shfl_sync(kFull, di, slot);
+            const uint32_t slocal = __shfl_sync(kFull, local, slot);
+            const bool svalid = base + static_cast<uint32_t>(slot) < b.total_strands;
+            const BatchDesc &sd = b.d[sdi];
+            if (svalid && sd.g.roots) { sd.g.roots[static_cast<uint64_t>(slocal) * 12u + (word - slot * 12)] = staged[warp][word]; }
+        }
+        if (valid) {
+            if (d.g.root_uvs) { d.g.root_uvs[local] = make_float2(r.u, r.v); }
+            if (d.g.point_counts) { d.g.point_counts[local] = d.g.p.cvs_per_strand; }
+        }
+        __syncwarp();
+    }
+}
+
+// Per-warp shared memory of the batched kernel.
+constexpr size_t kBatchTableBytes = sizeof(float4) * kTableFloat4;              // 4096
+constexpr size_t kBatchTvalBytes = sizeof(float) * 128u;                        // P <= 128
+constexpr size_t kBatchRecordBytes = sizeof(uint32_t) * kRecFields * 32u;       // 4096
+constexpr size_t kBatchStageBytes = sizeof(float4) * 32u * 4u;                  // 32 lanes x 4 CVs
+constexpr size_t kBatchLatticeBytes = sizeof(float2) * 384u;
+constexpr size_t kBatchWarpBytes =
+    kBatchTableBytes + kBatchTvalBytes + kBatchRecordBytes + kBatchStageBytes + kBatchLatticeBytes;
+
+template <int L, int PPT, bool NOISE>
+__device__ __noinline__ void batched_item(const BatchDesc &d, uint32_t batch, uint32_t end, int lane,
+                                             unsigned char *mine) {
+    const float4 *table = reinterpret_cast<const float4 *>(mine);
+    const float *tvals = reinterpret_cast<const float *>(mine + kBatchTableBytes);
+    const Records rec{reinterpret_cast<uint32_t *>(mine + kBatchTableBytes + kBatchTvalBytes)};
+    float4 *stage_base = reinterpret_cast<float4 *>(mine + kBatchTableBytes + kBatchTvalBytes + kBatchRecordBytes);
+    float2 *lattice_base = reinterpret_cast<float2 *>(mine + kBatchTableBytes + kBatchTvalBytes + kBatchRecordBytes +
+                                                      kBatchStageBytes);
+    constexpr int kGroups = 32 / L;
+    const int group = lane / L;
+    const int gl = lane % L;
+    const uint32_t item = batch + static_cast<uint32_t>(lane);
+    const bool valid = item < end;
+    setup_strand<NOISE>(d.g, rec, lane, valid ? item : batch, valid);
+    __syncwarp();
+    const uint32_t in_batch = end - batch;
+#pragma unroll 1
+    for (uint32_t r = 0; r < in_batch; r += kGroups) {
+        emit_strand<L, PPT, NOISE>(d.g, rec, static_cast<int>(r) + group, gl, table, d.offsets, tvals,
+                                   stage_base + group * (L * PPT), lattice_base + group * (384 / kGroups),
+                                   384 / 3 / kGroups);
+    }
+    __syncwarp();
+}
+
+template <int PPT, bool NOISE>
+__device__ __forceinline__ void batched_dispatch_lanes(const BatchDesc &d, uint32_t batch, uint32_t end, int lane,
+                                                       unsigned char *mine) {
+    switch (d.lanes) {
+        case 2: batched_item<2, PPT, NOISE>(d, batch, end, lane, mine); break;
+        case 4: batched_item<4, PPT, NOISE>(d, batch, end, lane, mine); break;
+        case 8: batched_item<8, PPT, NOISE>(d, batch, end, lane, mine); break;
+        case 16: batched_item<16, PPT, NOISE>(d, batch, end, lane, mine); break;
+        default: batched_item<32, PPT, NOISE>(d, batch, end, lane, mine); break;
+    }
+}
+
+template <int PPT>
+__global__ void batched_generate_kernel(const __grid_constant__ BatchArgs b) {
+    extern __shared__ float4 smem[];
+    __shared__ uint32_t claimed;
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const uint32_t warps = blockDim.x >> 5;
+    unsigned char *mine = reinterpret_cast<unsigned char *>(smem) + kBatchWarpBytes * warp;
+    float4 *table = reinterpret_cast<float4 *>(mine);
+    float *tvals = reinterpret_cast<float *>(mine + kBatchTableBytes);
+    int current = -1;
+    // A work item is a contiguous slice of one description's strand order,
+    // one 32-strand batch per warp of the CTA, so the CTA's strands share
+    // guide-offset rows in L1.  Each pass of the loop consumes one item.
+    for (uint32_t guard = 0; guard <= b.total_items; ++guard) {
+        if (threadIdx.x == 0) { claimed = atomicAdd(b.item_counter, 1u); }
+        __syncthreads();
+        const uint32_t item = claimed;
+        __syncthreads();
+        if (item >= b.total_items) { break; }
+        int di = 0;
+        while (di + 1 < static_cast<int>(b.count) && b.d[di + 1].item_begin <= item) { ++di; }
+        const BatchDesc &d = b.d[di];
+        const uint32_t batch = ((item - d.item_begin) * warps + static_cast<uint32_t>(warp)) * 32u;
+        if (batch >= d.g.count) { continue; }
+        if (di != current) {
+            __syncwarp();
+            const int P = static_cast<int>(d.g.p.cvs_per_strand);
+            if (d.noise) {
+                for (int i = lane; i < kTableFloat4; i += 32) {
+                    table[i] = make_float4(__ldg(d.g.a.gradients + 3 * i), __ldg(d.g.a.gradients + 3 * i + 1),
+                                           __ldg(d.g.a.gradients + 3 * i + 2), 0.0f);
+                }
+            }
+            for (int i = lane; i < P; i += 32) { tvals[i] = __fdiv_rn(static_cast<float>(i), static_cast<float>(P - 1)); }
+            __syncwarp();
+            current = di;
+        }
+        const uint32_t end = min(batch + 32u, d.g.count);
+        if (d.noise) {
+            batched_dispatch_lanes<PPT, true>(d, batch, end, lane, mine);
+        } else {
+            batched_dispatch_lanes<PPT, false>(d, batch, end, lane, mine);
+        }
+    }
+}
+
+} // namespace dev
+
+namespace {
+
+constexpr uint64_t kAlign = 256u;
+inline uint64_t up(uint64_t v) { return (v + kAlign - 1u) / kAlign * kAlign; }
+
+struct BatchLayout {
+    uint64_t counter;
+    std::vector<uint64_t> keys, order, bins, offsets;
+    uint64_t total;
+};
+
+BatchLayout batch_layout(const nxg_device_asset_desc *assets, const nxg_generation_params *params, uint32_t count) {
+    BatchLayout l{};
+    l.counter = 0u;
+    uint64_t at = kAlign;
+    for (uint32_t d = 0; d < count; ++d) {
+        const uint64_t S = params[d].strand_count, P = params[d].cvs_per_strand, G = assets[d].header.guide_count;
+        l.keys.push_back(at);
+        at += up(S * 4u);
+        l.order.push_back(at);
+        at += up(S * 4u);
+        l.bins.push_back(at);
+        at += up((G + 1u) * 4u);
+        l.offsets.push_back(at);
+        at += up(G * P * 16u);
+    }
+    l.total = at;
+    return l;
+}
+
+// Lanes per strand of a description in a batched launch whose CVs per lane
+// are `ppt`: the registered tile's lanes when it uses the same CVs per lane,
+// else the narrowest power-of-two group holding the strand.
+uint32_t batch_lanes(uint32_t P, bool noise, uint32_t ppt) {
+    nxg_tile t{};
+    nxg_get_tile(P, noise ? 1u : 0u, &t);
+    if (t.cvs_per_lane == ppt && t.lanes_per_strand * ppt >= P) { return t.lanes_per_strand; }
+    uint32_t l = 2u;
+    while (l * ppt < P) { l *= 2u; }
+    return l;
+}
+
+int sm_count() {
+    int device = 0, sms = 148;
+    if (cudaGetDevice(&device) == cudaSuccess) { cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device); }
+    return sms > 0 ? sms : 148;
+}
+
+} // namespace
+} // namespace nxg
+
+extern "C" uint64_t nxg_batched_workspace_size(const nxg_device_asset_desc *assets,
+                                               const nxg_generation_params *params, uint32_t count) {
+    if (!assets || !params || count == 0u || count > NXG_MAX_BATCH) { return 0u; }
+    return nxg::batch_layout(assets, params, count).total;
+}
+
+extern "C" uint32_t nxg_generate_batched(const nxg_device_asset_desc *assets, const nxg_deformed_desc *deformed,
+                                         const nxg_generation_params *params,
+                                         const nxg_packed_output_desc *outputs, uint32_t count,
+                                         const nxg_launch_config *config, void *workspace,
+                                         uint64_t workspace_bytes, void *stream) {
+    using namespace nxg;
+    if (!assets || !params || !outputs || count == 0u || count > NXG_MAX_BATCH) { return NXG_ERROR_INVALID_ARGUMENT; }
+    const nxg_launch_config cfg = config ? *config : nxg_launch_config{128u};
+    for (uint32_t d = 0; d < count; ++d) {
+        const uint32_t error = nxg_validate_packed_request(&assets[d], deformed ? &deformed[d] : nullptr, &params[d],
+                                                           &outputs[d], &cfg);
+        if (error != NXG_ERROR_NONE) { return error; }
+        if (!sections_in_bounds(assets[d].header)) { return NXG_ERROR_INVALID_ASSET_METADATA; }
+        if (reinterpret_cast<std::uintptr_t>(outputs[d].points) % 16u != 0u ||
+            reinterpret_cast<std::uintptr_t>(outputs[d].roots) % 4u != 0u ||
+            reinterpret_cast<std::uintptr_t>(outputs[d].root_uvs) % 8u != 0u ||
+            reinterpret_cast<std::uintptr_t>(outputs[d].point_counts) % 4u != 0u) {
+            return NXG_ERROR_MISALIGNED_OUTPUT;
+        }
+        if (params[d].cvs_per_strand > 128u ||
+            uint64_t{assets[d].header.guide_count} * params[d].cvs_per_strand * 16u > (uint64_t{1} << 30)) {
+            return NXG_ERROR_INVALID_ARGUMENT;  // long strands take nxg_generate_packed's serial kernel
+        }
+    }
+    const BatchLayout layout = batch_layout(assets, params, count);
+    if (!workspace || workspace_bytes < layout.total) { return NXG_ERROR_WORKSPACE_TOO_SMALL; }
+    if (reinterpret_cast<std::uintptr_t>(workspace) % kAlign != 0u) { return NXG_ERROR_MISALIGNED_OUTPUT; }
+
+    // CTA size of the generate kernel (work items are one 32-strand batch per warp).
+    uint32_t max_cvs = 0u;
+    for (uint32_t d = 0; d < count; ++d) { max_cvs = std::max(max_cvs, params[d].cvs_per_strand); }
+    const uint32_t ppt = max_cvs <= 64u ? 2u : 4u;
+    const void *fn = ppt == 2u ? reinterpret_cast<const void *>(dev::batched_generate_kernel<2>)
+                               : reinterpret_cast<const void *>(dev::batched_generate_kernel<4>);
+    uint32_t status = NXG_ERROR_NONE;
+    cudaFuncAttributes attr{};
+    if ((status = record_cuda(cudaFuncGetAttributes(&attr, fn)))) { return status; }
+    int device = 0, smem_optin = 48 * 1024;
+    if (cudaGetDevice(&device) == cudaSuccess) {
+        cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    }
+    uint32_t block = std::min(static_cast<uint32_t>(attr.maxThreadsPerBlock) / 32u * 32u,
+                              std::max<uint32_t>(32u, (cfg.block_size + 31u) / 32u * 32u));
+    while (block > 32u && dev::kBatchWarpBytes * (block / 32u) + 64u > static_cast<size_t>(smem_optin)) { block -= 32u; }
+    const uint32_t warps_per_cta = block / 32u;
+
+    auto *w = static_cast<unsigned char *>(workspace);
+    dev::BatchArgs b{};
+    b.count = count;
+    b.item_counter = reinterpret_cast<uint32_t *>(w + layout.counter);
+    // Costliest descriptions first (CVs per strand, tripled with noise), so the
+    // longest work items start early and the tail is made of cheap ones.
+    std::vector<uint32_t> rank(count);
+    std::iota(rank.begin(), rank.end(), 0u);
+    auto cost = [&](uint32_t d) {
+        const bool noise = params[d].noise_amplitude != 0.0f && params[d].noise_mask != 0.0f;
+        return uint64_t{params[d].cvs_per_strand} * (noise ? 3u : 1u);
+    };
+    std::stable_sort(rank.begin(), rank.end(), [&](uint32_t x, uint32_t y) { return cost(x) > cost(y); });
+    uint32_t strands = 0u, items = 0u;
+    uint64_t offsets = 0u;
+    for (uint32_t k = 0; k < count; ++k) {
+        const uint32_t d = rank[k];
+        dev::BatchDesc &bd = b.d[k];
+        const nxg_deformed_desc none{};
+        bd.g.a = resolve_asset(assets[d]);
+        bd.g.f = resolve_frame(bd.g.a, deformed ? deformed[d] : none);
+        bd.g.p = resolve_params(params[d], outputs[d].radius_scale);
+        bd.g.first_strand = 0u;
+        bd.g.count = params[d].strand_count;
+        bd.g.points = reinterpret_cast<float4 *>(outputs[d].points);
+        bd.g.vec3_points = nullptr;
+        bd.g.roots = reinterpret_cast<uint32_t *>(outputs[d].roots);
+        bd.g.root_uvs = reinterpret_cast<float2 *>(outputs[d].root_uvs);
+        bd.g.point_counts = outputs[d].point_counts;
+        bd.g.order = reinterpret_cast<const uint32_t *>(w + layout.order[d]);
+        bd.offsets = reinterpret_cast<const float4 *>(w + layout.offsets[d]);
+        bd.keys = reinterpret_cast<uint32_t *>(w + layout.keys[d]);
+        bd.bins = reinterpret_cast<uint32_t *>(w + layout.bins[d]);
+        bd.noise = bd.g.p.noise;
+        bd.want_roots = (outputs[d].roots || outputs[d].root_uvs || outputs[d].point_counts) ? 1u : 0u;
+        bd.strand_begin = strands;
+        bd.item_begin = items;
+        bd.offset_begin = offsets;
+        strands += params[d].strand_count;
+        items += (params[d].strand_count + 32u * warps_per_cta - 1u) / (32u * warps_per_cta);
+        offsets += uint64_t{assets[d].header.guide_count} * params[d].cvs_per_strand;
+    }
+    b.total_strands = strands;
+    b.total_items = items;
+    b.total_offsets = offsets;
+    // One CVs-per-lane value per launch keeps the kernel's register footprint
+    // that of a single tile family: two when every strand fits 32 lanes x 2.
+    for (uint32_t k = 0; k < count; ++k) {
+        b.d[k].ppt = ppt;
+        b.d[k].lanes = batch_lanes(b.d[k].g.p.cvs_per_strand, b.d[k].noise != 0u, ppt);
+    }
+
+    const auto s = static_cast<cudaStream_t>(stream);
+    const int sms = sm_count();
+    set_last_cuda_error(0);
+    const uint32_t flat_blocks = static_cast<uint32_t>(std::min<uint64_t>((strands + 255u) / 256u, uint64_t(sms) * 8u));
+    dev::batched_clear_kernel<<<std::max(1, sms), 256, 0, s>>>(b);
+    if ((status = record_cuda(cudaGetLastError()))) { return status; }
+    dev::batched_keys_kernel<<<flat_blocks, 256, 0, s>>>(b);
+    if ((status = record_cuda(cudaGetLastError()))) { return status; }
+    dev::batched_scan_kernel<<<count, 1024, 0, s>>>(b);
+    if ((status = record_cuda(cudaGetLastError()))) { return status; }
+    dev::batched_scatter_kernel<<<flat_blocks, 256, 0, s>>>(b);
+    if ((status = record_cuda(cudaGetLastError()))) { return status; }
+    const uint32_t offset_blocks = static_cast<uint32_t>(std::min<uint64_t>((offsets + 255u) / 256u, uint64_t(sms) * 16u));
+    dev::batched_offsets_kernel<<<std::max(1u, offset_blocks), 256, 0, s>>>(b);
+    if ((status = record_cuda(cudaGetLastError()))) { return status; }
+    dev::batched_roots_kernel<<<std::max(1u, static_cast<uint32_t>(std::min<uint64_t>((strands + 255u) / 256u,
+                                                                                    uint64_t(sms) * 16u))),
+                                256, 0, s>>>(b);
+    if ((status = record_cuda(cudaGetLastError()))) { return status; }
+
+    const size_t shm = dev::kBatchWarpBytes * (block / 32u);
+    if ((status = record_cuda(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   static_cast<int>(shm))))) {
+        return status;
+    }
+    int per_sm = 0;
+    if ((status = record_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, static_cast<int>(block),
+                                                                            shm)))) {
+        return status;
+    }
+    const uint32_t grid = static_cast<uint32_t>(std::max(1, sms * std::max(per_sm, 1)));
+    if (ppt == 2u) {
+        dev::batched_generate_kernel<2><<<grid, block, shm, s>>>(b);
+    } else {
+        dev::batched_generate_kernel<4><<<grid, block, shm, s>>>(b);
+    }
+    return record_cuda(cudaGetLastError());
+}

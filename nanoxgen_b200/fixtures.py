@@ -239,3 +239,54 @@ def motion_frames(build_input: AssetBuildInput, samples: int = 5, amplitude: flo
                      disp[t3[bound, 2]] * bary[bound, 1:2])
         frames.guide_cvs.append((cvs + gd[owner]).astype(np.float32))
     return frames
+
+
+@dataclasses.dataclass
+class Batch:
+    """Several descriptions on one mesh, each with its own guides and settings."""
+    name: str
+    workloads: list   # of Workload
+
+    @property
+    def points(self) -> int:
+        return sum(w.points for w in self.workloads)
+
+    @property
+    def strands(self) -> int:
+        return sum(int(w.params.strand_count) for w in self.workloads)
+
+
+BATCH_CVS = (8, 12, 16, 24, 32, 48, 64)
+
+
+def batched_descriptions(count: int = 9, n_lon: int = 1000, n_rings: int = 251, strands=(20_000, 1_000_000),
+                         guides=(512, 2048), seed: int = 2026, size_seed: int = 2590) -> Batch:
+    """Multi-description frame: `count` descriptions on one displaced sphere
+    (1000 x 251 -> 500,000 triangles), each with its own seeded guides
+    (count drawn from `guides`), stencil size 4 or 8, strand count
+    log-uniform in `strands`, CVs per strand from {8,12,16,24,32,48,64}, and
+    its own taper and noise (two in three descriptions noisy).  Strand and CV
+    counts come from their own stream (`size_seed`; the default gives
+    2,493,172 strands and 46,200,484 points for nine descriptions)."""
+    sizes = np.random.default_rng(size_seed)
+    lo, hi = math.log(strands[0]), math.log(strands[1])
+    counts = [int(round(math.exp(sizes.uniform(lo, hi)))) for _ in range(count)]
+    cv_counts = [int(sizes.choice(BATCH_CVS)) for _ in range(count)]
+    rng = np.random.default_rng(seed)
+    pos, uv, tris = sphere_mesh(n_lon, n_rings, displaced_sphere_radius)
+    out = []
+    for d in range(count):
+        cvs, S = cv_counts[d], counts[d]
+        g = int(rng.integers(guides[0], guides[1] + 1))
+        gcv = max(cvs, 8)
+        gs = surface_guides(pos, tris, g, gcv, rng, texcoords=uv, jitter=0.1 * 0.45 / (gcv - 1))
+        noisy = rng.random() < 2.0 / 3.0
+        params = GenerationParams(strand_count=S, cvs_per_strand=cvs, seed=100 + d,
+                                  root_width=float(rng.uniform(0.005, 0.03)), tip_width=0.001,
+                                  noise_amplitude=float(rng.uniform(0.05, 0.2)) if noisy else 0.0,
+                                  noise_frequency=float(rng.uniform(4.0, 12.0)))
+        k = int(rng.choice([4, 8]))
+        out.append(Workload("desc%d/%d-guides/k%d/%d-strands-x%d%s" % (d, g, k, S, cvs, "/noise" if noisy else ""),
+                            AssetBuildInput(pos, tris, gs, None, uv), k, params))
+    total_tris = tris.shape[0]
+    return Batch("%d-descriptions-on-%dk-tris" % (count, total_tris // 1000), out)

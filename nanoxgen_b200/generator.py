@@ -356,3 +356,40 @@ def generate_motion(dasset: DeviceAsset, params: GenerationParams, frames: Seque
                                     ctypes.byref(out), ctypes.byref(LaunchConfig(block_size)), ws.data_ptr(),
                                     ws.numel(), _stream_handle(stream)), "nxg_generate_motion")
     return points
+
+
+class BatchRunner:
+    """nxg_generate_batched over several uploaded descriptions, with the
+    output buffers and the workspace allocated once."""
+
+    def __init__(self, dassets: Sequence[DeviceAsset], params: Sequence[GenerationParams],
+                 radius_scale: float = 1.0, with_roots: bool = True):
+        self.dassets = list(dassets)
+        self.params = list(params)
+        device = self.dassets[0].device
+        n = len(self.dassets)
+        self._assets = (DeviceAssetDesc * n)()
+        for i, d in enumerate(self.dassets):
+            ctypes.memmove(ctypes.byref(self._assets[i]), ctypes.byref(d.desc), ctypes.sizeof(DeviceAssetDesc))
+        self._params = (GenerationParams * n)(*self.params)
+        self.outputs = [allocate_outputs(int(p.strand_count), int(p.cvs_per_strand), device, with_roots, with_roots,
+                                         with_roots) for p in self.params]
+        self._outs = (PackedOutputDesc * n)(*[packed_output_descriptor(o[0], o[1], o[2], o[3], radius_scale)
+                                              for o in self.outputs])
+        need = int(lib().nxg_batched_workspace_size(self._assets, self._params, n))
+        if need == 0:
+            raise ValueError("batch of %d descriptions is empty or exceeds NXG_MAX_BATCH" % n)
+        self.workspace = torch.empty(need, dtype=torch.uint8, device=device)
+
+    @property
+    def points(self) -> int:
+        return sum(int(p.strand_count) * int(p.cvs_per_strand) for p in self.params)
+
+    def run(self, block_size: int = 128, stream: Optional[torch.cuda.Stream] = None) -> None:
+        check(lib().nxg_generate_batched(self._assets, None, self._params, self._outs, len(self.dassets),
+                                         ctypes.byref(LaunchConfig(block_size)), self.workspace.data_ptr(),
+                                         self.workspace.numel(), _stream_handle(stream)), "nxg_generate_batched")
+
+    def curves(self) -> list:
+        return [PackedCurves(int(p.strand_count), int(p.cvs_per_strand), o[0], o[3], o[1], o[2])
+                for p, o in zip(self.params, self.outputs)]
