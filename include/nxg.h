@@ -223,6 +223,11 @@ typedef enum nxg_error {
     NXG_ERROR_WORKSPACE_TOO_SMALL = 66,   /* workspace missing or below the queried size */
     NXG_ERROR_MISALIGNED_OUTPUT = 67,     /* points not 16-byte aligned, or workspace not 256-byte aligned */
     NXG_ERROR_STATIC_SCRATCH_LIMIT = 68,  /* request needs more than NXG_STATIC_SCRATCH_BYTES of scratch */
+    NXG_ERROR_EXPRESSION_SYNTAX = 69,     /* expression did not compile; see the message buffer */
+    NXG_ERROR_EXPRESSION_LIMIT = 70,      /* program exceeds the device form's limits */
+    NXG_ERROR_EXPRESSION_INPUT = 71,      /* expression uses a variable this runtime cannot bind */
+    NXG_ERROR_EXPRESSION_DOMAIN = 72,     /* device evaluation gave a non-finite value or negative length */
+    NXG_ERROR_SURROGATE = 73,             /* surrogate model missing, untrained or misconfigured */
     NXG_ERROR_CUDA = 96                   /* a CUDA runtime call failed; see nxg_last_cuda_error */
 } nxg_error;
 

@@ -1,0 +1,140 @@
+/*
+ * nxg_classic.h -- Classic-expression per-root scalars on the GPU.
+ *
+ * Part of libnxg_b200.so; include after nxg.h.  Three layers:
+ *
+ *  1. The scalar-expression compiler.  nxg_expression_compile replaces the
+ *     reference's compile_xgen_scalar_expression + make_xgen_float_expression_program
+ *     (src/xgen_expression.cpp:771-818) and, with NXG_EXPRESSION_CLASSIC, the
+ *     Classic runtime's comment stripping and noise($Prefg*k) rewrite
+ *     (src/xgen_classic_runtime.cpp:138-347).  Same language, same SSA
+ *     program, same error texts.
+ *
+ *  2. The exact runtime.  nxg_classic_root_scalars evaluates a description's
+ *     SplinePrimitive length and width expressions for every root on the
+ *     device with the float semantics of evaluate_xgen_scalar_expression_float
+ *     (src/xgen_expression.cpp:984-1148) and xgen_classic_noise_float
+ *     (src/xgen_classic_runtime.cpp:803-837).  nxg_generate_packed_classic
+ *     applies the scalars inside the generator, as the reference's
+ *     apply_xgen_classic_float_runtime_plan_cpu does afterwards on the host
+ *     (src/xgen_classic_runtime.cpp:1650-1678 length, :1827-1858 width profile,
+ *     :1670-1675 the drop rule).
+ *
+ *  3. The learned surrogate (no reference counterpart): a 3x64 MLP over the
+ *     root's position, normal and uv, BF16 weights on the tcgen05 tensor cores
+ *     with FP32 accumulation, trained on the device by the library's own
+ *     forward/backward/Adam kernels on samples of the exact runtime, and
+ *     spot-checked against the exact runtime on every batch with an exact
+ *     re-run of any batch whose check exceeds the tolerance.
+ */
+#ifndef NXG_CLASSIC_H
+#define NXG_CLASSIC_H
+
+#include "nxg.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- compiler */
+
+typedef struct nxg_expression nxg_expression; /* opaque, host memory */
+
+#define NXG_EXPRESSION_CLASSIC 1u /* apply the Classic source rewrites first */
+#define NXG_EXPRESSION_MAX_INPUTS 16u
+
+typedef struct nxg_expression_info {
+    uint32_t instruction_count;
+    uint32_t operand_count;
+    uint32_t input_count;
+    uint32_t ramp_count;
+    uint32_t ramp_point_count;
+    uint32_t result;
+    uint32_t expression_seed;   /* xgen_expression_seed(name, object type) */
+    uint32_t random_call_count;
+    uint32_t pref_noise_count;  /* distinct noise($Prefg*k) frequencies */
+    float pref_noise_frequencies[NXG_EXPRESSION_MAX_INPUTS];
+} nxg_expression_info;
+
+/* One SSA instruction of the float program (XgenFloatScalarInstruction,
+ * xgen_expression.h:84-90); op numbers follow XgenScalarOp (:12-40). */
+typedef struct nxg_expression_instruction {
+    uint32_t op;
+    uint32_t operand_offset;
+    uint32_t operand_count;
+    uint32_t auxiliary;
+    float immediate;
+} nxg_expression_instruction;
+
+typedef struct nxg_expression_ramp_point {
+    float position;
+    float value;
+    uint32_t interpolation;
+} nxg_expression_ramp_point;
+
+/* Compiles `source`.  expression_name / object_type seed rand() exactly as
+ * xgen_expression_seed (xgen_expression.cpp:730-737); the Classic runtime
+ * passes the attribute name ("length", "width") and the object type
+ * ("SplinePrimitive").  On failure returns NXG_ERROR_EXPRESSION_SYNTAX and
+ * writes the reference's message text to `message`. */
+uint32_t nxg_expression_compile(const char *source, const char *expression_name, const char *object_type,
+                                uint32_t flags, nxg_expression **out, char *message, size_t message_capacity);
+void nxg_expression_destroy(nxg_expression *expression);
+uint32_t nxg_expression_get_info(const nxg_expression *expression, nxg_expression_info *info);
+uint32_t nxg_expression_get_instruction(const nxg_expression *expression, uint32_t index,
+                                        nxg_expression_instruction *instruction);
+uint32_t nxg_expression_get_operand(const nxg_expression *expression, uint32_t index, uint32_t *operand);
+uint32_t nxg_expression_get_ramp_point(const nxg_expression *expression, uint32_t index,
+                                       nxg_expression_ramp_point *point);
+/* Name of input `index` (without '$'), or NULL. */
+const char *nxg_expression_input_name(const nxg_expression *expression, uint32_t index);
+
+/* xgen_string_seed (xgen_expression.cpp:716-728). */
+uint32_t nxg_xgen_string_seed(const char *text);
+
+/* ------------------------------------------------------------ exact runtime */
+
+/* A description's per-root scalar expressions.  Bound inputs:
+ * $__nxg_pref_noise_<k> (from noise($Prefg*k)), $id (strand index), $u/$v
+ * (root uv), $cWidth (0, as in the reference while length and width are
+ * evaluated).  $cLength needs the generated curve and is refused here. */
+typedef struct nxg_classic_scalar_plan {
+    const nxg_expression *length; /* SplinePrimitive.length or NULL (scale 1) */
+    const nxg_expression *width;  /* SplinePrimitive.width or NULL */
+    uint32_t description_id;      /* rand() face seed (xgen_expression.cpp:702-714) */
+    uint32_t reserved;
+    const char *patch_name;       /* rand() face seed; NULL = "" */
+} nxg_classic_scalar_plan;
+
+/* scalars[2*i] = length scale, scalars[2*i+1] = width of strand first+i
+ * (float2 per strand, 8-byte aligned).  device_status (2 x uint32, zeroed
+ * by the caller) receives NXG_ERROR_EXPRESSION_DOMAIN in [0] and the number
+ * of failing strands in [1] when an expression yields a non-finite value or
+ * a negative length (the reference throws there). */
+uint32_t nxg_classic_root_scalars(const nxg_device_asset_desc *asset, const nxg_generation_params *params,
+                                  const nxg_classic_scalar_plan *plan, uint32_t first_strand,
+                                  uint32_t strand_count, float *scalars, uint32_t *device_status,
+                                  void *stream);
+
+/* Classic application fused into generation.  With apply_length the strand
+ * is scaled about its first point by scalars[2i]; with apply_width every
+ * radius becomes 0.5 * max(scalars[2i+1], 0) * radius_scale; a strand whose
+ * scaled spline length or width is below 1e-4 gets point_counts = 0 (the
+ * reference removes it from the set instead). */
+typedef struct nxg_classic_apply_desc {
+    const float *root_scalars; /* from nxg_classic_root_scalars or the surrogate */
+    uint32_t apply_length;
+    uint32_t apply_width;
+} nxg_classic_apply_desc;
+
+uint32_t nxg_generate_packed_classic(const nxg_device_asset_desc *asset, const nxg_deformed_desc *deformed,
+                                     const nxg_generation_params *params, const nxg_packed_output_desc *output,
+                                     const nxg_classic_apply_desc *classic, const nxg_launch_config *config,
+                                     uint32_t first_strand, uint32_t strand_count, void *workspace,
+                                     uint64_t workspace_bytes, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NXG_CLASSIC_H */

@@ -140,6 +140,47 @@ class Tile(ctypes.Structure):
                 ("block_size", ctypes.c_uint32)]
 
 
+EXPRESSION_CLASSIC = 1
+EXPRESSION_MAX_INPUTS = 16
+
+# XgenScalarOp order (xgen_expression.h:12-40).
+EXPRESSION_OPS = ["constant", "input", "negate", "logical_not", "add", "subtract", "multiply", "divide",
+                  "less", "less_equal", "greater", "greater_equal", "equal", "not_equal", "logical_and",
+                  "logical_or", "select", "hash", "random", "minimum", "maximum", "clamp", "fit", "gamma",
+                  "contrast", "smoothstep", "ramp"]
+
+
+class ExpressionInfo(ctypes.Structure):
+    """nxg_expression_info (nxg_classic.h)."""
+    _fields_ = [("instruction_count", ctypes.c_uint32), ("operand_count", ctypes.c_uint32),
+                ("input_count", ctypes.c_uint32), ("ramp_count", ctypes.c_uint32),
+                ("ramp_point_count", ctypes.c_uint32), ("result", ctypes.c_uint32),
+                ("expression_seed", ctypes.c_uint32), ("random_call_count", ctypes.c_uint32),
+                ("pref_noise_count", ctypes.c_uint32),
+                ("pref_noise_frequencies", ctypes.c_float * EXPRESSION_MAX_INPUTS)]
+
+
+class ExpressionInstruction(ctypes.Structure):
+    _fields_ = [("op", ctypes.c_uint32), ("operand_offset", ctypes.c_uint32), ("operand_count", ctypes.c_uint32),
+                ("auxiliary", ctypes.c_uint32), ("immediate", ctypes.c_float)]
+
+
+class ExpressionRampPoint(ctypes.Structure):
+    _fields_ = [("position", ctypes.c_float), ("value", ctypes.c_float), ("interpolation", ctypes.c_uint32)]
+
+
+class ClassicScalarPlan(ctypes.Structure):
+    """nxg_classic_scalar_plan (nxg_classic.h)."""
+    _fields_ = [("length", ctypes.c_void_p), ("width", ctypes.c_void_p), ("description_id", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32), ("patch_name", ctypes.c_char_p)]
+
+
+class ClassicApplyDesc(ctypes.Structure):
+    """nxg_classic_apply_desc (nxg_classic.h)."""
+    _fields_ = [("root_scalars", ctypes.c_void_p), ("apply_length", ctypes.c_uint32),
+                ("apply_width", ctypes.c_uint32)]
+
+
 class AssetBuildInput(ctypes.Structure):
     """nxg_asset_build_input: the flattened AssetBuildInput of asset.h:14-44."""
     _fields_ = [
@@ -185,7 +226,8 @@ ERROR_NAMES = [
 ]
 ERRORS = {name: code for code, name in enumerate(ERROR_NAMES)}
 ERRORS.update(InvalidArgument=64, InvalidStrandRange=65, WorkspaceTooSmall=66,
-              MisalignedOutput=67, StaticScratchLimit=68, Cuda=96)
+              MisalignedOutput=67, StaticScratchLimit=68, ExpressionSyntax=69, ExpressionLimit=70,
+              ExpressionInput=71, ExpressionDomain=72, Surrogate=73, Cuda=96)
 STATIC_SCRATCH_BYTES = 4 << 20  # NXG_STATIC_SCRATCH_BYTES
 ERROR_BY_CODE = {code: name for name, code in ERRORS.items()}
 
@@ -267,6 +309,24 @@ _SIGNATURES = {
                                                   ctypes.POINTER(DeformedDesc),
                                                   ctypes.POINTER(GenerationParams), _P, ctypes.c_uint32,
                                                   _P, _P]),
+    # nxg_classic.h
+    "nxg_expression_compile": (ctypes.c_uint32, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_uint32,
+                                                 ctypes.POINTER(ctypes.c_void_p), ctypes.c_char_p, ctypes.c_size_t]),
+    "nxg_expression_destroy": (None, [_P]),
+    "nxg_expression_get_info": (ctypes.c_uint32, [_P, ctypes.POINTER(ExpressionInfo)]),
+    "nxg_expression_get_instruction": (ctypes.c_uint32, [_P, ctypes.c_uint32, ctypes.POINTER(ExpressionInstruction)]),
+    "nxg_expression_get_operand": (ctypes.c_uint32, [_P, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)]),
+    "nxg_expression_get_ramp_point": (ctypes.c_uint32, [_P, ctypes.c_uint32, ctypes.POINTER(ExpressionRampPoint)]),
+    "nxg_expression_input_name": (ctypes.c_char_p, [_P, ctypes.c_uint32]),
+    "nxg_xgen_string_seed": (ctypes.c_uint32, [ctypes.c_char_p]),
+    "nxg_classic_root_scalars": (ctypes.c_uint32, [ctypes.POINTER(DeviceAssetDesc), ctypes.POINTER(GenerationParams),
+                                                   ctypes.POINTER(ClassicScalarPlan), ctypes.c_uint32,
+                                                   ctypes.c_uint32, _P, _P, _P]),
+    "nxg_generate_packed_classic": (ctypes.c_uint32, [ctypes.POINTER(DeviceAssetDesc), ctypes.POINTER(DeformedDesc),
+                                                      ctypes.POINTER(GenerationParams),
+                                                      ctypes.POINTER(PackedOutputDesc),
+                                                      ctypes.POINTER(ClassicApplyDesc), ctypes.POINTER(LaunchConfig),
+                                                      ctypes.c_uint32, ctypes.c_uint32, _P, ctypes.c_uint64, _P]),
 }
 
 
@@ -294,6 +354,8 @@ def lib() -> ctypes.CDLL:
                               "this package has no CPU fallback")
         handle = ctypes.CDLL(LIBRARY_PATH)
         for name, (restype, argtypes) in _SIGNATURES.items():
+            if not hasattr(handle, name):
+                raise ImportError("libnxg_b200.so lacks %s; rebuild it" % name)
             fn = getattr(handle, name)
             fn.restype = restype
             fn.argtypes = argtypes

@@ -27,9 +27,10 @@ NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-
                      "-Xptxas", "-warn-spills"]
 CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-ffp-contract=off", "-Wall", "-Wextra", "-I" + INCLUDE]
 
-CUDA_SOURCES = ["generate.cu", "batched.cu"]
-HOST_SOURCES = ["host.cpp"]
-HEADERS = ["nxg_internal.h", "strand_math.cuh", "generator_core.cuh", "seexpr_gradients.inc"]
+CUDA_SOURCES = ["generate.cu", "batched.cu", "classic.cu"]
+HOST_SOURCES = ["host.cpp", "expression.cpp"]
+HEADERS = ["nxg_internal.h", "strand_math.cuh", "generator_core.cuh", "seexpr_gradients.inc", "expression.h",
+           "seexpr_permutation.inc"]
 
 
 def _stale(target: str, deps: list[str]) -> bool:
@@ -48,7 +49,7 @@ def _run(cmd: list[str], verbose: bool) -> None:
 def build_library(verbose: bool = False, force: bool = False) -> str:
     """Compiles and links libnxg_b200.so when any source is newer than it."""
     os.makedirs(OBJ, exist_ok=True)
-    common = [os.path.join(INCLUDE, "nxg.h")] + [os.path.join(CSRC, h) for h in HEADERS]
+    common = [os.path.join(INCLUDE, "nxg.h"), os.path.join(INCLUDE, "nxg_classic.h")] + [os.path.join(CSRC, h) for h in HEADERS]
     objects = []
     for src in CUDA_SOURCES:
         path = os.path.join(CSRC, src)

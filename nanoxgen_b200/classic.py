@@ -1,0 +1,174 @@
+"""Classic-expression per-root scalars (include/nxg_classic.h).
+
+``Expression`` compiles an XGen scalar expression with the library's host
+compiler (the reference's compile_xgen_scalar_expression +
+make_xgen_float_expression_program, src/xgen_expression.cpp:771-818, and the
+Classic noise($Prefg*k) rewrite, src/xgen_classic_runtime.cpp:237-347).
+``root_scalars`` evaluates a description's length / width expressions for
+every root on the device, and ``generate_packed_classic`` generates strands
+with the scalars applied inside the generator (the reference applies them
+afterwards on the host in apply_xgen_classic_float_runtime_plan_cpu,
+src/xgen_classic_runtime.cpp:1650-1678 and :1827-1858).
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+from typing import Optional
+
+import numpy as np
+import torch
+
+from . import _abi
+from ._abi import (ClassicApplyDesc, ClassicScalarPlan, DeformedDesc, ExpressionInfo, ExpressionInstruction,
+                   ExpressionRampPoint, GenerationParams, LaunchConfig, check, lib)
+from .generator import (DeformedGeometry, DeviceAsset, PackedCurves, _stream_handle, allocate_outputs,
+                        packed_output_descriptor)
+
+
+class ExpressionError(ValueError):
+    """The compiler rejected the source; the message is the reference's text."""
+
+
+class Expression:
+    """A compiled scalar expression (host handle of nxg_expression)."""
+
+    def __init__(self, source: str, name: str = "", object_type: str = "", classic: bool = False):
+        handle = ctypes.c_void_p()
+        msg = ctypes.create_string_buffer(512)
+        code = lib().nxg_expression_compile(source.encode(), name.encode(), object_type.encode(),
+                                            _abi.EXPRESSION_CLASSIC if classic else 0, ctypes.byref(handle), msg,
+                                            512)
+        if code == _abi.ERRORS["ExpressionSyntax"]:
+            raise ExpressionError(msg.value.decode())
+        check(code, "nxg_expression_compile")
+        self.handle = handle
+        self.source = source
+
+    @classmethod
+    def classic(cls, source: str, attribute: str, object_type: str = "SplinePrimitive") -> "Expression":
+        """An attribute of a Classic object, as the Classic runtime compiles
+        it (seed from attribute name + object type, noise($Prefg*k) bound)."""
+        return cls(source, attribute, object_type, classic=True)
+
+    def close(self) -> None:
+        if getattr(self, "handle", None) and self.handle.value:
+            lib().nxg_expression_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self) -> ExpressionInfo:
+        out = ExpressionInfo()
+        check(lib().nxg_expression_get_info(self.handle, ctypes.byref(out)), "nxg_expression_get_info")
+        return out
+
+    @property
+    def inputs(self) -> list[str]:
+        n = self.info().input_count
+        return [lib().nxg_expression_input_name(self.handle, i).decode() for i in range(n)]
+
+    def describe(self) -> dict:
+        """Every field of the float program as plain Python values (floats as
+        their bit patterns), laid out like the reference's program."""
+        info = self.info()
+        ins = []
+        for i in range(info.instruction_count):
+            x = ExpressionInstruction()
+            check(lib().nxg_expression_get_instruction(self.handle, i, ctypes.byref(x)), "get_instruction")
+            ins.append((x.op, x.operand_offset, x.operand_count, x.auxiliary,
+                        np.float32(x.immediate).view(np.uint32).item()))
+        ops = []
+        for i in range(info.operand_count):
+            v = ctypes.c_uint32()
+            check(lib().nxg_expression_get_operand(self.handle, i, ctypes.byref(v)), "get_operand")
+            ops.append(int(v.value))
+        pts = []
+        for i in range(info.ramp_point_count):
+            p = ExpressionRampPoint()
+            check(lib().nxg_expression_get_ramp_point(self.handle, i, ctypes.byref(p)), "get_ramp_point")
+            pts.append((np.float32(p.position).view(np.uint32).item(), np.float32(p.value).view(np.uint32).item(),
+                        p.interpolation))
+        return dict(instructions=ins, operands=ops, inputs=self.inputs, ramp_points=pts, ramp_count=info.ramp_count,
+                    result=info.result, expression_seed=info.expression_seed,
+                    random_call_count=info.random_call_count)
+
+    @property
+    def pref_noise_frequencies(self) -> np.ndarray:
+        info = self.info()
+        return np.array(info.pref_noise_frequencies[:info.pref_noise_count], np.float32)
+
+
+@dataclasses.dataclass
+class ScalarPlan:
+    """A description's SplinePrimitive length / width expressions."""
+    length: Optional[Expression] = None
+    width: Optional[Expression] = None
+    description_id: int = 0
+    patch_name: str = ""
+
+    def descriptor(self) -> ClassicScalarPlan:
+        d = ClassicScalarPlan()
+        d.length = self.length.handle.value if self.length is not None else None
+        d.width = self.width.handle.value if self.width is not None else None
+        d.description_id = self.description_id
+        self._patch = self.patch_name.encode()
+        d.patch_name = self._patch
+        return d
+
+
+def root_scalars(dasset: DeviceAsset, params: GenerationParams, plan: ScalarPlan, *, first_strand: int = 0,
+                 count: Optional[int] = None, out: Optional[torch.Tensor] = None,
+                 status: Optional[torch.Tensor] = None,
+                 stream: Optional[torch.cuda.Stream] = None) -> tuple[torch.Tensor, torch.Tensor]:
+    """Exact per-root (length scale, width) as an (n, 2) float32 tensor, and
+    the 2-word device status (error code, failing strands).  Enqueue only."""
+    n = int(params.strand_count) - first_strand if count is None else int(count)
+    if out is None:
+        out = torch.empty((max(n, 1), 2), dtype=torch.float32, device=dasset.device)
+    if status is None:
+        status = torch.zeros(2, dtype=torch.int32, device=dasset.device)
+    desc = plan.descriptor()
+    check(lib().nxg_classic_root_scalars(ctypes.byref(dasset.desc), ctypes.byref(params), ctypes.byref(desc),
+                                         first_strand, n, out.data_ptr(), status.data_ptr(), _stream_handle(stream)),
+          "nxg_classic_root_scalars")
+    return out, status
+
+
+def check_status(status: torch.Tensor) -> None:
+    """Raises NxgError if a root_scalars launch reported a domain error."""
+    code, failing = (int(v) for v in status.cpu().tolist())
+    if code:
+        raise _abi.NxgError(code, "root scalars (%d strands)" % failing)
+
+
+def generate_packed_classic(dasset: DeviceAsset, params: GenerationParams, scalars: torch.Tensor,
+                            apply_length: bool = True, apply_width: bool = True, radius_scale: float = 1.0,
+                            deformed: Optional[DeformedGeometry] = None, *, first_strand: int = 0,
+                            count: Optional[int] = None, points: Optional[torch.Tensor] = None,
+                            roots: Optional[torch.Tensor] = None, root_uvs: Optional[torch.Tensor] = None,
+                            point_counts: Optional[torch.Tensor] = None, want_roots: bool = True,
+                            block_size: int = 128, stream: Optional[torch.cuda.Stream] = None) -> PackedCurves:
+    """Generation with the Classic length / width application fused in; a
+    dropped strand keeps its points and gets point count 0."""
+    n = int(params.strand_count) - first_strand if count is None else int(count)
+    cvs = int(params.cvs_per_strand)
+    if points is None:
+        points, r, uv, pc = allocate_outputs(n, cvs, dasset.device, want_roots, want_roots, True)
+        roots = roots if roots is not None else r
+        root_uvs = root_uvs if root_uvs is not None else uv
+        point_counts = point_counts if point_counts is not None else pc
+    out = packed_output_descriptor(points, roots, root_uvs, point_counts, radius_scale)
+    ddesc = deformed.descriptor() if deformed is not None else DeformedDesc()
+    apply = ClassicApplyDesc(scalars.data_ptr(), int(apply_length), int(apply_width))
+    cfg = LaunchConfig(block_size)
+    ws = dasset.workspace(params, max(n, 1))
+    check(lib().nxg_generate_packed_classic(ctypes.byref(dasset.desc), ctypes.byref(ddesc), ctypes.byref(params),
+                                            ctypes.byref(out), ctypes.byref(apply), ctypes.byref(cfg), first_strand,
+                                            n, ws.data_ptr(), ws.numel(), _stream_handle(stream)),
+          "nxg_generate_packed_classic")
+    return PackedCurves(n, cvs, points, point_counts, roots, root_uvs)

@@ -40,7 +40,7 @@ namespace dev {
 // Persistent CTAs over contiguous ranges of the strand order.  Each warp
 // takes 32 strands at a time: phase A sets them up one lane per strand,
 // phase B emits them one L-lane group per strand.
-template <int L, int PPT, bool NOISE>
+template <int L, int PPT, bool NOISE, bool CLASSIC>
 __global__ void generate_kernel(LaunchArgs g, const float4 *offsets) {
     extern __shared__ float4 smem[];
     constexpr int kGroups = 32 / L;
@@ -85,10 +85,40 @@ __global__ void generate_kernel(LaunchArgs g, const float4 *offsets) {
         const uint32_t in_batch = min(32u, end - batch);
 #pragma unroll 1
         for (uint32_t r = 0; r < in_batch; r += kGroups) {
-            emit_strand<L, PPT, NOISE>(g, rec, static_cast<int>(r) + group, gl, table, offsets, tvals, stage,
+            emit_strand<L, PPT, NOISE, CLASSIC>(g, rec, static_cast<int>(r) + group, gl, table, offsets, tvals, stage,
                                        lattice, kLatticeMax);
         }
         __syncwarp();
+    }
+}
+
+// The Classic application for the serial generator (P > 128): one thread
+// per strand re-reads its written points (xgen_classic_runtime.cpp:1650-1678,
+// :1827-1858), measuring cLength for every strand.
+__global__ void classic_serial_apply_kernel(LaunchArgs g) {
+    const int P = static_cast<int>(g.p.cvs_per_strand);
+    const float rs = g.p.radius_scale;
+    for (uint32_t local = blockIdx.x * blockDim.x + threadIdx.x; local < g.count; local += gridDim.x * blockDim.x) {
+        float4 *pts = g.points + static_cast<uint64_t>(local) * static_cast<uint32_t>(P);
+        const float2 sc = g.scalars[local];
+        const float s = g.classic_length ? sc.x : 1.0f;
+        const float raw_width = g.classic_width ? sc.y : (rs > 0.0f ? __fdiv_rn(__fmul_rn(2.0f, pts[0].w), rs) : 0.0f);
+        bool keep = !(raw_width < 1.0e-4f);
+        if (keep) { keep = !(__fmul_rn(classic_spline_length(pts, P), s) < 1.0e-4f); }
+        const F3 front = xyz(pts[0]);
+        const float radius = __fmul_rn(__fmul_rn(0.5f, raw_width < 0.0f ? 0.0f : raw_width), rs);
+        for (int cv = 0; cv < P; ++cv) {
+            float4 q = pts[cv];
+            if (g.classic_length) {
+                const F3 v = xadd(front, xmul(xsub(xyz(q), front), s));
+                q.x = v.x;
+                q.y = v.y;
+                q.z = v.z;
+            }
+            if (g.classic_width) { q.w = radius; }
+            pts[cv] = q;
+        }
+        if (!keep && g.point_counts != nullptr) { g.point_counts[local] = 0u; }
     }
 }
 
@@ -457,6 +487,8 @@ WorkspaceLayout workspace_layout(uint32_t guide_count, uint32_t count, uint32_t 
     return w;
 }
 
+} // namespace
+
 int device_sm_count() {
     int device = 0;
     if (cudaGetDevice(&device) != cudaSuccess) { return 148; }
@@ -466,8 +498,6 @@ int device_sm_count() {
     }
     return sms;
 }
-
-} // namespace
 
 dev::AssetArgs resolve_asset(const nxg_device_asset_desc &desc) {
     const auto *base = static_cast<const unsigned char *>(desc.asset);
@@ -535,19 +565,24 @@ namespace {
 
 using KernelFn = void (*)(LaunchArgs, const float4 *);
 
+// Classic variants (scalars applied in the kernel) are separate
+// instantiations, so the plain generator keeps its register budget.
 template <int L, int PPT>
-KernelFn pick_noise(bool noise) {
-    return noise ? dev::generate_kernel<L, PPT, true> : dev::generate_kernel<L, PPT, false>;
+KernelFn pick_noise(bool noise, bool classic) {
+    if (classic) {
+        return noise ? dev::generate_kernel<L, PPT, true, true> : dev::generate_kernel<L, PPT, false, true>;
+    }
+    return noise ? dev::generate_kernel<L, PPT, true, false> : dev::generate_kernel<L, PPT, false, false>;
 }
 
 template <int PPT>
-KernelFn pick_lanes(int lanes, bool noise) {
+KernelFn pick_lanes(int lanes, bool noise, bool classic) {
     switch (lanes) {
-        case 2: return pick_noise<2, PPT>(noise);
-        case 4: return pick_noise<4, PPT>(noise);
-        case 8: return pick_noise<8, PPT>(noise);
-        case 16: return pick_noise<16, PPT>(noise);
-        default: return pick_noise<32, PPT>(noise);
+        case 2: return pick_noise<2, PPT>(noise, classic);
+        case 4: return pick_noise<4, PPT>(noise, classic);
+        case 8: return pick_noise<8, PPT>(noise, classic);
+        case 16: return pick_noise<16, PPT>(noise, classic);
+        default: return pick_noise<32, PPT>(noise, classic);
     }
 }
 
@@ -579,11 +614,11 @@ void default_tile(uint32_t P, bool noise, int *lanes, int *ppt, uint32_t *block)
     *block = 0u;
 }
 
-KernelFn pick_kernel(int lanes, int ppt, bool noise) {
+KernelFn pick_kernel(int lanes, int ppt, bool noise, bool classic) {
     switch (ppt) {
-        case 1: return pick_lanes<1>(lanes, noise);
-        case 2: return pick_lanes<2>(lanes, noise);
-        default: return pick_lanes<4>(lanes, noise);
+        case 1: return pick_lanes<1>(lanes, noise, classic);
+        case 2: return pick_lanes<2>(lanes, noise, classic);
+        default: return pick_lanes<4>(lanes, noise, classic);
     }
 }
 
@@ -601,7 +636,6 @@ uint32_t record_cuda(cudaError_t e) {
     return NXG_ERROR_CUDA;
 }
 
-namespace {
 
 uint32_t check_launch_inputs(const nxg_device_asset_desc &asset, const nxg_packed_output_desc *output) {
     if (!sections_in_bounds(asset.header)) { return NXG_ERROR_INVALID_ASSET_METADATA; }
@@ -653,7 +687,7 @@ uint32_t launch_order(const nxg_device_asset_desc &asset, uint32_t seed, uint32_
 uint32_t launch_generate(const nxg_device_asset_desc &asset, const nxg_deformed_desc &deformed,
                          const nxg_generation_params &params, const nxg_packed_output_desc &output,
                          const nxg_launch_config &config, uint32_t first, uint32_t count, void *workspace,
-                         cudaStream_t stream, float *vec3_points = nullptr) {
+                         cudaStream_t stream, float *vec3_points, const nxg_classic_apply_desc *classic) {
     set_last_cuda_error(0);
     const uint32_t P = params.cvs_per_strand;
     const WorkspaceLayout ws = workspace_layout(asset.header.guide_count, count, P);
@@ -670,6 +704,11 @@ uint32_t launch_generate(const nxg_device_asset_desc &asset, const nxg_deformed_
     g.root_uvs = reinterpret_cast<float2 *>(output.root_uvs);
     g.point_counts = output.point_counts;
     g.order = reinterpret_cast<const uint32_t *>(wbase + ws.order);
+    if (classic != nullptr) {
+        g.scalars = reinterpret_cast<const float2 *>(classic->root_scalars);
+        g.classic_length = classic->apply_length != 0u;
+        g.classic_width = classic->apply_width != 0u;
+    }
     const int sms = device_sm_count();
     uint32_t status = NXG_ERROR_NONE;
     if (!parallel_path(asset.header.guide_count, P)) {
@@ -677,6 +716,8 @@ uint32_t launch_generate(const nxg_device_asset_desc &asset, const nxg_deformed_
         const uint32_t blocks = static_cast<uint32_t>(std::min<uint64_t>((count + threads - 1u) / threads,
                                                                           static_cast<uint64_t>(sms) * 8u));
         dev::generate_serial_kernel<<<blocks, threads, 0, stream>>>(g);
+        if ((status = record_cuda(cudaGetLastError())) || g.scalars == nullptr) { return status; }
+        dev::classic_serial_apply_kernel<<<blocks, threads, 0, stream>>>(g);
         return record_cuda(cudaGetLastError());
     }
     auto *offsets = reinterpret_cast<float4 *>(wbase + ws.offsets);
@@ -700,7 +741,7 @@ uint32_t launch_generate(const nxg_device_asset_desc &asset, const nxg_deformed_
     uint32_t tile_block = 0u;
     const bool noise = g.p.noise != 0u;
     default_tile(P, noise, &lanes, &ppt, &tile_block);
-    KernelFn fn = pick_kernel(lanes, ppt, noise);
+    KernelFn fn = pick_kernel(lanes, ppt, noise, g.scalars != nullptr);
     // block_size in [1, 1024] is a request: rounded up to whole warps, then
     // capped at what this kernel's register footprint can launch.
     cudaFuncAttributes attr{};
@@ -765,7 +806,6 @@ uint32_t validate_range_request(const nxg_device_asset_desc *asset, const nxg_de
     return NXG_ERROR_NONE;
 }
 
-} // namespace
 } // namespace nxg
 
 extern "C" {
@@ -808,7 +848,8 @@ uint32_t nxg_generate_packed_range(const nxg_device_asset_desc *asset, const nxg
     const nxg_deformed_desc none{};
     const nxg_launch_config default_config{128u};
     return nxg::launch_generate(*asset, deformed ? *deformed : none, *params, *output,
-                                config ? *config : default_config, first_strand, strand_count, workspace, s);
+                                config ? *config : default_config, first_strand, strand_count, workspace, s,
+                                nullptr, nullptr);
 }
 
 uint32_t nxg_prepare_strand_order(const nxg_device_asset_desc *asset, const nxg_generation_params *params,
@@ -851,7 +892,7 @@ uint32_t nxg_generate_packed_ordered(const nxg_device_asset_desc *asset, const n
     const nxg_launch_config default_config{128u};
     return nxg::launch_generate(*asset, deformed ? *deformed : none, *params, *output,
                                 config ? *config : default_config, first_strand, strand_count, workspace,
-                                static_cast<cudaStream_t>(stream));
+                                static_cast<cudaStream_t>(stream), nullptr, nullptr);
 }
 
 uint32_t nxg_query_strand_states(const nxg_device_asset_desc *asset, const nxg_deformed_desc *deformed,
@@ -1027,7 +1068,7 @@ extern "C" uint32_t nxg_generate_motion_packed(const nxg_device_asset_desc *asse
     }
     for (uint32_t i = 0; i < sample_count && !error; ++i) {
         error = nxg::launch_generate(*asset, samples[i].deformation, *params, outputs[i], cfg, 0u,
-                                     params->strand_count, workspace, s);
+                                     params->strand_count, workspace, s, nullptr, nullptr);
     }
     return error;
 }
@@ -1057,7 +1098,7 @@ extern "C" uint32_t nxg_generate_motion(const nxg_device_asset_desc *asset, cons
     for (uint32_t i = 0; i < sample_count && !error; ++i) {
         float *dst = reinterpret_cast<float *>(output->points) + per_sample * i;
         error = nxg::launch_generate(*asset, samples[i].deformation, *params, none, cfg, 0u, params->strand_count,
-                                     workspace, s, dst);
+                                     workspace, s, dst, nullptr);
     }
     return error;
 }

@@ -11,6 +11,7 @@
 #pragma once
 
 #include "nxg_internal.h"
+#include "nxg_classic.h"
 #include "strand_math.cuh"
 
 #include <cuda_runtime.h>
@@ -32,6 +33,9 @@ struct LaunchArgs {
     float2 *root_uvs;
     uint32_t *point_counts;
     const uint32_t *order;   // permutation of [0, count), or nullptr for identity
+    const float2 *scalars;   // Classic per-root (length scale, width), or nullptr
+    uint32_t classic_length; // scale each strand about its first point by scalars.x
+    uint32_t classic_width;  // radius = 0.5 * max(scalars.y, 0) * radius_scale
 };
 
 constexpr int kTableFloat4 = NXG_NOISE_GRADIENT_COUNT;  // float4 entries of the staged table
@@ -217,9 +221,53 @@ __device__ __forceinline__ float2 lattice_column(const float4 *table, int axis, 
     return make_float2(A, B);
 }
 
+// ---------------------------------------------------------------------------
+// Classic cLength (xgen_classic_runtime.cpp:591-662): the uniform cubic
+// B-spline through the CVs, with mirrored phantom end CVs, sampled at
+// 2P + 4 intervals whose first and last samples are the raw end CVs.  Every
+// operation is rounded as the reference's, so a strand's measured length
+// matches the CPU runtime's for the same points.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ F3 xyz(float4 v) { return {v.x, v.y, v.z}; }
+
+__device__ inline F3 classic_curve_eval(const float4 *pts, int P, float t) {
+    if (t < 1.0e-7f) { return xyz(pts[0]); }
+    if (t > 1.0f - 1.0e-7f) { return xyz(pts[P - 1]); }
+    const float scaled = __fmul_rn(t, static_cast<float>(P - 1));
+    const int span = static_cast<int>(static_cast<uint32_t>(scaled));
+    const float f = __fsub_rn(scaled, static_cast<float>(span));
+    const float f2 = __fmul_rn(f, f);
+    const float f3 = __fmul_rn(f2, f);
+    const float omf = __fsub_rn(1.0f, f);
+    const float b0 = __fmul_rn(__fmul_rn(omf, omf), omf);
+    const float b1 = __fadd_rn(__fsub_rn(__fmul_rn(3.0f, f3), __fmul_rn(6.0f, f2)), 4.0f);
+    const float b2 =
+        __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(-3.0f, f3), __fmul_rn(3.0f, f2)), __fmul_rn(3.0f, f)), 1.0f);
+    const F3 p0 = span == 0 ? xsub(xmul(xyz(pts[0]), 2.0f), xyz(pts[1])) : xyz(pts[span - 1]);
+    const F3 p1 = xyz(pts[span]);
+    const F3 p2 = xyz(pts[span + 1]);
+    const F3 p3 = span + 2 == P ? xsub(xmul(xyz(pts[P - 1]), 2.0f), xyz(pts[P - 2])) : xyz(pts[span + 2]);
+    return xmul(xadd(xadd(xadd(xmul(p0, b0), xmul(p1, b1)), xmul(p2, b2)), xmul(p3, f3)), 1.0f / 6.0f);
+}
+
+__device__ inline float classic_spline_length(const float4 *pts, int P) {
+    const int intervals = 2 * P + 4;
+    const float step = __fdiv_rn(1.0f, static_cast<float>(intervals));
+    F3 previous = xyz(pts[0]);
+    float length = 0.0f;
+    for (int k = 1; k < intervals; ++k) {
+        const F3 current = classic_curve_eval(pts, P, __fmul_rn(step, static_cast<float>(k)));
+        const F3 d = xsub(current, previous);
+        length = __fadd_rn(length, __fsqrt_rn(xdot(d, d)));
+        previous = current;
+    }
+    const F3 d = xsub(xyz(pts[P - 1]), previous);
+    return __fadd_rn(length, __fsqrt_rn(xdot(d, d)));
+}
+
 // Phase B: strand b of the batch on an L-lane group; lane gl owns the
 // consecutive CVs gl*PPT .. gl*PPT+PPT-1.
-template <int L, int PPT, bool NOISE>
+template <int L, int PPT, bool NOISE, bool CLASSIC = false>
 __device__ __forceinline__ void emit_strand(const LaunchArgs &g, const Records &rec, int b, int gl,
                                             const float4 *table, const float4 *offsets, const float *tvals,
                                             float4 *stage, float2 *lattice_area, int lattice_max) {
@@ -447,12 +495,61 @@ __device__ __forceinline__ void emit_strand(const LaunchArgs &g, const Records &
         }
     }
 
+    // Classic length and width (xgen_classic_runtime.cpp:1650-1678,
+    // :1827-1858) from the strand's per-root scalars: scale about the first
+    // point, override the radius, and drop (point count 0) a strand whose
+    // scaled cLength or width is below 1e-4.
+    bool width_override = false;
+    float override_radius = 0.0f;
+    if constexpr (CLASSIC) {
+        const float2 sc = __ldg(g.scalars + local);
+        const F3 front = group_shfl<L>(point[0], 0);
+        F3 last = point[0];
+#pragma unroll
+        for (int j = 1; j < PPT; ++j) {
+            if (cv0 + j == P - 1) { last = point[j]; }
+        }
+        const F3 back = group_shfl<L>(last, (P - 1) / PPT);
+        const float s = g.classic_length ? sc.x : 1.0f;
+        const float raw_width = g.classic_width ? sc.y
+            : (p.radius_scale > 0.0f ? __fdiv_rn(__fmul_rn(2.0f, strand_radius(p, 0.0f)), p.radius_scale) : 0.0f);
+        bool keep = !(raw_width < 1.0e-4f);
+        // cLength is at least the root-tip chord, so only strands near the
+        // threshold measure the sampled spline (group-uniform branch).
+        const F3 chord = back - front;
+        if (keep && !(sqrtf(dot(chord, chord)) * s > 1.01e-4f)) {
+            const int lane = static_cast<int>(threadIdx.x & 31u);
+            const unsigned group_mask = L == 32 ? kFull : (((1u << L) - 1u) << (lane - gl));
+#pragma unroll
+            for (int j = 0; j < PPT; ++j) {
+                if (cv0 + j < P) { stage[cv0 + j] = make_float4(point[j].x, point[j].y, point[j].z, 0.0f); }
+            }
+            __syncwarp(group_mask);
+            float c_length = gl == 0 ? classic_spline_length(stage, P) : 0.0f;
+            c_length = __shfl_sync(group_mask, c_length, 0, L);
+            __syncwarp(group_mask);
+            keep = !(__fmul_rn(c_length, s) < 1.0e-4f);
+        }
+        if (g.classic_length) {
+#pragma unroll
+            for (int j = 0; j < PPT; ++j) { point[j] = xadd(front, xmul(xsub(point[j], front), s)); }
+        }
+        if (g.classic_width) {
+            width_override = true;
+            override_radius = __fmul_rn(__fmul_rn(0.5f, raw_width < 0.0f ? 0.0f : raw_width), p.radius_scale);
+        }
+        if (!keep && active && gl == 0 && g.point_counts != nullptr) { g.point_counts[local] = 0u; }
+    }
+
     // Stage the strand's float4s in shared memory, then write them with
     // consecutive lanes on consecutive CVs (coalesced streaming stores).
 #pragma unroll
     for (int j = 0; j < PPT; ++j) {
         const int cv = cv0 + j;
-        if (cv < P) { stage[cv] = make_float4(point[j].x, point[j].y, point[j].z, strand_radius(p, tcv[j])); }
+        if (cv < P) {
+            stage[cv] = make_float4(point[j].x, point[j].y, point[j].z,
+                                    width_override ? override_radius : strand_radius(p, tcv[j]));
+        }
     }
     __syncwarp();
     if (active) {
@@ -517,5 +614,18 @@ dev::AssetArgs resolve_asset(const nxg_device_asset_desc &desc);
 dev::FrameArgs resolve_frame(const dev::AssetArgs &a, const nxg_deformed_desc &d);
 dev::ParamArgs resolve_params(const nxg_generation_params &p, float radius_scale);
 uint32_t record_cuda(cudaError_t e);
+int device_sm_count();
+uint32_t validate_range_request(const nxg_device_asset_desc *asset, const nxg_deformed_desc *deformed,
+                                const nxg_generation_params *params, const nxg_packed_output_desc *output,
+                                const nxg_launch_config *config, uint32_t first, uint32_t count);
+uint32_t check_launch_inputs(const nxg_device_asset_desc &asset, const nxg_packed_output_desc *output);
+uint32_t check_workspace(const nxg_device_asset_desc &asset, uint32_t count, uint32_t P, const void *workspace,
+                         uint64_t bytes);
+uint32_t launch_order(const nxg_device_asset_desc &asset, uint32_t seed, uint32_t first, uint32_t count,
+                      uint32_t P, void *workspace, cudaStream_t stream);
+uint32_t launch_generate(const nxg_device_asset_desc &asset, const nxg_deformed_desc &deformed,
+                         const nxg_generation_params &params, const nxg_packed_output_desc &output,
+                         const nxg_launch_config &config, uint32_t first, uint32_t count, void *workspace,
+                         cudaStream_t stream, float *vec3_points, const nxg_classic_apply_desc *classic);
 
 } // namespace nxg

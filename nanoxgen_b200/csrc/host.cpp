@@ -425,6 +425,12 @@ const char *nxg_error_message(uint32_t code) {
             return "device point output must be 16-byte aligned and workspace 256-byte aligned";
         case NXG_ERROR_STATIC_SCRATCH_LIMIT:
             return "request needs more scratch than the library's static scratch holds (NXG_STATIC_SCRATCH_BYTES)";
+        case NXG_ERROR_EXPRESSION_SYNTAX: return "scalar expression did not compile";
+        case NXG_ERROR_EXPRESSION_LIMIT: return "scalar expression exceeds the device program limits";
+        case NXG_ERROR_EXPRESSION_INPUT: return "scalar expression uses a variable the runtime cannot bind";
+        case NXG_ERROR_EXPRESSION_DOMAIN:
+            return "scalar expression produced a non-finite value or a negative length";
+        case NXG_ERROR_SURROGATE: return "surrogate model is missing, untrained or misconfigured";
         case NXG_ERROR_CUDA: return "a CUDA runtime call failed";
         default: return "unknown device generation error";
     }

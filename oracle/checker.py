@@ -249,3 +249,163 @@ class Reference:
 
     def gradient_noise(self, handle, x, y, z) -> float:
         return float(self.lib.ref_gradient_noise(handle.ptr, x, y, z))
+
+    # ------------------------------------------------ scalar expressions
+    # (ref_classic_shim.cpp over src/xgen_expression.cpp and
+    # src/xgen_classic_runtime.cpp)
+
+    def _expression_prototypes(self):
+        lib = self.lib
+        if getattr(self, "_expr_ready", False):
+            return lib
+        u32, f32, c_p = ctypes.c_uint32, ctypes.c_float, ctypes.c_char_p
+        lib.ref_expr_compile.restype = _P
+        lib.ref_expr_compile.argtypes = [c_p, c_p, c_p, c_p, ctypes.c_uint64]
+        lib.ref_expr_free.argtypes = [_P]
+        lib.ref_expr_info.argtypes = [_P, _P]
+        lib.ref_expr_instruction.argtypes = [_P, u32, _P, ctypes.POINTER(f32)]
+        lib.ref_expr_operand.restype = u32
+        lib.ref_expr_operand.argtypes = [_P, u32]
+        lib.ref_expr_ramp_point.argtypes = [_P, u32, ctypes.POINTER(f32), ctypes.POINTER(f32), ctypes.POINTER(u32)]
+        lib.ref_expr_input.restype = c_p
+        lib.ref_expr_input.argtypes = [_P, u32]
+        lib.ref_expr_eval_batch.argtypes = [_P, _P, u32, ctypes.c_uint64, _P, _P, _P, f32, _P, _P, _P]
+        lib.ref_seexpr_hash_finish.restype = u32
+        lib.ref_seexpr_hash_finish.argtypes = [u32]
+        lib.ref_runtime_hash_component.restype = u32
+        lib.ref_runtime_hash_component.argtypes = [f32]
+        lib.ref_runtime_hash.restype = f32
+        lib.ref_runtime_hash.argtypes = [_P, u32]
+        lib.ref_runtime_face_seed.restype = f32
+        lib.ref_runtime_face_seed.argtypes = [u32, c_p, u32]
+        lib.ref_string_seed.restype = u32
+        lib.ref_string_seed.argtypes = [c_p]
+        lib.ref_classic_noise_batch.argtypes = [_P, ctypes.c_uint64, f32, _P]
+        lib.ref_classic_plan.restype = _P
+        lib.ref_classic_plan.argtypes = [c_p, c_p, u32, c_p, c_p, ctypes.c_uint64]
+        lib.ref_classic_plan_free.argtypes = [_P]
+        lib.ref_classic_plan_info.argtypes = [_P, _P, _P]
+        lib.ref_classic_plan_program.restype = _P
+        lib.ref_classic_plan_program.argtypes = [_P, u32]
+        lib.ref_classic_apply.restype = u32
+        lib.ref_classic_apply.argtypes = [_P, _P, _P, _P, _P, u32, u32, f32, _P, ctypes.c_uint64, u32, _P, c_p,
+                                          ctypes.c_uint64]
+        self._expr_ready = True
+        return lib
+
+    class Program:
+        """A reference XgenFloatExpressionProgram."""
+
+        def __init__(self, ref, ptr, owned=True):
+            self.ref, self.ptr, self.owned = ref, ptr, owned
+
+        def __del__(self):
+            if getattr(self, "owned", False) and self.ptr:
+                self.ref.lib.ref_expr_free(self.ptr)
+                self.ptr = None
+
+        def describe(self) -> dict:
+            """Every field of the program, as plain Python values."""
+            lib = self.ref.lib
+            info = np.zeros(8, np.uint32)
+            lib.ref_expr_info(self.ptr, info.ctypes.data)
+            n_ins, n_ops, n_in, n_ramps, n_pts, result, seed, calls = (int(v) for v in info)
+            ins = []
+            for i in range(n_ins):
+                w = np.zeros(4, np.uint32)
+                imm = ctypes.c_float()
+                lib.ref_expr_instruction(self.ptr, i, w.ctypes.data, ctypes.byref(imm))
+                ins.append((int(w[0]), int(w[1]), int(w[2]), int(w[3]), np.float32(imm.value).view(np.uint32).item()))
+            pts = []
+            for i in range(n_pts):
+                a, b, c = ctypes.c_float(), ctypes.c_float(), ctypes.c_uint32()
+                lib.ref_expr_ramp_point(self.ptr, i, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
+                pts.append((np.float32(a.value).view(np.uint32).item(), np.float32(b.value).view(np.uint32).item(),
+                            int(c.value)))
+            return dict(instructions=ins, operands=[int(lib.ref_expr_operand(self.ptr, i)) for i in range(n_ops)],
+                        inputs=[lib.ref_expr_input(self.ptr, i).decode() for i in range(n_in)],
+                        ramp_points=pts, ramp_count=n_ramps, result=result, expression_seed=seed,
+                        random_call_count=calls)
+
+        def evaluate(self, inputs, u=None, v=None, face_seed=None, t=0.0):
+            """evaluate_xgen_scalar_expression_float per row; (values, ok)."""
+            inputs = np.ascontiguousarray(inputs, np.float32)
+            count = inputs.shape[0]
+            cols = inputs.shape[1] if inputs.ndim == 2 else 0
+            out = np.zeros(count, np.float32)
+            ok = np.zeros(count, np.uint8)
+            keep = [None if a is None else np.ascontiguousarray(a, np.float32) for a in (u, v, face_seed)]
+            p = lambda a: None if a is None else a.ctypes.data
+            self.ref.lib.ref_expr_eval_batch(self.ptr, inputs.ctypes.data, cols, count, p(keep[0]), p(keep[1]),
+                                             p(keep[2]), t, None, out.ctypes.data, ok.ctypes.data)
+            return out, ok.astype(bool)
+
+    def compile_expression(self, source: str, name: str = "", object_type: str = ""):
+        """compile + make_float_program; returns (Program or None, message)."""
+        lib = self._expression_prototypes()
+        msg = ctypes.create_string_buffer(512)
+        ptr = lib.ref_expr_compile(source.encode(), name.encode(), object_type.encode(), msg, 512)
+        return (Reference.Program(self, ptr) if ptr else None), msg.value.decode()
+
+    def classic_noise(self, points, frequency: float) -> np.ndarray:
+        """xgen_classic_noise_float(p * frequency) per point."""
+        lib = self._expression_prototypes()
+        pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+        out = np.zeros(pts.shape[0], np.float32)
+        lib.ref_classic_noise_batch(pts.ctypes.data, pts.shape[0], frequency, out.ctypes.data)
+        return out
+
+    def runtime_face_seed(self, description_id: int, patch: str, face: int) -> float:
+        return float(self._expression_prototypes().ref_runtime_face_seed(description_id, patch.encode(), face))
+
+    class Plan:
+        def __init__(self, ref, ptr, reasons):
+            self.ref, self.ptr, self.fallback_reasons = ref, ptr, reasons
+
+        def __del__(self):
+            if getattr(self, "ptr", None):
+                self.ref.lib.ref_classic_plan_free(self.ptr)
+                self.ptr = None
+
+        def info(self) -> dict:
+            out = np.zeros(4, np.uint32)
+            freqs = np.zeros(64, np.float32)
+            self.ref.lib.ref_classic_plan_info(self.ptr, out.ctypes.data, freqs.ctypes.data)
+            return dict(has_length=bool(out[0]), has_width=bool(out[1]), ptex=int(out[2]),
+                        pref_noise=freqs[:int(out[3])].copy())
+
+        def program(self, which: str):
+            ptr = self.ref.lib.ref_classic_plan_program(self.ptr, 0 if which == "length" else 1)
+            return Reference.Program(self.ref, ptr, owned=False) if ptr else None
+
+    def classic_plan(self, length=None, width=None, description_id: int = 0, name: str = "description"):
+        """compile_xgen_classic_float_runtime_plan for one SplinePrimitive."""
+        lib = self._expression_prototypes()
+        msg = ctypes.create_string_buffer(2048)
+        enc = lambda s: None if s is None else s.encode()
+        ptr = lib.ref_classic_plan(enc(length), enc(width), description_id, name.encode(), msg, 2048)
+        if not ptr:
+            raise ValueError(msg.value.decode())
+        return Reference.Plan(self, ptr, [r for r in msg.value.decode().split("\n") if r])
+
+    def classic_apply(self, plan, points, counts, roots, uvs, cvs: int, radius_scale: float,
+                      runtime_inputs=None, workers: int = 1):
+        """apply_xgen_classic_float_runtime_plan_cpu; returns the compacted
+        (points, counts, roots, uvs)."""
+        lib = self._expression_prototypes()
+        points = np.ascontiguousarray(points, np.float32).copy()
+        counts = np.ascontiguousarray(counts, np.uint32).copy()
+        roots = np.ascontiguousarray(roots).copy()
+        uvs = np.ascontiguousarray(uvs, np.float32).copy()
+        S = counts.size
+        inputs = None if runtime_inputs is None else np.ascontiguousarray(runtime_inputs, np.float32)
+        kept = ctypes.c_uint32()
+        msg = ctypes.create_string_buffer(512)
+        rc = lib.ref_classic_apply(plan.ptr, points.ctypes.data, counts.ctypes.data, roots.ctypes.data,
+                                   uvs.ctypes.data, S, cvs, radius_scale,
+                                   None if inputs is None else inputs.ctypes.data,
+                                   0 if inputs is None else inputs.size, workers, ctypes.byref(kept), msg, 512)
+        if rc != 0:
+            raise ValueError(msg.value.decode())
+        k = kept.value
+        return points[:k * cvs], counts[:k], roots[:k], uvs[:k]

@@ -1,0 +1,228 @@
+// ref_classic_shim.cpp -- extern "C" shim over the reference's scalar
+// expression compiler/evaluator and its Classic float runtime.
+//
+// TEST INFRASTRUCTURE ONLY.  oracle/Makefile links this file with the
+// unmodified reference sources src/xgen_expression.cpp,
+// src/xgen_classic_runtime.cpp and their support files (xgen_classic.cpp,
+// context.cpp, task_executor.cpp) into oracle/_ref/libnxg_ref.so.  Tests pin
+// the product's compiler, device evaluator and fused Classic application
+// against it; make_permutation_table.py derives the SeExpr permutation from
+// ref_seexpr_hash_finish.  Nothing here is product code.
+#include "nanoxgen/asset.h"
+#include "nanoxgen/context.h"
+#include "nanoxgen/xgen_classic.h"
+#include "nanoxgen/xgen_classic_runtime.h"
+#include "nanoxgen/xgen_expression.h"
+
+#include <cstdint>
+#include <cstring>
+#include <exception>
+#include <span>
+#include <string>
+#include <vector>
+
+using namespace nanoxgen;
+
+namespace {
+
+void copy_text(const std::string &text, char *out, std::uint64_t cap) {
+    if (!out || cap == 0u) { return; }
+    const std::size_t n = std::min<std::size_t>(text.size(), static_cast<std::size_t>(cap - 1u));
+    std::memcpy(out, text.data(), n);
+    out[n] = '\0';
+}
+
+const XgenFloatExpressionProgram *program_of(const void *p) {
+    return static_cast<const XgenFloatExpressionProgram *>(p);
+}
+
+} // namespace
+
+extern "C" {
+
+// compile_xgen_scalar_expression + make_xgen_float_expression_program.
+void *ref_expr_compile(const char *source, const char *name, const char *type, char *msg, std::uint64_t cap) {
+    try {
+        XgenExpressionCompileOptions options{};
+        options.expression_name = name ? name : "";
+        options.object_type = type ? type : "";
+        auto *p = new XgenFloatExpressionProgram(
+            make_xgen_float_expression_program(compile_xgen_scalar_expression(source, options)));
+        copy_text("", msg, cap);
+        return p;
+    } catch (const std::exception &e) {
+        copy_text(e.what(), msg, cap);
+        return nullptr;
+    }
+}
+
+void ref_expr_free(void *p) { delete static_cast<XgenFloatExpressionProgram *>(p); }
+
+// instructions, operands, inputs, ramps, ramp points, result, seed, rand calls
+void ref_expr_info(const void *p, std::uint32_t *out) {
+    const XgenFloatExpressionProgram &g = *program_of(p);
+    out[0] = static_cast<std::uint32_t>(g.instructions.size());
+    out[1] = static_cast<std::uint32_t>(g.operands.size());
+    out[2] = static_cast<std::uint32_t>(g.inputs.size());
+    out[3] = static_cast<std::uint32_t>(g.ramps.size());
+    out[4] = static_cast<std::uint32_t>(g.ramp_points.size());
+    out[5] = g.result;
+    out[6] = g.expression_seed;
+    out[7] = g.random_call_count;
+}
+
+// op, operand offset, operand count, auxiliary; immediate separately.
+void ref_expr_instruction(const void *p, std::uint32_t index, std::uint32_t *out, float *immediate) {
+    const XgenFloatScalarInstruction &in = program_of(p)->instructions.at(index);
+    out[0] = static_cast<std::uint32_t>(in.op);
+    out[1] = in.operand_offset;
+    out[2] = in.operand_count;
+    out[3] = in.auxiliary;
+    *immediate = in.immediate;
+}
+
+std::uint32_t ref_expr_operand(const void *p, std::uint32_t index) { return program_of(p)->operands.at(index); }
+
+void ref_expr_ramp_point(const void *p, std::uint32_t index, float *position, float *value, std::uint32_t *interp) {
+    const XgenFloatRampPoint &rp = program_of(p)->ramp_points.at(index);
+    *position = rp.position;
+    *value = rp.value;
+    *interp = rp.interpolation;
+}
+
+const char *ref_expr_input(const void *p, std::uint32_t index) { return program_of(p)->inputs.at(index).c_str(); }
+
+// evaluate_xgen_scalar_expression_float over `count` rows; inputs is
+// row-major [count x input_count].  ok[i] = 0 where the reference throws.
+void ref_expr_eval_batch(const void *p, const float *inputs, std::uint32_t input_count, std::uint64_t count,
+                         const float *u, const float *v, const float *face_seed, float t,
+                         const std::uint32_t *random_prefix, float *out, std::uint8_t *ok) {
+    const XgenFloatExpressionProgram &g = *program_of(p);
+    std::vector<float> scratch(g.instructions.size());
+    for (std::uint64_t i = 0; i < count; ++i) {
+        XgenExpressionFloatContext context{};
+        context.inputs = std::span<const float>(inputs + i * input_count, input_count);
+        context.u = u ? u[i] : 0.0f;
+        context.v = v ? v[i] : 0.0f;
+        context.face_seed = face_seed ? face_seed[i] : 0.0f;
+        context.t = t;
+        context.random_prefix = random_prefix ? random_prefix[i] : 0u;
+        context.has_random_prefix = random_prefix != nullptr;
+        try {
+            out[i] = evaluate_xgen_scalar_expression_float(g, context, scratch);
+            ok[i] = 1u;
+        } catch (const std::exception &) {
+            out[i] = 0.0f;
+            ok[i] = 0u;
+        }
+    }
+}
+
+std::uint32_t ref_seexpr_hash_finish(std::uint32_t state) { return xgen_seexpr_hash_finish(state); }
+
+std::uint32_t ref_runtime_hash_component(float argument) { return xgen_runtime_hash_component(argument); }
+
+float ref_runtime_hash(const float *arguments, std::uint32_t count) {
+    return xgen_runtime_hash(std::span<const float>(arguments, count));
+}
+
+float ref_runtime_face_seed(std::uint32_t description_id, const char *patch, std::uint32_t face) {
+    return xgen_runtime_face_seed(description_id, patch ? patch : "", face);
+}
+
+std::uint32_t ref_string_seed(const char *text) { return xgen_string_seed(text ? text : ""); }
+
+// xgen_classic_noise_float(p * frequency) for n points (xyz interleaved).
+void ref_classic_noise_batch(const float *xyz, std::uint64_t n, float frequency, float *out) {
+    for (std::uint64_t i = 0; i < n; ++i) {
+        const Vec3 p{xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]};
+        out[i] = xgen_classic_noise_float(p * frequency);
+    }
+}
+
+// compile_xgen_classic_float_runtime_plan for a description whose
+// SplinePrimitive carries the given length / width expressions (either may
+// be NULL).  msg receives the fallback reasons joined by '\n'.
+void *ref_classic_plan(const char *length, const char *width, std::uint32_t description_id,
+                       const char *description_name, char *msg, std::uint64_t cap) {
+    try {
+        ClassicDescription description{};
+        description.name = description_name ? description_name : "description";
+        description.attributes.push_back({"descriptionId", std::to_string(description_id), 0u});
+        ClassicObject primitive{};
+        primitive.type = "SplinePrimitive";
+        if (length) { primitive.attributes.push_back({"length", length, 0u}); }
+        if (width) { primitive.attributes.push_back({"width", width, 0u}); }
+        description.objects.push_back(primitive);
+        auto *plan = new ClassicFloatRuntimePlan(compile_xgen_classic_float_runtime_plan(description, {}));
+        std::string reasons;
+        for (const std::string &r : plan->fallback_reasons) { reasons += r + "\n"; }
+        copy_text(reasons, msg, cap);
+        return plan;
+    } catch (const std::exception &e) {
+        copy_text(e.what(), msg, cap);
+        return nullptr;
+    }
+}
+
+void ref_classic_plan_free(void *plan) { delete static_cast<ClassicFloatRuntimePlan *>(plan); }
+
+// has length, has width, PTEX paths, pref-noise inputs; frequencies out.
+void ref_classic_plan_info(const void *plan, std::uint32_t *out, float *frequencies) {
+    const ClassicFloatRuntimePlan &p = *static_cast<const ClassicFloatRuntimePlan *>(plan);
+    out[0] = p.length.has_value();
+    out[1] = p.width.has_value();
+    out[2] = static_cast<std::uint32_t>(p.ptex_paths.size());
+    out[3] = static_cast<std::uint32_t>(p.pref_noise_inputs.size());
+    for (std::size_t i = 0; i < p.pref_noise_inputs.size(); ++i) { frequencies[i] = p.pref_noise_inputs[i].frequency; }
+}
+
+// The compiled float program of the plan's length (0) or width (1).
+const void *ref_classic_plan_program(const void *plan, std::uint32_t which) {
+    const ClassicFloatRuntimePlan &p = *static_cast<const ClassicFloatRuntimePlan *>(plan);
+    const auto &e = which == 0u ? p.length : p.width;
+    return e ? &e->program : nullptr;
+}
+
+// apply_xgen_classic_float_runtime_plan_cpu on a packed curve set.  points
+// is [S*P] PackedCurvePoint, roots [S] RootSample, root_uvs [S] Vec2 (may be
+// NULL); runtime_inputs is [S x (PTEX + pref-noise)] in the plan's order.
+// The surviving strands are compacted to the front; *kept receives their
+// number.  Returns 0, or 1 with the exception text in msg.
+std::uint32_t ref_classic_apply(const void *plan, float *points, std::uint32_t *counts, void *roots,
+                                float *root_uvs, std::uint32_t strands, std::uint32_t cvs, float radius_scale,
+                                const float *runtime_inputs, std::uint64_t runtime_input_count,
+                                std::uint32_t workers, std::uint32_t *kept, char *msg, std::uint64_t cap) {
+    try {
+        const ClassicFloatRuntimePlan &p = *static_cast<const ClassicFloatRuntimePlan *>(plan);
+        PackedGeneratedCurves curves{};
+        curves.strand_count = strands;
+        curves.cvs_per_strand = cvs;
+        const auto *pts = reinterpret_cast<const PackedCurvePoint *>(points);
+        curves.points.assign(pts, pts + static_cast<std::size_t>(strands) * cvs);
+        curves.point_counts.assign(counts, counts + strands);
+        const auto *rs = static_cast<const RootSample *>(roots);
+        curves.roots.assign(rs, rs + strands);
+        if (root_uvs) {
+            const auto *uv = reinterpret_cast<const Vec2 *>(root_uvs);
+            curves.root_uvs.assign(uv, uv + strands);
+        }
+        NanoXGenContext context(workers == 0u ? 1u : workers);
+        apply_xgen_classic_float_runtime_plan_cpu(
+            curves, p, radius_scale, {}, {}, {}, {},
+            std::span<const float>(runtime_inputs, runtime_inputs ? runtime_input_count : 0u), {}, false,
+            &context);
+        std::memcpy(points, curves.points.data(), curves.points.size() * sizeof(PackedCurvePoint));
+        std::memcpy(counts, curves.point_counts.data(), curves.point_counts.size() * 4u);
+        std::memcpy(roots, curves.roots.data(), curves.roots.size() * sizeof(RootSample));
+        if (root_uvs) { std::memcpy(root_uvs, curves.root_uvs.data(), curves.root_uvs.size() * sizeof(Vec2)); }
+        *kept = curves.strand_count;
+        copy_text("", msg, cap);
+        return 0u;
+    } catch (const std::exception &e) {
+        copy_text(e.what(), msg, cap);
+        return 1u;
+    }
+}
+
+} // extern "C"

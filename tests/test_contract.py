@@ -20,7 +20,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def test_library_exports_every_declared_symbol(nxg_lib):
-    header = open(os.path.join(ROOT, "include", "nxg.h")).read()
+    header = "".join(open(os.path.join(ROOT, "include", name)).read()
+                     for name in sorted(os.listdir(os.path.join(ROOT, "include"))) if name.endswith(".h"))
     declared = set(re.findall(r"^\s*(?:const\s+)?[a-z_0-9]+\s+\*?\s*(nxg_[a-z_0-9]+)\(", header, re.M))
     assert declared, "no declarations parsed"
     assert declared == set(_abi.declared_symbols()), declared ^ set(_abi.declared_symbols())
