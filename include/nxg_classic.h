@@ -133,6 +133,91 @@ uint32_t nxg_generate_packed_classic(const nxg_device_asset_desc *asset, const n
                                      uint32_t first_strand, uint32_t strand_count, void *workspace,
                                      uint64_t workspace_bytes, void *stream);
 
+/* ---------------------------------------------------------------- surrogate */
+
+/* The model is one caller-owned device buffer of nxg_surrogate_model_bytes()
+ * bytes (256-byte aligned): header (input/output normalisation, Adam step),
+ * FP32 parameters, Adam moments and the BF16 weight tiles the kernels copy
+ * into shared memory.  Parameters are the augmented matrices W1a 64x16,
+ * W2a 64x80, W3a 64x80, W4a 16x80 (row-major, concatenated; the bias is the
+ * column after the inputs: 8 for W1a, 64 for the others; W4a rows 0-1 are
+ * the length and width outputs). */
+#define NXG_SURROGATE_INPUTS 8u        /* rest position xyz, normal xyz, u, v */
+#define NXG_SURROGATE_HIDDEN 64u
+#define NXG_SURROGATE_PARAMETERS 12544u
+
+typedef struct nxg_surrogate_config {
+    float input_offset[NXG_SURROGATE_INPUTS]; /* the network sees (feature - offset) * scale */
+    float input_scale[NXG_SURROGATE_INPUTS];
+    uint32_t seed;                            /* initial weights */
+    uint32_t reserved;
+} nxg_surrogate_config;
+
+typedef struct nxg_surrogate_train_config {
+    uint32_t epochs;
+    uint32_t batch;          /* samples per Adam step, a multiple of 128 */
+    float learning_rate;
+    float lr_decay;          /* learning-rate factor per epoch (0 = 1) */
+    float beta1, beta2, epsilon; /* Adam (0 = 0.9, 0.999, 1e-8) */
+    uint32_t seed;           /* sample order */
+} nxg_surrogate_train_config;
+
+/* Per-batch judge.  A batch is one 128-root tile: `checks_per_batch` of its
+ * roots are evaluated by the exact runtime and, if any relative error
+ * exceeds its tolerance (or the exact runtime fails there), every root of
+ * the tile is re-run exactly.  mode 0 = checked surrogate, 1 = exact
+ * runtime only, 2 = surrogate without checks. */
+typedef struct nxg_surrogate_check {
+    float length_tolerance;
+    float width_tolerance;
+    uint32_t checks_per_batch; /* 0..128 */
+    uint32_t mode;
+} nxg_surrogate_check;
+
+uint64_t nxg_surrogate_model_bytes(void);
+uint64_t nxg_surrogate_workspace_bytes(void);
+
+/* Header, He-uniform weights, zero Adam state; synchronises `stream`. */
+uint32_t nxg_surrogate_init(void *model, const nxg_surrogate_config *config, void *stream);
+
+/* Raw features of strands [first, first + count): count x 8 floats. */
+uint32_t nxg_surrogate_features(const nxg_device_asset_desc *asset, const nxg_generation_params *params,
+                                uint32_t first_strand, uint32_t count, float *features, void *stream);
+
+/* Output normalisation from training targets (count x 2: length, width). */
+uint32_t nxg_surrogate_fit_outputs(void *model, const float *targets, uint32_t count, void *stream);
+
+/* Mini-batch Adam on the squared error of the normalised outputs, forward,
+ * backward and weight gradients on the tensor cores.  loss_history (device,
+ * `epochs` floats, optional) receives per epoch the sum over its steps of
+ * the step's mean loss.  A set-up call: synchronises `stream`. */
+uint32_t nxg_surrogate_train(void *model, const float *features, const float *targets, uint32_t count,
+                             const nxg_surrogate_train_config *config, void *workspace, uint64_t workspace_bytes,
+                             float *loss_history, void *stream);
+
+/* Gradient of the mean loss over all `count` samples with respect to every
+ * parameter (NXG_SURROGATE_PARAMETERS floats, device) and the loss itself;
+ * the same kernels as training, without the update. */
+uint32_t nxg_surrogate_gradients(const void *model, const float *features, const float *targets, uint32_t count,
+                                 float *gradients, float *loss, void *stream);
+
+/* Network outputs (length, width) for raw features (count x 2 floats). */
+uint32_t nxg_surrogate_forward(const void *model, const float *features, uint32_t count, float *outputs,
+                               void *stream);
+
+/* Per-root (length scale, width) of strands [first, first + count) by the
+ * surrogate, judged per batch by the exact runtime of `plan`.
+ * device_status (4 x uint32, zeroed by the caller): [0] error code, [1]
+ * roots whose exact evaluation failed, [2] batches re-run exactly, [3]
+ * batches checked. */
+uint32_t nxg_surrogate_root_scalars(const void *model, const nxg_device_asset_desc *asset,
+                                    const nxg_generation_params *params, const nxg_classic_scalar_plan *plan,
+                                    const nxg_surrogate_check *check, uint32_t first_strand, uint32_t count,
+                                    float *scalars, uint32_t *device_status, void *stream);
+
+/* Device address of the FP32 parameter array inside the model. */
+uint32_t nxg_surrogate_parameters(void *model, float **parameters);
+
 #ifdef __cplusplus
 }
 #endif

@@ -181,6 +181,30 @@ class ClassicApplyDesc(ctypes.Structure):
                 ("apply_width", ctypes.c_uint32)]
 
 
+SURROGATE_INPUTS = 8
+SURROGATE_PARAMETERS = 12544
+
+
+class SurrogateConfig(ctypes.Structure):
+    """nxg_surrogate_config (nxg_classic.h)."""
+    _fields_ = [("input_offset", ctypes.c_float * SURROGATE_INPUTS),
+                ("input_scale", ctypes.c_float * SURROGATE_INPUTS), ("seed", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32)]
+
+
+class SurrogateTrainConfig(ctypes.Structure):
+    """nxg_surrogate_train_config (nxg_classic.h)."""
+    _fields_ = [("epochs", ctypes.c_uint32), ("batch", ctypes.c_uint32), ("learning_rate", ctypes.c_float),
+                ("lr_decay", ctypes.c_float), ("beta1", ctypes.c_float), ("beta2", ctypes.c_float),
+                ("epsilon", ctypes.c_float), ("seed", ctypes.c_uint32)]
+
+
+class SurrogateCheck(ctypes.Structure):
+    """nxg_surrogate_check (nxg_classic.h)."""
+    _fields_ = [("length_tolerance", ctypes.c_float), ("width_tolerance", ctypes.c_float),
+                ("checks_per_batch", ctypes.c_uint32), ("mode", ctypes.c_uint32)]
+
+
 class AssetBuildInput(ctypes.Structure):
     """nxg_asset_build_input: the flattened AssetBuildInput of asset.h:14-44."""
     _fields_ = [
@@ -327,6 +351,21 @@ _SIGNATURES = {
                                                       ctypes.POINTER(PackedOutputDesc),
                                                       ctypes.POINTER(ClassicApplyDesc), ctypes.POINTER(LaunchConfig),
                                                       ctypes.c_uint32, ctypes.c_uint32, _P, ctypes.c_uint64, _P]),
+    "nxg_surrogate_model_bytes": (ctypes.c_uint64, []),
+    "nxg_surrogate_workspace_bytes": (ctypes.c_uint64, []),
+    "nxg_surrogate_init": (ctypes.c_uint32, [_P, ctypes.POINTER(SurrogateConfig), _P]),
+    "nxg_surrogate_features": (ctypes.c_uint32, [ctypes.POINTER(DeviceAssetDesc), ctypes.POINTER(GenerationParams),
+                                                 ctypes.c_uint32, ctypes.c_uint32, _P, _P]),
+    "nxg_surrogate_fit_outputs": (ctypes.c_uint32, [_P, _P, ctypes.c_uint32, _P]),
+    "nxg_surrogate_train": (ctypes.c_uint32, [_P, _P, _P, ctypes.c_uint32, ctypes.POINTER(SurrogateTrainConfig), _P,
+                                              ctypes.c_uint64, _P, _P]),
+    "nxg_surrogate_gradients": (ctypes.c_uint32, [_P, _P, _P, ctypes.c_uint32, _P, _P, _P]),
+    "nxg_surrogate_forward": (ctypes.c_uint32, [_P, _P, ctypes.c_uint32, _P, _P]),
+    "nxg_surrogate_root_scalars": (ctypes.c_uint32, [_P, ctypes.POINTER(DeviceAssetDesc),
+                                                     ctypes.POINTER(GenerationParams),
+                                                     ctypes.POINTER(ClassicScalarPlan), ctypes.POINTER(SurrogateCheck),
+                                                     ctypes.c_uint32, ctypes.c_uint32, _P, _P, _P]),
+    "nxg_surrogate_parameters": (ctypes.c_uint32, [_P, ctypes.POINTER(ctypes.c_void_p)]),
 }
 
 

@@ -1,0 +1,937 @@
+// surrogate.cu -- the learned per-root scalar surrogate (no reference
+// counterpart): a 3 x 64 ReLU MLP from a root's rest position, normal and
+// uv to its Classic (length scale, width), run on the tcgen05 tensor cores.
+//
+// Network (augmented weights, bias folded into the product):
+//   x  = [ (features - offset) * scale, 1, 0 x 7 ]          16 columns
+//   h1 = relu(W1a x),  W1a 64 x 16   (column 8 = bias)
+//   h2 = relu(W2a [h1, 1, 0..]),  W2a 64 x 80 (column 64 = bias)
+//   h3 = relu(W3a [h2, 1, 0..]),  W3a 64 x 80
+//   y  = W4a [h3, 1, 0..],  W4a 16 x 80 (rows 0-1 used)
+//   (length, width) = y * output_scale + output_offset
+// Weights and activations are BF16, every product accumulates in FP32 in
+// TMEM.  A CTA of 128 threads owns one 128-row tile: thread r is row r and
+// TMEM lane r.
+//
+// Training computes forward, backward and weight gradients on the tensor
+// cores: dH_{l-1} = dZ_l W_l reads the weight tile as an MN-major operand,
+// and dW_l = dZ_l^T [H_{l-1}, 1] reads the activation and gradient tiles as
+// MN-major operands (the ones column yields the bias gradient).  dW_l
+// accumulates in TMEM across the tiles a CTA processes and is added to the
+// global gradient once per step.
+#include "classic_eval.cuh"
+#include "expression.h"
+#include "generator_core.cuh"
+#include "nxg_classic.h"
+#include "nxg_internal.h"
+#include "strand_math.cuh"
+#include "umma.cuh"
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstddef>
+#include <cstdint>
+
+namespace nxg {
+namespace surrogate {
+
+constexpr uint32_t kRows = 128;      // tile rows = MMA M = threads per CTA
+constexpr uint32_t kIn = 8;          // features
+constexpr uint32_t kK1 = 16;         // layer-1 K (features, bias one, padding)
+constexpr uint32_t kHidden = 64;
+constexpr uint32_t kKh = 80;         // hidden K (64 activations, bias one, padding)
+constexpr uint32_t kOutRows = 16;    // output rows of W4a (2 used)
+
+// Parameter (and gradient, and image element) offsets: W1a | W2a | W3a | W4a.
+constexpr uint32_t kP1 = 0, kP2 = kP1 + kHidden * kK1, kP3 = kP2 + kHidden * kKh, kP4 = kP3 + kHidden * kKh;
+constexpr uint32_t kParams = kP4 + kOutRows * kKh;
+static_assert(kParams == NXG_SURROGATE_PARAMETERS, "parameter count");
+
+// Image bytes (bf16 tiles in the UMMA layout), contiguous in the model and
+// copied as one block into shared memory.
+constexpr uint32_t kImg1 = 0, kImg2 = kImg1 + kHidden * kK1 * 2, kImg3 = kImg2 + kHidden * kKh * 2,
+                   kImg4 = kImg3 + kHidden * kKh * 2, kImgBytes = kImg4 + kOutRows * kKh * 2;
+
+constexpr uint32_t kMagic = 0x5347584eu;  // "NXGS"
+
+struct Header {
+    uint32_t magic, version, parameters, step;
+    float input_offset[kIn];
+    float input_scale[kIn];
+    float output_offset[2];
+    float output_scale[2];
+    uint32_t initialised, trained;
+    uint32_t reserved[38];
+};
+static_assert(sizeof(Header) == 256, "model header");
+
+constexpr uint64_t kHeaderBytes = 256, kParamBytes = uint64_t{kParams} * 4;
+constexpr uint64_t kOffParams = kHeaderBytes, kOffM = kOffParams + kParamBytes, kOffV = kOffM + kParamBytes,
+                   kOffImages = kOffV + kParamBytes, kModelBytes = kOffImages + kImgBytes;
+static_assert(kOffImages % 16 == 0, "images are copied in 16-byte units");
+
+// Layer geometry of a parameter index: (image rows, K, row, column, image byte offset).
+__host__ __device__ inline void param_place(uint32_t i, uint32_t *rows, uint32_t *k, uint32_t *row, uint32_t *col,
+                                            uint32_t *base) {
+    if (i < kP2) {
+        *rows = kHidden; *k = kK1; *base = kImg1; i -= kP1;
+    } else if (i < kP3) {
+        *rows = kHidden; *k = kKh; *base = kImg2; i -= kP2;
+    } else if (i < kP4) {
+        *rows = kHidden; *k = kKh; *base = kImg3; i -= kP3;
+    } else {
+        *rows = kOutRows; *k = kKh; *base = kImg4; i -= kP4;
+    }
+    *row = i / *k;
+    *col = i % *k;
+}
+
+// Parameters that exist in the network (the rest stay zero).
+__host__ __device__ inline bool param_used(uint32_t i) {
+    uint32_t rows, k, row, col, base;
+    param_place(i, &rows, &k, &row, &col, &base);
+    if (k == kK1) { return col <= kIn; }
+    return col <= kHidden && (rows == kHidden || row < 2u);
+}
+
+__device__ inline uint32_t image_offset(uint32_t i) {
+    uint32_t rows, k, row, col, base;
+    param_place(i, &rows, &k, &row, &col, &base);
+    return base + umma::tile_offset(row, col, rows);
+}
+
+__device__ inline float uniform_hash(uint32_t seed, uint32_t i) {
+    return __uint2float_rn(dev::hash32(seed ^ dev::hash32(i + 0x9e3779b9u)) >> 8) * (1.0f / 16777216.0f);
+}
+
+// ------------------------------------------------------------ small kernels
+
+__global__ void init_kernel(unsigned char *model, uint32_t seed) {
+    float *params = reinterpret_cast<float *>(model + kOffParams);
+    float *m = reinterpret_cast<float *>(model + kOffM);
+    float *v = reinterpret_cast<float *>(model + kOffV);
+    __nv_bfloat16 *img = reinterpret_cast<__nv_bfloat16 *>(model + kOffImages);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < kParams; i += gridDim.x * blockDim.x) {
+        uint32_t rows, k, row, col, base;
+        param_place(i, &rows, &k, &row, &col, &base);
+        float w = 0.0f;
+        const bool bias = (k == kK1 && col == kIn) || (k == kKh && col == kHidden);
+        if (param_used(i) && !bias) {  // He-uniform on fan-in; the output layer half as wide
+            const float fan_in = k == kK1 ? static_cast<float>(kIn) : static_cast<float>(kHidden);
+            const float bound = sqrtf(6.0f / fan_in) * (rows == kOutRows ? 0.5f : 1.0f);
+            w = (2.0f * uniform_hash(seed, i) - 1.0f) * bound;
+        }
+        params[i] = w;
+        m[i] = 0.0f;
+        v[i] = 0.0f;
+        img[image_offset(i) / 2] = __float2bfloat16_rn(w);
+    }
+}
+
+// Mean and standard deviation of the two target columns (one block).
+__global__ void output_stats_kernel(unsigned char *model, const float *targets, uint32_t count) {
+    __shared__ double sums[4][256];
+    double s0 = 0, s1 = 0, q0 = 0, q1 = 0;
+    for (uint32_t i = threadIdx.x; i < count; i += blockDim.x) {
+        const double a = targets[2 * i], b = targets[2 * i + 1];
+        s0 += a;
+        s1 += b;
+        q0 += a * a;
+        q1 += b * b;
+    }
+    sums[0][threadIdx.x] = s0;
+    sums[1][threadIdx.x] = s1;
+    sums[2][threadIdx.x] = q0;
+    sums[3][threadIdx.x] = q1;
+    __syncthreads();
+    for (uint32_t s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) {
+            for (int j = 0; j < 4; ++j) { sums[j][threadIdx.x] += sums[j][threadIdx.x + s]; }
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        Header *h = reinterpret_cast<Header *>(model);
+        for (int j = 0; j < 2; ++j) {
+            const double mean = sums[j][0] / count;
+            const double var = fmax(sums[2 + j][0] / count - mean * mean, 0.0);
+            const double sd = sqrt(var);
+            h->output_offset[j] = static_cast<float>(mean);
+            h->output_scale[j] = static_cast<float>(sd > 1e-12 * fmax(fabs(mean), 1e-30) ? sd : 1.0);
+        }
+    }
+}
+
+// Raw features of strands [first, first + count): rest position, normal, uv.
+__global__ void features_kernel(dev::AssetArgs a, dev::FrameArgs f, uint32_t seed, uint32_t first, uint32_t count,
+                                float *features) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        const dev::Root r = dev::sample_root(a, f, seed, first + i);
+        float *out = features + 8ull * i;
+        out[0] = r.position.x;
+        out[1] = r.position.y;
+        out[2] = r.position.z;
+        out[3] = r.normal.x;
+        out[4] = r.normal.y;
+        out[5] = r.normal.z;
+        out[6] = r.u;
+        out[7] = r.v;
+    }
+}
+
+// One Adam step over every parameter, then the parameter's BF16 image
+// element; the gradient is cleared for the next step.
+__global__ void adam_kernel(unsigned char *model, float *grad, float lr_t, float beta1, float beta2, float epsilon) {
+    float *params = reinterpret_cast<float *>(model + kOffParams);
+    float *m = reinterpret_cast<float *>(model + kOffM);
+    float *v = reinterpret_cast<float *>(model + kOffV);
+    __nv_bfloat16 *img = reinterpret_cast<__nv_bfloat16 *>(model + kOffImages);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < kParams; i += gridDim.x * blockDim.x) {
+        const float g = grad[i];
+        grad[i] = 0.0f;
+        if (!param_used(i)) { continue; }
+        const float mi = beta1 * m[i] + (1.0f - beta1) * g;
+        const float vi = beta2 * v[i] + (1.0f - beta2) * g * g;
+        m[i] = mi;
+        v[i] = vi;
+        const float p = params[i] - lr_t * mi / (sqrtf(vi) + epsilon);
+        params[i] = p;
+        img[image_offset(i) / 2] = __float2bfloat16_rn(p);
+    }
+}
+
+// ---------------------------------------------------------- tile helpers
+
+__device__ inline uint32_t pack2(float a, float b) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<const uint32_t *>(&h);
+}
+
+// Normalised features of one row into the input tile: 8 features, the bias
+// one, zeros.
+__device__ inline void store_input_row(__nv_bfloat16 *x, uint32_t r, const float *raw, const Header &h, bool active) {
+    float f[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) { f[j] = active ? (raw[j] - h.input_offset[j]) * h.input_scale[j] : 0.0f; }
+    const uint4 lo = make_uint4(pack2(f[0], f[1]), pack2(f[2], f[3]), pack2(f[4], f[5]), pack2(f[6], f[7]));
+    const uint4 hi = make_uint4(pack2(active ? 1.0f : 0.0f, 0.0f), 0u, 0u, 0u);
+    unsigned char *base = reinterpret_cast<unsigned char *>(x);
+    *reinterpret_cast<uint4 *>(base + umma::tile_offset(r, 0, kRows)) = lo;
+    *reinterpret_cast<uint4 *>(base + umma::tile_offset(r, 8, kRows)) = hi;
+}
+
+// Constant columns 64..79 of an activation tile: the bias one and zeros.
+__device__ inline void store_bias_columns(__nv_bfloat16 *t, uint32_t r) {
+    unsigned char *base = reinterpret_cast<unsigned char *>(t);
+    *reinterpret_cast<uint4 *>(base + umma::tile_offset(r, 64, kRows)) = make_uint4(pack2(1.0f, 0.0f), 0u, 0u, 0u);
+    *reinterpret_cast<uint4 *>(base + umma::tile_offset(r, 72, kRows)) = make_uint4(0u, 0u, 0u, 0u);
+}
+
+// Row r of TMEM columns [col, col + 64) -> relu -> BF16 columns 0..63 of t.
+__device__ inline void relu_epilogue(uint32_t tmem_row, uint32_t col, __nv_bfloat16 *t, uint32_t r) {
+    unsigned char *base = reinterpret_cast<unsigned char *>(t);
+#pragma unroll
+    for (uint32_t q = 0; q < 4; ++q) {
+        float v[16];
+        umma::load16(tmem_row + col + 16u * q, v);
+#pragma unroll
+        for (uint32_t c = 0; c < 2; ++c) {
+            const float *w = v + 8 * c;
+            const uint4 packed = make_uint4(pack2(fmaxf(w[0], 0.0f), fmaxf(w[1], 0.0f)),
+                                            pack2(fmaxf(w[2], 0.0f), fmaxf(w[3], 0.0f)),
+                                            pack2(fmaxf(w[4], 0.0f), fmaxf(w[5], 0.0f)),
+                                            pack2(fmaxf(w[6], 0.0f), fmaxf(w[7], 0.0f)));
+            *reinterpret_cast<uint4 *>(base + umma::tile_offset(r, 16u * q + 8u * c, kRows)) = packed;
+        }
+    }
+}
+
+// dZ = dH * (h > 0): TMEM row of dH, activation tile h, into gradient tile dz.
+__device__ inline void relu_backward(uint32_t tmem_row, uint32_t col, const __nv_bfloat16 *h, __nv_bfloat16 *dz,
+                                     uint32_t r) {
+    const unsigned char *hb = reinterpret_cast<const unsigned char *>(h);
+    unsigned char *db = reinterpret_cast<unsigned char *>(dz);
+#pragma unroll
+    for (uint32_t q = 0; q < 4; ++q) {
+        float v[16];
+        umma::load16(tmem_row + col + 16u * q, v);
+#pragma unroll
+        for (uint32_t c = 0; c < 2; ++c) {
+            const uint32_t k = 16u * q + 8u * c;
+            const uint4 hv = *reinterpret_cast<const uint4 *>(hb + umma::tile_offset(r, k, kRows));
+            const uint32_t hw[4] = {hv.x, hv.y, hv.z, hv.w};
+            uint32_t out[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const __nv_bfloat162 pair = *reinterpret_cast<const __nv_bfloat162 *>(&hw[e]);
+                const float a = __bfloat162float(pair.x) > 0.0f ? v[8 * c + 2 * e] : 0.0f;
+                const float b = __bfloat162float(pair.y) > 0.0f ? v[8 * c + 2 * e + 1] : 0.0f;
+                out[e] = pack2(a, b);
+            }
+            *reinterpret_cast<uint4 *>(db + umma::tile_offset(r, k, kRows)) = make_uint4(out[0], out[1], out[2], out[3]);
+        }
+    }
+}
+
+// Issue the four forward products of one tile (layer `layer`, 1-based) into
+// TMEM column `col`.
+__device__ inline void issue_forward(uint32_t layer, uint32_t d, uint32_t x, uint32_t h, uint32_t img) {
+    if (layer == 1) {
+        umma::mma(d, umma::kmajor(x, kRows, 0), umma::kmajor(img + kImg1, kHidden, 0),
+                  umma::instr_bf16(kRows, kHidden, false, false), 0u);
+        return;
+    }
+    const uint32_t w = layer == 2 ? img + kImg2 : (layer == 3 ? img + kImg3 : img + kImg4);
+    const uint32_t rows = layer == 4 ? kOutRows : kHidden;
+    const uint32_t instr = umma::instr_bf16(kRows, rows, false, false);
+#pragma unroll
+    for (uint32_t s = 0; s < kKh / 16; ++s) {
+        umma::mma(d, umma::kmajor(h, kRows, s), umma::kmajor(w, rows, s), instr, s > 0 ? 1u : 0u);
+    }
+}
+
+// Bounded wait on the tile barrier, uniform across the CTA: false when any
+// thread's wait ran out.
+__device__ inline bool wait_round(uint64_t *bar, uint32_t &phase) {
+    const bool ok = __syncthreads_and(umma::mbar_wait(bar, phase)) != 0;
+    if (ok) { phase ^= 1u; }  // on a timeout the final drain waits on the same phase
+    umma::fence_after_sync();
+    return ok;
+}
+
+// Hand the operands written by every thread to the tensor cores.
+__device__ inline void publish_operands() {
+    umma::fence_before_sync();
+    umma::fence_shared_to_async();
+    __syncthreads();
+}
+
+// -------------------------------------------------------------- inference
+
+struct InferArgs {
+    const unsigned char *model;
+    const float *features;   // features mode: [count x 8], else nullptr
+    float2 *out;
+    uint32_t count;
+    uint32_t *status;        // [error, failing roots, fallback tiles, checked tiles]
+    // roots mode
+    dev::AssetArgs a;
+    dev::FrameArgs f;
+    uint32_t seed, first;
+    float description_id, patch_seed;
+    float length_tolerance, width_tolerance;
+    uint32_t checks, mode;   // checks per tile; mode 0 checked, 1 exact, 2 unchecked
+    DeviceExpression length;
+    DeviceExpression width;
+};
+
+// Shared memory ends with a guard band as large as the furthest any operand
+// descriptor of the last tile could reach with its two byte offsets
+// exchanged, so every product stays inside the CTA's allocation.
+constexpr uint32_t kGuardBytes = 32768;
+constexpr uint32_t kInferSmem = kImgBytes + kRows * kK1 * 2 + kRows * kKh * 2 + 256 * 16 + 256 + 64 + kGuardBytes;
+constexpr uint32_t kInferTmemColumns = 64;
+
+template <bool ROOTS>
+__global__ void __launch_bounds__(kRows) infer_kernel(const __grid_constant__ InferArgs k) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    unsigned char *images = smem;
+    auto *x = reinterpret_cast<__nv_bfloat16 *>(smem + kImgBytes);
+    auto *h = reinterpret_cast<__nv_bfloat16 *>(smem + kImgBytes + kRows * kK1 * 2);
+    auto *table = reinterpret_cast<float4 *>(smem + kImgBytes + kRows * kK1 * 2 + kRows * kKh * 2);
+    auto *perm = reinterpret_cast<uint8_t *>(table + 256);
+    auto *bar = reinterpret_cast<uint64_t *>(perm + 256);
+    auto *tmem_slot = reinterpret_cast<uint32_t *>(bar + 1);
+    auto *fail_flag = tmem_slot + 1;
+    const uint32_t r = threadIdx.x;
+    const Header &hd = *reinterpret_cast<const Header *>(k.model);
+
+    // Weight images (one block copy), constant columns, exact-check tables.
+    const uint4 *src = reinterpret_cast<const uint4 *>(k.model + kOffImages);
+    for (uint32_t i = r; i < kImgBytes / 16; i += kRows) { reinterpret_cast<uint4 *>(images)[i] = src[i]; }
+    store_bias_columns(h, r);
+    if constexpr (ROOTS) { dev::stage_classic_tables(table, perm); }
+    if (r == 0) { umma::mbar_init(bar, 1); }
+    if (r < 32) { umma::tmem_alloc(tmem_slot, kInferTmemColumns); }
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t tmem = *tmem_slot;
+    const uint32_t lane_base = tmem + ((32u * (r >> 5)) << 16);
+    const uint32_t sx = umma::smem_address(x), sh = umma::smem_address(h), simg = umma::smem_address(images);
+    const bool random = k.length.uses_random || k.width.uses_random;
+    uint32_t phase = 0;
+    bool healthy = true;
+    const uint32_t tiles = (k.count + kRows - 1) / kRows;
+    for (uint32_t t = blockIdx.x; t < tiles && healthy; t += gridDim.x) {
+        const uint32_t row = t * kRows + r;
+        const bool active = row < k.count;
+        dev::Root root{};
+        float raw[8];
+        if constexpr (ROOTS) {
+            if (active) { root = dev::sample_root(k.a, k.f, k.seed, k.first + row); }
+            raw[0] = root.position.x; raw[1] = root.position.y; raw[2] = root.position.z;
+            raw[3] = root.normal.x; raw[4] = root.normal.y; raw[5] = root.normal.z;
+            raw[6] = root.u; raw[7] = root.v;
+        } else {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) { raw[j] = active ? k.features[8ull * row + j] : 0.0f; }
+        }
+        float y0 = 0.0f, y1 = 0.0f;
+        if (!ROOTS || k.mode != 1u) {
+            store_input_row(x, r, raw, hd, active);
+            for (uint32_t layer = 1; layer <= 4 && healthy; ++layer) {
+                publish_operands();
+                if (r == 0) {
+                    umma::fence_after_sync();
+                    issue_forward(layer, tmem, sx, sh, simg);
+                    umma::commit(bar);
+                }
+                healthy = wait_round(bar, phase);
+                if (!healthy) { break; }
+                if (layer < 4) {
+                    relu_epilogue(lane_base, 0, h, r);
+                } else {
+                    umma::load2(lane_base, y0, y1);
+                }
+            }
+            if (!healthy) { break; }
+            y0 = y0 * hd.output_scale[0] + hd.output_offset[0];
+            y1 = y1 * hd.output_scale[1] + hd.output_offset[1];
+        }
+        if constexpr (ROOTS) {
+            // Spot check: `checks` rows of the tile against the exact runtime;
+            // any miss, or exact mode, re-runs the whole tile exactly.
+            bool exact_tile = k.mode == 1u;
+            if (!exact_tile && k.mode == 0u && k.checks > 0u) {
+                if (r == 0) { *fail_flag = 0u; }
+                __syncthreads();
+                const uint32_t stride = kRows / k.checks;
+                const uint32_t pick = dev::hash32(t * 0x9e3779b9u + k.seed) % stride;
+                if (active && r % stride == pick && r / stride < k.checks) {
+                    const float fs = random ? dev::classic_face_seed(k.description_id, k.patch_seed, root.triangle, perm)
+                                            : 0.0f;
+                    float el, ew;
+                    const bool ok = dev::classic_root_scalars(k.length, k.width, table, perm, root, k.first + row, fs,
+                                                              &el, &ew);
+                    const bool miss = !ok || !(fabsf(y0 - el) <= k.length_tolerance * fabsf(el)) ||
+                                      !(fabsf(y1 - ew) <= k.width_tolerance * fabsf(ew));
+                    if (miss) { atomicOr(fail_flag, 1u); }
+                }
+                __syncthreads();
+                exact_tile = *fail_flag != 0u;
+                if (r == 0) { atomicAdd(k.status + 3, 1u); }
+            }
+            if (exact_tile) {
+                if (active) {
+                    const float fs = random ? dev::classic_face_seed(k.description_id, k.patch_seed, root.triangle, perm)
+                                            : 0.0f;
+                    if (!dev::classic_root_scalars(k.length, k.width, table, perm, root, k.first + row, fs, &y0, &y1)) {
+                        atomicCAS(k.status, 0u, static_cast<uint32_t>(NXG_ERROR_EXPRESSION_DOMAIN));
+                        atomicAdd(k.status + 1, 1u);
+                    }
+                }
+                if (r == 0 && k.mode == 0u) { atomicAdd(k.status + 2, 1u); }
+            }
+        }
+        if (active) { k.out[row] = make_float2(y0, y1); }
+    }
+    if (!healthy && r == 0) { atomicCAS(k.status, 0u, static_cast<uint32_t>(NXG_ERROR_SURROGATE)); }
+    if (!healthy) { umma::mbar_wait(bar, phase); }  // let a product still in flight land
+    umma::fence_before_sync();
+    __syncthreads();
+    if (r < 32) {
+        umma::fence_after_sync();
+        umma::tmem_free(tmem, kInferTmemColumns);
+    }
+}
+
+// --------------------------------------------------------------- training
+
+struct TrainArgs {
+    const unsigned char *model;
+    const float *features;   // [count x 8]
+    const float *targets;    // [count x 2]
+    uint32_t count;          // samples in the set
+    uint32_t begin, length;  // positions [begin, begin + length) of this step
+    uint32_t multiplier, shift;  // sample = (position * multiplier + shift) % count
+    float inv_batch;         // 1 / samples in the step
+    float *grad;             // [kParams], accumulated with atomics
+    float *loss;             // += mean squared error of the step
+    uint32_t *status;
+};
+
+constexpr uint32_t kTrainSmem = kImgBytes + kRows * kK1 * 2 + 3 * kRows * kKh * 2 + 2 * kRows * kRows * 2 + 64 + kGuardBytes;
+static_assert(kTrainSmem <= 227u * 1024u, "training tiles fit one CTA");
+constexpr uint32_t kTrainTmemColumns = 512;
+// TMEM columns: working product | dW1 | dW2 | dW3 | dW4
+constexpr uint32_t kColWork = 0, kColW1 = 64, kColW2 = 96, kColW3 = 192, kColW4 = 288;
+
+__device__ inline void zero_tile(__nv_bfloat16 *t, uint32_t bytes) {
+    for (uint32_t i = threadIdx.x; i < bytes / 16; i += blockDim.x) {
+        reinterpret_cast<uint4 *>(t)[i] = make_uint4(0u, 0u, 0u, 0u);
+    }
+}
+
+// Adds rows [0, rows) x columns [0, k) of the TMEM accumulator at `col` to
+// the gradient at `offset` (row-major rows x k).  Warps 0-1 hold lanes 0-63.
+__device__ inline void flush_gradient(uint32_t lane_base, uint32_t col, uint32_t rows, uint32_t k, float *grad,
+                                      uint32_t offset) {
+    const uint32_t r = threadIdx.x;
+    if (r >= 64) { return; }
+    for (uint32_t q = 0; q < k / 16; ++q) {
+        float v[16];
+        umma::load16(lane_base + col + 16u * q, v);
+        if (r < rows) {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) { atomicAdd(grad + offset + r * k + 16u * q + j, v[j]); }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kRows, 1) train_kernel(const __grid_constant__ TrainArgs k) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    unsigned char *images = smem;
+    auto *x = reinterpret_cast<__nv_bfloat16 *>(smem + kImgBytes);
+    auto *h1 = reinterpret_cast<__nv_bfloat16 *>(smem + kImgBytes + kRows * kK1 * 2);
+    auto *h2 = h1 + kRows * kKh;
+    auto *h3 = h2 + kRows * kKh;
+    auto *dza = h3 + kRows * kKh;           // 128 x 128 gradient tiles (columns 64+ stay zero)
+    auto *dzb = dza + kRows * kRows;
+    auto *bar = reinterpret_cast<uint64_t *>(dzb + kRows * kRows);
+    auto *tmem_slot = reinterpret_cast<uint32_t *>(bar + 1);
+    auto *loss_slot = reinterpret_cast<float *>(tmem_slot + 1);
+    const uint32_t r = threadIdx.x;
+    const Header &hd = *reinterpret_cast<const Header *>(k.model);
+
+    const uint4 *src = reinterpret_cast<const uint4 *>(k.model + kOffImages);
+    for (uint32_t i = r; i < kImgBytes / 16; i += kRows) { reinterpret_cast<uint4 *>(images)[i] = src[i]; }
+    zero_tile(dza, kRows * kRows * 2);
+    zero_tile(dzb, kRows * kRows * 2);
+    store_bias_columns(h1, r);
+    store_bias_columns(h2, r);
+    store_bias_columns(h3, r);
+    if (r == 0) {
+        umma::mbar_init(bar, 1);
+        *loss_slot = 0.0f;
+    }
+    if (r < 32) { umma::tmem_alloc(tmem_slot, kTrainTmemColumns); }
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t tmem = *tmem_slot;
+    const uint32_t lane_base = tmem + ((32u * (r >> 5)) << 16);
+    const uint32_t sx = umma::smem_address(x), simg = umma::smem_address(images);
+    const uint32_t sh[4] = {sx, umma::smem_address(h1), umma::smem_address(h2), umma::smem_address(h3)};
+    __nv_bfloat16 *hs[4] = {x, h1, h2, h3};
+    const uint32_t sdz[2] = {umma::smem_address(dza), umma::smem_address(dzb)};
+    __nv_bfloat16 *dzs[2] = {dza, dzb};
+    const uint32_t img_layer[5] = {0, kImg1, kImg2, kImg3, kImg4};
+    const uint32_t col_dw[5] = {0, kColW1, kColW2, kColW3, kColW4};
+    uint32_t phase = 0;
+    bool healthy = true;
+    bool first_tile = true;
+    float my_loss = 0.0f;
+    const uint32_t tiles = (k.length + kRows - 1) / kRows;
+    for (uint32_t t = blockIdx.x; t < tiles && healthy; t += gridDim.x) {
+        const uint32_t position = k.begin + t * kRows + r;
+        const bool active = t * kRows + r < k.length;
+        const uint32_t sample =
+            active ? static_cast<uint32_t>((uint64_t{position} * k.multiplier + k.shift) % k.count) : 0u;
+        float raw[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) { raw[j] = active ? k.features[8ull * sample + j] : 0.0f; }
+        store_input_row(x, r, raw, hd, active);
+        // Forward: h1, h2, h3 kept for the backward pass.
+        float y0 = 0.0f, y1 = 0.0f;
+        for (uint32_t layer = 1; layer <= 4 && healthy; ++layer) {
+            publish_operands();
+            if (r == 0) {
+                umma::fence_after_sync();
+                issue_forward(layer, tmem + kColWork, sx, sh[layer - 1], simg);
+                umma::commit(bar);
+            }
+            healthy = wait_round(bar, phase);
+            if (!healthy) { break; }
+            if (layer < 4) {
+                relu_epilogue(lane_base, kColWork, hs[layer], r);
+            } else {
+                umma::load2(lane_base + kColWork, y0, y1);
+            }
+        }
+        if (!healthy) { break; }
+        // Loss gradient on the normalised outputs.
+        float g0 = 0.0f, g1 = 0.0f;
+        if (active) {
+            const float t0 = (k.targets[2ull * sample] - hd.output_offset[0]) / hd.output_scale[0];
+            const float t1 = (k.targets[2ull * sample + 1] - hd.output_offset[1]) / hd.output_scale[1];
+            g0 = 2.0f * (y0 - t0) * k.inv_batch;
+            g1 = 2.0f * (y1 - t1) * k.inv_batch;
+            my_loss += ((y0 - t0) * (y0 - t0) + (y1 - t1) * (y1 - t1)) * k.inv_batch;
+        }
+        {
+            unsigned char *db = reinterpret_cast<unsigned char *>(dza);
+            *reinterpret_cast<uint4 *>(db + umma::tile_offset(r, 0, kRows)) = make_uint4(pack2(g0, g1), 0u, 0u, 0u);
+#pragma unroll
+            for (uint32_t c = 1; c < 8; ++c) {
+                *reinterpret_cast<uint4 *>(db + umma::tile_offset(r, 8u * c, kRows)) = make_uint4(0u, 0u, 0u, 0u);
+            }
+        }
+        // Backward, layer l = 4 .. 1: dW_l += dZ_l^T [H_{l-1}, 1] and, for l > 1,
+        // dH_{l-1} = dZ_l W_l, then dZ_{l-1} = dH_{l-1} * (H_{l-1} > 0).
+        for (uint32_t layer = 4; layer >= 1 && healthy; --layer) {
+            const uint32_t cur = (4u - layer) & 1u;  // dZ4 in A, dZ3 in B, ...
+            publish_operands();
+            if (r == 0) {
+                umma::fence_after_sync();
+                const uint32_t n_in = layer == 1 ? kK1 : kKh;
+                const uint32_t acc = first_tile ? 0u : 1u;
+                const uint32_t dw_instr = umma::instr_bf16(kRows, n_in, true, true);
+#pragma unroll 1
+                for (uint32_t s = 0; s < kRows / 16; ++s) {
+                    umma::mma(tmem + col_dw[layer], umma::mnmajor(sdz[cur], kRows, s),
+                              umma::mnmajor(sh[layer - 1], kRows, s), dw_instr, (s > 0 || acc) ? 1u : 0u);
+                }
+                if (layer > 1) {
+                    const uint32_t w_rows = layer == 4 ? kOutRows : kHidden;
+                    const uint32_t k_steps = layer == 4 ? 1u : kHidden / 16;
+                    const uint32_t dh_instr = umma::instr_bf16(kRows, kHidden, false, true);
+#pragma unroll 1
+                    for (uint32_t s = 0; s < k_steps; ++s) {
+                        umma::mma(tmem + kColWork, umma::kmajor(sdz[cur], kRows, s),
+                                  umma::mnmajor(simg + img_layer[layer], w_rows, s), dh_instr, s > 0 ? 1u : 0u);
+                    }
+                }
+                umma::commit(bar);
+            }
+            healthy = wait_round(bar, phase);
+            if (!healthy || layer == 1) { break; }
+            relu_backward(lane_base, kColWork, hs[layer - 1], dzs[cur ^ 1u], r);
+        }
+        first_tile = false;
+    }
+    if (healthy && !first_tile) {
+        publish_operands();
+        umma::fence_after_sync();
+        flush_gradient(lane_base, kColW1, kHidden, kK1, k.grad, kP1);
+        flush_gradient(lane_base, kColW2, kHidden, kKh, k.grad, kP2);
+        flush_gradient(lane_base, kColW3, kHidden, kKh, k.grad, kP3);
+        flush_gradient(lane_base, kColW4, kOutRows, kKh, k.grad, kP4);
+    }
+    if (!healthy) {
+        if (r == 0 && k.status) { atomicCAS(k.status, 0u, static_cast<uint32_t>(NXG_ERROR_SURROGATE)); }
+        umma::mbar_wait(bar, phase);
+    }
+    for (int d = 16; d > 0; d >>= 1) { my_loss += __shfl_xor_sync(0xffffffffu, my_loss, d); }
+    if ((r & 31) == 0) { atomicAdd(loss_slot, my_loss); }
+    umma::fence_before_sync();
+    __syncthreads();
+    if (r == 0 && k.loss) { atomicAdd(k.loss, *loss_slot); }
+    if (r < 32) {
+        umma::fence_after_sync();
+        umma::tmem_free(tmem, kTrainTmemColumns);
+    }
+}
+
+} // namespace surrogate
+} // namespace nxg
+
+// ------------------------------------------------------------ entry points
+
+namespace {
+
+using nxg::surrogate::Header;
+
+bool model_ok(const void *model) {
+    return model != nullptr && reinterpret_cast<std::uintptr_t>(model) % 256u == 0u;
+}
+
+uint32_t launch_status(cudaError_t e) { return nxg::record_cuda(e); }
+
+uint32_t configure_smem(const void *fn, uint32_t bytes) {
+    return launch_status(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)));
+}
+
+uint32_t host_hash(uint32_t x) {
+    x ^= x >> 16u;
+    x *= 0x7feb352du;
+    x ^= x >> 15u;
+    x *= 0x846ca68bu;
+    x ^= x >> 16u;
+    return x;
+}
+
+uint32_t coprime_multiplier(uint32_t count, uint32_t seed) {
+    static const uint32_t primes[] = {2654435761u, 2246822519u, 3266489917u, 668265263u, 374761393u, 1103515245u};
+    for (uint32_t i = 0; i < 6; ++i) {
+        const uint32_t p = primes[(seed + i) % 6];
+        uint64_t a = p % count, b = count;
+        while (b) {
+            const uint64_t t = a % b;
+            a = b;
+            b = t;
+        }
+        if (a == 1u && p % count != 0u) { return p % count; }
+    }
+    return 1u;
+}
+
+} // namespace
+
+extern "C" {
+
+uint64_t nxg_surrogate_model_bytes(void) { return nxg::surrogate::kModelBytes; }
+
+uint64_t nxg_surrogate_workspace_bytes(void) {
+    return (uint64_t{nxg::surrogate::kParams} + 64u) * 4u;  // gradient + loss slots
+}
+
+uint32_t nxg_surrogate_init(void *model, const nxg_surrogate_config *config, void *stream) {
+    if (!model_ok(model) || !config) { return NXG_ERROR_INVALID_ARGUMENT; }
+    Header h{};
+    h.magic = nxg::surrogate::kMagic;
+    h.version = 1u;
+    h.parameters = nxg::surrogate::kParams;
+    for (int j = 0; j < 8; ++j) {
+        if (!std::isfinite(config->input_offset[j]) || !std::isfinite(config->input_scale[j])) {
+            return NXG_ERROR_INVALID_ARGUMENT;
+        }
+        h.input_offset[j] = config->input_offset[j];
+        h.input_scale[j] = config->input_scale[j];
+    }
+    h.output_scale[0] = h.output_scale[1] = 1.0f;
+    h.initialised = 1u;
+    const auto s = static_cast<cudaStream_t>(stream);
+    nxg::set_last_cuda_error(0);
+    // the header is small and copied from a stack object: synchronise before returning
+    uint32_t e = launch_status(cudaMemcpyAsync(model, &h, sizeof h, cudaMemcpyHostToDevice, s));
+    if (e) { return e; }
+    nxg::surrogate::init_kernel<<<64, 256, 0, s>>>(static_cast<unsigned char *>(model), config->seed);
+    if ((e = launch_status(cudaGetLastError()))) { return e; }
+    return launch_status(cudaStreamSynchronize(s));
+}
+
+uint32_t nxg_surrogate_fit_outputs(void *model, const float *targets, uint32_t count, void *stream) {
+    if (!model_ok(model) || !targets || count == 0u) { return NXG_ERROR_INVALID_ARGUMENT; }
+    nxg::set_last_cuda_error(0);
+    nxg::surrogate::output_stats_kernel<<<1, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<unsigned char *>(model), targets, count);
+    return launch_status(cudaGetLastError());
+}
+
+uint32_t nxg_surrogate_features(const nxg_device_asset_desc *asset, const nxg_generation_params *params,
+                                uint32_t first_strand, uint32_t count, float *features, void *stream) {
+    if (!asset || !params || !features) { return NXG_ERROR_INVALID_ARGUMENT; }
+    const nxg_deformed_desc none{};
+    const nxg_launch_config cfg{128u};
+    uint32_t e = nxg::validate_common(*asset, none, *params, cfg);
+    if (e) { return e; }
+    if (first_strand > params->strand_count || count > params->strand_count - first_strand) {
+        return NXG_ERROR_INVALID_STRAND_RANGE;
+    }
+    if ((e = nxg::check_launch_inputs(*asset, nullptr))) { return e; }
+    if (count == 0u) { return NXG_ERROR_NONE; }
+    const nxg::dev::AssetArgs a = nxg::resolve_asset(*asset);
+    const nxg::dev::FrameArgs f = nxg::resolve_frame(a, none);
+    nxg::set_last_cuda_error(0);
+    const uint32_t blocks = std::min<uint32_t>((count + 255u) / 256u, static_cast<uint32_t>(nxg::device_sm_count()) * 8u);
+    nxg::surrogate::features_kernel<<<blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(a, f, params->seed,
+                                                                                          first_strand, count, features);
+    return launch_status(cudaGetLastError());
+}
+
+uint32_t nxg_surrogate_forward(const void *model, const float *features, uint32_t count, float *outputs,
+                               void *stream) {
+    if (!model_ok(model) || !features || !outputs) { return NXG_ERROR_INVALID_ARGUMENT; }
+    if (reinterpret_cast<std::uintptr_t>(outputs) % 8u != 0u) { return NXG_ERROR_MISALIGNED_OUTPUT; }
+    if (count == 0u) { return NXG_ERROR_NONE; }
+    nxg::surrogate::InferArgs k{};
+    k.model = static_cast<const unsigned char *>(model);
+    k.features = features;
+    k.out = reinterpret_cast<float2 *>(outputs);
+    k.count = count;
+    nxg::set_last_cuda_error(0);
+    const void *fn = reinterpret_cast<const void *>(nxg::surrogate::infer_kernel<false>);
+    uint32_t e = configure_smem(fn, nxg::surrogate::kInferSmem);
+    if (e) { return e; }
+    const uint32_t tiles = (count + 127u) / 128u;
+    const uint32_t blocks = std::min<uint32_t>(tiles, static_cast<uint32_t>(nxg::device_sm_count()) * 4u);
+    nxg::surrogate::infer_kernel<false><<<blocks, 128, nxg::surrogate::kInferSmem, static_cast<cudaStream_t>(stream)>>>(k);
+    return launch_status(cudaGetLastError());
+}
+
+uint32_t nxg_surrogate_gradients(const void *model, const float *features, const float *targets, uint32_t count,
+                                 float *gradients, float *loss, void *stream) {
+    if (!model_ok(model) || !features || !targets || !gradients || !loss || count == 0u) {
+        return NXG_ERROR_INVALID_ARGUMENT;
+    }
+    const auto s = static_cast<cudaStream_t>(stream);
+    nxg::set_last_cuda_error(0);
+    uint32_t e = launch_status(cudaMemsetAsync(gradients, 0, nxg::surrogate::kParams * 4u, s));
+    if (e || (e = launch_status(cudaMemsetAsync(loss, 0, 4u, s)))) { return e; }
+    const void *fn = reinterpret_cast<const void *>(nxg::surrogate::train_kernel);
+    if ((e = configure_smem(fn, nxg::surrogate::kTrainSmem))) { return e; }
+    nxg::surrogate::TrainArgs k{};
+    k.model = static_cast<const unsigned char *>(model);
+    k.features = features;
+    k.targets = targets;
+    k.count = count;
+    k.begin = 0u;
+    k.length = count;
+    k.multiplier = 1u;
+    k.shift = 0u;
+    k.inv_batch = 1.0f / static_cast<float>(count);
+    k.grad = gradients;
+    k.loss = loss;
+    k.status = nullptr;
+    const uint32_t tiles = (count + 127u) / 128u;
+    const uint32_t blocks = std::min<uint32_t>(tiles, static_cast<uint32_t>(nxg::device_sm_count()));
+    nxg::surrogate::train_kernel<<<blocks, 128, nxg::surrogate::kTrainSmem, s>>>(k);
+    return launch_status(cudaGetLastError());
+}
+
+uint32_t nxg_surrogate_train(void *model, const float *features, const float *targets, uint32_t count,
+                             const nxg_surrogate_train_config *config, void *workspace, uint64_t workspace_bytes,
+                             float *loss_history, void *stream) {
+    if (!model_ok(model) || !features || !targets || !config || count == 0u) { return NXG_ERROR_INVALID_ARGUMENT; }
+    if (!workspace || workspace_bytes < nxg_surrogate_workspace_bytes() ||
+        reinterpret_cast<std::uintptr_t>(workspace) % 256u != 0u) {
+        return NXG_ERROR_WORKSPACE_TOO_SMALL;
+    }
+    const uint32_t batch = config->batch;
+    if (batch == 0u || batch % 128u != 0u || config->epochs == 0u || !(config->learning_rate > 0.0f)) {
+        return NXG_ERROR_INVALID_ARGUMENT;
+    }
+    const auto s = static_cast<cudaStream_t>(stream);
+    nxg::set_last_cuda_error(0);
+    auto *grad = static_cast<float *>(workspace);
+    float *loss = grad + nxg::surrogate::kParams;
+    uint32_t *status = reinterpret_cast<uint32_t *>(loss + 16);
+    uint32_t e = launch_status(cudaMemsetAsync(workspace, 0, nxg_surrogate_workspace_bytes(), s));
+    if (e) { return e; }
+    if (loss_history && (e = launch_status(cudaMemsetAsync(loss_history, 0, config->epochs * 4u, s)))) { return e; }
+    // Adam's step count lives in the model header; training is a set-up call
+    // and synchronises the stream to read and write it.
+    Header h{};
+    if ((e = launch_status(cudaMemcpyAsync(&h, model, sizeof h, cudaMemcpyDeviceToHost, s)))) { return e; }
+    if ((e = launch_status(cudaStreamSynchronize(s)))) { return e; }
+    if (h.magic != nxg::surrogate::kMagic || !h.initialised) { return NXG_ERROR_SURROGATE; }
+    const void *fn = reinterpret_cast<const void *>(nxg::surrogate::train_kernel);
+    if ((e = configure_smem(fn, nxg::surrogate::kTrainSmem))) { return e; }
+    const uint32_t sms = static_cast<uint32_t>(nxg::device_sm_count());
+    const uint32_t multiplier = coprime_multiplier(count, config->seed);
+    const float b1 = config->beta1 > 0.0f ? config->beta1 : 0.9f;
+    const float b2 = config->beta2 > 0.0f ? config->beta2 : 0.999f;
+    const float eps = config->epsilon > 0.0f ? config->epsilon : 1e-8f;
+    const float decay = config->lr_decay > 0.0f ? config->lr_decay : 1.0f;
+    float lr = config->learning_rate;
+    uint32_t step = h.step;
+    for (uint32_t epoch = 0; epoch < config->epochs; ++epoch) {
+        const uint32_t shift = host_hash(config->seed * 0x9e3779b9u + epoch) % count;
+        for (uint32_t begin = 0; begin < count; begin += batch) {
+            nxg::surrogate::TrainArgs k{};
+            k.model = static_cast<const unsigned char *>(model);
+            k.features = features;
+            k.targets = targets;
+            k.count = count;
+            k.begin = begin;
+            k.length = std::min(batch, count - begin);
+            k.multiplier = multiplier;
+            k.shift = shift;
+            k.inv_batch = 1.0f / static_cast<float>(k.length);
+            k.grad = grad;
+            k.loss = loss_history ? loss_history + epoch : loss;
+            k.status = status;
+            const uint32_t tiles = (k.length + 127u) / 128u;
+            nxg::surrogate::train_kernel<<<std::min(tiles, sms), 128, nxg::surrogate::kTrainSmem, s>>>(k);
+            if ((e = launch_status(cudaGetLastError()))) { return e; }
+            ++step;
+            const double bc1 = 1.0 - std::pow(static_cast<double>(b1), static_cast<double>(step));
+            const double bc2 = 1.0 - std::pow(static_cast<double>(b2), static_cast<double>(step));
+            const float lr_t = static_cast<float>(lr * std::sqrt(bc2) / bc1);
+            nxg::surrogate::adam_kernel<<<(nxg::surrogate::kParams + 255u) / 256u, 256, 0, s>>>(
+                static_cast<unsigned char *>(model), grad, lr_t, b1, b2, eps);
+            if ((e = launch_status(cudaGetLastError()))) { return e; }
+        }
+        lr *= decay;
+    }
+    h.step = step;
+    h.trained = 1u;
+    uint32_t device_status = 0u;
+    if ((e = launch_status(cudaMemcpyAsync(reinterpret_cast<unsigned char *>(model) + offsetof(Header, step), &h.step,
+                                           4u, cudaMemcpyHostToDevice, s)))) {
+        return e;
+    }
+    if ((e = launch_status(cudaMemcpyAsync(reinterpret_cast<unsigned char *>(model) + offsetof(Header, trained),
+                                           &h.trained, 4u, cudaMemcpyHostToDevice, s)))) {
+        return e;
+    }
+    if ((e = launch_status(cudaMemcpyAsync(&device_status, status, 4u, cudaMemcpyDeviceToHost, s)))) { return e; }
+    if ((e = launch_status(cudaStreamSynchronize(s)))) { return e; }
+    return device_status;
+}
+
+uint32_t nxg_surrogate_root_scalars(const void *model, const nxg_device_asset_desc *asset,
+                                    const nxg_generation_params *params, const nxg_classic_scalar_plan *plan,
+                                    const nxg_surrogate_check *check, uint32_t first_strand, uint32_t count,
+                                    float *scalars, uint32_t *device_status, void *stream) {
+    if (!model_ok(model) || !asset || !params || !plan || !check) { return NXG_ERROR_INVALID_ARGUMENT; }
+    const nxg_deformed_desc none{};
+    const nxg_launch_config cfg{128u};
+    uint32_t e = nxg::validate_common(*asset, none, *params, cfg);
+    if (e) { return e; }
+    if (first_strand > params->strand_count || count > params->strand_count - first_strand) {
+        return NXG_ERROR_INVALID_STRAND_RANGE;
+    }
+    if (!scalars || !device_status) { return NXG_ERROR_MISSING_OUTPUT; }
+    if (reinterpret_cast<std::uintptr_t>(scalars) % 8u != 0u ||
+        reinterpret_cast<std::uintptr_t>(device_status) % 4u != 0u) {
+        return NXG_ERROR_MISALIGNED_OUTPUT;
+    }
+    if (check->mode > 2u || check->checks_per_batch > 128u ||
+        (check->mode == 0u && (!(check->length_tolerance >= 0.0f) || !(check->width_tolerance >= 0.0f)))) {
+        return NXG_ERROR_INVALID_ARGUMENT;
+    }
+    if ((e = nxg::check_launch_inputs(*asset, nullptr))) { return e; }
+    nxg::surrogate::InferArgs k{};
+    if (plan->length && (e = nxg::pack_device_expression(plan->length, k.length))) { return e; }
+    if (plan->width && (e = nxg::pack_device_expression(plan->width, k.width))) { return e; }
+    if (k.length.uses_clength || k.width.uses_clength) { return NXG_ERROR_EXPRESSION_INPUT; }
+    if (count == 0u) { return NXG_ERROR_NONE; }
+    k.model = static_cast<const unsigned char *>(model);
+    k.out = reinterpret_cast<float2 *>(scalars);
+    k.count = count;
+    k.status = device_status;
+    k.a = nxg::resolve_asset(*asset);
+    k.f = nxg::resolve_frame(k.a, none);
+    k.seed = params->seed;
+    k.first = first_strand;
+    k.description_id = static_cast<float>(plan->description_id);
+    const char *patch = plan->patch_name ? plan->patch_name : "";
+    for (const char *p = patch; *p; ++p) {
+        if (*p == ':') { patch = p + 1; }
+    }
+    k.patch_seed = static_cast<float>(nxg_xgen_string_seed(patch));
+    k.length_tolerance = check->length_tolerance;
+    k.width_tolerance = check->width_tolerance;
+    k.checks = check->checks_per_batch;
+    k.mode = check->mode;
+    nxg::set_last_cuda_error(0);
+    const void *fn = reinterpret_cast<const void *>(nxg::surrogate::infer_kernel<true>);
+    if ((e = configure_smem(fn, nxg::surrogate::kInferSmem))) { return e; }
+    const uint32_t tiles = (count + 127u) / 128u;
+    const uint32_t blocks = std::min<uint32_t>(tiles, static_cast<uint32_t>(nxg::device_sm_count()) * 4u);
+    nxg::surrogate::infer_kernel<true><<<blocks, 128, nxg::surrogate::kInferSmem, static_cast<cudaStream_t>(stream)>>>(k);
+    return launch_status(cudaGetLastError());
+}
+
+uint32_t nxg_surrogate_parameters(void *model, float **parameters) {
+    if (!model_ok(model) || !parameters) { return NXG_ERROR_INVALID_ARGUMENT; }
+    *parameters = reinterpret_cast<float *>(static_cast<unsigned char *>(model) + nxg::surrogate::kOffParams);
+    return NXG_ERROR_NONE;
+}
+
+} // extern "C"

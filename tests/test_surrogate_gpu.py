@@ -1,0 +1,144 @@
+"""The tensor-core surrogate (nxg_surrogate_*) against its float64 CPU
+oracle (oracle/mlp_reference.py) and the exact Classic runtime.
+
+Bars: forward outputs and full-batch gradients match the oracle evaluated on
+the same BF16-rounded weights, inputs and activations (the remaining
+difference is FP32 accumulation order: outputs within 1e-2 of the output
+scale, every layer's gradient within 2e-2 relative L2 and cosine >= 0.999);
+training lowers the loss; exact mode reproduces nxg_classic_root_scalars
+bit for bit; a fully checked batch never returns a root outside the
+tolerance.
+"""
+import numpy as np
+import pytest
+
+from oracle import mlp_reference as ref
+
+pytestmark = pytest.mark.gpu
+
+LENGTH = "0.5*(1+0.4*noise($Prefg*6))*clamp(1-$v,0.2,1)"
+WIDTH = "0.01*(1+0.3*noise($Prefg*20))"
+
+
+@pytest.fixture(scope="module")
+def sphere(cuda, nxg_lib):
+    from nanoxgen_b200 import fixtures
+    from nanoxgen_b200.asset import build_asset
+    from nanoxgen_b200.generator import DeviceAsset
+    w = fixtures.plain_sphere()
+    asset = build_asset(w.build_input, w.stencil_slots)
+    return w, asset, DeviceAsset(asset)
+
+
+def _params(w, strands):
+    from nanoxgen_b200._abi import GenerationParams
+    p = GenerationParams()
+    for name, _ in GenerationParams._fields_:
+        setattr(p, name, getattr(w.params, name))
+    p.strand_count = strands
+    return p
+
+
+def _plan():
+    from nanoxgen_b200.classic import Expression, ScalarPlan
+    return ScalarPlan(Expression.classic(LENGTH, "length"), Expression.classic(WIDTH, "width"))
+
+
+def _model(sphere, seed=3):
+    from nanoxgen_b200.surrogate import Surrogate, asset_input_normalisation
+    off, sc = asset_input_normalisation(sphere[1])
+    return Surrogate("cuda", off, sc, seed)
+
+
+def _data(sphere, strands, seed=7):
+    """Features of `strands` roots and their exact (length, width)."""
+    import torch
+    from nanoxgen_b200.classic import check_status, root_scalars
+    from nanoxgen_b200.surrogate import Surrogate
+    w, _, dasset = sphere
+    params = _params(w, strands)
+    params.seed = seed
+    feats = Surrogate.features(dasset, params)
+    targets, status = root_scalars(dasset, params, _plan())
+    torch.cuda.synchronize()
+    check_status(status)
+    return params, feats, targets[:strands].contiguous()
+
+
+def test_forward_matches_oracle(sphere):
+    import torch
+    m = _model(sphere)
+    params, feats, targets = _data(sphere, 1000)
+    m.fit_outputs(targets)
+    out = m.forward(feats).cpu().numpy()
+    h = m.header()
+    theirs, _ = ref.forward(m.parameters(), feats.cpu().numpy(), h, emulate=True)
+    scale = np.asarray(h["output_scale"], np.float64)
+    err = np.abs(out - theirs) / scale
+    print("forward: max %.3g mean %.3g (output-scale units)" % (err.max(), err.mean()))
+    assert err.max() <= 1e-2 and err.mean() <= 1e-3
+
+
+def test_gradients_match_oracle(sphere):
+    m = _model(sphere, seed=11)
+    params, feats, targets = _data(sphere, 4096)
+    m.fit_outputs(targets)
+    loss, grad = m.gradients(feats, targets)
+    rloss, rgrad = ref.loss_and_gradients(m.parameters(), feats.cpu().numpy(), targets.cpu().numpy(), m.header())
+    assert abs(loss - rloss) <= 1e-3 * abs(rloss)
+    bounds = [(ref.P1, ref.P2), (ref.P2, ref.P3), (ref.P3, ref.P4), (ref.P4, ref.PARAMETERS)]
+    for layer, (a, b) in enumerate(bounds, 1):
+        g, r = grad[a:b].astype(np.float64), rgrad[a:b]
+        rel = np.linalg.norm(g - r) / np.linalg.norm(r)
+        cos = float(g @ r / (np.linalg.norm(g) * np.linalg.norm(r)))
+        print("layer %d: relative L2 %.3g, cosine %.6f" % (layer, rel, cos))
+        assert rel <= 2e-2 and cos >= 0.999, layer
+    assert np.all(grad[~ref.used_mask()] == 0.0)
+
+
+def test_training_lowers_loss(sphere):
+    m = _model(sphere, seed=5)
+    params, feats, targets = _data(sphere, 65536)
+    m.fit_outputs(targets)
+    before, _ = m.gradients(feats, targets)
+    result = m.train(feats, targets, epochs=6, batch=8192, learning_rate=3e-3, lr_decay=0.85)
+    after, _ = m.gradients(feats, targets)
+    print("loss %.4f -> %.4f; per epoch %s" % (before, after, np.round(result.epoch_losses, 4)))
+    assert after < 0.25 * before
+    assert m.header()["step"] == result.steps
+
+
+def test_exact_mode_is_the_exact_runtime(sphere):
+    import torch
+    from nanoxgen_b200.classic import root_scalars
+    w, _, dasset = sphere
+    m = _model(sphere)
+    params = _params(w, 5000)
+    exact, _ = root_scalars(dasset, params, _plan())
+    mine, status = m.root_scalars(dasset, params, _plan(), mode=1)
+    torch.cuda.synchronize()
+    assert status.cpu().tolist() == [0, 0, 0, 0]
+    np.testing.assert_array_equal(mine[:5000].cpu().numpy().view(np.uint32), exact[:5000].cpu().numpy().view(np.uint32))
+
+
+def test_fully_checked_batches_stay_within_tolerance(sphere):
+    import torch
+    from nanoxgen_b200.classic import root_scalars
+    w, _, dasset = sphere
+    m = _model(sphere, seed=9)
+    _, feats, targets = _data(sphere, 32768, seed=101)
+    m.fit_outputs(targets)
+    m.train(feats, targets, epochs=4, batch=8192)
+    params = _params(w, 20000)
+    exact, _ = root_scalars(dasset, params, _plan())
+    for tol in (1e-3, 5e-2):
+        got, status = m.root_scalars(dasset, params, _plan(), length_tolerance=tol, width_tolerance=tol,
+                                     checks_per_batch=128)
+        torch.cuda.synchronize()
+        g, e = got[:20000].cpu().numpy(), exact[:20000].cpu().numpy()
+        rel = np.abs(g - e) / np.abs(e)
+        st = status.cpu().tolist()
+        print("tolerance %g: %d of %d batches re-run exactly, max relative error %.3g / %.3g"
+              % (tol, st[2], st[3], rel[:, 0].max(), rel[:, 1].max()))
+        assert st[0] == 0 and st[3] == (20000 + 127) // 128
+        assert rel.max() <= tol * (1 + 1e-6)
