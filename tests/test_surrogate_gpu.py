@@ -97,15 +97,30 @@ def test_gradients_match_oracle(sphere):
 
 
 def test_training_lowers_loss(sphere):
+    # The length depends smoothly on v and on noise at frequency 6, which the
+    # network learns; the width is noise at frequency 20 over the sphere, which
+    # a 3 x 64 network cannot resolve (it stays near the mean), so the summed
+    # loss falls towards the width's share (1 in normalised units).
     m = _model(sphere, seed=5)
     params, feats, targets = _data(sphere, 65536)
     m.fit_outputs(targets)
     before, _ = m.gradients(feats, targets)
+    first = _relative_errors(m, feats, targets)
     result = m.train(feats, targets, epochs=6, batch=8192, learning_rate=3e-3, lr_decay=0.85)
     after, _ = m.gradients(feats, targets)
+    last = _relative_errors(m, feats, targets)
     print("loss %.4f -> %.4f; per epoch %s" % (before, after, np.round(result.epoch_losses, 4)))
-    assert after < 0.25 * before
+    print("mean relative length error %.4f -> %.4f, width %.4f -> %.4f"
+          % (first[0].mean(), last[0].mean(), first[1].mean(), last[1].mean()))
+    assert after < 0.6 * before
+    assert last[0].mean() < 0.3 * first[0].mean()
     assert m.header()["step"] == result.steps
+
+
+def _relative_errors(m, feats, targets):
+    out = m.forward(feats).cpu().numpy()
+    t = targets.cpu().numpy()
+    return (np.abs(out - t) / np.abs(t)).T
 
 
 def test_exact_mode_is_the_exact_runtime(sphere):
