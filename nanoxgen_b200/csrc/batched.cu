@@ -3,21 +3,18 @@
 // A frame of several descriptions (each its own .nxg asset, strand count,
 // CV count, stencil and noise settings) is generated by:
 //   batched_clear      zero the per-description bins and the work counter;
-//   batched_records    one pass over every strand of every description:
-//                      root sample, stencil row and (with noise) surface
-//                      frame inputs as a strand record, the sort key (first
-//                      stencil guide) with its histogram, and the
-//                      RootSample / root UV / point count outputs;
+//   batched_keys       alias-sample every strand's triangle, key it by its
+//                      first stencil guide (all descriptions, one grid);
 //   batched_scan       one CTA per description: bin offsets;
 //   batched_scatter    per-description strand-locality orders;
 //   batched_offsets    every description's guide-offset table;
+//   batched_roots      RootSample / root UV / point count, strand order;
 //   batched_generate   persistent warps pull (description, 32-strand batch)
 //                      items from an atomic counter -- items of the costliest
 //                      descriptions first -- and run each item with its
 //                      description's tile (lanes per strand x CVs per lane)
-//                      and noise setting, reading each strand's record
-//                      instead of re-sampling its root.
-// Six launches per frame whatever the description count, all enqueue-only
+//                      and noise setting.
+// Seven launches per frame whatever the description count, all enqueue-only
 // and capturable in one CUDA graph.
 #include "generator_core.cuh"
 #include "nxg_internal.h"
@@ -72,6 +69,18 @@ __global__ void batched_clear_kernel(const __grid_constant__ BatchArgs b) {
         for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < bins; i += gridDim.x * blockDim.x) {
             b.d[d].bins[i] = 0u;
         }
+    }
+}
+
+__global__ void batched_keys_kernel(const __grid_constant__ BatchArgs b) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < b.total_strands; i += gridDim.x * blockDim.x) {
+        const BatchDesc &d = b.d[desc_of_strand(b, i)];
+        const uint32_t local = i - d.strand_begin;
+        const uint32_t tri = sample_triangle(d.g.a, d.g.p.seed, d.g.first_strand + local);
+        const uint32_t gi = __ldg(d.g.a.stencil + static_cast<uint64_t>(tri) * kSlots);
+        const uint32_t key = gi < d.g.a.guide_count ? gi : d.g.a.guide_count;
+        d.keys[local] = key;
+        atomicAdd(&d.bins[key], 1u);
     }
 }
 
@@ -137,85 +146,38 @@ __global__ void batched_offsets_kernel(const __grid_constant__ BatchArgs b) {
     }
 }
 
-// Per flat strand: the strand record (generator_core.cuh) in its
-// description's output order, the sort key (first stencil guide) with the
-// description's key histogram, and the RootSample / root UV / point count
-// outputs.  Block b owns the contiguous flat range [b*chunk, (b+1)*chunk),
-// so its strands are mostly one description's and that description's
-// histogram is kept in shared memory.  Records and roots of a warp whose 32
-// strands share a description are written as consecutive words.
-constexpr uint32_t kBatchPrivateBins = 4096u;
-
-__global__ void __launch_bounds__(256) batched_records_kernel(const __grid_constant__ BatchArgs b, uint32_t chunk) {
-    __shared__ uint32_t staged[8][32 * kRecordStride];
-    __shared__ uint32_t hist[kBatchPrivateBins];
-    const uint32_t begin = blockIdx.x * chunk;
-    const uint32_t end = min(begin + chunk, b.total_strands);
-    if (begin >= end) { return; }
-    const int home = desc_of_strand(b, begin);
-    const uint32_t home_bins = b.d[home].g.a.guide_count + 1u;
-    const bool priv = home_bins <= kBatchPrivateBins;
-    if (priv) {
-        for (uint32_t i = threadIdx.x; i < home_bins; i += blockDim.x) { hist[i] = 0u; }
-    }
-    __syncthreads();
+// RootSample / root UV / point count per strand, strand order.  A warp
+// stages its 32 records in shared memory and writes them as consecutive
+// words (a warp may straddle two descriptions; each word goes to its own).
+__global__ void batched_roots_kernel(const __grid_constant__ BatchArgs b) {
+    __shared__ uint32_t staged[8][32 * 12];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    for (uint32_t base = begin + static_cast<uint32_t>(warp) * 32u; base < end; base += (blockDim.x >> 5) * 32u) {
+    for (uint32_t base = (blockIdx.x * (blockDim.x >> 5) + warp) * 32u; base < b.total_strands;
+         base += gridDim.x * (blockDim.x >> 5) * 32u) {
         const uint32_t i = base + static_cast<uint32_t>(lane);
-        const bool valid = i < end;
-        const uint32_t fi = valid ? i : base;
-        const int di = desc_of_strand(b, fi);
+        const bool valid = i < b.total_strands;
+        const int di = desc_of_strand(b, valid ? i : base);
         const BatchDesc &d = b.d[di];
-        const uint32_t local = fi - d.strand_begin;
-        uint32_t *row = staged[warp] + lane * kRecordStride;
-        stage_record(d.g.a, d.g.f, d.g.p, d.g.first_strand + local, row);
+        const uint32_t local = (valid ? i : base) - d.strand_begin;
+        const Root r = sample_root(d.g.a, d.g.f, d.g.p.seed, d.g.first_strand + local);
+        uint32_t *rec = staged[warp] + lane * 12;
+        for (int w = 0; w < 12; ++w) { rec[w] = root_word(r, w); }
+        __syncwarp();
+        for (int k = 0; k < 12; ++k) {
+            const int word = k * 32 + lane;           // word of the warp's staged records
+            const int slot = word / 12;               // which lane's strand
+            const int sdi = __shfl_sync(kFull, di, slot);
+            const uint32_t slocal = __shfl_sync(kFull, local, slot);
+            const bool svalid = base + static_cast<uint32_t>(slot) < b.total_strands;
+            const BatchDesc &sd = b.d[sdi];
+            if (svalid && sd.g.roots) { sd.g.roots[static_cast<uint64_t>(slocal) * 12u + (word - slot * 12)] = staged[warp][word]; }
+        }
         if (valid) {
-            const uint32_t gi = row[12];
-            const uint32_t key = gi < d.g.a.guide_count ? gi : d.g.a.guide_count;
-            d.keys[local] = key;
-            if (priv && di == home) {
-                atomicAdd(&hist[key], 1u);
-            } else {
-                atomicAdd(&d.bins[key], 1u);
-            }
-            if (d.g.root_uvs) { d.g.root_uvs[local] = make_float2(__uint_as_float(row[6]), __uint_as_float(row[7])); }
+            if (d.g.root_uvs) { d.g.root_uvs[local] = make_float2(r.u, r.v); }
             if (d.g.point_counts) { d.g.point_counts[local] = d.g.p.cvs_per_strand; }
         }
         __syncwarp();
-        const int d0 = __shfl_sync(kFull, di, 0);
-        if (__all_sync(kFull, di == d0)) {
-            const BatchDesc &dd = b.d[d0];
-            const uint32_t local0 = __shfl_sync(kFull, local, 0);
-            const uint32_t n = min(32u, end - base);
-            const uint32_t words = record_words(dd.g.p);
-            uint32_t *dst = reinterpret_cast<uint32_t *>(const_cast<uint4 *>(dd.g.records)) +
-                            static_cast<uint64_t>(local0) * words;
-            for (uint32_t w = lane; w < n * words; w += 32u) {
-                dst[w] = staged[warp][(w / words) * kRecordStride + w % words];
-            }
-            if (dd.g.roots) {
-                uint32_t *rd = dd.g.roots + static_cast<uint64_t>(local0) * 12u;
-                for (uint32_t w = lane; w < n * 12u; w += 32u) {
-                    rd[w] = staged[warp][(w / 12u) * kRecordStride + w % 12u];
-                }
-            }
-        } else if (valid) {  // the warp straddles two descriptions
-            const uint32_t words = record_words(d.g.p);
-            uint32_t *dst = reinterpret_cast<uint32_t *>(const_cast<uint4 *>(d.g.records)) +
-                            static_cast<uint64_t>(local) * words;
-            for (uint32_t w = 0; w < words; ++w) { dst[w] = row[w]; }
-            if (d.g.roots) {
-                for (uint32_t w = 0; w < 12u; ++w) { d.g.roots[static_cast<uint64_t>(local) * 12u + w] = row[w]; }
-            }
-        }
-        __syncwarp();
-    }
-    __syncthreads();
-    if (priv) {
-        for (uint32_t k = threadIdx.x; k < home_bins; k += blockDim.x) {
-            if (hist[k]) { atomicAdd(&b.d[home].bins[k], hist[k]); }
-        }
     }
 }
 
@@ -322,7 +284,7 @@ inline uint64_t up(uint64_t v) { return (v + kAlign - 1u) / kAlign * kAlign; }
 
 struct BatchLayout {
     uint64_t counter;
-    std::vector<uint64_t> keys, order, bins, offsets, records;
+    std::vector<uint64_t> keys, order, bins, offsets;
     uint64_t total;
 };
 
@@ -340,8 +302,6 @@ BatchLayout batch_layout(const nxg_device_asset_desc *assets, const nxg_generati
         at += up((G + 1u) * 4u);
         l.offsets.push_back(at);
         at += up(G * P * 16u);
-        l.records.push_back(at);
-        at += up(S * dev::kNoiseRecordWords * 4u);
     }
     l.total = at;
     return l;
@@ -450,7 +410,6 @@ extern "C" uint32_t nxg_generate_batched(const nxg_device_asset_desc *assets, co
         bd.g.root_uvs = reinterpret_cast<float2 *>(outputs[d].root_uvs);
         bd.g.point_counts = outputs[d].point_counts;
         bd.g.order = reinterpret_cast<const uint32_t *>(w + layout.order[d]);
-        bd.g.records = reinterpret_cast<const uint4 *>(w + layout.records[d]);
         bd.offsets = reinterpret_cast<const float4 *>(w + layout.offsets[d]);
         bd.keys = reinterpret_cast<uint32_t *>(w + layout.keys[d]);
         bd.bins = reinterpret_cast<uint32_t *>(w + layout.bins[d]);
@@ -479,19 +438,18 @@ extern "C" uint32_t nxg_generate_batched(const nxg_device_asset_desc *assets, co
     const uint32_t flat_blocks = static_cast<uint32_t>(std::min<uint64_t>((strands + 255u) / 256u, uint64_t(sms) * 8u));
     dev::batched_clear_kernel<<<std::max(1, sms), 256, 0, s>>>(b);
     if ((status = record_cuda(cudaGetLastError()))) { return status; }
-    {
-        const uint32_t record_blocks = static_cast<uint32_t>(std::min<uint64_t>((strands + 255u) / 256u,
-                                                                                uint64_t(sms) * 8u));
-        const uint32_t chunk = ((strands + record_blocks - 1u) / record_blocks + 31u) / 32u * 32u;
-        dev::batched_records_kernel<<<std::max(1u, record_blocks), 256, 0, s>>>(b, chunk);
-        if ((status = record_cuda(cudaGetLastError()))) { return status; }
-    }
+    dev::batched_keys_kernel<<<flat_blocks, 256, 0, s>>>(b);
+    if ((status = record_cuda(cudaGetLastError()))) { return status; }
     dev::batched_scan_kernel<<<count, 1024, 0, s>>>(b);
     if ((status = record_cuda(cudaGetLastError()))) { return status; }
     dev::batched_scatter_kernel<<<flat_blocks, 256, 0, s>>>(b);
     if ((status = record_cuda(cudaGetLastError()))) { return status; }
     const uint32_t offset_blocks = static_cast<uint32_t>(std::min<uint64_t>((offsets + 255u) / 256u, uint64_t(sms) * 16u));
     dev::batched_offsets_kernel<<<std::max(1u, offset_blocks), 256, 0, s>>>(b);
+    if ((status = record_cuda(cudaGetLastError()))) { return status; }
+    dev::batched_roots_kernel<<<std::max(1u, static_cast<uint32_t>(std::min<uint64_t>((strands + 255u) / 256u,
+                                                                                    uint64_t(sms) * 16u))),
+                                256, 0, s>>>(b);
     if ((status = record_cuda(cudaGetLastError()))) { return status; }
 
     const size_t shm = dev::kBatchWarpBytes * (block / 32u);

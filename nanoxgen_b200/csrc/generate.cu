@@ -122,32 +122,39 @@ __global__ void classic_serial_apply_kernel(LaunchArgs g) {
     }
 }
 
-// Per strand of the range, in output order: the strand record phase A
-// reads (generator_core.cuh), and the RootSample / root UV / point count
-// outputs (generate.h:101-135, :621-623), each written as consecutive words.
-// Launched with 256 threads.
-__global__ void strand_records_kernel(LaunchArgs g, uint32_t *records) {
-    __shared__ uint32_t staged[8][32 * kRecordStride];
+// RootSample, root UV and point count of every strand of the range, in
+// output order (coalesced), for the frame (generate.h:101-135, :621-623).
+__global__ void strand_roots_kernel(LaunchArgs g) {
+    __shared__ uint32_t staged[8][32 * 12];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const uint32_t P = g.p.cvs_per_strand;
-    const uint32_t words = record_words(g.p);
     for (uint32_t base = (blockIdx.x * (blockDim.x >> 5) + warp) * 32u; base < g.count;
          base += gridDim.x * (blockDim.x >> 5) * 32u) {
         const uint32_t i = base + lane;
         const bool valid = i < g.count;
-        stage_record(g.a, g.f, g.p, g.first_strand + (valid ? i : base), staged[warp] + lane * kRecordStride);
+        const Root r = sample_root(g.a, g.f, g.p.seed, g.first_strand + (valid ? i : base));
+        uint32_t *rec = staged[warp] + lane * 12;
+        rec[0] = __float_as_uint(r.position.x);
+        rec[1] = __float_as_uint(r.position.y);
+        rec[2] = __float_as_uint(r.position.z);
+        rec[3] = __float_as_uint(r.normal.x);
+        rec[4] = __float_as_uint(r.normal.y);
+        rec[5] = __float_as_uint(r.normal.z);
+        rec[6] = __float_as_uint(r.u);
+        rec[7] = __float_as_uint(r.v);
+        rec[8] = r.triangle;
+        rec[9] = __float_as_uint(r.b1);
+        rec[10] = __float_as_uint(r.b2);
+        rec[11] = r.triangle;  // surface_face_id == triangle_index (generate.h:134)
         __syncwarp();
         const uint32_t n = min(32u, g.count - base);
-        uint32_t *dst = records + static_cast<uint64_t>(base) * words;
-        for (uint32_t w = lane; w < n * words; w += 32u) { dst[w] = staged[warp][(w / words) * kRecordStride + w % words]; }
         if (g.roots) {
-            uint32_t *rd = g.roots + static_cast<uint64_t>(base) * 12u;
-            for (uint32_t w = lane; w < n * 12u; w += 32u) { rd[w] = staged[warp][(w / 12u) * kRecordStride + w % 12u]; }
+            uint32_t *dst = g.roots + static_cast<uint64_t>(base) * 12u;
+            for (uint32_t w = lane; w < n * 12u; w += 32u) { dst[w] = staged[warp][w]; }
         }
         if (valid) {
-            const uint32_t *row = staged[warp] + lane * kRecordStride;
-            if (g.root_uvs) { g.root_uvs[i] = make_float2(__uint_as_float(row[6]), __uint_as_float(row[7])); }
+            if (g.root_uvs) { g.root_uvs[i] = make_float2(r.u, r.v); }
             if (g.point_counts) { g.point_counts[i] = P; }
         }
         __syncwarp();
@@ -456,7 +463,7 @@ constexpr uint64_t kWorkspaceAlign = 256u;
 inline uint64_t align_up(uint64_t v, uint64_t a) { return (v + a - 1u) / a * a; }
 
 struct WorkspaceLayout {
-    uint64_t keys, order, hist, offsets, offset_bytes, records, total;
+    uint64_t keys, order, hist, offsets, offset_bytes, total;
 };
 
 // Largest guide-offset table the warp-parallel generator stages; beyond it
@@ -469,18 +476,14 @@ bool parallel_path(uint32_t guide_count, uint32_t P) {
 }
 
 // keys[count] | order[count] | bins[guides + 1] | offsets[guides * P] (float4)
-// | records[count] (strand records of the warp-parallel path, 112 bytes)
 WorkspaceLayout workspace_layout(uint32_t guide_count, uint32_t count, uint32_t P) {
     WorkspaceLayout w{};
     w.keys = 0u;
     w.order = align_up(uint64_t{count} * 4u, kWorkspaceAlign);
     w.hist = w.order + align_up(uint64_t{count} * 4u, kWorkspaceAlign);
     w.offsets = w.hist + align_up((uint64_t{guide_count} + 1u) * 4u, kWorkspaceAlign);
-    const bool parallel = parallel_path(guide_count, P);
-    w.offset_bytes = parallel ? uint64_t{guide_count} * P * 16u : 0u;
-    w.records = w.offsets + align_up(w.offset_bytes, kWorkspaceAlign);
-    const uint64_t record_bytes = parallel ? uint64_t{count} * dev::kNoiseRecordWords * 4u : 0u;
-    w.total = w.records + align_up(record_bytes, kWorkspaceAlign);
+    w.offset_bytes = parallel_path(guide_count, P) ? uint64_t{guide_count} * P * 16u : 0u;
+    w.total = w.offsets + align_up(w.offset_bytes, kWorkspaceAlign);
     return w;
 }
 
@@ -726,14 +729,13 @@ uint32_t launch_generate(const nxg_device_asset_desc &asset, const nxg_deformed_
         dev::guide_offsets_kernel<<<blocks, threads, 0, stream>>>(g.a, g.f, P, offsets);
         if ((status = record_cuda(cudaGetLastError()))) { return status; }
     }
-    {
-        auto *records = reinterpret_cast<uint32_t *>(wbase + ws.records);
+    if (g.roots || g.root_uvs || g.point_counts) {
         const uint32_t threads = 256u;
-        const uint32_t blocks = static_cast<uint32_t>(std::min<uint64_t>((count + threads - 1u) / threads,
+        const uint32_t per_block = threads;  // one strand per thread
+        const uint32_t blocks = static_cast<uint32_t>(std::min<uint64_t>((count + per_block - 1u) / per_block,
                                                                           static_cast<uint64_t>(sms) * 8u));
-        dev::strand_records_kernel<<<blocks, threads, 0, stream>>>(g, records);
+        dev::strand_roots_kernel<<<blocks, threads, 0, stream>>>(g);
         if ((status = record_cuda(cudaGetLastError()))) { return status; }
-        g.records = reinterpret_cast<const uint4 *>(records);
     }
     int lanes = 32, ppt = 4;
     uint32_t tile_block = 0u;

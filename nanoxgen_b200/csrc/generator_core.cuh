@@ -33,24 +33,12 @@ struct LaunchArgs {
     float2 *root_uvs;
     uint32_t *point_counts;
     const uint32_t *order;   // permutation of [0, count), or nullptr for identity
-    const uint4 *records;    // per-strand records of this frame (output order), or nullptr
     const float2 *scalars;   // Classic per-root (length scale, width), or nullptr
     uint32_t classic_length; // scale each strand about its first point by scalars.x
     uint32_t classic_width;  // radius = 0.5 * max(scalars.y, 0) * radius_scale
 };
 
 constexpr int kTableFloat4 = NXG_NOISE_GRADIENT_COUNT;  // float4 entries of the staged table
-
-// Strand record: what phase A needs about a strand's root, computed once per
-// frame by a coalesced pass in output order.  Words 0-11 are the RootSample
-// (position, normal, uv, triangle, b1, b2, surface face), 12-19 the root
-// triangle's stencil row; with noise, 20-22 the surface tangent and 23-25
-// the rest-pose root position (generate.h:312-351).
-constexpr uint32_t kRecordWords = 20, kNoiseRecordWords = 28;
-
-__device__ __forceinline__ uint32_t record_words(const ParamArgs &p) {
-    return p.noise ? kNoiseRecordWords : kRecordWords;
-}
 
 __device__ __forceinline__ uint32_t root_word(const Root &r, int w) {
     switch (w) {
@@ -114,40 +102,14 @@ __device__ __forceinline__ void setup_strand(const LaunchArgs &g, const Records 
         local = 0u;
         valid = false;
     }
-    Root root;
-    uint32_t stencil[kSlots];
-    F3 record_su = {0.0f, 0.0f, 0.0f}, record_rest = {0.0f, 0.0f, 0.0f};
-    if (g.records != nullptr) {
-        const uint4 *rp = g.records + static_cast<uint64_t>(local) * (record_words(p) / 4u);
-        const uint4 q0 = __ldg(rp), q1 = __ldg(rp + 1), q2 = __ldg(rp + 2), q3 = __ldg(rp + 3), q4 = __ldg(rp + 4);
-        root.position = {__uint_as_float(q0.x), __uint_as_float(q0.y), __uint_as_float(q0.z)};
-        root.normal = {__uint_as_float(q0.w), __uint_as_float(q1.x), __uint_as_float(q1.y)};
-        root.u = __uint_as_float(q1.z);
-        root.v = __uint_as_float(q1.w);
-        root.triangle = q2.x;
-        root.b1 = __uint_as_float(q2.y);
-        root.b2 = __uint_as_float(q2.z);
-        stencil[0] = q3.x; stencil[1] = q3.y; stencil[2] = q3.z; stencil[3] = q3.w;
-        stencil[4] = q4.x; stencil[5] = q4.y; stencil[6] = q4.z; stencil[7] = q4.w;
-        if constexpr (NOISE) {
-            const uint4 q5 = __ldg(rp + 5), q6 = __ldg(rp + 6);
-            record_su = {__uint_as_float(q5.x), __uint_as_float(q5.y), __uint_as_float(q5.z)};
-            record_rest = {__uint_as_float(q5.w), __uint_as_float(q6.x), __uint_as_float(q6.y)};
-        }
-    } else {
-        root = sample_root(a, f, p.seed, g.first_strand + local);
-        const uint4 *row = reinterpret_cast<const uint4 *>(a.stencil + static_cast<uint64_t>(root.triangle) * kSlots);
-        const uint4 s0 = __ldg(row), s1 = __ldg(row + 1);
-        stencil[0] = s0.x; stencil[1] = s0.y; stencil[2] = s0.z; stencil[3] = s0.w;
-        stencil[4] = s1.x; stencil[5] = s1.y; stencil[6] = s1.z; stencil[7] = s1.w;
-    }
+    const Root root = sample_root(a, f, p.seed, g.first_strand + local);
     float wsum = 0.0f;
     float nearest_d2 = FLT_MAX;
     uint32_t nearest = kInvalid;
     uint32_t blended = 0u;
 #pragma unroll 1
     for (uint32_t j = 0; j < kSlots; ++j) {
-        const Slot s = eval_slot_guide(a, f, p, root, stencil[j]);
+        const Slot s = eval_slot(a, f, p, root, j);
         if ((s.flags & kSlotEligible) && s.d2 < nearest_d2) {  // strict first minimum (generate.h:234)
             nearest_d2 = s.d2;
             nearest = s.guide;
@@ -171,43 +133,16 @@ __device__ __forceinline__ void setup_strand(const LaunchArgs &g, const Records 
     rec.setf(kRecNz, lane, root.normal.z);
     rec.u(kRecLocal, lane) = local | (valid ? 0u : 0x80000000u);
     if constexpr (NOISE) {
-        const F3 su = g.records != nullptr ? record_su : root_surface_u(a, f, root);
-        const F3 rest = g.records != nullptr ? record_rest : rest_root_position(a, root);
+        const F3 su = root_surface_u(a, f, root);
         const float decorrelation = 1.0f - p.noise_correlation;
         const float domain_scale = 100.0f * decorrelation * decorrelation;
-        const F3 dom = (rest + F3{0.419276f, 0.184247f, 0.805721f}) * domain_scale;
+        const F3 dom = (rest_root_position(a, root) + F3{0.419276f, 0.184247f, 0.805721f}) * domain_scale;
         rec.setf(kRecSUx, lane, su.x);
         rec.setf(kRecSUy, lane, su.y);
         rec.setf(kRecSUz, lane, su.z);
         rec.setf(kRecDx, lane, dom.x);
         rec.setf(kRecDy, lane, dom.y);
         rec.setf(kRecDz, lane, dom.z);
-    }
-}
-
-// One strand's record into a warp's staging row (stride kRecordStride words).
-constexpr uint32_t kRecordStride = kNoiseRecordWords + 1;  // odd stride: conflict-free staging
-
-__device__ __forceinline__ void stage_record(const AssetArgs &a, const FrameArgs &f, const ParamArgs &p,
-                                             uint32_t strand, uint32_t *row) {
-    const Root r = sample_root(a, f, p.seed, strand);
-#pragma unroll
-    for (int w = 0; w < 12; ++w) { row[w] = root_word(r, w); }
-    const uint4 *st = reinterpret_cast<const uint4 *>(a.stencil + static_cast<uint64_t>(r.triangle) * kSlots);
-    const uint4 s0 = __ldg(st), s1 = __ldg(st + 1);
-    row[12] = s0.x; row[13] = s0.y; row[14] = s0.z; row[15] = s0.w;
-    row[16] = s1.x; row[17] = s1.y; row[18] = s1.z; row[19] = s1.w;
-    if (p.noise) {
-        const F3 su = root_surface_u(a, f, r);
-        const F3 rest = rest_root_position(a, r);
-        row[20] = __float_as_uint(su.x);
-        row[21] = __float_as_uint(su.y);
-        row[22] = __float_as_uint(su.z);
-        row[23] = __float_as_uint(rest.x);
-        row[24] = __float_as_uint(rest.y);
-        row[25] = __float_as_uint(rest.z);
-        row[26] = 0u;
-        row[27] = 0u;
     }
 }
 

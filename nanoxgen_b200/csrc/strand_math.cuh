@@ -199,9 +199,8 @@ struct Slot {             // 48 bytes, staged in shared memory per strand
     uint32_t guide, first_cv, cv_count, flags;
 };
 
-// Slot of stencil guide `gi` (the root triangle's stencil entry).
-__device__ __forceinline__ Slot eval_slot_guide(const AssetArgs &a, const FrameArgs &f, const ParamArgs &p,
-                                                const Root &root, uint32_t gi) {
+__device__ __forceinline__ Slot eval_slot(const AssetArgs &a, const FrameArgs &f, const ParamArgs &p,
+                                          const Root &root, uint32_t j) {
     Slot s;
     s.gx = s.gy = s.gz = s.w = 0.0f;
     s.rx = s.ry = s.rz = s.d2 = 0.0f;
@@ -209,6 +208,7 @@ __device__ __forceinline__ Slot eval_slot_guide(const AssetArgs &a, const FrameA
     s.first_cv = 0u;
     s.cv_count = 0u;
     s.flags = 0u;
+    const uint32_t gi = __ldg(a.stencil + static_cast<uint64_t>(root.triangle) * kSlots + j);
     if (gi == kInvalid || gi >= a.guide_count) { return s; }
     const uint32_t *g = a.guides + 14u * static_cast<uint64_t>(gi);
     const uint32_t first = __ldg(g + 0);
@@ -269,11 +269,6 @@ __device__ __forceinline__ Slot eval_slot_guide(const AssetArgs &a, const FrameA
     s.w = powf(__fsub_rn(1.0f, __fdiv_rn(__fsqrt_rn(d2), radius)), p.weight_power);
     s.flags |= kSlotBlended;
     return s;
-}
-
-__device__ __forceinline__ Slot eval_slot(const AssetArgs &a, const FrameArgs &f, const ParamArgs &p,
-                                          const Root &root, uint32_t j) {
-    return eval_slot_guide(a, f, p, root, __ldg(a.stencil + static_cast<uint64_t>(root.triangle) * kSlots + j));
 }
 
 // generate.h:189-205 sample_guide, minus the current guide root (the
