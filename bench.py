@@ -41,7 +41,8 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["nxg", "reference"], default="nxg")
-    ap.add_argument("--workload", choices=["large", "batched", "motion"], default="large",
+    ap.add_argument("--workload", choices=["large", "batched", "motion", "classic", "batched_classic"],
+                    default="large",
                     help="large: the single large description (headline); batched: nine descriptions in one "
                          "persistent launch vs. one launch per description; motion: five shutter samples of the "
                          "large description in one graph")
@@ -477,10 +478,217 @@ def run_motion(args):
     print(json.dumps(line), flush=True)
 
 
+def _train_surrogate(dasset, asset, params, plan, samples: int, epochs: int):
+    """A surrogate trained on `samples` roots of `params` (training seed) with
+    targets from the exact runtime; returns (model, seconds)."""
+    import torch
+
+    from nanoxgen_b200.classic import check_status, root_scalars
+    from nanoxgen_b200.surrogate import Surrogate, asset_input_normalisation
+    tp = params.copy(strand_count=samples, seed=int(params.seed) + 7919)
+    off, sc = asset_input_normalisation(asset)
+    t0 = time.perf_counter()
+    model = Surrogate(dasset.device, off, sc, seed=3)
+    feats = Surrogate.features(dasset, tp)
+    targets, status = root_scalars(dasset, tp, plan)
+    torch.cuda.synchronize()
+    check_status(status)
+    targets = targets[:samples].contiguous()
+    model.fit_outputs(targets)
+    result = model.train(feats, targets, epochs=epochs, batch=16384, learning_rate=3e-3, lr_decay=0.85)
+    torch.cuda.synchronize()
+    return model, time.perf_counter() - t0, result
+
+
+def _relative_errors(got, exact):
+    import numpy as np
+    g = got.cpu().numpy().astype(np.float64)
+    e = exact.cpu().numpy().astype(np.float64)
+    rel = np.abs(g - e) / np.abs(e)
+    return {"length_max": float(rel[:, 0].max()), "length_p99": float(np.percentile(rel[:, 0], 99)),
+            "length_mean": float(rel[:, 0].mean()), "width_max": float(rel[:, 1].max()),
+            "width_p99": float(np.percentile(rel[:, 1], 99))}
+
+
+def run_classic(args):
+    """Learned-expression workload: 4,000,000 strands x 24 points on the
+    200,000-triangle sphere with Classic length / width expressions.  The
+    exact runtime (nxg_classic_root_scalars) and the tensor-core surrogate
+    (trained here on 1M exact samples, judged per 128-root batch at 1e-3
+    relative error, adaptive) feed nxg_generate_packed_classic; each path is
+    one CUDA graph replay per step."""
+    import numpy as np
+    import torch
+
+    from nanoxgen_b200 import fixtures
+    from nanoxgen_b200.asset import build_asset
+    from nanoxgen_b200.classic import Expression, ScalarPlan, generate_packed_classic, root_scalars
+    from nanoxgen_b200.generator import DeviceAsset, allocate_outputs
+    device = torch.device("cuda", 0)
+    torch.cuda.set_device(device)
+    strands = args.strands if args.strands != STRANDS_PER_GPU else 4_000_000
+    w = fixtures.classic_sphere(strands=strands)
+    asset = build_asset(w.build_input, w.stencil_slots)
+    d = DeviceAsset(asset, device)
+    params = w.params
+    S, P = int(params.strand_count), int(params.cvs_per_strand)
+    plan = ScalarPlan(Expression.classic(fixtures.CLASSIC_LENGTH, "length"),
+                      Expression.classic(fixtures.CLASSIC_WIDTH, "width"))
+    model, train_s, result = _train_surrogate(d, asset, params, plan, 1_000_000, 8)
+    out = allocate_outputs(S, P, device)
+    scal = torch.empty((S, 2), dtype=torch.float32, device=device)
+    status2 = torch.zeros(2, dtype=torch.int32, device=device)
+    status4 = torch.zeros(4, dtype=torch.int32, device=device)
+    tol = 1e-3
+
+    def exact_scalars(s):
+        root_scalars(d, params, plan, out=scal, status=status2, stream=s)
+
+    def surrogate_scalars(mode):
+        return lambda s: model.root_scalars(d, params, plan, length_tolerance=tol, width_tolerance=tol,
+                                            checks_per_batch=4, mode=mode, out=scal, status=status4, stream=s)
+
+    def gen(s):
+        generate_packed_classic(d, params, scal, points=out[0], roots=out[1], root_uvs=out[2],
+                                point_counts=out[3], stream=s)
+
+    # accuracy of the network alone and of the judged output, against the exact runtime
+    exact_scalars(None)
+    exact = scal.clone()
+    surrogate_scalars(2)(None)
+    network = scal.clone()
+    status4.zero_()
+    surrogate_scalars(3)(None)
+    torch.cuda.synchronize()
+    judged = scal.clone()
+    tiles = (S + 127) // 128
+    adaptive_status = status4.cpu().tolist()
+    status4.zero_()
+    surrogate_scalars(0)(None)
+    torch.cuda.synchronize()
+    checked_status = status4.cpu().tolist()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=device)
+    sampler = ClockSampler(0)
+    sampler.start()
+    t = {}
+    t["scalars_exact"] = _graph_time(device, exact_scalars, args.steps, args.warmup, flush)
+    t["scalars_network_only"] = _graph_time(device, surrogate_scalars(2), args.steps, args.warmup, flush)
+    t["scalars_judged_adaptive"] = _graph_time(device, surrogate_scalars(3), args.steps, args.warmup, flush)
+    t["scalars_judged_every_batch"] = _graph_time(device, surrogate_scalars(0), args.steps, args.warmup, flush)
+    t["exact_path"] = _graph_time(device, lambda s: (exact_scalars(s), gen(s)), args.steps, args.warmup, flush)
+    t["surrogate_path"] = _graph_time(device, lambda s: (surrogate_scalars(3)(s), gen(s)), args.steps,
+                                      args.warmup, flush)
+    clocks = sampler.stop()
+    ms = {k: statistics.mean(v) for k, v in t.items()}
+    points = S * P
+    line = {"metric": "points/sec", "value": points / (ms["surrogate_path"] / 1e3), "unit": "points/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms["surrogate_path"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (network bf16)",
+            "data": "synthetic",
+            "config": {"workload": w.name, "strands": S, "cvs_per_strand": P, "length": fixtures.CLASSIC_LENGTH,
+                       "width": fixtures.CLASSIC_WIDTH, "tolerance": tol, "checks_per_batch": 4,
+                       "l2": "flushed between timed replays (256 MiB write)"},
+            "exact_path": {"ms_per_step": ms["exact_path"], "value": points / (ms["exact_path"] / 1e3)},
+            "scalar_stage_ms": {k[len("scalars_"):]: v for k, v in ms.items() if k.startswith("scalars_")},
+            "surrogate": {"training_s": train_s, "training_samples": 1_000_000, "epochs": 8,
+                          "epoch_losses": [float(x) for x in result.epoch_losses],
+                          "network_only_error": _relative_errors(network, exact),
+                          "judged_error": _relative_errors(judged, exact),
+                          "batches": tiles,
+                          "adaptive": {"checked": adaptive_status[3], "rerun_exactly": adaptive_status[2],
+                                       "served_exactly_unchecked": tiles - adaptive_status[3]},
+                          "every_batch": {"checked": checked_status[3], "rerun_exactly": checked_status[2]}},
+            "clocks": clocks, "gpu_launches": 7 * args.steps}
+    print(json.dumps(line), flush=True)
+
+
+def run_batched_classic(args):
+    """The nine-description workload with Classic length / width expressions:
+    the plain path (per description: exact scalars + generate_packed_classic)
+    against the batched form (per description surrogate scalars, adaptive,
+    judged at 1e-3, then one batched generate launch with the scalars fused),
+    each one CUDA graph; also batched with exact scalars."""
+    import torch
+
+    from nanoxgen_b200 import fixtures
+    from nanoxgen_b200.asset import build_asset
+    from nanoxgen_b200.classic import Expression, ScalarPlan, generate_packed_classic, root_scalars
+    from nanoxgen_b200.generator import BatchRunner, DeviceAsset, autotune
+    device = torch.device("cuda", 0)
+    torch.cuda.set_device(device)
+    batch = fixtures.batched_descriptions()
+    assets = [build_asset(w.build_input, w.stencil_slots) for w in batch.workloads]
+    dassets = [DeviceAsset(a, device) for a in assets]
+    params = [w.params for w in batch.workloads]
+    plan = ScalarPlan(Expression.classic(fixtures.CLASSIC_LENGTH, "length"),
+                      Expression.classic(fixtures.CLASSIC_WIDTH, "width"))
+    runner = BatchRunner(dassets, params)
+    for w, d, o in zip(batch.workloads, dassets, runner.outputs):
+        autotune(d, w.params, o[0], repeats=2)
+    # One network for every description: they share the mesh and the expressions.
+    model, train_s, _ = _train_surrogate(dassets[0], assets[0], params[0].copy(noise_amplitude=0.0), plan,
+                                         1_000_000, 8)
+    scal = [torch.empty((int(p.strand_count), 2), dtype=torch.float32, device=device) for p in params]
+    st2 = [torch.zeros(2, dtype=torch.int32, device=device) for _ in params]
+    st4 = [torch.zeros(4, dtype=torch.int32, device=device) for _ in params]
+
+    def exact(s):
+        for d, p, t, st in zip(dassets, params, scal, st2):
+            root_scalars(d, p, plan, out=t, status=st, stream=s)
+
+    def surrogate(s):
+        for d, p, t, st in zip(dassets, params, scal, st4):
+            model.root_scalars(d, p, plan, length_tolerance=1e-3, width_tolerance=1e-3, checks_per_batch=4,
+                               mode=3, out=t, status=st, stream=s)
+
+    def plain(s):
+        exact(s)
+        for d, p, t, o in zip(dassets, params, scal, runner.outputs):
+            generate_packed_classic(d, p, t, points=o[0], roots=o[1], root_uvs=o[2], point_counts=o[3], stream=s)
+
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=device)
+    sampler = ClockSampler(0)
+    sampler.start()
+    t_batched = _graph_time(device, lambda s: (surrogate(s), runner.run(stream=s, scalars=scal)), args.steps,
+                            args.warmup, flush)
+    t_batched_exact = _graph_time(device, lambda s: (exact(s), runner.run(stream=s, scalars=scal)), args.steps,
+                                  args.warmup, flush)
+    t_plain = _graph_time(device, plain, args.steps, args.warmup, flush)
+    clocks = sampler.stop()
+    # the judged scalars against the exact runtime, per strand
+    exact(None)
+    ref = [t.clone() for t in scal]
+    for st in st4:
+        st.zero_()
+    surrogate(None)
+    torch.cuda.synchronize()
+    worst = max(_relative_errors(t, r)["length_max"] for t, r in zip(scal, ref))
+    fallback = [s.cpu().tolist() for s in st4]
+    ms, pms, ems = statistics.mean(t_batched), statistics.mean(t_plain), statistics.mean(t_batched_exact)
+    points = batch.points
+    line = {"metric": "points/sec", "value": points / (ms / 1e3), "unit": "points/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (network bf16)", "data": "synthetic",
+            "config": {"workload": batch.name + "/classic-length-width", "strands": batch.strands, "points": points,
+                       "tolerance": 1e-3, "checks_per_batch": 4, "judge": "adaptive",
+                       "l2": "flushed between timed replays (256 MiB write)"},
+            "plain_path": {"ms_per_step": pms, "value": points / (pms / 1e3),
+                           "how": "per description nxg_classic_root_scalars + nxg_generate_packed_classic, one graph"},
+            "batched_exact": {"ms_per_step": ems, "value": points / (ems / 1e3)},
+            "speedup_vs_plain": pms / ms, "max_relative_length_error": worst,
+            "surrogate": {"training_s": train_s, "status_per_description": fallback},
+            "clocks": clocks, "gpu_launches": (len(params) + 6) * args.steps}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
         run_reference_arm(args)
+    elif args.workload == "classic":
+        run_classic(args)
+    elif args.workload == "batched_classic":
+        run_batched_classic(args)
     elif args.workload == "batched":
         run_batched(args)
     elif args.workload == "motion":

@@ -133,6 +133,14 @@ uint32_t nxg_generate_packed_classic(const nxg_device_asset_desc *asset, const n
                                      uint32_t first_strand, uint32_t strand_count, void *workspace,
                                      uint64_t workspace_bytes, void *stream);
 
+/* nxg_generate_batched (nxg.h) with per-description Classic scalars:
+ * classic[d].root_scalars may be NULL for descriptions without them. */
+uint32_t nxg_generate_batched_classic(const nxg_device_asset_desc *assets, const nxg_deformed_desc *deformed,
+                                      const nxg_generation_params *params, const nxg_packed_output_desc *outputs,
+                                      const nxg_classic_apply_desc *classic, uint32_t count,
+                                      const nxg_launch_config *config, void *workspace, uint64_t workspace_bytes,
+                                      void *stream);
+
 /* ---------------------------------------------------------------- surrogate */
 
 /* The model is one caller-owned device buffer of nxg_surrogate_model_bytes()
@@ -166,7 +174,10 @@ typedef struct nxg_surrogate_train_config {
  * roots are evaluated by the exact runtime and, if any relative error
  * exceeds its tolerance (or the exact runtime fails there), every root of
  * the tile is re-run exactly.  mode 0 = checked surrogate, 1 = exact
- * runtime only, 2 = surrogate without checks. */
+ * runtime only, 2 = surrogate without checks, 3 = adaptive: as 0, but a
+ * CTA whose check fails serves its next 15 batches exactly before it tries
+ * the network again (a surrogate that misses the tolerance then costs a
+ * sixteenth of its inference). */
 typedef struct nxg_surrogate_check {
     float length_tolerance;
     float width_tolerance;

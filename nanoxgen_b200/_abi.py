@@ -351,6 +351,8 @@ _SIGNATURES = {
                                                       ctypes.POINTER(PackedOutputDesc),
                                                       ctypes.POINTER(ClassicApplyDesc), ctypes.POINTER(LaunchConfig),
                                                       ctypes.c_uint32, ctypes.c_uint32, _P, ctypes.c_uint64, _P]),
+    "nxg_generate_batched_classic": (ctypes.c_uint32, [_P, _P, _P, _P, _P, ctypes.c_uint32,
+                                                       ctypes.POINTER(LaunchConfig), _P, ctypes.c_uint64, _P]),
     "nxg_surrogate_model_bytes": (ctypes.c_uint64, []),
     "nxg_surrogate_workspace_bytes": (ctypes.c_uint64, []),
     "nxg_surrogate_init": (ctypes.c_uint32, [_P, ctypes.POINTER(SurrogateConfig), _P]),

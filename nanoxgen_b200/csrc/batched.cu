@@ -3,20 +3,21 @@
 // A frame of several descriptions (each its own .nxg asset, strand count,
 // CV count, stencil and noise settings) is generated by:
 //   batched_clear      zero the per-description bins and the work counter;
-//   batched_keys       alias-sample every strand's triangle, key it by its
-//                      first stencil guide (all descriptions, one grid);
+//   batched_prepare    one pass over every strand of every description:
+//                      root sample, sort key (first stencil guide) with its
+//                      histogram, RootSample / root UV / point count outputs;
 //   batched_scan       one CTA per description: bin offsets;
 //   batched_scatter    per-description strand-locality orders;
 //   batched_offsets    every description's guide-offset table;
-//   batched_roots      RootSample / root UV / point count, strand order;
 //   batched_generate   persistent warps pull (description, 32-strand batch)
 //                      items from an atomic counter -- items of the costliest
 //                      descriptions first -- and run each item with its
 //                      description's tile (lanes per strand x CVs per lane)
 //                      and noise setting.
-// Seven launches per frame whatever the description count, all enqueue-only
+// Six launches per frame whatever the description count, all enqueue-only
 // and capturable in one CUDA graph.
 #include "generator_core.cuh"
+#include "nxg_classic.h"
 #include "nxg_internal.h"
 #include "strand_math.cuh"
 
@@ -69,18 +70,6 @@ __global__ void batched_clear_kernel(const __grid_constant__ BatchArgs b) {
         for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < bins; i += gridDim.x * blockDim.x) {
             b.d[d].bins[i] = 0u;
         }
-    }
-}
-
-__global__ void batched_keys_kernel(const __grid_constant__ BatchArgs b) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < b.total_strands; i += gridDim.x * blockDim.x) {
-        const BatchDesc &d = b.d[desc_of_strand(b, i)];
-        const uint32_t local = i - d.strand_begin;
-        const uint32_t tri = sample_triangle(d.g.a, d.g.p.seed, d.g.first_strand + local);
-        const uint32_t gi = __ldg(d.g.a.stencil + static_cast<uint64_t>(tri) * kSlots);
-        const uint32_t key = gi < d.g.a.guide_count ? gi : d.g.a.guide_count;
-        d.keys[local] = key;
-        atomicAdd(&d.bins[key], 1u);
     }
 }
 
@@ -146,38 +135,71 @@ __global__ void batched_offsets_kernel(const __grid_constant__ BatchArgs b) {
     }
 }
 
-// RootSample / root UV / point count per strand, strand order.  A warp
-// stages its 32 records in shared memory and writes them as consecutive
-// words (a warp may straddle two descriptions; each word goes to its own).
-__global__ void batched_roots_kernel(const __grid_constant__ BatchArgs b) {
-    __shared__ uint32_t staged[8][32 * 12];
+// Per flat strand: the root sample, its sort key (first stencil guide)
+// with the description's key histogram, and the RootSample / root UV /
+// point count outputs.  Block b owns the contiguous flat range
+// [b*chunk, (b+1)*chunk), so its strands are mostly one description's and
+// that description's histogram is kept in shared memory.  Roots of a warp
+// whose 32 strands share a description are written as consecutive words.
+constexpr uint32_t kBatchPrivateBins = 4096u;
+
+__global__ void __launch_bounds__(256) batched_prepare_kernel(const __grid_constant__ BatchArgs b, uint32_t chunk) {
+    __shared__ uint32_t staged[8][32 * 12 + 1];
+    __shared__ uint32_t hist[kBatchPrivateBins];
+    const uint32_t begin = blockIdx.x * chunk;
+    const uint32_t end = min(begin + chunk, b.total_strands);
+    if (begin >= end) { return; }
+    const int home = desc_of_strand(b, begin);
+    const uint32_t home_bins = b.d[home].g.a.guide_count + 1u;
+    const bool priv = home_bins <= kBatchPrivateBins;
+    if (priv) {
+        for (uint32_t i = threadIdx.x; i < home_bins; i += blockDim.x) { hist[i] = 0u; }
+    }
+    __syncthreads();
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    for (uint32_t base = (blockIdx.x * (blockDim.x >> 5) + warp) * 32u; base < b.total_strands;
-         base += gridDim.x * (blockDim.x >> 5) * 32u) {
+    for (uint32_t base = begin + static_cast<uint32_t>(warp) * 32u; base < end; base += (blockDim.x >> 5) * 32u) {
         const uint32_t i = base + static_cast<uint32_t>(lane);
-        const bool valid = i < b.total_strands;
-        const int di = desc_of_strand(b, valid ? i : base);
+        const bool valid = i < end;
+        const uint32_t fi = valid ? i : base;
+        const int di = desc_of_strand(b, fi);
         const BatchDesc &d = b.d[di];
-        const uint32_t local = (valid ? i : base) - d.strand_begin;
+        const uint32_t local = fi - d.strand_begin;
         const Root r = sample_root(d.g.a, d.g.f, d.g.p.seed, d.g.first_strand + local);
         uint32_t *rec = staged[warp] + lane * 12;
         for (int w = 0; w < 12; ++w) { rec[w] = root_word(r, w); }
-        __syncwarp();
-        for (int k = 0; k < 12; ++k) {
-            const int word = k * 32 + lane;           // word of the warp's staged records
-            const int slot = word / 12;               // which lane's strand
-            const int sdi = __shfl_sync(kFull, di, slot);
-            const uint32_t slocal = __shfl_sync(kFull, local, slot);
-            const bool svalid = base + static_cast<uint32_t>(slot) < b.total_strands;
-            const BatchDesc &sd = b.d[sdi];
-            if (svalid && sd.g.roots) { sd.g.roots[static_cast<uint64_t>(slocal) * 12u + (word - slot * 12)] = staged[warp][word]; }
-        }
         if (valid) {
+            const uint32_t gi = __ldg(d.g.a.stencil + static_cast<uint64_t>(r.triangle) * kSlots);
+            const uint32_t key = gi < d.g.a.guide_count ? gi : d.g.a.guide_count;
+            d.keys[local] = key;
+            if (priv && di == home) {
+                atomicAdd(&hist[key], 1u);
+            } else {
+                atomicAdd(&d.bins[key], 1u);
+            }
             if (d.g.root_uvs) { d.g.root_uvs[local] = make_float2(r.u, r.v); }
             if (d.g.point_counts) { d.g.point_counts[local] = d.g.p.cvs_per_strand; }
         }
         __syncwarp();
+        const int d0 = __shfl_sync(kFull, di, 0);
+        if (__all_sync(kFull, di == d0)) {
+            const BatchDesc &dd = b.d[d0];
+            if (dd.g.roots) {
+                const uint32_t local0 = __shfl_sync(kFull, local, 0);
+                const uint32_t n = min(32u, end - base);
+                uint32_t *dst = dd.g.roots + static_cast<uint64_t>(local0) * 12u;
+                for (uint32_t w = lane; w < n * 12u; w += 32u) { dst[w] = staged[warp][w]; }
+            }
+        } else if (valid && d.g.roots) {  // the warp straddles two descriptions
+            for (int w = 0; w < 12; ++w) { d.g.roots[static_cast<uint64_t>(local) * 12u + w] = rec[w]; }
+        }
+        __syncwarp();
+    }
+    __syncthreads();
+    if (priv) {
+        for (uint32_t k = threadIdx.x; k < home_bins; k += blockDim.x) {
+            if (hist[k]) { atomicAdd(&b.d[home].bins[k], hist[k]); }
+        }
     }
 }
 
@@ -190,7 +212,7 @@ constexpr size_t kBatchLatticeBytes = sizeof(float2) * 384u;
 constexpr size_t kBatchWarpBytes =
     kBatchTableBytes + kBatchTvalBytes + kBatchRecordBytes + kBatchStageBytes + kBatchLatticeBytes;
 
-template <int L, int PPT, bool NOISE>
+template <int L, int PPT, bool NOISE, bool CLASSIC>
 __device__ __noinline__ void batched_item(const BatchDesc &d, uint32_t batch, uint32_t end, int lane,
                                              unsigned char *mine) {
     const float4 *table = reinterpret_cast<const float4 *>(mine);
@@ -209,26 +231,28 @@ __device__ __noinline__ void batched_item(const BatchDesc &d, uint32_t batch, ui
     const uint32_t in_batch = end - batch;
 #pragma unroll 1
     for (uint32_t r = 0; r < in_batch; r += kGroups) {
-        emit_strand<L, PPT, NOISE>(d.g, rec, static_cast<int>(r) + group, gl, table, d.offsets, tvals,
+        emit_strand<L, PPT, NOISE, CLASSIC>(d.g, rec, static_cast<int>(r) + group, gl, table, d.offsets, tvals,
                                    stage_base + group * (L * PPT), lattice_base + group * (384 / kGroups),
                                    384 / 3 / kGroups);
     }
     __syncwarp();
 }
 
-template <int PPT, bool NOISE>
+template <int PPT, bool NOISE, bool CLASSIC>
 __device__ __forceinline__ void batched_dispatch_lanes(const BatchDesc &d, uint32_t batch, uint32_t end, int lane,
                                                        unsigned char *mine) {
     switch (d.lanes) {
-        case 2: batched_item<2, PPT, NOISE>(d, batch, end, lane, mine); break;
-        case 4: batched_item<4, PPT, NOISE>(d, batch, end, lane, mine); break;
-        case 8: batched_item<8, PPT, NOISE>(d, batch, end, lane, mine); break;
-        case 16: batched_item<16, PPT, NOISE>(d, batch, end, lane, mine); break;
-        default: batched_item<32, PPT, NOISE>(d, batch, end, lane, mine); break;
+        case 2: batched_item<2, PPT, NOISE, CLASSIC>(d, batch, end, lane, mine); break;
+        case 4: batched_item<4, PPT, NOISE, CLASSIC>(d, batch, end, lane, mine); break;
+        case 8: batched_item<8, PPT, NOISE, CLASSIC>(d, batch, end, lane, mine); break;
+        case 16: batched_item<16, PPT, NOISE, CLASSIC>(d, batch, end, lane, mine); break;
+        default: batched_item<32, PPT, NOISE, CLASSIC>(d, batch, end, lane, mine); break;
     }
 }
 
-template <int PPT>
+// CLASSIC: some description applies Classic per-root scalars; descriptions
+// without scalars still take the plain item.
+template <int PPT, bool CLASSIC>
 __global__ void batched_generate_kernel(const __grid_constant__ BatchArgs b) {
     extern __shared__ float4 smem[];
     __shared__ uint32_t claimed;
@@ -267,10 +291,16 @@ __global__ void batched_generate_kernel(const __grid_constant__ BatchArgs b) {
             current = di;
         }
         const uint32_t end = min(batch + 32u, d.g.count);
-        if (d.noise) {
-            batched_dispatch_lanes<PPT, true>(d, batch, end, lane, mine);
+        if (CLASSIC && d.g.scalars != nullptr) {
+            if (d.noise) {
+                batched_dispatch_lanes<PPT, true, CLASSIC>(d, batch, end, lane, mine);
+            } else {
+                batched_dispatch_lanes<PPT, false, CLASSIC>(d, batch, end, lane, mine);
+            }
+        } else if (d.noise) {
+            batched_dispatch_lanes<PPT, true, false>(d, batch, end, lane, mine);
         } else {
-            batched_dispatch_lanes<PPT, false>(d, batch, end, lane, mine);
+            batched_dispatch_lanes<PPT, false, false>(d, batch, end, lane, mine);
         }
     }
 }
@@ -334,13 +364,24 @@ extern "C" uint64_t nxg_batched_workspace_size(const nxg_device_asset_desc *asse
     return nxg::batch_layout(assets, params, count).total;
 }
 
-extern "C" uint32_t nxg_generate_batched(const nxg_device_asset_desc *assets, const nxg_deformed_desc *deformed,
-                                         const nxg_generation_params *params,
-                                         const nxg_packed_output_desc *outputs, uint32_t count,
-                                         const nxg_launch_config *config, void *workspace,
-                                         uint64_t workspace_bytes, void *stream) {
-    using namespace nxg;
+namespace nxg {
+namespace {
+
+uint32_t generate_batched(const nxg_device_asset_desc *assets, const nxg_deformed_desc *deformed,
+                          const nxg_generation_params *params, const nxg_packed_output_desc *outputs,
+                          const nxg_classic_apply_desc *classic, uint32_t count, const nxg_launch_config *config,
+                          void *workspace, uint64_t workspace_bytes, void *stream) {
     if (!assets || !params || !outputs || count == 0u || count > NXG_MAX_BATCH) { return NXG_ERROR_INVALID_ARGUMENT; }
+    bool any_classic = false;
+    if (classic) {
+        for (uint32_t d = 0; d < count; ++d) {
+            if (classic[d].root_scalars == nullptr) { continue; }
+            if (reinterpret_cast<std::uintptr_t>(classic[d].root_scalars) % 8u != 0u) {
+                return NXG_ERROR_MISALIGNED_OUTPUT;
+            }
+            any_classic = true;
+        }
+    }
     const nxg_launch_config cfg = config ? *config : nxg_launch_config{128u};
     for (uint32_t d = 0; d < count; ++d) {
         const uint32_t error = nxg_validate_packed_request(&assets[d], deformed ? &deformed[d] : nullptr, &params[d],
@@ -366,8 +407,11 @@ extern "C" uint32_t nxg_generate_batched(const nxg_device_asset_desc *assets, co
     uint32_t max_cvs = 0u;
     for (uint32_t d = 0; d < count; ++d) { max_cvs = std::max(max_cvs, params[d].cvs_per_strand); }
     const uint32_t ppt = max_cvs <= 64u ? 2u : 4u;
-    const void *fn = ppt == 2u ? reinterpret_cast<const void *>(dev::batched_generate_kernel<2>)
-                               : reinterpret_cast<const void *>(dev::batched_generate_kernel<4>);
+    const void *fn = any_classic
+        ? (ppt == 2u ? reinterpret_cast<const void *>(dev::batched_generate_kernel<2, true>)
+                     : reinterpret_cast<const void *>(dev::batched_generate_kernel<4, true>))
+        : (ppt == 2u ? reinterpret_cast<const void *>(dev::batched_generate_kernel<2, false>)
+                     : reinterpret_cast<const void *>(dev::batched_generate_kernel<4, false>));
     uint32_t status = NXG_ERROR_NONE;
     cudaFuncAttributes attr{};
     if ((status = record_cuda(cudaFuncGetAttributes(&attr, fn)))) { return status; }
@@ -410,6 +454,11 @@ extern "C" uint32_t nxg_generate_batched(const nxg_device_asset_desc *assets, co
         bd.g.root_uvs = reinterpret_cast<float2 *>(outputs[d].root_uvs);
         bd.g.point_counts = outputs[d].point_counts;
         bd.g.order = reinterpret_cast<const uint32_t *>(w + layout.order[d]);
+        if (classic && classic[d].root_scalars) {
+            bd.g.scalars = reinterpret_cast<const float2 *>(classic[d].root_scalars);
+            bd.g.classic_length = classic[d].apply_length != 0u;
+            bd.g.classic_width = classic[d].apply_width != 0u;
+        }
         bd.offsets = reinterpret_cast<const float4 *>(w + layout.offsets[d]);
         bd.keys = reinterpret_cast<uint32_t *>(w + layout.keys[d]);
         bd.bins = reinterpret_cast<uint32_t *>(w + layout.bins[d]);
@@ -438,18 +487,19 @@ extern "C" uint32_t nxg_generate_batched(const nxg_device_asset_desc *assets, co
     const uint32_t flat_blocks = static_cast<uint32_t>(std::min<uint64_t>((strands + 255u) / 256u, uint64_t(sms) * 8u));
     dev::batched_clear_kernel<<<std::max(1, sms), 256, 0, s>>>(b);
     if ((status = record_cuda(cudaGetLastError()))) { return status; }
-    dev::batched_keys_kernel<<<flat_blocks, 256, 0, s>>>(b);
-    if ((status = record_cuda(cudaGetLastError()))) { return status; }
+    {
+        const uint32_t prepare_blocks = static_cast<uint32_t>(std::min<uint64_t>((strands + 255u) / 256u,
+                                                                                 uint64_t(sms) * 8u));
+        const uint32_t chunk = ((strands + prepare_blocks - 1u) / prepare_blocks + 31u) / 32u * 32u;
+        dev::batched_prepare_kernel<<<std::max(1u, prepare_blocks), 256, 0, s>>>(b, chunk);
+        if ((status = record_cuda(cudaGetLastError()))) { return status; }
+    }
     dev::batched_scan_kernel<<<count, 1024, 0, s>>>(b);
     if ((status = record_cuda(cudaGetLastError()))) { return status; }
     dev::batched_scatter_kernel<<<flat_blocks, 256, 0, s>>>(b);
     if ((status = record_cuda(cudaGetLastError()))) { return status; }
     const uint32_t offset_blocks = static_cast<uint32_t>(std::min<uint64_t>((offsets + 255u) / 256u, uint64_t(sms) * 16u));
     dev::batched_offsets_kernel<<<std::max(1u, offset_blocks), 256, 0, s>>>(b);
-    if ((status = record_cuda(cudaGetLastError()))) { return status; }
-    dev::batched_roots_kernel<<<std::max(1u, static_cast<uint32_t>(std::min<uint64_t>((strands + 255u) / 256u,
-                                                                                    uint64_t(sms) * 16u))),
-                                256, 0, s>>>(b);
     if ((status = record_cuda(cudaGetLastError()))) { return status; }
 
     const size_t shm = dev::kBatchWarpBytes * (block / 32u);
@@ -463,10 +513,40 @@ extern "C" uint32_t nxg_generate_batched(const nxg_device_asset_desc *assets, co
         return status;
     }
     const uint32_t grid = static_cast<uint32_t>(std::max(1, sms * std::max(per_sm, 1)));
-    if (ppt == 2u) {
-        dev::batched_generate_kernel<2><<<grid, block, shm, s>>>(b);
+    if (any_classic) {
+        if (ppt == 2u) {
+            dev::batched_generate_kernel<2, true><<<grid, block, shm, s>>>(b);
+        } else {
+            dev::batched_generate_kernel<4, true><<<grid, block, shm, s>>>(b);
+        }
+    } else if (ppt == 2u) {
+        dev::batched_generate_kernel<2, false><<<grid, block, shm, s>>>(b);
     } else {
-        dev::batched_generate_kernel<4><<<grid, block, shm, s>>>(b);
+        dev::batched_generate_kernel<4, false><<<grid, block, shm, s>>>(b);
     }
     return record_cuda(cudaGetLastError());
+}
+
+} // namespace
+} // namespace nxg
+
+extern "C" uint32_t nxg_generate_batched(const nxg_device_asset_desc *assets, const nxg_deformed_desc *deformed,
+                                         const nxg_generation_params *params,
+                                         const nxg_packed_output_desc *outputs, uint32_t count,
+                                         const nxg_launch_config *config, void *workspace,
+                                         uint64_t workspace_bytes, void *stream) {
+    return nxg::generate_batched(assets, deformed, params, outputs, nullptr, count, config, workspace,
+                                 workspace_bytes, stream);
+}
+
+extern "C" uint32_t nxg_generate_batched_classic(const nxg_device_asset_desc *assets,
+                                                 const nxg_deformed_desc *deformed,
+                                                 const nxg_generation_params *params,
+                                                 const nxg_packed_output_desc *outputs,
+                                                 const nxg_classic_apply_desc *classic, uint32_t count,
+                                                 const nxg_launch_config *config, void *workspace,
+                                                 uint64_t workspace_bytes, void *stream) {
+    if (!classic) { return NXG_ERROR_INVALID_ARGUMENT; }
+    return nxg::generate_batched(assets, deformed, params, outputs, classic, count, config, workspace,
+                                 workspace_bytes, stream);
 }

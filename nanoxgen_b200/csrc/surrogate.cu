@@ -323,7 +323,7 @@ struct InferArgs {
     uint32_t seed, first;
     float description_id, patch_seed;
     float length_tolerance, width_tolerance;
-    uint32_t checks, mode;   // checks per tile; mode 0 checked, 1 exact, 2 unchecked
+    uint32_t checks, mode;   // checks per tile; mode 0 checked, 1 exact, 2 unchecked, 3 adaptive
     DeviceExpression length;
     DeviceExpression width;
 };
@@ -334,6 +334,9 @@ struct InferArgs {
 constexpr uint32_t kGuardBytes = 32768;
 constexpr uint32_t kInferSmem = kImgBytes + kRows * kK1 * 2 + kRows * kKh * 2 + 256 * 16 + 256 + 64 + kGuardBytes;
 constexpr uint32_t kInferTmemColumns = 64;
+// Adaptive judging: after a failed check a CTA serves this many batches
+// exactly before it tries the network again.
+constexpr uint32_t kAdaptiveSkip = 15;
 
 template <bool ROOTS>
 __global__ void __launch_bounds__(kRows) infer_kernel(const __grid_constant__ InferArgs k) {
@@ -365,6 +368,7 @@ __global__ void __launch_bounds__(kRows) infer_kernel(const __grid_constant__ In
     const bool random = k.length.uses_random || k.width.uses_random;
     uint32_t phase = 0;
     bool healthy = true;
+    uint32_t skip = 0;  // adaptive mode: batches left to serve exactly (uniform across the CTA)
     const uint32_t tiles = (k.count + kRows - 1) / kRows;
     for (uint32_t t = blockIdx.x; t < tiles && healthy; t += gridDim.x) {
         const uint32_t row = t * kRows + r;
@@ -381,7 +385,9 @@ __global__ void __launch_bounds__(kRows) infer_kernel(const __grid_constant__ In
             for (int j = 0; j < 8; ++j) { raw[j] = active ? k.features[8ull * row + j] : 0.0f; }
         }
         float y0 = 0.0f, y1 = 0.0f;
-        if (!ROOTS || k.mode != 1u) {
+        bool run_network = !ROOTS || k.mode != 1u;
+        if (ROOTS && k.mode == 3u && skip > 0u) { run_network = false; }
+        if (run_network) {
             store_input_row(x, r, raw, hd, active);
             for (uint32_t layer = 1; layer <= 4 && healthy; ++layer) {
                 publish_operands();
@@ -404,9 +410,11 @@ __global__ void __launch_bounds__(kRows) infer_kernel(const __grid_constant__ In
         }
         if constexpr (ROOTS) {
             // Spot check: `checks` rows of the tile against the exact runtime;
-            // any miss, or exact mode, re-runs the whole tile exactly.
-            bool exact_tile = k.mode == 1u;
-            if (!exact_tile && k.mode == 0u && k.checks > 0u) {
+            // any miss re-runs the whole tile exactly (as do exact mode and the
+            // adaptive mode's skipped batches).
+            bool exact_tile = !run_network;
+            const bool judged = k.mode == 0u || k.mode == 3u;
+            if (run_network && judged && k.checks > 0u) {
                 if (r == 0) { *fail_flag = 0u; }
                 __syncthreads();
                 const uint32_t stride = kRows / k.checks;
@@ -434,8 +442,9 @@ __global__ void __launch_bounds__(kRows) infer_kernel(const __grid_constant__ In
                         atomicAdd(k.status + 1, 1u);
                     }
                 }
-                if (r == 0 && k.mode == 0u) { atomicAdd(k.status + 2, 1u); }
+                if (r == 0 && run_network) { atomicAdd(k.status + 2, 1u); }
             }
+            if (k.mode == 3u) { skip = run_network ? (exact_tile ? kAdaptiveSkip : 0u) : skip - 1u; }
         }
         if (active) { k.out[row] = make_float2(y0, y1); }
     }
@@ -891,8 +900,9 @@ uint32_t nxg_surrogate_root_scalars(const void *model, const nxg_device_asset_de
         reinterpret_cast<std::uintptr_t>(device_status) % 4u != 0u) {
         return NXG_ERROR_MISALIGNED_OUTPUT;
     }
-    if (check->mode > 2u || check->checks_per_batch > 128u ||
-        (check->mode == 0u && (!(check->length_tolerance >= 0.0f) || !(check->width_tolerance >= 0.0f)))) {
+    const bool judged = check->mode == 0u || check->mode == 3u;
+    if (check->mode > 3u || check->checks_per_batch > 128u ||
+        (judged && (!(check->length_tolerance >= 0.0f) || !(check->width_tolerance >= 0.0f)))) {
         return NXG_ERROR_INVALID_ARGUMENT;
     }
     if ((e = nxg::check_launch_inputs(*asset, nullptr))) { return e; }

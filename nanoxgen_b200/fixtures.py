@@ -146,6 +146,23 @@ def large_sphere(strands: int = 1_000_000, cvs: int = 32, guides: int = 4096, se
     return Workload(name, AssetBuildInput(pos, tris, gs, None, uv), 8, params)
 
 
+# The Classic per-root expressions of the surrogate workload (SplinePrimitive
+# length and width; $v is the root's v texture coordinate).
+CLASSIC_LENGTH = "0.5*(1+0.4*noise($Prefg*6))*clamp(1-$v,0.2,1)"
+CLASSIC_WIDTH = "0.01*(1+0.3*noise($Prefg*20))"
+
+
+def classic_sphere(strands: int = 4_000_000, cvs: int = 24) -> Workload:
+    """Learned-expression workload: the large displaced sphere (200,000
+    triangles, 4,096 guides of 32 CVs, 8-guide stencils), 4,000,000 strands x
+    24 points, generator noise off (the reference's default), per-root length
+    and width from CLASSIC_LENGTH / CLASSIC_WIDTH."""
+    w = large_sphere(strands=strands, cvs=cvs)
+    params = w.params.copy(noise_amplitude=0.0)
+    name = "displaced-sphere-200k-tris/4096-guides/k8/%d-strands-x%d/classic-length-width" % (strands, cvs)
+    return Workload(name, w.build_input, w.stencil_slots, params)
+
+
 def reference_unit_fixture() -> AssetBuildInput:
     """The one-triangle, one-guide asset the reference's unit tests use
     (tests/test_main.cpp:39-53)."""

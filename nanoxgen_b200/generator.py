@@ -385,10 +385,26 @@ class BatchRunner:
     def points(self) -> int:
         return sum(int(p.strand_count) * int(p.cvs_per_strand) for p in self.params)
 
-    def run(self, block_size: int = 128, stream: Optional[torch.cuda.Stream] = None) -> None:
-        check(lib().nxg_generate_batched(self._assets, None, self._params, self._outs, len(self.dassets),
-                                         ctypes.byref(LaunchConfig(block_size)), self.workspace.data_ptr(),
-                                         self.workspace.numel(), _stream_handle(stream)), "nxg_generate_batched")
+    def run(self, block_size: int = 128, stream: Optional[torch.cuda.Stream] = None,
+            scalars: Optional[Sequence[Optional[torch.Tensor]]] = None, apply_length: bool = True,
+            apply_width: bool = True) -> None:
+        """One batched frame; with `scalars` (per description an (n, 2) Classic
+        (length scale, width) tensor or None) the Classic application is fused
+        into generation (nxg_generate_batched_classic)."""
+        cfg = ctypes.byref(LaunchConfig(block_size))
+        if scalars is None:
+            check(lib().nxg_generate_batched(self._assets, None, self._params, self._outs, len(self.dassets), cfg,
+                                             self.workspace.data_ptr(), self.workspace.numel(),
+                                             _stream_handle(stream)), "nxg_generate_batched")
+            return
+        classic = (_abi.ClassicApplyDesc * len(self.dassets))()
+        for i, t in enumerate(scalars):
+            if t is not None:
+                classic[i] = _abi.ClassicApplyDesc(t.data_ptr(), int(apply_length), int(apply_width))
+        check(lib().nxg_generate_batched_classic(self._assets, None, self._params, self._outs, classic,
+                                                 len(self.dassets), cfg, self.workspace.data_ptr(),
+                                                 self.workspace.numel(), _stream_handle(stream)),
+              "nxg_generate_batched_classic")
 
     def curves(self) -> list:
         return [PackedCurves(int(p.strand_count), int(p.cvs_per_strand), o[0], o[3], o[1], o[2])

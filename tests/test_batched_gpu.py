@@ -61,3 +61,37 @@ def test_batched_graph_replay_and_single_description_agreement(batch):
         single = generate_packed(d, w.params)
         torch.cuda.synchronize()
         assert max_position_error(single.points.cpu().numpy(), e.cpu().numpy()) <= 1e-5 * a.bbox_diagonal()
+
+
+def test_batched_classic_matches_single_description_classic(batch):
+    # nxg_generate_batched_classic with per-description Classic scalars (one
+    # description left without) against nxg_generate_packed_classic per
+    # description: identical drop decisions and point counts, positions and
+    # radii within 1e-5 of the bounding-box diagonal.
+    import torch
+
+    from nanoxgen_b200 import fixtures
+    from nanoxgen_b200.classic import Expression, ScalarPlan, generate_packed_classic, root_scalars
+    from nanoxgen_b200.generator import BatchRunner, generate_packed
+    b, assets, dassets = batch
+    plan = ScalarPlan(Expression.classic("hash($id) * 0.0005 + " + fixtures.CLASSIC_LENGTH, "length"),
+                      Expression.classic("hash($id, 3) * 0.0002 + 0.00005", "width"))
+    params = [w.params for w in b.workloads]
+    scalars = [root_scalars(d, p, plan)[0] for d, p in zip(dassets, params)]
+    scalars[2] = None
+    runner = BatchRunner(dassets, params)
+    runner.run(scalars=scalars)
+    torch.cuda.synchronize()
+    dropped = 0
+    for i, (c, d, p, a) in enumerate(zip(runner.curves(), dassets, params, assets)):
+        if scalars[i] is None:
+            single = generate_packed(d, p)
+        else:
+            single = generate_packed_classic(d, p, scalars[i])
+        torch.cuda.synchronize()
+        assert torch.equal(c.point_counts, single.point_counts), i
+        dropped += int((c.point_counts == 0).sum())
+        diag = a.bbox_diagonal()
+        assert max_position_error(c.points.cpu().numpy(), single.points.cpu().numpy()) <= 1e-5 * diag
+        assert float((c.points[:, 3] - single.points[:, 3]).abs().max()) <= 1e-5 * diag
+    assert dropped > 0
