@@ -174,10 +174,11 @@ typedef struct nxg_surrogate_train_config {
  * roots are evaluated by the exact runtime and, if any relative error
  * exceeds its tolerance (or the exact runtime fails there), every root of
  * the tile is re-run exactly.  mode 0 = checked surrogate, 1 = exact
- * runtime only, 2 = surrogate without checks, 3 = adaptive: as 0, but a
- * CTA whose check fails serves its next 15 batches exactly before it tries
- * the network again (a surrogate that misses the tolerance then costs a
- * sixteenth of its inference). */
+ * runtime only, 2 = surrogate without checks, 3 = adaptive: as 0 while the
+ * model is trusted; after a launch in which a check failed, the next launch
+ * runs the network (checked) on one batch in 16 and the exact kernel on the
+ * rest, and trust returns when those probes pass.  Adaptive launches update
+ * state in the model buffer, so they are ordered on one stream. */
 typedef struct nxg_surrogate_check {
     float length_tolerance;
     float width_tolerance;
@@ -221,7 +222,7 @@ uint32_t nxg_surrogate_forward(const void *model, const float *features, uint32_
  * device_status (4 x uint32, zeroed by the caller): [0] error code, [1]
  * roots whose exact evaluation failed, [2] batches re-run exactly, [3]
  * batches checked. */
-uint32_t nxg_surrogate_root_scalars(const void *model, const nxg_device_asset_desc *asset,
+uint32_t nxg_surrogate_root_scalars(void *model, const nxg_device_asset_desc *asset,
                                     const nxg_generation_params *params, const nxg_classic_scalar_plan *plan,
                                     const nxg_surrogate_check *check, uint32_t first_strand, uint32_t count,
                                     float *scalars, uint32_t *device_status, void *stream);

@@ -36,6 +36,8 @@ struct ScalarArgs {
     float patch_seed;
     float2 *out;
     uint32_t *status;
+    const uint32_t *distrust;  // surrogate split: skip the network's batches (see surrogate.cu)
+    uint32_t probe_period;
     DeviceExpression length;
     DeviceExpression width;
 };
@@ -46,7 +48,13 @@ __global__ void __launch_bounds__(256) classic_scalars_kernel(const __grid_const
     stage_classic_tables(table, perm);
     __syncthreads();
     const bool random = k.length.uses_random || k.width.uses_random;
+    // With a surrogate split, this kernel takes the 128-root batches the
+    // network does not: none while the model is trusted, else all but the
+    // probes (every probe_period-th batch).
+    const bool split = k.distrust != nullptr;
+    if (split && *k.distrust == 0u) { return; }
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < k.count; i += gridDim.x * blockDim.x) {
+        if (split && (i / 128u) % k.probe_period == 0u) { continue; }
         const uint32_t strand = k.first + i;
         const Root root = sample_root(k.a, k.f, k.seed, strand);
         const float face_seed = random ? classic_face_seed(k.description_id, k.patch_seed, root.triangle, perm) : 0.0f;
@@ -61,6 +69,45 @@ __global__ void __launch_bounds__(256) classic_scalars_kernel(const __grid_const
 }
 
 } // namespace dev
+} // namespace nxg
+
+namespace nxg {
+
+uint32_t launch_classic_root_scalars(const nxg_device_asset_desc &asset, const nxg_generation_params &params,
+                                     const nxg_classic_scalar_plan &plan, uint32_t first, uint32_t count,
+                                     float *scalars, uint32_t *status, cudaStream_t stream,
+                                     const uint32_t *distrust, uint32_t probe_period) {
+    dev::ScalarArgs k{};
+    uint32_t error = NXG_ERROR_NONE;
+    if (plan.length && (error = pack_device_expression(plan.length, k.length))) { return error; }
+    if (plan.width && (error = pack_device_expression(plan.width, k.width))) { return error; }
+    if (k.length.uses_clength || k.width.uses_clength) { return NXG_ERROR_EXPRESSION_INPUT; }
+    if (count == 0u) { return NXG_ERROR_NONE; }
+    const nxg_deformed_desc none{};
+    k.a = resolve_asset(asset);
+    k.f = resolve_frame(k.a, none);
+    k.seed = params.seed;
+    k.first = first;
+    k.count = count;
+    k.description_id = static_cast<float>(plan.description_id);
+    // xgen_runtime_face_seed keeps the patch name after its last ':'
+    const char *patch = plan.patch_name ? plan.patch_name : "";
+    for (const char *p = patch; *p; ++p) {
+        if (*p == ':') { patch = p + 1; }
+    }
+    k.patch_seed = static_cast<float>(nxg_xgen_string_seed(patch));
+    k.out = reinterpret_cast<float2 *>(scalars);
+    k.status = status;
+    k.distrust = distrust;
+    k.probe_period = probe_period;
+    set_last_cuda_error(0);
+    const uint32_t threads = 256u;
+    const uint32_t blocks = static_cast<uint32_t>(std::min<uint64_t>(
+        (uint64_t{count} + threads - 1u) / threads, static_cast<uint64_t>(device_sm_count()) * 8u));
+    dev::classic_scalars_kernel<<<blocks, threads, 0, stream>>>(k);
+    return record_cuda(cudaGetLastError());
+}
+
 } // namespace nxg
 
 extern "C" {
@@ -82,31 +129,8 @@ uint32_t nxg_classic_root_scalars(const nxg_device_asset_desc *asset, const nxg_
         return NXG_ERROR_MISALIGNED_OUTPUT;
     }
     if ((error = nxg::check_launch_inputs(*asset, nullptr)) != NXG_ERROR_NONE) { return error; }
-    nxg::dev::ScalarArgs k{};
-    if (plan->length && (error = nxg::pack_device_expression(plan->length, k.length))) { return error; }
-    if (plan->width && (error = nxg::pack_device_expression(plan->width, k.width))) { return error; }
-    if (k.length.uses_clength || k.width.uses_clength) { return NXG_ERROR_EXPRESSION_INPUT; }
-    if (strand_count == 0u) { return NXG_ERROR_NONE; }
-    k.a = nxg::resolve_asset(*asset);
-    k.f = nxg::resolve_frame(k.a, none);
-    k.seed = params->seed;
-    k.first = first_strand;
-    k.count = strand_count;
-    k.description_id = static_cast<float>(plan->description_id);
-    // xgen_runtime_face_seed keeps the patch name after its last ':'
-    const char *patch = plan->patch_name ? plan->patch_name : "";
-    for (const char *p = patch; *p; ++p) {
-        if (*p == ':') { patch = p + 1; }
-    }
-    k.patch_seed = static_cast<float>(nxg_xgen_string_seed(patch));
-    k.out = reinterpret_cast<float2 *>(scalars);
-    k.status = device_status;
-    nxg::set_last_cuda_error(0);
-    const uint32_t threads = 256u;
-    const uint32_t blocks = static_cast<uint32_t>(std::min<uint64_t>(
-        (uint64_t{strand_count} + threads - 1u) / threads, static_cast<uint64_t>(nxg::device_sm_count()) * 8u));
-    nxg::dev::classic_scalars_kernel<<<blocks, threads, 0, static_cast<cudaStream_t>(stream)>>>(k);
-    return nxg::record_cuda(cudaGetLastError());
+    return nxg::launch_classic_root_scalars(*asset, *params, *plan, first_strand, strand_count, scalars,
+                                            device_status, static_cast<cudaStream_t>(stream), nullptr, 0u);
 }
 
 uint32_t nxg_generate_packed_classic(const nxg_device_asset_desc *asset, const nxg_deformed_desc *deformed,

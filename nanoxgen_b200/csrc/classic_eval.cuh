@@ -9,6 +9,7 @@
 #pragma once
 
 #include "expression.h"
+#include "nxg_classic.h"
 #include "strand_math.cuh"
 
 #include <cuda_runtime.h>
@@ -303,4 +304,12 @@ __device__ inline bool classic_root_scalars(const DeviceExpression &length_progr
 }
 
 } // namespace dev
+
+// The exact per-root scalar kernel over strands [first, first + count)
+// (classic.cu).  With `distrust`, it skips the batches a surrogate launch
+// serves (see nxg_surrogate_root_scalars, adaptive mode).
+uint32_t launch_classic_root_scalars(const nxg_device_asset_desc &asset, const nxg_generation_params &params,
+                                     const nxg_classic_scalar_plan &plan, uint32_t first, uint32_t count,
+                                     float *scalars, uint32_t *status, cudaStream_t stream,
+                                     const uint32_t *distrust, uint32_t probe_period);
 } // namespace nxg

@@ -64,7 +64,9 @@ struct Header {
     float output_offset[2];
     float output_scale[2];
     uint32_t initialised, trained;
-    uint32_t reserved[38];
+    uint32_t distrust;  // adaptive judging: the last launch's probed batches failed
+    uint32_t failed;    // set by the current launch's failed checks
+    uint32_t reserved[36];
 };
 static_assert(sizeof(Header) == 256, "model header");
 
@@ -328,15 +330,12 @@ struct InferArgs {
     DeviceExpression width;
 };
 
-// Shared memory ends with a guard band as large as the furthest any operand
-// descriptor of the last tile could reach with its two byte offsets
-// exchanged, so every product stays inside the CTA's allocation.
-constexpr uint32_t kGuardBytes = 32768;
-constexpr uint32_t kInferSmem = kImgBytes + kRows * kK1 * 2 + kRows * kKh * 2 + 256 * 16 + 256 + 64 + kGuardBytes;
+constexpr uint32_t kInferSmem = kImgBytes + kRows * kK1 * 2 + kRows * kKh * 2 + 256 * 16 + 256 + 64;
 constexpr uint32_t kInferTmemColumns = 64;
-// Adaptive judging: after a failed check a CTA serves this many batches
-// exactly before it tries the network again.
-constexpr uint32_t kAdaptiveSkip = 15;
+// Adaptive judging: while the model is distrusted (its last launch's probed
+// batches failed), the network serves one batch in this many -- the probes --
+// and the exact kernel the rest.
+constexpr uint32_t kProbePeriod = 16;
 
 template <bool ROOTS>
 __global__ void __launch_bounds__(kRows) infer_kernel(const __grid_constant__ InferArgs k) {
@@ -368,9 +367,11 @@ __global__ void __launch_bounds__(kRows) infer_kernel(const __grid_constant__ In
     const bool random = k.length.uses_random || k.width.uses_random;
     uint32_t phase = 0;
     bool healthy = true;
-    uint32_t skip = 0;  // adaptive mode: batches left to serve exactly (uniform across the CTA)
+    const bool adaptive = ROOTS && k.mode == 3u;
+    const bool distrusted = adaptive && hd.distrust != 0u;
     const uint32_t tiles = (k.count + kRows - 1) / kRows;
     for (uint32_t t = blockIdx.x; t < tiles && healthy; t += gridDim.x) {
+        if (distrusted && t % kProbePeriod != 0u) { continue; }  // the exact kernel's batch
         const uint32_t row = t * kRows + r;
         const bool active = row < k.count;
         dev::Root root{};
@@ -385,8 +386,7 @@ __global__ void __launch_bounds__(kRows) infer_kernel(const __grid_constant__ In
             for (int j = 0; j < 8; ++j) { raw[j] = active ? k.features[8ull * row + j] : 0.0f; }
         }
         float y0 = 0.0f, y1 = 0.0f;
-        bool run_network = !ROOTS || k.mode != 1u;
-        if (ROOTS && k.mode == 3u && skip > 0u) { run_network = false; }
+        const bool run_network = !ROOTS || k.mode != 1u;
         if (run_network) {
             store_input_row(x, r, raw, hd, active);
             for (uint32_t layer = 1; layer <= 4 && healthy; ++layer) {
@@ -410,8 +410,7 @@ __global__ void __launch_bounds__(kRows) infer_kernel(const __grid_constant__ In
         }
         if constexpr (ROOTS) {
             // Spot check: `checks` rows of the tile against the exact runtime;
-            // any miss re-runs the whole tile exactly (as do exact mode and the
-            // adaptive mode's skipped batches).
+            // any miss re-runs the whole tile exactly.
             bool exact_tile = !run_network;
             const bool judged = k.mode == 0u || k.mode == 3u;
             if (run_network && judged && k.checks > 0u) {
@@ -431,7 +430,10 @@ __global__ void __launch_bounds__(kRows) infer_kernel(const __grid_constant__ In
                 }
                 __syncthreads();
                 exact_tile = *fail_flag != 0u;
-                if (r == 0) { atomicAdd(k.status + 3, 1u); }
+                if (r == 0) {
+                    atomicAdd(k.status + 3, 1u);
+                    if (adaptive && exact_tile) { atomicOr(&const_cast<Header &>(hd).failed, 1u); }
+                }
             }
             if (exact_tile) {
                 if (active) {
@@ -444,7 +446,6 @@ __global__ void __launch_bounds__(kRows) infer_kernel(const __grid_constant__ In
                 }
                 if (r == 0 && run_network) { atomicAdd(k.status + 2, 1u); }
             }
-            if (k.mode == 3u) { skip = run_network ? (exact_tile ? kAdaptiveSkip : 0u) : skip - 1u; }
         }
         if (active) { k.out[row] = make_float2(y0, y1); }
     }
@@ -456,6 +457,14 @@ __global__ void __launch_bounds__(kRows) infer_kernel(const __grid_constant__ In
         umma::fence_after_sync();
         umma::tmem_free(tmem, kInferTmemColumns);
     }
+}
+
+// Adaptive judging's state after a launch: the next launch distrusts the
+// model exactly when one of this launch's checks failed.
+__global__ void trust_update_kernel(unsigned char *model) {
+    Header *h = reinterpret_cast<Header *>(model);
+    h->distrust = h->failed;
+    h->failed = 0u;
 }
 
 // --------------------------------------------------------------- training
@@ -473,7 +482,7 @@ struct TrainArgs {
     uint32_t *status;
 };
 
-constexpr uint32_t kTrainSmem = kImgBytes + kRows * kK1 * 2 + 3 * kRows * kKh * 2 + 2 * kRows * kRows * 2 + 64 + kGuardBytes;
+constexpr uint32_t kTrainSmem = kImgBytes + kRows * kK1 * 2 + 3 * kRows * kKh * 2 + 2 * kRows * kRows * 2 + 64;
 static_assert(kTrainSmem <= 227u * 1024u, "training tiles fit one CTA");
 constexpr uint32_t kTrainTmemColumns = 512;
 // TMEM columns: working product | dW1 | dW2 | dW3 | dW4
@@ -883,7 +892,7 @@ uint32_t nxg_surrogate_train(void *model, const float *features, const float *ta
     return device_status;
 }
 
-uint32_t nxg_surrogate_root_scalars(const void *model, const nxg_device_asset_desc *asset,
+uint32_t nxg_surrogate_root_scalars(void *model, const nxg_device_asset_desc *asset,
                                     const nxg_generation_params *params, const nxg_classic_scalar_plan *plan,
                                     const nxg_surrogate_check *check, uint32_t first_strand, uint32_t count,
                                     float *scalars, uint32_t *device_status, void *stream) {
@@ -932,9 +941,21 @@ uint32_t nxg_surrogate_root_scalars(const void *model, const nxg_device_asset_de
     nxg::set_last_cuda_error(0);
     const void *fn = reinterpret_cast<const void *>(nxg::surrogate::infer_kernel<true>);
     if ((e = configure_smem(fn, nxg::surrogate::kInferSmem))) { return e; }
+    const auto s = static_cast<cudaStream_t>(stream);
     const uint32_t tiles = (count + 127u) / 128u;
     const uint32_t blocks = std::min<uint32_t>(tiles, static_cast<uint32_t>(nxg::device_sm_count()) * 4u);
-    nxg::surrogate::infer_kernel<true><<<blocks, 128, nxg::surrogate::kInferSmem, static_cast<cudaStream_t>(stream)>>>(k);
+    nxg::surrogate::infer_kernel<true><<<blocks, 128, nxg::surrogate::kInferSmem, s>>>(k);
+    if ((e = launch_status(cudaGetLastError())) || check->mode != 3u) { return e; }
+    // Adaptive: the exact kernel serves the batches the network did not
+    // (all but the probes while the model is distrusted), then the model's
+    // trust follows this launch's probes.
+    auto *bytes = static_cast<unsigned char *>(model);
+    const auto *distrust = reinterpret_cast<const uint32_t *>(bytes + offsetof(Header, distrust));
+    if ((e = nxg::launch_classic_root_scalars(*asset, *params, *plan, first_strand, count, scalars, device_status, s,
+                                              distrust, nxg::surrogate::kProbePeriod))) {
+        return e;
+    }
+    nxg::surrogate::trust_update_kernel<<<1, 1, 0, s>>>(bytes);
     return launch_status(cudaGetLastError());
 }
 

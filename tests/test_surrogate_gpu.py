@@ -157,3 +157,24 @@ def test_fully_checked_batches_stay_within_tolerance(sphere):
               % (tol, st[2], st[3], rel[:, 0].max(), rel[:, 1].max()))
         assert st[0] == 0 and st[3] == (20000 + 127) // 128
         assert rel.max() <= tol * (1 + 1e-6)
+
+
+def test_adaptive_judge_routes_distrusted_batches_to_the_exact_kernel(sphere):
+    # A freshly initialised network misses 1e-3 everywhere.  The first
+    # adaptive launch checks every batch and re-runs each exactly; the next
+    # launch probes one batch in 16 with the network and leaves the rest to
+    # the exact kernel.  Both return the exact runtime's values bit for bit.
+    import torch
+    from nanoxgen_b200.classic import root_scalars
+    w, _, dasset = sphere
+    m = _model(sphere, seed=13)
+    params = _params(w, 30000)
+    exact, _ = root_scalars(dasset, params, _plan())
+    tiles = (30000 + 127) // 128
+    for launch, checked in ((1, tiles), (2, (tiles + 15) // 16), (3, (tiles + 15) // 16)):
+        got, status = m.root_scalars(dasset, params, _plan(), checks_per_batch=4, mode=3)
+        torch.cuda.synchronize()
+        st = status.cpu().tolist()
+        assert st == [0, 0, checked, checked], (launch, st)
+        np.testing.assert_array_equal(got[:30000].cpu().numpy().view(np.uint32),
+                                      exact[:30000].cpu().numpy().view(np.uint32))
