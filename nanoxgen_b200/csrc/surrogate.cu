@@ -370,8 +370,12 @@ __global__ void __launch_bounds__(kRows) infer_kernel(const __grid_constant__ In
     const bool adaptive = ROOTS && k.mode == 3u;
     const bool distrusted = adaptive && hd.distrust != 0u;
     const uint32_t tiles = (k.count + kRows - 1) / kRows;
-    for (uint32_t t = blockIdx.x; t < tiles && healthy; t += gridDim.x) {
-        if (distrusted && t % kProbePeriod != 0u) { continue; }  // the exact kernel's batch
+    // A distrusted model runs only the probe batches (every kProbePeriod-th),
+    // spread over the CTAs; the exact kernel takes the rest.
+    const uint32_t step = distrusted ? kProbePeriod : 1u;
+    const uint32_t units = (tiles + step - 1u) / step;
+    for (uint32_t u = blockIdx.x; u < units && healthy; u += gridDim.x) {
+        const uint32_t t = u * step;
         const uint32_t row = t * kRows + r;
         const bool active = row < k.count;
         dev::Root root{};
