@@ -30,7 +30,7 @@ CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-ffp-contract=off", "-Wall", "-Wextr
 CUDA_SOURCES = ["generate.cu", "batched.cu", "classic.cu", "surrogate.cu"]
 HOST_SOURCES = ["host.cpp", "expression.cpp"]
 HEADERS = ["nxg_internal.h", "strand_math.cuh", "generator_core.cuh", "seexpr_gradients.inc", "expression.h",
-           "seexpr_permutation.inc", "classic_eval.cuh", "umma.cuh"]
+           "seexpr_permutation.inc", "classic_eval.cuh", "umma.cuh", "walk.cuh"]
 
 
 def _stale(target: str, deps: list[str]) -> bool:

@@ -21,6 +21,7 @@
 // Strands longer than 128 CVs take a serial per-thread kernel that walks the
 // reference's cursor directly.
 #include "generator_core.cuh"
+#include "walk.cuh"
 #include "nxg_internal.h"
 #include "strand_math.cuh"
 
@@ -88,6 +89,67 @@ __global__ void generate_kernel(LaunchArgs g, const float4 *offsets) {
             emit_strand<L, PPT, NOISE, CLASSIC>(g, rec, static_cast<int>(r) + group, gl, table, offsets, tvals, stage,
                                        lattice, kLatticeMax);
         }
+        __syncwarp();
+    }
+}
+
+// Strands of 2..32 CVs: the lane-walk generator (walk.cuh).  Persistent CTAs
+// over contiguous ranges of the strand order; each warp takes 32 strands at a
+// time through setup (which also writes the roots, root UVs and point
+// counts), base, frame (with noise) and store.
+template <bool NOISE, bool CLASSIC>
+__global__ void __launch_bounds__(256, 1) generate_walk_kernel(LaunchArgs g, const float4 *offsets) {
+    extern __shared__ float4 smem[];
+    const int P = static_cast<int>(g.p.cvs_per_strand);
+    const int warps = blockDim.x >> 5;
+    float4 *table = smem;
+    float *tvals = reinterpret_cast<float *>(reinterpret_cast<unsigned char *>(smem) +
+                                             (NOISE ? sizeof(float4) * kTableFloat4 : 0u));
+    float *rvals = tvals + kWalkMaxCvs;
+    unsigned char *warp_base = reinterpret_cast<unsigned char *>(rvals + kWalkMaxCvs);
+    if constexpr (NOISE) {
+        for (int i = threadIdx.x; i < kTableFloat4; i += blockDim.x) {
+            table[i] = make_float4(__ldg(g.a.gradients + 3 * i), __ldg(g.a.gradients + 3 * i + 1),
+                                   __ldg(g.a.gradients + 3 * i + 2), 0.0f);
+        }
+    }
+    for (int i = threadIdx.x; i < P; i += blockDim.x) {  // t = cv / (P - 1) (generate.h:295-298)
+        tvals[i] = __fdiv_rn(static_cast<float>(i), static_cast<float>(P - 1));
+        rvals[i] = strand_radius(g.p, tvals[i]);
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    unsigned char *mine = warp_base + walk_warp_bytes(NOISE) * warp;
+    float4 *stage = reinterpret_cast<float4 *>(mine);
+    float4 *records = reinterpret_cast<float4 *>(mine + kWalkStageBytes);
+    float2 *lattice = reinterpret_cast<float2 *>(mine + kWalkStageBytes);
+    uint32_t *locals = reinterpret_cast<uint32_t *>(mine + walk_warp_bytes(NOISE) - kWalkLocalBytes);
+    const float inv_p = 1.0f / static_cast<float>(P);
+    const uint32_t begin = static_cast<uint32_t>(static_cast<uint64_t>(blockIdx.x) * g.count / gridDim.x);
+    const uint32_t end = static_cast<uint32_t>(static_cast<uint64_t>(blockIdx.x + 1u) * g.count / gridDim.x);
+    for (uint32_t batch = begin + static_cast<uint32_t>(warp) * 32u; batch < end;
+         batch += static_cast<uint32_t>(warps) * 32u) {
+        const uint32_t item = batch + static_cast<uint32_t>(lane);
+        const bool valid = item < end;
+        const int in_batch = static_cast<int>(min(32u, end - batch));
+        uint32_t *root_words = reinterpret_cast<uint32_t *>(stage);  // the stage is free until the base step
+        const WalkRoot wr = walk_setup<NOISE>(g, records, locals, root_words, lane, valid ? item : batch, valid,
+                                              static_cast<uint32_t>(P));
+        __syncwarp();
+        if (g.roots) {
+            walk_store_roots(g, root_words, locals, lane, in_batch);
+            __syncwarp();
+        }
+        walk_base(g, records, stage, tvals, rvals, offsets, lane, in_batch, P, inv_p);
+        __syncwarp();
+        if constexpr (NOISE) {
+            if (lane < in_batch) {
+                walk_frame(g.p, wr, stage + lane * kWalkStride, lattice + lane, tvals, rvals, table, P);
+            }
+            __syncwarp();
+        }
+        walk_store<CLASSIC>(g, stage, locals, lane, in_batch, P, inv_p);
         __syncwarp();
     }
 }
@@ -592,19 +654,27 @@ KernelFn pick_lanes(int lanes, bool noise, bool classic) {
 std::atomic<uint32_t> g_tiles[kMaxParallelCvs + 1][2];
 
 bool valid_tile(uint32_t P, uint32_t lanes, uint32_t ppt) {
+    if (lanes == 1u) { return ppt == 1u && P >= 2u && P <= static_cast<uint32_t>(dev::kWalkMaxCvs); }
     const bool lanes_ok = lanes == 2u || lanes == 4u || lanes == 8u || lanes == 16u || lanes == 32u;
     const bool ppt_ok = ppt == 1u || ppt == 2u || ppt == 4u;
     return lanes_ok && ppt_ok && lanes * ppt >= P && P >= 2u && P <= kMaxParallelCvs;
 }
 
-// Tile shape for P CVs: the registered one, else four CVs per lane on the
-// narrowest power-of-two group that holds the strand.
+// Tile shape for P CVs: the registered one, else the lane-walk generator for
+// 2..32 CVs (lanes_per_strand 1, 128-thread CTAs), else four CVs per lane on
+// the narrowest power-of-two group that holds the strand.
 void default_tile(uint32_t P, bool noise, int *lanes, int *ppt, uint32_t *block) {
     const uint32_t packed = P <= kMaxParallelCvs ? g_tiles[P][noise ? 1 : 0].load(std::memory_order_relaxed) : 0u;
     if (packed) {
         *lanes = static_cast<int>(packed & 0xffu);
         *ppt = static_cast<int>((packed >> 8) & 0xffu);
         *block = ((packed >> 16) & 0xffu) * 32u;
+        return;
+    }
+    if (P >= 2u && P <= static_cast<uint32_t>(dev::kWalkMaxCvs)) {  // the lane-walk generator
+        *lanes = 1;
+        *ppt = 1;
+        *block = 128u;
         return;
     }
     *ppt = 4;
@@ -615,6 +685,10 @@ void default_tile(uint32_t P, bool noise, int *lanes, int *ppt, uint32_t *block)
 }
 
 KernelFn pick_kernel(int lanes, int ppt, bool noise, bool classic) {
+    if (lanes == 1) {
+        if (classic) { return noise ? dev::generate_walk_kernel<true, true> : dev::generate_walk_kernel<false, true>; }
+        return noise ? dev::generate_walk_kernel<true, false> : dev::generate_walk_kernel<false, false>;
+    }
     switch (ppt) {
         case 1: return pick_lanes<1>(lanes, noise, classic);
         case 2: return pick_lanes<2>(lanes, noise, classic);
@@ -623,6 +697,7 @@ KernelFn pick_kernel(int lanes, int ppt, bool noise, bool classic) {
 }
 
 size_t generate_smem_bytes(uint32_t P, int lanes, int ppt, bool noise, uint32_t warps) {
+    if (lanes == 1) { return dev::walk_head_bytes(noise) + dev::walk_warp_bytes(noise) * warps; }
     const size_t per_warp = sizeof(uint32_t) * dev::kRecFields * 32u + sizeof(float4) * 32u / lanes * lanes * ppt +
                             (noise ? sizeof(float2) * 384u : 0u);
     return sizeof(float4) * dev::kTableFloat4 + sizeof(float) * ((P + 3u) & ~3u) + per_warp * warps;
@@ -729,7 +804,11 @@ uint32_t launch_generate(const nxg_device_asset_desc &asset, const nxg_deformed_
         dev::guide_offsets_kernel<<<blocks, threads, 0, stream>>>(g.a, g.f, P, offsets);
         if ((status = record_cuda(cudaGetLastError()))) { return status; }
     }
-    if (g.roots || g.root_uvs || g.point_counts) {
+    int lanes = 32, ppt = 4;
+    uint32_t tile_block = 0u;
+    const bool noise = g.p.noise != 0u;
+    default_tile(P, noise, &lanes, &ppt, &tile_block);
+    if (lanes != 1 && (g.roots || g.root_uvs || g.point_counts)) {  // the lane-walk kernel writes its own
         const uint32_t threads = 256u;
         const uint32_t per_block = threads;  // one strand per thread
         const uint32_t blocks = static_cast<uint32_t>(std::min<uint64_t>((count + per_block - 1u) / per_block,
@@ -737,10 +816,6 @@ uint32_t launch_generate(const nxg_device_asset_desc &asset, const nxg_deformed_
         dev::strand_roots_kernel<<<blocks, threads, 0, stream>>>(g);
         if ((status = record_cuda(cudaGetLastError()))) { return status; }
     }
-    int lanes = 32, ppt = 4;
-    uint32_t tile_block = 0u;
-    const bool noise = g.p.noise != 0u;
-    default_tile(P, noise, &lanes, &ppt, &tile_block);
     KernelFn fn = pick_kernel(lanes, ppt, noise, g.scalars != nullptr);
     // block_size in [1, 1024] is a request: rounded up to whole warps, then
     // capped at what this kernel's register footprint can launch.
@@ -972,7 +1047,7 @@ uint32_t nxg_autotune_packed(const nxg_device_asset_desc *asset, const nxg_defor
     float winner_ms = 0.0f;
     const uint32_t reps = std::max(1u, repeats);
     const uint32_t blocks[3] = {64u, 128u, 256u};
-    for (uint32_t lanes = 2u; lanes <= 32u && !error; lanes *= 2u) {
+    for (uint32_t lanes = 1u; lanes <= 32u && !error; lanes *= 2u) {
         for (uint32_t ppt = 1u; ppt <= 4u && !error; ppt *= 2u) {
             // tiles that hold the strand without idling half of their lanes
             if (!nxg::valid_tile(P, lanes, ppt) || (lanes > 2u && lanes * ppt >= 2u * P)) { continue; }

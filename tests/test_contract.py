@@ -257,7 +257,13 @@ def test_tile_registry(nxg_lib):
     from nanoxgen_b200._abi import Tile
     L = lib()
     t = Tile()
-    assert L.nxg_get_tile(32, 1, ctypes.byref(t)) == 0 and t.lanes_per_strand * t.cvs_per_lane >= 32
+    # built-in choice for 2..32 CVs: the lane-walk generator (one lane per strand)
+    assert L.nxg_get_tile(32, 1, ctypes.byref(t)) == 0
+    assert (t.lanes_per_strand, t.cvs_per_lane, t.block_size) == (1, 1, 128)
+    assert L.nxg_get_tile(64, 1, ctypes.byref(t)) == 0 and t.lanes_per_strand * t.cvs_per_lane >= 64
+    assert L.nxg_set_tile(32, 1, ctypes.byref(Tile(1, 1, 256))) == 0
+    assert L.nxg_set_tile(33, 1, ctypes.byref(Tile(1, 1, 256))) == ERRORS["InvalidArgument"]
+    assert L.nxg_set_tile(32, 1, ctypes.byref(Tile(1, 2, 256))) == ERRORS["InvalidArgument"]
     assert L.nxg_set_tile(32, 1, ctypes.byref(Tile(16, 2, 256))) == 0
     assert L.nxg_get_tile(32, 1, ctypes.byref(t)) == 0
     assert (t.lanes_per_strand, t.cvs_per_lane, t.block_size) == (16, 2, 256)
@@ -266,4 +272,4 @@ def test_tile_registry(nxg_lib):
         assert L.nxg_set_tile(32, 1, ctypes.byref(bad)) == ERRORS["InvalidArgument"]
     assert L.nxg_set_tile(200, 1, ctypes.byref(Tile(32, 4, 128))) == ERRORS["InvalidArgument"]
     assert L.nxg_set_tile(32, 1, None) == 0
-    assert L.nxg_get_tile(32, 1, ctypes.byref(t)) == 0 and t.block_size == 0
+    assert L.nxg_get_tile(32, 1, ctypes.byref(t)) == 0 and t.lanes_per_strand == 1

@@ -265,12 +265,12 @@ def test_every_tile_matches_oracle_and_autotuner(torch_cuda, oracle, sphere):
     theirs = oracle.generate(asset.buffer, w.params, threads=8)
     P = w.params.cvs_per_strand
     try:
-        for lanes, ppt in ((4, 4), (8, 2), (8, 4), (16, 1), (16, 2), (32, 1)):
+        for lanes, ppt in ((1, 1), (4, 4), (8, 2), (8, 4), (16, 1), (16, 2), (32, 1)):
             set_tile(P, True, lanes, ppt, 128)
             _compare(asset, w.params, _gen(torch_cuda, d, w.params), theirs)
         pts, *_ = allocate_outputs(w.params.strand_count, P, "cuda")
         (lanes, ppt, block), ms = autotune(d, w.params, pts, repeats=2)
-        assert lanes * ppt >= P and ms > 0.0
+        assert (lanes == 1 or lanes * ppt >= P) and ms > 0.0
         assert get_tile(P, True) == (lanes, ppt, block)
         _compare(asset, w.params, _gen(torch_cuda, d, w.params), theirs)
     finally:
