@@ -383,7 +383,12 @@ uint32_t nxg_generate_packed_ordered(const nxg_device_asset_desc *asset,
 /* Tile of the warp-parallel generator: a group of `lanes_per_strand` lanes
  * (2, 4, 8, 16 or 32) owns one strand, each lane `cvs_per_lane` consecutive
  * CVs (1, 2 or 4; lanes * cvs <= 128 and >= the strand's CVs); a CTA has
- * `block_size` threads (0: take nxg_launch_config::block_size). */
+ * `block_size` threads (0: take nxg_launch_config::block_size).
+ * lanes_per_strand 1 (with cvs_per_lane 1, strands of 2..32 CVs) selects the
+ * lane-walk generator: base curve and stores lane-parallel, one lane walking
+ * each strand's noise frame; with noise and block_size 64 (or below) its
+ * CTAs are producer/consumer warp pairs.  It is the built-in choice for
+ * 2..32 CVs. */
 typedef struct nxg_tile {
     uint32_t lanes_per_strand;
     uint32_t cvs_per_lane;
@@ -464,7 +469,7 @@ uint32_t nxg_generate_batched(const nxg_device_asset_desc *assets, const nxg_def
  * nxg_generate_packed; returns NXG_ERROR_STATIC_SCRATCH_LIMIT, before
  * touching the device, when nxg_packed_workspace_size for the request
  * exceeds NXG_STATIC_SCRATCH_BYTES (for a 4,096-guide description at 32
- * CVs, about 260,000 strands fit and a million do not).  Allocates
+ * CVs, about 240,000 strands fit and a million do not).  Allocates
  * nothing.  The first call on each device looks up the scratch's device
  * address (once per device), so make that first call before any stream
  * capture.  Every call shares the one scratch: calls that can overlap on

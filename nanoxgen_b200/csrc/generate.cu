@@ -94,20 +94,25 @@ __global__ void generate_kernel(LaunchArgs g, const float4 *offsets) {
 }
 
 // Strands of 2..32 CVs: the lane-walk generator (walk.cuh).  Persistent CTAs
-// over contiguous ranges of the strand order; each warp takes 32 strands at a
-// time through setup (which also writes the roots, root UVs and point
-// counts), base, frame (with noise) and store.
+// over contiguous ranges of the strand order positions [range_begin,
+// range_end); each warp takes 32 strands at a time through setup (which also
+// writes the roots, root UVs and point counts), base, frame (with noise) and
+// store.  Without noise or Classic scalars the base step writes the output
+// directly (no stage); with noise and no scalars this kernel runs without
+// noise and frame_walk_kernel adds it.
 template <bool NOISE, bool CLASSIC>
 __global__ void __launch_bounds__(256, 1) generate_walk_kernel(LaunchArgs g, const float4 *offsets) {
+    constexpr bool kStaged = NOISE || CLASSIC;
+    constexpr bool kWalk = NOISE;  // noise walk inside this kernel
     extern __shared__ float4 smem[];
     const int P = static_cast<int>(g.p.cvs_per_strand);
     const int warps = blockDim.x >> 5;
     float4 *table = smem;
-    float *tvals = reinterpret_cast<float *>(reinterpret_cast<unsigned char *>(smem) +
-                                             (NOISE ? sizeof(float4) * kTableFloat4 : 0u));
+    float *tvals = reinterpret_cast<float *>(reinterpret_cast<unsigned char *>(smem) + walk_head_bytes(kWalk) -
+                                             2u * sizeof(float) * kWalkMaxCvs);
     float *rvals = tvals + kWalkMaxCvs;
     unsigned char *warp_base = reinterpret_cast<unsigned char *>(rvals + kWalkMaxCvs);
-    if constexpr (NOISE) {
+    if constexpr (kWalk) {
         for (int i = threadIdx.x; i < kTableFloat4; i += blockDim.x) {
             table[i] = make_float4(__ldg(g.a.gradients + 3 * i), __ldg(g.a.gradients + 3 * i + 1),
                                    __ldg(g.a.gradients + 3 * i + 2), 0.0f);
@@ -120,20 +125,23 @@ __global__ void __launch_bounds__(256, 1) generate_walk_kernel(LaunchArgs g, con
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    unsigned char *mine = warp_base + walk_warp_bytes(NOISE) * warp;
-    float4 *stage = reinterpret_cast<float4 *>(mine);
-    float4 *records = reinterpret_cast<float4 *>(mine + kWalkStageBytes);
+    constexpr size_t kWarpBytes = walk_warp_bytes(kWalk, kStaged);
+    unsigned char *mine = warp_base + kWarpBytes * warp;
+    float4 *stage = reinterpret_cast<float4 *>(mine);  // staged variants only
+    float4 *records = reinterpret_cast<float4 *>(kStaged ? mine + kWalkStageBytes : mine);
     float2 *lattice = reinterpret_cast<float2 *>(mine + kWalkStageBytes);
-    uint32_t *locals = reinterpret_cast<uint32_t *>(mine + walk_warp_bytes(NOISE) - kWalkLocalBytes);
+    uint32_t *root_words = reinterpret_cast<uint32_t *>(kStaged ? mine : mine + kWalkRecordBytes);
+    uint32_t *locals = reinterpret_cast<uint32_t *>(mine + kWarpBytes - kWalkLocalBytes);
     const float inv_p = 1.0f / static_cast<float>(P);
-    const uint32_t begin = static_cast<uint32_t>(static_cast<uint64_t>(blockIdx.x) * g.count / gridDim.x);
-    const uint32_t end = static_cast<uint32_t>(static_cast<uint64_t>(blockIdx.x + 1u) * g.count / gridDim.x);
+    const uint32_t span = g.range_end - g.range_begin;
+    const uint32_t begin = g.range_begin + static_cast<uint32_t>(static_cast<uint64_t>(blockIdx.x) * span / gridDim.x);
+    const uint32_t end =
+        g.range_begin + static_cast<uint32_t>(static_cast<uint64_t>(blockIdx.x + 1u) * span / gridDim.x);
     for (uint32_t batch = begin + static_cast<uint32_t>(warp) * 32u; batch < end;
          batch += static_cast<uint32_t>(warps) * 32u) {
         const uint32_t item = batch + static_cast<uint32_t>(lane);
         const bool valid = item < end;
         const int in_batch = static_cast<int>(min(32u, end - batch));
-        uint32_t *root_words = reinterpret_cast<uint32_t *>(stage);  // the stage is free until the base step
         const WalkRoot wr = walk_setup<NOISE>(g, records, locals, root_words, lane, valid ? item : batch, valid,
                                               static_cast<uint32_t>(P));
         __syncwarp();
@@ -141,16 +149,106 @@ __global__ void __launch_bounds__(256, 1) generate_walk_kernel(LaunchArgs g, con
             walk_store_roots(g, root_words, locals, lane, in_batch);
             __syncwarp();
         }
-        walk_base(g, records, stage, tvals, rvals, offsets, lane, in_batch, P, inv_p);
+        walk_base<!kStaged>(g, records, stage, locals, tvals, rvals, offsets, lane, in_batch, P, inv_p);
         __syncwarp();
-        if constexpr (NOISE) {
-            if (lane < in_batch) {
-                walk_frame(g.p, wr, stage + lane * kWalkStride, lattice + lane, tvals, rvals, table, P);
-            }
+        if constexpr (kWalk) {
+            walk_frame(g.p, wr, lane < in_batch, stage + lane * kWalkStride, lattice + lane, tvals, rvals, table, P);
             __syncwarp();
         }
-        walk_store<CLASSIC>(g, stage, locals, lane, in_batch, P, inv_p);
-        __syncwarp();
+        if constexpr (kStaged) {
+            walk_store<CLASSIC>(g, stage, locals, lane, in_batch, P, inv_p);
+            __syncwarp();
+        }
+    }
+}
+
+// Noise on strands of 2..32 CVs without Classic scalars: one producer warp
+// and one consumer warp per 64-thread CTA over the CTA's contiguous range of
+// the strand order, sharing two stage buffers.  The producer runs setup and
+// base (the latency-bound gathers) into one buffer while the consumer runs
+// the noise frame and the stores (the arithmetic) from the other; hardware
+// named barriers hand the buffers over (1, 2: buffer full; 3, 4: buffer
+// empty).  Both warps step through the same batches, so every bar.sync has
+// its matching arrivals.
+__device__ __forceinline__ void named_sync(uint32_t id) { asm volatile("bar.sync %0, 64;" ::"r"(id) : "memory"); }
+__device__ __forceinline__ void named_arrive(uint32_t id) {
+    __threadfence_block();  // this warp's shared-memory reads and writes are done before the other warp proceeds
+    asm volatile("bar.arrive %0, 64;" ::"r"(id) : "memory");
+}
+
+__global__ void __launch_bounds__(64, 1) generate_pipe_kernel(LaunchArgs g, const float4 *offsets) {
+    extern __shared__ float4 smem[];
+    const int P = static_cast<int>(g.p.cvs_per_strand);
+    float4 *table = smem;
+    float *tvals = reinterpret_cast<float *>(smem + kTableFloat4);
+    float *rvals = tvals + kWalkMaxCvs;
+    unsigned char *base = reinterpret_cast<unsigned char *>(rvals + kWalkMaxCvs);
+    for (int i = threadIdx.x; i < kTableFloat4; i += blockDim.x) {
+        table[i] = make_float4(__ldg(g.a.gradients + 3 * i), __ldg(g.a.gradients + 3 * i + 1),
+                               __ldg(g.a.gradients + 3 * i + 2), 0.0f);
+    }
+    for (int i = threadIdx.x; i < P; i += blockDim.x) {  // t = cv / (P - 1) (generate.h:295-298)
+        tvals[i] = __fdiv_rn(static_cast<float>(i), static_cast<float>(P - 1));
+        rvals[i] = strand_radius(g.p, tvals[i]);
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const bool producer = threadIdx.x < 32;
+    unsigned char *tail = base + 2 * kPipeBufferBytes;
+    float4 *records = reinterpret_cast<float4 *>(tail);                    // producer
+    float2 *lattice = reinterpret_cast<float2 *>(tail + kWalkRecordBytes);  // consumer
+    const float inv_p = 1.0f / static_cast<float>(P);
+    const uint32_t span = g.range_end - g.range_begin;
+    const uint32_t begin = g.range_begin + static_cast<uint32_t>(static_cast<uint64_t>(blockIdx.x) * span / gridDim.x);
+    const uint32_t end =
+        g.range_begin + static_cast<uint32_t>(static_cast<uint64_t>(blockIdx.x + 1u) * span / gridDim.x);
+    const uint32_t iterations = (end - begin + 31u) / 32u;
+    for (uint32_t it = 0; it < iterations; ++it) {
+        const uint32_t batch = begin + it * 32u;
+        const int in_batch = static_cast<int>(min(32u, end - batch));
+        const int b = static_cast<int>(it & 1u);
+        unsigned char *buf = base + b * kPipeBufferBytes;
+        float4 *stage = reinterpret_cast<float4 *>(buf);
+        float *fr = reinterpret_cast<float *>(buf + kWalkStageBytes);  // 12 x 32: root position, normal, surface_u, domain
+        uint32_t *locals = reinterpret_cast<uint32_t *>(buf + kWalkStageBytes + kPipeFrameBytes);
+        if (producer) {
+            if (it >= 2u) { named_sync(3u + b); }
+            const uint32_t item = batch + static_cast<uint32_t>(lane);
+            const bool valid = item < end;
+            uint32_t *root_words = reinterpret_cast<uint32_t *>(stage);  // free until the base step
+            const WalkRoot wr = walk_setup<true>(g, records, locals, root_words, lane, valid ? item : batch,
+                                                 valid, static_cast<uint32_t>(P));
+            fr[0 * 32 + lane] = wr.position.x;
+            fr[1 * 32 + lane] = wr.position.y;
+            fr[2 * 32 + lane] = wr.position.z;
+            fr[3 * 32 + lane] = wr.normal.x;
+            fr[4 * 32 + lane] = wr.normal.y;
+            fr[5 * 32 + lane] = wr.normal.z;
+            fr[6 * 32 + lane] = wr.surface_u.x;
+            fr[7 * 32 + lane] = wr.surface_u.y;
+            fr[8 * 32 + lane] = wr.surface_u.z;
+            fr[9 * 32 + lane] = wr.domain.x;
+            fr[10 * 32 + lane] = wr.domain.y;
+            fr[11 * 32 + lane] = wr.domain.z;
+            __syncwarp();
+            if (g.roots) {
+                walk_store_roots(g, root_words, locals, lane, in_batch);
+                __syncwarp();
+            }
+            walk_base<false>(g, records, stage, locals, tvals, rvals, offsets, lane, in_batch, P, inv_p);
+            named_arrive(1u + b);
+        } else {
+            named_sync(1u + b);
+            WalkRoot wr;
+            wr.position = F3{fr[0 * 32 + lane], fr[1 * 32 + lane], fr[2 * 32 + lane]};
+            wr.normal = F3{fr[3 * 32 + lane], fr[4 * 32 + lane], fr[5 * 32 + lane]};
+            wr.surface_u = F3{fr[6 * 32 + lane], fr[7 * 32 + lane], fr[8 * 32 + lane]};
+            wr.domain = F3{fr[9 * 32 + lane], fr[10 * 32 + lane], fr[11 * 32 + lane]};
+            walk_frame(g.p, wr, lane < in_batch, stage + lane * kWalkStride, lattice + lane, tvals, rvals, table, P);
+            __syncwarp();
+            walk_store<false>(g, stage, locals, lane, in_batch, P, inv_p);
+            if (it + 2u < iterations) { named_arrive(3u + b); }
+        }
     }
 }
 
@@ -223,11 +321,17 @@ __global__ void strand_roots_kernel(LaunchArgs g) {
     }
 }
 
-__global__ void guide_offsets_kernel(AssetArgs a, FrameArgs f, uint32_t P, float4 *offsets) {
+// The frame's guide-offset table (G x P float4) and, after it, the guide
+// frame records (2 float4 per guide) the lane-walk generator reads.
+__global__ void guide_offsets_kernel(AssetArgs a, FrameArgs f, uint32_t P, float support_scale, float4 *offsets) {
     const uint64_t n = static_cast<uint64_t>(a.guide_count) * P;
-    for (uint64_t idx = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; idx < n;
-         idx += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    const uint64_t first = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    for (uint64_t idx = first; idx < n; idx += stride) {
         offsets[idx] = guide_offset_entry(a, f, P, static_cast<uint32_t>(idx / P), static_cast<uint32_t>(idx % P));
+    }
+    for (uint64_t gi = first; gi < a.guide_count; gi += stride) {
+        guide_frame_entry(a, f, support_scale, static_cast<uint32_t>(gi), offsets + n + 2u * gi);
     }
 }
 
@@ -538,13 +642,14 @@ bool parallel_path(uint32_t guide_count, uint32_t P) {
 }
 
 // keys[count] | order[count] | bins[guides + 1] | offsets[guides * P] (float4)
+// followed by the guide frame records [guides * 2] (float4)
 WorkspaceLayout workspace_layout(uint32_t guide_count, uint32_t count, uint32_t P) {
     WorkspaceLayout w{};
     w.keys = 0u;
     w.order = align_up(uint64_t{count} * 4u, kWorkspaceAlign);
     w.hist = w.order + align_up(uint64_t{count} * 4u, kWorkspaceAlign);
     w.offsets = w.hist + align_up((uint64_t{guide_count} + 1u) * 4u, kWorkspaceAlign);
-    w.offset_bytes = parallel_path(guide_count, P) ? uint64_t{guide_count} * P * 16u : 0u;
+    w.offset_bytes = parallel_path(guide_count, P) ? uint64_t{guide_count} * (P + 2u) * 16u : 0u;
     w.total = w.offsets + align_up(w.offset_bytes, kWorkspaceAlign);
     return w;
 }
@@ -696,8 +801,21 @@ KernelFn pick_kernel(int lanes, int ppt, bool noise, bool classic) {
     }
 }
 
-size_t generate_smem_bytes(uint32_t P, int lanes, int ppt, bool noise, uint32_t warps) {
-    if (lanes == 1) { return dev::walk_head_bytes(noise) + dev::walk_warp_bytes(noise) * warps; }
+// Dynamic shared memory of the generate kernels; for the lane-walk kernel,
+// `staged` says whether its stage is used and `noise` whether it walks the
+// noise frame itself.
+uint32_t launch_kernel(void (*fn)(LaunchArgs, const float4 *), uint32_t grid, uint32_t block, size_t shm,
+                       cudaStream_t stream, const LaunchArgs &g, const float4 *offsets) {
+    fn<<<grid, block, shm, stream>>>(g, offsets);
+    return record_cuda(cudaGetLastError());
+}
+
+
+size_t generate_smem_bytes(uint32_t P, int lanes, int ppt, bool noise, bool staged, uint32_t warps) {
+    if (lanes == 1) {
+        const bool walk = noise && staged;
+        return dev::walk_head_bytes(walk) + dev::walk_warp_bytes(walk, staged) * warps;
+    }
     const size_t per_warp = sizeof(uint32_t) * dev::kRecFields * 32u + sizeof(float4) * 32u / lanes * lanes * ppt +
                             (noise ? sizeof(float2) * 384u : 0u);
     return sizeof(float4) * dev::kTableFloat4 + sizeof(float) * ((P + 3u) & ~3u) + per_warp * warps;
@@ -796,12 +914,13 @@ uint32_t launch_generate(const nxg_device_asset_desc &asset, const nxg_deformed_
         return record_cuda(cudaGetLastError());
     }
     auto *offsets = reinterpret_cast<float4 *>(wbase + ws.offsets);
+    g.guide_frames = offsets + uint64_t{asset.header.guide_count} * P;
     {
         const uint64_t n = uint64_t{asset.header.guide_count} * P;
         const uint32_t threads = 256u;
         const uint32_t blocks = static_cast<uint32_t>(std::min<uint64_t>((n + threads - 1u) / threads,
                                                                           static_cast<uint64_t>(sms) * 16u));
-        dev::guide_offsets_kernel<<<blocks, threads, 0, stream>>>(g.a, g.f, P, offsets);
+        dev::guide_offsets_kernel<<<blocks, threads, 0, stream>>>(g.a, g.f, P, g.p.support_scale, offsets);
         if ((status = record_cuda(cudaGetLastError()))) { return status; }
     }
     int lanes = 32, ppt = 4;
@@ -816,40 +935,49 @@ uint32_t launch_generate(const nxg_device_asset_desc &asset, const nxg_deformed_
         dev::strand_roots_kernel<<<blocks, threads, 0, stream>>>(g);
         if ((status = record_cuda(cudaGetLastError()))) { return status; }
     }
-    KernelFn fn = pick_kernel(lanes, ppt, noise, g.scalars != nullptr);
-    // block_size in [1, 1024] is a request: rounded up to whole warps, then
-    // capped at what this kernel's register footprint can launch.
-    cudaFuncAttributes attr{};
-    if ((status = record_cuda(cudaFuncGetAttributes(&attr, reinterpret_cast<const void *>(fn))))) { return status; }
-    const uint32_t launchable = std::max<uint32_t>(32u, static_cast<uint32_t>(attr.maxThreadsPerBlock) / 32u * 32u);
-    const uint32_t requested = tile_block ? tile_block : config.block_size;
-    uint32_t block = std::min(launchable, std::max<uint32_t>(32u, (requested + 31u) / 32u * 32u));
+    g.range_begin = 0u;
+    g.range_end = count;
     int device = 0, smem_optin = 48 * 1024;
     if (cudaGetDevice(&device) == cudaSuccess) {
         cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
     }
-    while (block > 32u && generate_smem_bytes(P, lanes, ppt, noise, block / 32u) > static_cast<size_t>(smem_optin)) {
-        block -= 32u;
-    }
-    const uint32_t warps = block / 32u;
-    const size_t shm = generate_smem_bytes(P, lanes, ppt, noise, warps);
-    if (shm > 48u * 1024u) {
-        if ((status = record_cuda(cudaFuncSetAttribute(reinterpret_cast<const void *>(fn),
-                                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                       static_cast<int>(shm))))) {
-            return status;
+    // Launches `fn` persistently over the order positions [g.range_begin,
+    // g.range_end).  block_size in [1, 1024] is a request: rounded up to whole
+    // warps, then capped at what the kernel's registers and shared memory
+    // (smem(warps) bytes) can launch.
+    auto launch = [&](auto fn, uint32_t requested, auto smem) -> uint32_t {
+        cudaFuncAttributes attr{};
+        uint32_t st = record_cuda(cudaFuncGetAttributes(&attr, reinterpret_cast<const void *>(fn)));
+        if (st) { return st; }
+        const uint32_t launchable =
+            std::max<uint32_t>(32u, static_cast<uint32_t>(attr.maxThreadsPerBlock) / 32u * 32u);
+        uint32_t block = std::min(launchable, std::max<uint32_t>(32u, (requested + 31u) / 32u * 32u));
+        while (block > 32u && smem(block / 32u) > static_cast<size_t>(smem_optin)) { block -= 32u; }
+        const uint32_t warps = block / 32u;
+        const size_t shm = smem(warps);
+        if (shm > 48u * 1024u) {
+            st = record_cuda(cudaFuncSetAttribute(reinterpret_cast<const void *>(fn),
+                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(shm)));
+            if (st) { return st; }
         }
+        int per_sm = 0;
+        st = record_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, reinterpret_cast<const void *>(fn),
+                                                                       static_cast<int>(block), shm));
+        if (st) { return st; }
+        per_sm = std::max(per_sm, 1);
+        const uint64_t n = g.range_end - g.range_begin;
+        const uint64_t needed = (n + 32u * warps - 1u) / (32u * warps);
+        const uint32_t grid = static_cast<uint32_t>(std::min<uint64_t>(needed, static_cast<uint64_t>(sms) * per_sm));
+        return grid ? launch_kernel(fn, grid, block, shm, stream, g, offsets) : NXG_ERROR_NONE;
+    };
+    const uint32_t requested = tile_block ? tile_block : config.block_size;
+    const bool classic_scalars = g.scalars != nullptr;
+    if (lanes == 1 && noise && !classic_scalars && requested <= 64u) {  // producer/consumer warp pairs
+        return launch(dev::generate_pipe_kernel, 64u, [](uint32_t) { return dev::kPipeSmemBytes; });
     }
-    int per_sm = 0;
-    if ((status = record_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-             &per_sm, reinterpret_cast<const void *>(fn), static_cast<int>(block), shm)))) {
-        return status;
-    }
-    per_sm = std::max(per_sm, 1);
-    const uint64_t needed = (uint64_t{count} + 32u * warps - 1u) / (32u * warps);
-    const uint32_t grid = static_cast<uint32_t>(std::min<uint64_t>(needed, static_cast<uint64_t>(sms) * per_sm));
-    fn<<<grid, block, shm, stream>>>(g, offsets);
-    return record_cuda(cudaGetLastError());
+    const bool staged = noise || classic_scalars;
+    return launch(pick_kernel(lanes, ppt, noise, classic_scalars), requested,
+                  [&](uint32_t w) { return generate_smem_bytes(P, lanes, ppt, noise, staged, w); });
 }
 
 uint32_t validate_range_request(const nxg_device_asset_desc *asset, const nxg_deformed_desc *deformed,

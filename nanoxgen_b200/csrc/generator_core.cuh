@@ -27,12 +27,15 @@ struct LaunchArgs {
     ParamArgs p;
     uint32_t first_strand;   // global id of output record 0
     uint32_t count;          // strands in this launch
+    uint32_t range_begin;    // lane-walk kernels: positions [range_begin, range_end) of the order
+    uint32_t range_end;
     float4 *points;
     float *vec3_points;      // when set: sample-major Vec3 output instead of float4 (motion contract)
     uint32_t *roots;         // 12 words per strand, or nullptr
     float2 *root_uvs;
     uint32_t *point_counts;
     const uint32_t *order;   // permutation of [0, count), or nullptr for identity
+    const float4 *guide_frames;  // 2 per guide (guide_frame_entry), or nullptr
     const float2 *scalars;   // Classic per-root (length scale, width), or nullptr
     uint32_t classic_length; // scale each strand about its first point by scalars.x
     uint32_t classic_width;  // radius = 0.5 * max(scalars.y, 0) * radius_scale

@@ -199,6 +199,58 @@ struct Slot {             // 48 bytes, staged in shared memory per strand
     uint32_t guide, first_cv, cv_count, flags;
 };
 
+// The frame's guide root (generate.h:137-151) and guide normal
+// (generate.h:153-172) from the guide record's fields.
+__device__ __forceinline__ void frame_guide(const AssetArgs &a, const FrameArgs &f, uint32_t first, uint32_t gtri,
+                                            float gb1, float gb2, F3 rest_root, F3 rest_normal, F3 &groot,
+                                            F3 &gnormal) {
+    const bool bound = gtri < a.triangle_count;
+    groot = rest_root;
+    if (f.deformed_guide_cvs) {
+        groot = ld3(f.guide_cvs, first);
+    } else if (f.deformed_positions && bound) {
+        const uint3 t = load_triangle(a, gtri);
+        const float gb0 = __fsub_rn(__fsub_rn(1.0f, gb1), gb2);
+        groot = xbary(ld3(f.positions, t.x), ld3(f.positions, t.y), ld3(f.positions, t.z), gb0, gb1, gb2);
+    }
+    gnormal = rest_normal;
+    if (bound && (f.deformed_positions || f.deformed_normals)) {
+        const uint3 t = load_triangle(a, gtri);
+        const float gb0 = __fsub_rn(__fsub_rn(1.0f, gb1), gb2);
+        if (f.deformed_normals) {
+            gnormal = xnormalize(xbary(ld3(f.normals, t.x), ld3(f.normals, t.y), ld3(f.normals, t.z),
+                                       gb0, gb1, gb2));
+        } else {
+            const F3 p0 = ld3(f.positions, t.x);
+            gnormal = xnormalize(xcross(xsub(ld3(f.positions, t.y), p0), xsub(ld3(f.positions, t.z), p0)));
+        }
+    }
+}
+
+// Per-frame guide record for the lane-walk generator: (guide root, support
+// radius * support_scale) and (guide normal, 1), or a zero second word for a
+// corrupt record (first CV past the CV array).
+__device__ __forceinline__ void guide_frame_entry(const AssetArgs &a, const FrameArgs &f, float support_scale,
+                                                  uint32_t gi, float4 *out) {
+    const uint32_t *g = a.guides + 14u * static_cast<uint64_t>(gi);
+    const uint32_t first = __ldg(g + 0);
+    if (first >= a.guide_cv_count) {
+        out[0] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        out[1] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        return;
+    }
+    const float support = __uint_as_float(__ldg(g + 3));
+    const F3 rest_root = {__uint_as_float(__ldg(g + 8)), __uint_as_float(__ldg(g + 9)),
+                          __uint_as_float(__ldg(g + 10))};
+    const F3 rest_normal = {__uint_as_float(__ldg(g + 11)), __uint_as_float(__ldg(g + 12)),
+                            __uint_as_float(__ldg(g + 13))};
+    F3 groot, gnormal;
+    frame_guide(a, f, first, __ldg(g + 2), __uint_as_float(__ldg(g + 4)), __uint_as_float(__ldg(g + 5)), rest_root,
+                rest_normal, groot, gnormal);
+    out[0] = make_float4(groot.x, groot.y, groot.z, __fmul_rn(support, support_scale));
+    out[1] = make_float4(gnormal.x, gnormal.y, gnormal.z, __uint_as_float(1u));
+}
+
 __device__ __forceinline__ Slot eval_slot(const AssetArgs &a, const FrameArgs &f, const ParamArgs &p,
                                           const Root &root, uint32_t j) {
     Slot s;
@@ -224,28 +276,8 @@ __device__ __forceinline__ Slot eval_slot(const AssetArgs &a, const FrameArgs &f
     const F3 rest_normal = {__uint_as_float(__ldg(g + 11)), __uint_as_float(__ldg(g + 12)),
                             __uint_as_float(__ldg(g + 13))};
     const bool bound = gtri < a.triangle_count;
-    // guide_root (generate.h:137-151)
-    F3 groot = rest_root;
-    if (f.deformed_guide_cvs) {
-        groot = ld3(f.guide_cvs, first);
-    } else if (f.deformed_positions && bound) {
-        const uint3 t = load_triangle(a, gtri);
-        const float gb0 = __fsub_rn(__fsub_rn(1.0f, gb1), gb2);
-        groot = xbary(ld3(f.positions, t.x), ld3(f.positions, t.y), ld3(f.positions, t.z), gb0, gb1, gb2);
-    }
-    // guide_normal (generate.h:153-172)
-    F3 gnormal = rest_normal;
-    if (bound && (f.deformed_positions || f.deformed_normals)) {
-        const uint3 t = load_triangle(a, gtri);
-        const float gb0 = __fsub_rn(__fsub_rn(1.0f, gb1), gb2);
-        if (f.deformed_normals) {
-            gnormal = xnormalize(xbary(ld3(f.normals, t.x), ld3(f.normals, t.y), ld3(f.normals, t.z),
-                                       gb0, gb1, gb2));
-        } else {
-            const F3 p0 = ld3(f.positions, t.x);
-            gnormal = xnormalize(xcross(xsub(ld3(f.positions, t.y), p0), xsub(ld3(f.positions, t.z), p0)));
-        }
-    }
+    F3 groot, gnormal;
+    frame_guide(a, f, first, gtri, gb1, gb2, rest_root, rest_normal, groot, gnormal);
     const F3 delta = xsub(root.position, groot);
     const float d2 = xdot(delta, delta);
     s.gx = groot.x;

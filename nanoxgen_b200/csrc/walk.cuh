@@ -34,15 +34,21 @@ constexpr int kWalkStride = kWalkMaxCvs + 1;   // float4 per staged strand row
 constexpr int kWalkAxisColumns = 12;           // noise lattice columns per axis and strand
 constexpr int kWalkRecords = 6;                // float4 setup records per strand
 
-// Shared-memory bytes per warp: stage | records (aliased by the lattice once
-// the base step has read them) | output words.
+// Shared-memory bytes per warp.  Staged variants (noise or Classic scalars):
+// stage | records (aliased by the lattice once the base step has read them) |
+// output words; the RootSample words use the stage.  The plain variant has no
+// stage -- its base step writes the output directly -- so: records | RootSample
+// words | output words.
 constexpr size_t kWalkStageBytes = sizeof(float4) * 32u * kWalkStride;
 constexpr size_t kWalkRecordBytes = sizeof(float4) * kWalkRecords * 32u;
 constexpr size_t kWalkLatticeBytes = sizeof(float2) * 3u * kWalkAxisColumns * 32u;
+constexpr size_t kWalkRootWordBytes = sizeof(uint32_t) * 12u * 32u;
 constexpr size_t kWalkLocalBytes = sizeof(uint32_t) * 32u;
-__host__ __device__ constexpr size_t walk_warp_bytes(bool noise) {
-    return kWalkStageBytes + (noise && kWalkLatticeBytes > kWalkRecordBytes ? kWalkLatticeBytes : kWalkRecordBytes) +
-           kWalkLocalBytes;
+__host__ __device__ constexpr size_t walk_warp_bytes(bool noise, bool staged) {
+    return staged ? kWalkStageBytes + (noise && kWalkLatticeBytes > kWalkRecordBytes ? kWalkLatticeBytes
+                                                                                     : kWalkRecordBytes) +
+                        kWalkLocalBytes
+                  : kWalkRecordBytes + kWalkRootWordBytes + kWalkLocalBytes;
 }
 // Per CTA, before the warps: gradient table (noise) | t values | radii.
 __host__ __device__ constexpr size_t walk_head_bytes(bool noise) {
@@ -61,8 +67,69 @@ struct WalkRoot {
     F3 position, normal, surface_u, domain;
 };
 
-// Also writes the strand's root UV and point count, and stages its twelve
-// RootSample words at root_words[lane * 12] for walk_store_roots.
+// sample_root (generate.h:101-135) plus, with noise, the root's surface_u
+// (generate.h:312-341) and rest position (generate.h:343-351), reusing the
+// triangle's vertex data instead of loading it again.
+template <bool NOISE>
+__device__ __forceinline__ Root walk_root(const AssetArgs &a, const FrameArgs &f, uint32_t seed, uint32_t strand,
+                                          F3 &surface_u, F3 &rest_position) {
+    Root r;
+    r.triangle = sample_triangle(a, seed, strand);
+    const float r1 = random01(seed, strand, 2u);
+    const float r2 = random01(seed, strand, 3u);
+    const float s = __fsqrt_rn(r1);
+    const float b0 = __fsub_rn(1.0f, s);
+    r.b1 = __fmul_rn(s, __fsub_rn(1.0f, r2));
+    r.b2 = __fmul_rn(s, r2);
+    const uint3 t = load_triangle(a, r.triangle);
+    const F3 p0 = ld3(f.positions, t.x), p1 = ld3(f.positions, t.y), p2 = ld3(f.positions, t.z);
+    r.position = xbary(p0, p1, p2, b0, r.b1, r.b2);
+    r.normal = xnormalize(xcross(xsub(p1, p0), xsub(p2, p0)));
+    if (a.flags & NXG_ASSET_HAS_NORMALS) {
+        r.normal = xnormalize(xbary(ld3(f.normals, t.x), ld3(f.normals, t.y), ld3(f.normals, t.z),
+                                    b0, r.b1, r.b2));
+    }
+    r.u = 0.0f;
+    r.v = 0.0f;
+    const bool uvs = (a.flags & NXG_ASSET_HAS_TEXCOORDS) && a.texcoords;
+    float2 uv0 = make_float2(0.0f, 0.0f), uv1 = uv0, uv2 = uv0;
+    if (uvs) {
+        uv0 = make_float2(__ldg(a.texcoords + 2u * static_cast<uint64_t>(t.x)),
+                          __ldg(a.texcoords + 2u * static_cast<uint64_t>(t.x) + 1u));
+        uv1 = make_float2(__ldg(a.texcoords + 2u * static_cast<uint64_t>(t.y)),
+                          __ldg(a.texcoords + 2u * static_cast<uint64_t>(t.y) + 1u));
+        uv2 = make_float2(__ldg(a.texcoords + 2u * static_cast<uint64_t>(t.z)),
+                          __ldg(a.texcoords + 2u * static_cast<uint64_t>(t.z) + 1u));
+        r.u = __fadd_rn(__fadd_rn(__fmul_rn(uv0.x, b0), __fmul_rn(uv1.x, r.b1)), __fmul_rn(uv2.x, r.b2));
+        r.v = __fadd_rn(__fadd_rn(__fmul_rn(uv0.y, b0), __fmul_rn(uv1.y, r.b1)), __fmul_rn(uv2.y, r.b2));
+    }
+    if constexpr (NOISE) {
+        F3 tangent = {0.0f, 0.0f, 0.0f};
+        if (uvs) {
+            const F3 e1 = p1 - p0;
+            const F3 e2 = p2 - p0;
+            const float du1 = uv1.x - uv0.x, dv1 = uv1.y - uv0.y;
+            const float du2 = uv2.x - uv0.x, dv2 = uv2.y - uv0.y;
+            const float det = du1 * dv2 - dv1 * du2;
+            if (fabsf(det) > 1.0e-12f) {
+                tangent = (e1 * dv2 - e2 * dv1) * (1.0f / det);
+                tangent = tangent - r.normal * dot(tangent, r.normal);
+            }
+        }
+        surface_u = dot(tangent, tangent) > 1.0e-20f ? normalize(tangent) : fallback_surface_u(r.normal);
+        const float rb0 = __fsub_rn(__fsub_rn(1.0f, r.b1), r.b2);
+        rest_position = f.positions == a.positions
+            ? xbary(p0, p1, p2, rb0, r.b1, r.b2)
+            : xbary(ld3(a.positions, t.x), ld3(a.positions, t.y), ld3(a.positions, t.z), rb0, r.b1, r.b2);
+    }
+    return r;
+}
+
+// Setup step for this lane's strand.  The stencil slots follow eval_slot and
+// the loop of generate.h:214-244 with the frame's guide roots, normals and
+// support radii read from the per-frame guide records.  Also writes the
+// strand's root UV and point count, and stages its twelve RootSample words
+// at root_words[lane * 12] for walk_store_roots.
 template <bool NOISE>
 __device__ __forceinline__ WalkRoot walk_setup(const LaunchArgs &g, float4 *records, uint32_t *locals,
                                                uint32_t *root_words, int lane, uint32_t pick, bool valid,
@@ -75,7 +142,10 @@ __device__ __forceinline__ WalkRoot walk_setup(const LaunchArgs &g, float4 *reco
         local = 0u;
         valid = false;
     }
-    const Root root = sample_root(a, f, p.seed, g.first_strand + local);
+    WalkRoot r;
+    r.surface_u = F3{0.0f, 0.0f, 0.0f};
+    F3 rest_position = {0.0f, 0.0f, 0.0f};
+    const Root root = walk_root<NOISE>(a, f, p.seed, g.first_strand + local, r.surface_u, rest_position);
     if (g.roots) {
 #pragma unroll
         for (int w = 0; w < 12; ++w) { root_words[lane * 12 + w] = root_word(root, w); }
@@ -86,25 +156,44 @@ __device__ __forceinline__ WalkRoot walk_setup(const LaunchArgs &g, float4 *reco
     }
 #pragma unroll
     for (int q = 0; q < 4; ++q) { records[q * 32 + lane] = make_float4(0.0f, 0.0f, 0.0f, 0.0f); }
+    uint32_t stencil[kSlots];
+    const uint32_t *row = a.stencil + static_cast<uint64_t>(root.triangle) * kSlots;
+    if ((reinterpret_cast<std::uintptr_t>(a.stencil) & 15u) == 0u) {
+        const uint4 s0 = __ldg(reinterpret_cast<const uint4 *>(row));
+        const uint4 s1 = __ldg(reinterpret_cast<const uint4 *>(row) + 1);
+        stencil[0] = s0.x; stencil[1] = s0.y; stencil[2] = s0.z; stencil[3] = s0.w;
+        stencil[4] = s1.x; stencil[5] = s1.y; stencil[6] = s1.z; stencil[7] = s1.w;
+    } else {
+#pragma unroll
+        for (uint32_t j = 0; j < kSlots; ++j) { stencil[j] = __ldg(row + j); }
+    }
     float *slot_words = reinterpret_cast<float *>(records);
     float wsum = 0.0f;
     float nearest_d2 = FLT_MAX;
     uint32_t nearest = kInvalid;
     uint32_t blended = 0u;
-#pragma unroll 1
+#pragma unroll
     for (uint32_t j = 0; j < kSlots; ++j) {
-        const Slot s = eval_slot(a, f, p, root, j);
-        if ((s.flags & kSlotEligible) && s.d2 < nearest_d2) {  // strict first minimum (generate.h:234)
-            nearest_d2 = s.d2;
-            nearest = s.guide;
+        const uint32_t gi = stencil[j];
+        if (gi == kInvalid || gi >= a.guide_count) { continue; }
+        const float4 gr = __ldg(g.guide_frames + 2u * gi);
+        const float4 gn = __ldg(g.guide_frames + 2u * gi + 1u);
+        if (__float_as_uint(gn.w) == 0u) { continue; }  // corrupt record
+        const F3 delta = xsub(root.position, F3{gr.x, gr.y, gr.z});
+        const float d2 = xdot(delta, delta);
+        if (xdot(root.normal, F3{gn.x, gn.y, gn.z}) < p.rejection_cos) { continue; }
+        if (d2 < nearest_d2) {  // strict first minimum over eligible slots (generate.h:234)
+            nearest_d2 = d2;
+            nearest = gi;
         }
-        if (s.flags & kSlotBlended) {
-            float *dst = slot_words + ((blended >> 1) * 32u + lane) * 4u + (blended & 1u) * 2u;
-            dst[0] = __uint_as_float(s.guide * P);
-            dst[1] = s.w;
-            ++blended;
-            wsum = __fadd_rn(wsum, s.w);
-        }
+        const float radius = gr.w;
+        if (radius <= 0.0f || d2 >= __fmul_rn(radius, radius)) { continue; }
+        const float w = powf(__fsub_rn(1.0f, __fdiv_rn(__fsqrt_rn(d2), radius)), p.weight_power);
+        float *dst = slot_words + ((blended >> 1) * 32u + lane) * 4u + (blended & 1u) * 2u;
+        dst[0] = __uint_as_float(gi * P);
+        dst[1] = w;
+        ++blended;
+        wsum = __fadd_rn(wsum, w);
     }
     float inv = 0.0f;
     F3 normal_term = {0.0f, 0.0f, 0.0f};
@@ -122,16 +211,13 @@ __device__ __forceinline__ WalkRoot walk_setup(const LaunchArgs &g, float4 *reco
     records[4 * 32 + lane] = make_float4(root.position.x, root.position.y, root.position.z, inv);
     records[5 * 32 + lane] = make_float4(normal_term.x, normal_term.y, normal_term.z, __uint_as_float(nb));
     locals[lane] = local | (valid ? 0u : 0x80000000u);
-    WalkRoot r;
     r.position = root.position;
     r.normal = root.normal;
-    r.surface_u = F3{0.0f, 0.0f, 0.0f};
     r.domain = F3{0.0f, 0.0f, 0.0f};
     if constexpr (NOISE) {
-        r.surface_u = root_surface_u(a, f, root);
         const float decorrelation = 1.0f - p.noise_correlation;
         const float domain_scale = 100.0f * decorrelation * decorrelation;
-        r.domain = (rest_root_position(a, root) + F3{0.419276f, 0.184247f, 0.805721f}) * domain_scale;
+        r.domain = (rest_position + F3{0.419276f, 0.184247f, 0.805721f}) * domain_scale;
     }
     return r;
 }
@@ -147,16 +233,34 @@ __device__ __forceinline__ void walk_store_roots(const LaunchArgs &g, const uint
     }
 }
 
+// One output point of the strand whose output word is `word` (skipped when
+// the word is marked invalid): float4 (position, radius), or Vec3 positions,
+// 3P consecutive floats per strand (device_contract.h:47-52).
+__device__ __forceinline__ void walk_emit(const LaunchArgs &g, uint32_t word, int P, int c, float4 q) {
+    if (word >> 31) { return; }
+    const uint64_t index = static_cast<uint64_t>(word) * static_cast<uint32_t>(P) + static_cast<uint32_t>(c);
+    if (g.vec3_points) {
+        float *out3 = g.vec3_points + 3u * index;
+        __stcs(out3, q.x);
+        __stcs(out3 + 1, q.y);
+        __stcs(out3 + 2, q.z);
+    } else {
+        __stcs(g.points + index, q);
+    }
+}
+
 // Strand of a flattened (strand, CV) item: floor((item + 0.5) / P), exact for
 // item < 32 * 32 (the quotient is at least 0.5 / P from an integer).
 __device__ __forceinline__ int walk_strand(int item, float inv_p) {
     return static_cast<int>((static_cast<float>(item) + 0.5f) * inv_p);
 }
 
-// Base step: item = s * P + c over the batch, 32 consecutive items per pass.
+// Base step: item = s * P + c over the batch, 32 consecutive items per pass,
+// into the stage or (DIRECT) straight to the output.
+template <bool DIRECT>
 __device__ __forceinline__ void walk_base(const LaunchArgs &g, const float4 *records, float4 *stage,
-                                          const float *tvals, const float *rvals, const float4 *offsets, int lane,
-                                          int in_batch, int P, float inv_p) {
+                                          const uint32_t *locals, const float *tvals, const float *rvals,
+                                          const float4 *offsets, int lane, int in_batch, int P, float inv_p) {
     const int items = in_batch * P;
     const float ls = g.p.length_scale;
 #pragma unroll 2
@@ -182,7 +286,11 @@ __device__ __forceinline__ void walk_base(const LaunchArgs &g, const float4 *rec
         const float t = tvals[c];
         const F3 off = acc * head.w + F3{tail.x, tail.y, tail.z} * t;
         const F3 base = F3{head.x, head.y, head.z} + off * ls;
-        stage[s * kWalkStride + c] = make_float4(base.x, base.y, base.z, rvals[c]);
+        if constexpr (DIRECT) {
+            walk_emit(g, locals[s], P, c, make_float4(base.x, base.y, base.z, rvals[c]));
+        } else {
+            stage[s * kWalkStride + c] = make_float4(base.x, base.y, base.z, rvals[c]);
+        }
     }
 }
 
@@ -201,157 +309,228 @@ __device__ __forceinline__ float walk_lattice_delta(const float2 *lat, int axis,
     return 0.5f * (v0 + s * (v1 - v0));
 }
 
-// Frame step for the strand whose staged row is `row` (this lane's strand):
-// arc lengths into row[c].w, the lattice, then the cursor walk, leaving the
-// noisy points (with radii) in the row.
-__device__ __forceinline__ void walk_frame(const ParamArgs &p, const WalkRoot &wr, float4 *row, float2 *lat,
-                                           const float *tvals, const float *rvals, const float4 *table, int P) {
-    // Arc-length prefix of the base curve (generate.h:420-433, :465-468).
-    float arc = 0.0f;
-    {
-        F3 prev = xyz(row[0]);
-        reinterpret_cast<float *>(row)[3] = 0.0f;
-        for (int c = 1; c < P; ++c) {
-            const F3 cur = xyz(row[c]);
-            const F3 d = cur - prev;
-            arc += sqrtf(dot(d, d));
-            reinterpret_cast<float *>(row + c)[3] = arc;
-            prev = cur;
-        }
-    }
-    const float original_length = arc;
-    const float f_eff = original_length > 0.0f ? fmaxf(0.5f / original_length, p.noise_frequency)
-                                               : p.noise_frequency;
-
-    // Lattice columns (A, B) of the three noise axes (see lattice_noise):
-    // columns lo .. floor(d0 + span) + 2 cover every CV's X and X + 1 with one
-    // column of margin for rounding in the arc-length prefix.
-    const F3 dom = wr.domain;
-    const float span = original_length * f_eff;
+// Lattice columns (A, B) of the three noise axes for one strand (see
+// lattice_noise): columns lo .. floor(d0 + span) + 2 cover every CV's X and
+// X + 1 with one column of margin for rounding in the arc-length prefix.
+// `lat` is this lane's column 0 of axis 0; column k of axis a is at
+// lat[(a * kWalkAxisColumns + k) * 32].  fits is false when a strand needs
+// more columns than the lattice holds (it then takes direct noise).
+struct WalkLattice {
     int lo[3], n[3];
-    bool fits = true;
+    bool fits;
+};
+
+__device__ __forceinline__ WalkLattice walk_fill_lattice(F3 dom, float span, float2 *lat, const float4 *table) {
+    WalkLattice wl;
+    wl.fits = true;
 #pragma unroll
     for (int ax = 0; ax < 3; ++ax) {
         const float d0 = component(dom, ax);
-        lo[ax] = static_cast<int>(floorf(d0));
-        n[ax] = static_cast<int>(floorf(d0 + span)) + 3 - lo[ax];
-        fits = fits && n[ax] >= 2 && n[ax] <= kWalkAxisColumns;
+        wl.lo[ax] = static_cast<int>(floorf(d0));
+        wl.n[ax] = static_cast<int>(floorf(d0 + span)) + 3 - wl.lo[ax];
+        wl.fits = wl.fits && wl.n[ax] >= 2 && wl.n[ax] <= kWalkAxisColumns;
     }
-    if (fits) {
+    if (!wl.fits) {  // lattice reads stay in bounds (column 0 and 1) whatever the strand
+        wl.n[0] = wl.n[1] = wl.n[2] = 2;
+        return wl;
+    }
 #pragma unroll
-        for (int ax = 0; ax < 3; ++ax) {
-            const int ib = ax == 0 ? 1 : 0;  // the fixed axes, ascending
-            const int ic = ax == 2 ? 1 : 2;
-            const float db = component(dom, ib), dc = component(dom, ic);
-            const float fb = floorf(db), fc = floorf(dc);
-            const float wb = db - fb, wc = dc - fc;
-            const float sb = s_curve(wb), sc = s_curve(wc);
-            const int Yb = static_cast<int>(fb), Zc = static_cast<int>(fc);
-            // The corner seed is linear in the moving coordinate X (noise_hash's
-            // LCG chain): seed(X + 1) = seed(X) + step.
-            const uint32_t step = ax == 0 ? kLcgA2 : (ax == 1 ? kLcgA : 1u);
-            uint32_t seed[4];
-            float wgt[4], wdb[4], wdc[4];
+    for (int ax = 0; ax < 3; ++ax) {
+        const int ib = ax == 0 ? 1 : 0;  // the fixed axes, ascending
+        const int ic = ax == 2 ? 1 : 2;
+        const float db = component(dom, ib), dc = component(dom, ic);
+        const float fb = floorf(db), fc = floorf(dc);
+        const float wb = db - fb, wc = dc - fc;
+        const float sb = s_curve(wb), sc = s_curve(wc);
+        const int Yb = static_cast<int>(fb), Zc = static_cast<int>(fc);
+        // The corner seed is linear in the moving coordinate X (noise_hash's
+        // LCG chain): seed(X + 1) = seed(X) + step.
+        const uint32_t step = ax == 0 ? kLcgA2 : (ax == 1 ? kLcgA : 1u);
+        uint32_t seed[4];
+        float wgt[4], wdb[4], wdc[4];
+#pragma unroll
+        for (int corner = 0; corner < 4; ++corner) {
+            const int ob = corner & 1, oc = corner >> 1;
+            const int X = wl.lo[ax];
+            const int cx = ax == 0 ? X : Yb + ob;
+            const int cy = ax == 1 ? X : (ax == 0 ? Yb + ob : Zc + oc);
+            const int cz = ax == 2 ? X : Zc + oc;
+            seed[corner] = static_cast<uint32_t>(cx) * kLcgA2 + static_cast<uint32_t>(cy) * kLcgA +
+                           static_cast<uint32_t>(cz) + kLcgK;
+            wgt[corner] = (ob ? sb : 1.0f - sb) * (oc ? sc : 1.0f - sc);
+            wdb[corner] = wgt[corner] * (wb - static_cast<float>(ob));
+            wdc[corner] = wgt[corner] * (wc - static_cast<float>(oc));
+        }
+        for (int k = 0; k < wl.n[ax]; ++k) {
+            float A = 0.0f, B = 0.0f;
 #pragma unroll
             for (int corner = 0; corner < 4; ++corner) {
-                const int ob = corner & 1, oc = corner >> 1;
-                const int X = lo[ax];
-                const int cx = ax == 0 ? X : Yb + ob;
-                const int cy = ax == 1 ? X : (ax == 0 ? Yb + ob : Zc + oc);
-                const int cz = ax == 2 ? X : Zc + oc;
-                seed[corner] = static_cast<uint32_t>(cx) * kLcgA2 + static_cast<uint32_t>(cy) * kLcgA +
-                               static_cast<uint32_t>(cz) + kLcgK;
-                wgt[corner] = (ob ? sb : 1.0f - sb) * (oc ? sc : 1.0f - sc);
-                wdb[corner] = wgt[corner] * (wb - static_cast<float>(ob));
-                wdc[corner] = wgt[corner] * (wc - static_cast<float>(oc));
+                const float4 gr = table[temper_index(seed[corner] + static_cast<uint32_t>(k) * step)];
+                A += wgt[corner] * component4(gr, ax);
+                B += component4(gr, ib) * wdb[corner] + component4(gr, ic) * wdc[corner];
             }
-            for (int k = 0; k < n[ax]; ++k) {
-                float A = 0.0f, B = 0.0f;
-#pragma unroll
-                for (int corner = 0; corner < 4; ++corner) {
-                    const float4 gr = table[temper_index(seed[corner] + static_cast<uint32_t>(k) * step)];
-                    A += wgt[corner] * component4(gr, ax);
-                    B += component4(gr, ib) * wdb[corner] + component4(gr, ic) * wdc[corner];
-                }
-                lat[(ax * kWalkAxisColumns + k) * 32] = make_float2(A, B);
-            }
+            lat[(ax * kWalkAxisColumns + k) * 32] = make_float2(A, B);
         }
     }
+    return wl;
+}
 
-    // The cursor walk (generate.h:465-502).  Tangent after CV c: the next
-    // segment's direction, carried over zero-length segments and at the tip;
-    // the transported normal rotates by rotate_by(axis, acos(cos)) with
-    // cos(acos x) = x and sin(acos x) = sqrt(1 - x^2):
-    //   M v = cos v + (1 - cos)(axis . v) axis + sin (axis x v).
+__device__ __forceinline__ float walk_effective_frequency(const ParamArgs &p, float original_length) {
+    return original_length > 0.0f ? fmaxf(0.5f / original_length, p.noise_frequency) : p.noise_frequency;
+}
+
+// Square root by the PTX approximate instruction (one MUFU operation, no
+// special-case branch); its relative error (below 2^-22) is far inside the
+// position tolerance where it is used (arc lengths and sin(acos x)).
+__device__ __forceinline__ float sqrt_approx(float x) {
+    float r;
+    asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+// The cursor walk (generate.h:465-502) over base points base(0..P-1),
+// handing each noisy point to emit(c, point) in CV order; returns the noisy
+// length (generate.h:553-556) when PRESERVE, else 0.  Tangent after CV c: the
+// next segment's direction, carried over zero-length segments and at the
+// tip; the transported normal rotates by rotate_by(axis, acos(cos)) with
+// cos(acos x) = x and sin(acos x) = sqrt(1 - x^2):
+//   M v = cos v + (1 - cos)(axis . v) axis + sin (axis x v),
+// and is left unchanged when the axis is zero.  The body has no per-lane
+// branches (each decision is a select), so the compiler can overlap the
+// noise, tangent and frame chains of neighbouring CVs; noise at CV 0 is
+// multiplied by t_0 = 0.  LATTICE: every lane of the warp reads lattice
+// noise (else every lane evaluates gradient_noise).  Base points are
+// requested three CVs before they are used.
+template <bool LATTICE, bool PRESERVE, class Base, class Emit>
+__device__ __forceinline__ float walk_cursor(const ParamArgs &p, const WalkRoot &wr, float f_eff,
+                                             const WalkLattice &wl, const float2 *lat, const float *tvals,
+                                             const float4 *table, int P, Base base, Emit emit) {
     const float mscale = p.noise_mask * p.noise_amplitude;
-    const bool preserve = p.noise_preserve_length > 0.001f;
+    const F3 dom = wr.domain;
     F3 tan = wr.normal;
     F3 v = wr.surface_u;
-    float4 cur4 = row[0];
-    F3 nxt = xyz(row[1]);
-    F3 previous_point = xyz(cur4);
+    F3 cur = base(0);
+    F3 nxt = base(1);
+    F3 ahead = P > 2 ? base(2) : nxt;
+    F3 previous_base = cur;
+    F3 previous_point = cur;
     float noisy = 0.0f;
+    float arc = 0.0f;
+#pragma unroll 2
     for (int c = 0; c < P; ++c) {
-        const F3 cur = xyz(cur4);
-        F3 ntan = tan;
-        if (c + 1 < P) {
-            const F3 seg = xsub(nxt, cur);
-            if (xdot(seg, seg) > 0.0f) { ntan = normalize(seg); }
-        }
+        const F3 further = c + 3 < P ? base(c + 3) : ahead;
+        const F3 d = cur - previous_base;
+        arc += sqrt_approx(dot(d, d));
+        const F3 seg = xsub(nxt, cur);
+        const F3 ntan = (c + 1 < P && xdot(seg, seg) > 0.0f) ? normalize(seg) : tan;
         const F3 axis = xcross(tan, ntan);
-        if (xdot(axis, axis) > 0.0f) {
-            const float cs = fminf(fmaxf(dot(tan, ntan), -1.0f), 1.0f);
-            const float sn = sqrtf(fmaf(-cs, cs, 1.0f));
-            const float k = (1.0f - cs) * dot(axis, v);
-            const F3 axv = cross(axis, v);
-            v = normalize(F3{v.x * cs + axis.x * k + axv.x * sn, v.y * cs + axis.y * k + axv.y * sn,
-                             v.z * cs + axis.z * k + axv.z * sn});
-        }
+        const float cs = fminf(fmaxf(dot(tan, ntan), -1.0f), 1.0f);
+        const float sn = sqrt_approx(fmaf(-cs, cs, 1.0f));
+        const float k = (1.0f - cs) * dot(axis, v);
+        const F3 axv = cross(axis, v);
+        const F3 rotated = normalize(F3{v.x * cs + axis.x * k + axv.x * sn, v.y * cs + axis.y * k + axv.y * sn,
+                                        v.z * cs + axis.z * k + axv.z * sn});
+        v = xdot(axis, axis) > 0.0f ? rotated : v;
         const F3 bn = cross(v, ntan);
         const F3 tt = cross(bn, v);
-        F3 q = cur;
-        if (c > 0) {
-            const float distance = cur4.w * f_eff;
-            const float magnitude = mscale * tvals[c];
-            float gx, gy, gz;
-            if (fits) {
-                gx = walk_lattice_delta(lat, 0, lo[0], n[0], dom.x + distance);
-                gy = walk_lattice_delta(lat, 1, lo[1], n[1], dom.y + distance);
-                gz = walk_lattice_delta(lat, 2, lo[2], n[2], dom.z + distance);
-            } else {
-                gx = gradient_noise(table, dom.x + distance, dom.y, dom.z) - 0.5f;
-                gy = gradient_noise(table, dom.x, dom.y + distance, dom.z) - 0.5f;
-                gz = gradient_noise(table, dom.x, dom.y, dom.z + distance) - 0.5f;
-            }
-            q = q + v * (gx * magnitude) + bn * (gy * magnitude) + tt * (gz * magnitude);
+        const float distance = arc * f_eff;
+        const float magnitude = mscale * tvals[c];
+        float gx, gy, gz;
+        if constexpr (LATTICE) {
+            gx = walk_lattice_delta(lat, 0, wl.lo[0], wl.n[0], dom.x + distance);
+            gy = walk_lattice_delta(lat, 1, wl.lo[1], wl.n[1], dom.y + distance);
+            gz = walk_lattice_delta(lat, 2, wl.lo[2], wl.n[2], dom.z + distance);
+        } else {
+            gx = gradient_noise(table, dom.x + distance, dom.y, dom.z) - 0.5f;
+            gy = gradient_noise(table, dom.x, dom.y + distance, dom.z) - 0.5f;
+            gz = gradient_noise(table, dom.x, dom.y, dom.z + distance) - 0.5f;
         }
-        row[c] = make_float4(q.x, q.y, q.z, rvals[c]);
-        if (preserve) {
-            const F3 d = q - previous_point;
-            noisy += c > 0 ? sqrtf(dot(d, d)) : 0.0f;
+        const F3 q = cur + v * (gx * magnitude) + bn * (gy * magnitude) + tt * (gz * magnitude);
+        if constexpr (PRESERVE) {
+            const F3 e = q - previous_point;
+            noisy += sqrt_approx(dot(e, e));
             previous_point = q;
         }
+        emit(c, q);
         tan = ntan;
-        if (c + 1 < P) { cur4 = row[c + 1]; }
-        if (c + 2 < P) { nxt = xyz(row[c + 2]); }
+        previous_base = cur;
+        cur = nxt;
+        nxt = ahead;
+        ahead = further;
     }
+    return noisy;
+}
 
-    // preserveLength (generate.h:553-563) from the noisy points of the walk,
-    // scaling the strand about its root.
-    if (preserve && noisy > 0.0f) {
-        const float target = original_length * p.noise_preserve_length + noisy * (1.0f - p.noise_preserve_length);
-        if (fabsf(noisy - target) >= 0.0001f) {
-            const float scale = target / noisy;
-            const F3 root = wr.position;
-            for (int c = 0; c < P; ++c) {
-                const F3 q = root + (xyz(row[c]) - root) * scale;
-                row[c].x = q.x;
-                row[c].y = q.y;
-                row[c].z = q.z;
-            }
+// walk_cursor with its warp-uniform variant: lattice noise when every lane
+// whose strand counts (`counts`) fits its lattice.  Every lane of the warp
+// calls it.
+template <class Base, class Emit>
+__device__ __forceinline__ float walk_cursor_any(const ParamArgs &p, const WalkRoot &wr, float f_eff,
+                                                 const WalkLattice &wl, bool counts, const float2 *lat,
+                                                 const float *tvals, const float4 *table, int P, Base base,
+                                                 Emit emit) {
+    const bool lattice = __all_sync(kFull, wl.fits || !counts);
+    const bool preserve = p.noise_preserve_length > 0.001f;
+    if (lattice) {
+        return preserve ? walk_cursor<true, true>(p, wr, f_eff, wl, lat, tvals, table, P, base, emit)
+                        : walk_cursor<true, false>(p, wr, f_eff, wl, lat, tvals, table, P, base, emit);
+    }
+    return preserve ? walk_cursor<false, true>(p, wr, f_eff, wl, lat, tvals, table, P, base, emit)
+                    : walk_cursor<false, false>(p, wr, f_eff, wl, lat, tvals, table, P, base, emit);
+}
+
+// preserveLength scale (generate.h:553-563), or 1.
+__device__ __forceinline__ float walk_preserve_scale(const ParamArgs &p, float original_length, float noisy) {
+    if (!(p.noise_preserve_length > 0.001f) || !(noisy > 0.0f)) { return 1.0f; }
+    const float target = original_length * p.noise_preserve_length + noisy * (1.0f - p.noise_preserve_length);
+    return fabsf(noisy - target) >= 0.0001f ? target / noisy : 1.0f;
+}
+
+// Frame step for the strand whose staged row is `row` (this lane's strand):
+// the base curve's length, the lattice, then the cursor walk, leaving the
+// noisy points (with radii) in the row.  The walk reads CV c + 3 after
+// writing CV c, so it never reads a point it has replaced.  Every lane of the
+// warp calls it; lanes whose strand does not count (past the batch) work on
+// whatever their row holds and are ignored.
+__device__ __forceinline__ void walk_frame(const ParamArgs &p, const WalkRoot &wr, bool counts, float4 *row,
+                                           float2 *lat, const float *tvals, const float *rvals, const float4 *table,
+                                           int P) {
+    // Length of the base curve (generate.h:420-433); the walk accumulates the
+    // same prefix again as its arc length.
+    float original_length = 0.0f;
+    {
+        F3 prev = xyz(row[0]);
+        for (int c = 1; c < P; ++c) {
+            const F3 cur = xyz(row[c]);
+            const F3 d = cur - prev;
+            original_length += sqrt_approx(dot(d, d));
+            prev = cur;
+        }
+    }
+    const float f_eff = walk_effective_frequency(p, original_length);
+    const WalkLattice wl = walk_fill_lattice(wr.domain, original_length * f_eff, lat, table);
+    const float noisy = walk_cursor_any(
+        p, wr, f_eff, wl, counts, lat, tvals, table, P, [&](int c) { return xyz(row[c]); },
+        [&](int c, F3 q) { row[c] = make_float4(q.x, q.y, q.z, rvals[c]); });
+    const float scale = walk_preserve_scale(p, original_length, noisy);
+    if (scale != 1.0f) {
+        const F3 root = wr.position;
+        for (int c = 0; c < P; ++c) {
+            const F3 q = root + (xyz(row[c]) - root) * scale;
+            row[c].x = q.x;
+            row[c].y = q.y;
+            row[c].z = q.z;
         }
     }
 }
+
+// generate_pipe_kernel shared memory: table | t values | radii | two buffers
+// (stage, 12 x 32 frame floats, 32 output words) | producer records |
+// consumer lattice.
+constexpr size_t kPipeFrameBytes = sizeof(float) * 12u * 32u;
+constexpr size_t kPipeBufferBytes = kWalkStageBytes + kPipeFrameBytes + kWalkLocalBytes;
+constexpr size_t kPipeSmemBytes = sizeof(float4) * kTableFloat4 + 2u * sizeof(float) * kWalkMaxCvs +
+                                  2u * kPipeBufferBytes + kWalkRecordBytes + kWalkLatticeBytes;
 
 // Store step: item = s * P + c; the Classic application (scale about the
 // first point, width override, drop rule) as in emit_strand.
@@ -390,16 +569,7 @@ __device__ __forceinline__ void walk_store(const LaunchArgs &g, const float4 *st
             }
             if (!keep && c == 0 && g.point_counts != nullptr) { g.point_counts[word] = 0u; }
         }
-        const uint64_t index = static_cast<uint64_t>(word) * static_cast<uint32_t>(P) + static_cast<uint32_t>(c);
-        if (g.vec3_points) {
-            // Vec3 positions, 3P consecutive floats per strand (device_contract.h:47-52)
-            float *out3 = g.vec3_points + 3u * index;
-            __stcs(out3, q.x);
-            __stcs(out3 + 1, q.y);
-            __stcs(out3 + 2, q.z);
-        } else {
-            __stcs(g.points + index, q);
-        }
+        walk_emit(g, word, P, c, q);
     }
 }
 
