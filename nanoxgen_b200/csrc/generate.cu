@@ -97,12 +97,11 @@ __global__ void generate_kernel(LaunchArgs g, const float4 *offsets) {
 // over contiguous ranges of the strand order positions [range_begin,
 // range_end); each warp takes 32 strands at a time through setup (which also
 // writes the roots, root UVs and point counts), base, frame (with noise) and
-// store.  Without noise or Classic scalars the base step writes the output
-// directly (no stage); with noise and no scalars this kernel runs without
-// noise and frame_walk_kernel adds it.
+// store.  Without noise the base step writes the output directly (no
+// stage), applying Classic scalars itself when given.
 template <bool NOISE, bool CLASSIC>
 __global__ void __launch_bounds__(256, 1) generate_walk_kernel(LaunchArgs g, const float4 *offsets) {
-    constexpr bool kStaged = NOISE || CLASSIC;
+    constexpr bool kStaged = NOISE;
     constexpr bool kWalk = NOISE;  // noise walk inside this kernel
     extern __shared__ float4 smem[];
     const int P = static_cast<int>(g.p.cvs_per_strand);
@@ -149,7 +148,13 @@ __global__ void __launch_bounds__(256, 1) generate_walk_kernel(LaunchArgs g, con
             walk_store_roots(g, root_words, locals, lane, in_batch);
             __syncwarp();
         }
-        walk_base<!kStaged>(g, records, stage, locals, tvals, rvals, offsets, lane, in_batch, P, inv_p);
+        if constexpr (CLASSIC && !NOISE) {
+            walk_classic_setup(g, records, lane, valid, locals[lane] & 0x7fffffffu, tvals, offsets,
+                               reinterpret_cast<float4 *>(root_words), P);
+            __syncwarp();
+        }
+        walk_base<!kStaged, CLASSIC && !NOISE>(g, records, stage, locals, tvals, rvals, offsets, lane, in_batch, P,
+                                               inv_p);
         __syncwarp();
         if constexpr (kWalk) {
             walk_frame(g.p, wr, lane < in_batch, stage + lane * kWalkStride, lattice + lane, tvals, rvals, table, P);
@@ -975,7 +980,7 @@ uint32_t launch_generate(const nxg_device_asset_desc &asset, const nxg_deformed_
     if (lanes == 1 && noise && !classic_scalars && requested <= 64u) {  // producer/consumer warp pairs
         return launch(dev::generate_pipe_kernel, 64u, [](uint32_t) { return dev::kPipeSmemBytes; });
     }
-    const bool staged = noise || classic_scalars;
+    const bool staged = lanes == 1 ? noise : (noise || classic_scalars);
     return launch(pick_kernel(lanes, ppt, noise, classic_scalars), requested,
                   [&](uint32_t w) { return generate_smem_bytes(P, lanes, ppt, noise, staged, w); });
 }

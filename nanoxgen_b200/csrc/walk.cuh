@@ -32,7 +32,7 @@ namespace dev {
 constexpr int kWalkMaxCvs = 32;
 constexpr int kWalkStride = kWalkMaxCvs + 1;   // float4 per staged strand row
 constexpr int kWalkAxisColumns = 12;           // noise lattice columns per axis and strand
-constexpr int kWalkRecords = 6;                // float4 setup records per strand
+constexpr int kWalkRecords = 8;                // float4 setup records per strand
 
 // Shared-memory bytes per warp.  Staged variants (noise or Classic scalars):
 // stage | records (aliased by the lattice once the base step has read them) |
@@ -60,6 +60,8 @@ __host__ __device__ constexpr size_t walk_head_bytes(bool noise) {
 //             guide * P, the guide's first entry in the offset table
 //   q = 4     (root position, 1 / weight sum)
 //   q = 5     (root normal in normal mode else 0, slot count as bits)
+//   q = 6, 7  Classic scalars without noise (walk_classic_setup): (first
+//             point, length scale) and (width radius, width override flag)
 // Nearest mode becomes one slot of weight 1 and normal mode zero slots, so
 // the base step evaluates every strand as
 //   base = root + (inv * sum_j w_j offsets[row_j + c] + normal' * t_c) * length_scale.
@@ -255,9 +257,69 @@ __device__ __forceinline__ int walk_strand(int item, float inv_p) {
     return static_cast<int>((static_cast<float>(item) + 0.5f) * inv_p);
 }
 
+// Base point c of strand s from its records (generate.h:246-267, :300-310).
+__device__ __forceinline__ F3 walk_base_point(const float4 *records, int s, int c, float t, float ls,
+                                              const float4 *offsets) {
+    const float4 head = records[4 * 32 + s];
+    const float4 tail = records[5 * 32 + s];
+    const uint32_t nb = __float_as_uint(tail.w);
+    F3 acc = {0.0f, 0.0f, 0.0f};
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const float4 gw = records[q * 32 + s];
+        if (static_cast<uint32_t>(2 * q) < nb) {
+            const float4 d = __ldg(offsets + (__float_as_uint(gw.x) + static_cast<uint32_t>(c)));
+            acc = acc + F3{d.x, d.y, d.z} * gw.y;
+        }
+        if (static_cast<uint32_t>(2 * q + 1) < nb) {
+            const float4 d = __ldg(offsets + (__float_as_uint(gw.z) + static_cast<uint32_t>(c)));
+            acc = acc + F3{d.x, d.y, d.z} * gw.w;
+        }
+    }
+    const F3 off = acc * head.w + F3{tail.x, tail.y, tail.z} * t;
+    return F3{head.x, head.y, head.z} + off * ls;
+}
+
+// Classic scalars without noise (xgen_classic_runtime.cpp:1650-1678,
+// :1827-1858), for this lane's strand before its base step: the first and
+// last base points give the chord; a strand whose scaled chord is near the
+// 1e-4 threshold measures its sampled spline (lanes that need it take turns
+// on `scratch`, 32 float4); a dropped strand gets point count 0.  Leaves
+// records 6 and 7 for walk_base.  Every lane of the warp calls it.
+__device__ __forceinline__ void walk_classic_setup(const LaunchArgs &g, float4 *records, int lane, bool valid,
+                                                   uint32_t local, const float *tvals, const float4 *offsets,
+                                                   float4 *scratch, int P) {
+    const ParamArgs &p = g.p;
+    const float ls = p.length_scale;
+    const float2 sc = __ldg(g.scalars + local);
+    const F3 front = walk_base_point(records, lane, 0, tvals[0], ls, offsets);
+    const F3 back = walk_base_point(records, lane, P - 1, tvals[P - 1], ls, offsets);
+    const float scale = g.classic_length ? sc.x : 1.0f;
+    const float raw_width = g.classic_width ? sc.y
+        : (p.radius_scale > 0.0f ? __fdiv_rn(__fmul_rn(2.0f, strand_radius(p, 0.0f)), p.radius_scale) : 0.0f);
+    bool keep = !(raw_width < 1.0e-4f);
+    const F3 chord = back - front;
+    const bool measure = keep && !(sqrtf(dot(chord, chord)) * scale > 1.01e-4f);
+    for (unsigned todo = __ballot_sync(kFull, measure); todo != 0u; todo &= todo - 1u) {
+        if (lane == __ffs(todo) - 1) {
+            for (int c = 0; c < P; ++c) {
+                const F3 b = walk_base_point(records, lane, c, tvals[c], ls, offsets);
+                scratch[c] = make_float4(b.x, b.y, b.z, 0.0f);
+            }
+            keep = !(__fmul_rn(classic_spline_length(scratch, P), scale) < 1.0e-4f);
+        }
+        __syncwarp();
+    }
+    const float radius = __fmul_rn(__fmul_rn(0.5f, raw_width < 0.0f ? 0.0f : raw_width), p.radius_scale);
+    records[6 * 32 + lane] = make_float4(front.x, front.y, front.z, scale);
+    records[7 * 32 + lane] = make_float4(radius, g.classic_width ? 1.0f : 0.0f, 0.0f, 0.0f);
+    if (!keep && valid && g.point_counts != nullptr) { g.point_counts[local] = 0u; }
+}
+
 // Base step: item = s * P + c over the batch, 32 consecutive items per pass,
-// into the stage or (DIRECT) straight to the output.
-template <bool DIRECT>
+// into the stage or (DIRECT) straight to the output; CLASSIC (with DIRECT)
+// applies records 6 and 7: scale about the first point, width override.
+template <bool DIRECT, bool CLASSIC = false>
 __device__ __forceinline__ void walk_base(const LaunchArgs &g, const float4 *records, float4 *stage,
                                           const uint32_t *locals, const float *tvals, const float *rvals,
                                           const float4 *offsets, int lane, int in_batch, int P, float inv_p) {
@@ -267,29 +329,18 @@ __device__ __forceinline__ void walk_base(const LaunchArgs &g, const float4 *rec
     for (int item = lane; item < items; item += 32) {
         const int s = walk_strand(item, inv_p);
         const int c = item - s * P;
-        const float4 head = records[4 * 32 + s];
-        const float4 tail = records[5 * 32 + s];
-        const uint32_t nb = __float_as_uint(tail.w);
-        F3 acc = {0.0f, 0.0f, 0.0f};
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const float4 gw = records[q * 32 + s];
-            if (static_cast<uint32_t>(2 * q) < nb) {
-                const float4 d = __ldg(offsets + (__float_as_uint(gw.x) + static_cast<uint32_t>(c)));
-                acc = acc + F3{d.x, d.y, d.z} * gw.y;
-            }
-            if (static_cast<uint32_t>(2 * q + 1) < nb) {
-                const float4 d = __ldg(offsets + (__float_as_uint(gw.z) + static_cast<uint32_t>(c)));
-                acc = acc + F3{d.x, d.y, d.z} * gw.w;
-            }
+        F3 base = walk_base_point(records, s, c, tvals[c], ls, offsets);
+        float radius = rvals[c];
+        if constexpr (CLASSIC) {
+            const float4 front = records[6 * 32 + s];
+            const float4 width = records[7 * 32 + s];
+            if (g.classic_length) { base = xadd(xyz(front), xmul(xsub(base, xyz(front)), front.w)); }
+            if (width.y != 0.0f) { radius = width.x; }
         }
-        const float t = tvals[c];
-        const F3 off = acc * head.w + F3{tail.x, tail.y, tail.z} * t;
-        const F3 base = F3{head.x, head.y, head.z} + off * ls;
         if constexpr (DIRECT) {
-            walk_emit(g, locals[s], P, c, make_float4(base.x, base.y, base.z, rvals[c]));
+            walk_emit(g, locals[s], P, c, make_float4(base.x, base.y, base.z, radius));
         } else {
-            stage[s * kWalkStride + c] = make_float4(base.x, base.y, base.z, rvals[c]);
+            stage[s * kWalkStride + c] = make_float4(base.x, base.y, base.z, radius);
         }
     }
 }
