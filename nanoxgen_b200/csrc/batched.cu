@@ -8,15 +8,18 @@
 //                      histogram, RootSample / root UV / point count outputs;
 //   batched_scan       one CTA per description: bin offsets;
 //   batched_scatter    per-description strand-locality orders;
-//   batched_offsets    every description's guide-offset table;
+//   batched_offsets    every description's guide-offset table and guide
+//                      frame records;
 //   batched_generate   persistent warps pull (description, 32-strand batch)
 //                      items from an atomic counter -- items of the costliest
 //                      descriptions first -- and run each item with its
-//                      description's tile (lanes per strand x CVs per lane)
-//                      and noise setting.
+//                      description's tile (lanes per strand x CVs per lane,
+//                      or the lane walk for noise-free strands of up to 32
+//                      CVs) and noise setting.
 // Six launches per frame whatever the description count, all enqueue-only
 // and capturable in one CUDA graph.
 #include "generator_core.cuh"
+#include "walk.cuh"
 #include "nxg_classic.h"
 #include "nxg_internal.h"
 #include "strand_math.cuh"
@@ -121,6 +124,9 @@ __global__ void batched_scatter_kernel(const __grid_constant__ BatchArgs b) {
     }
 }
 
+// Every description's guide-offset table (G x P float4) and guide frame
+// records (2 float4 per guide, after the table): G x P + G flat entries per
+// description.
 __global__ void batched_offsets_kernel(const __grid_constant__ BatchArgs b) {
     for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < b.total_offsets;
          i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
@@ -129,9 +135,16 @@ __global__ void batched_offsets_kernel(const __grid_constant__ BatchArgs b) {
         const BatchDesc &d = b.d[di];
         const uint64_t local = i - d.offset_begin;
         const uint32_t P = d.g.p.cvs_per_strand;
-        const_cast<float4 *>(d.offsets)[local] = guide_offset_entry(d.g.a, d.g.f, P,
-                                                                    static_cast<uint32_t>(local / P),
-                                                                    static_cast<uint32_t>(local % P));
+        const uint64_t table = static_cast<uint64_t>(d.g.a.guide_count) * P;
+        if (local < table) {
+            const_cast<float4 *>(d.offsets)[local] = guide_offset_entry(d.g.a, d.g.f, P,
+                                                                        static_cast<uint32_t>(local / P),
+                                                                        static_cast<uint32_t>(local % P));
+        } else {
+            const uint64_t gi = local - table;
+            guide_frame_entry(d.g.a, d.g.f, d.g.p.support_scale, static_cast<uint32_t>(gi),
+                              const_cast<float4 *>(d.offsets) + table + 2u * gi);
+        }
     }
 }
 
@@ -212,6 +225,41 @@ constexpr size_t kBatchLatticeBytes = sizeof(float2) * 384u;
 constexpr size_t kBatchWarpBytes =
     kBatchTableBytes + kBatchTvalBytes + kBatchRecordBytes + kBatchStageBytes + kBatchLatticeBytes;
 
+static_assert(kBatchRecordBytes >= kWalkRecordBytes, "lane-walk records fit the record area");
+static_assert(kBatchStageBytes >= sizeof(float4) * kWalkMaxCvs, "spline scratch fits the stage area");
+static_assert(kBatchLatticeBytes >= kWalkLocalBytes, "output words fit the lattice area");
+
+// A noise-free description on the lane-walk tile (2..32 CVs): setup and the
+// lane-parallel base step writing the output directly (walk.cuh), with the
+// Classic application when the description has scalars.  Roots, root UVs
+// and point counts come from batched_prepare.
+template <bool CLASSIC>
+__device__ __noinline__ void batched_walk_item(const BatchDesc &d, uint32_t batch, uint32_t end, int lane,
+                                               unsigned char *mine) {
+    const float *tvals = reinterpret_cast<const float *>(mine + kBatchTableBytes);
+    const float *rvals = tvals + 2 * kWalkMaxCvs;
+    float4 *records = reinterpret_cast<float4 *>(mine + kBatchTableBytes + kBatchTvalBytes);
+    float4 *scratch = reinterpret_cast<float4 *>(mine + kBatchTableBytes + kBatchTvalBytes + kBatchRecordBytes);
+    uint32_t *locals = reinterpret_cast<uint32_t *>(mine + kBatchTableBytes + kBatchTvalBytes + kBatchRecordBytes +
+                                                    kBatchStageBytes);
+    const int P = static_cast<int>(d.g.p.cvs_per_strand);
+    const uint32_t item = batch + static_cast<uint32_t>(lane);
+    const bool valid = item < end;
+    const int in_batch = static_cast<int>(end - batch);
+    const float inv_p = 1.0f / static_cast<float>(P);
+    walk_setup<false>(d.g, records, locals, nullptr, lane, valid ? item : batch, valid, static_cast<uint32_t>(P),
+                      false);
+    __syncwarp();
+    if (CLASSIC && d.g.scalars != nullptr) {
+        walk_classic_setup(d.g, records, lane, valid, locals[lane] & 0x7fffffffu, tvals, d.offsets, scratch, P);
+        __syncwarp();
+        walk_base<true, true>(d.g, records, nullptr, locals, tvals, rvals, d.offsets, lane, in_batch, P, inv_p);
+    } else {
+        walk_base<true, false>(d.g, records, nullptr, locals, tvals, rvals, d.offsets, lane, in_batch, P, inv_p);
+    }
+    __syncwarp();
+}
+
 template <int L, int PPT, bool NOISE, bool CLASSIC>
 __device__ __noinline__ void batched_item(const BatchDesc &d, uint32_t batch, uint32_t end, int lane,
                                              unsigned char *mine) {
@@ -286,12 +334,17 @@ __global__ void batched_generate_kernel(const __grid_constant__ BatchArgs b) {
                                            __ldg(d.g.a.gradients + 3 * i + 2), 0.0f);
                 }
             }
-            for (int i = lane; i < P; i += 32) { tvals[i] = __fdiv_rn(static_cast<float>(i), static_cast<float>(P - 1)); }
+            for (int i = lane; i < P; i += 32) {
+                tvals[i] = __fdiv_rn(static_cast<float>(i), static_cast<float>(P - 1));
+                if (P <= kWalkMaxCvs) { tvals[2 * kWalkMaxCvs + i] = strand_radius(d.g.p, tvals[i]); }
+            }
             __syncwarp();
             current = di;
         }
         const uint32_t end = min(batch + 32u, d.g.count);
-        if (CLASSIC && d.g.scalars != nullptr) {
+        if (d.lanes == 1u) {
+            batched_walk_item<CLASSIC>(d, batch, end, lane, mine);
+        } else if (CLASSIC && d.g.scalars != nullptr) {
             if (d.noise) {
                 batched_dispatch_lanes<PPT, true, CLASSIC>(d, batch, end, lane, mine);
             } else {
@@ -331,18 +384,20 @@ BatchLayout batch_layout(const nxg_device_asset_desc *assets, const nxg_generati
         l.bins.push_back(at);
         at += up((G + 1u) * 4u);
         l.offsets.push_back(at);
-        at += up(G * P * 16u);
+        at += up(G * (P + 2u) * 16u);  // offset table, then 2 guide frame records per guide
     }
     l.total = at;
     return l;
 }
 
 // Lanes per strand of a description in a batched launch whose CVs per lane
-// are `ppt`: the registered tile's lanes when it uses the same CVs per lane,
-// else the narrowest power-of-two group holding the strand.
+// are `ppt`: 1 (a lane-walk item) for a noise-free description on the
+// lane-walk tile; the registered tile's lanes when it uses the same CVs per
+// lane; else the narrowest power-of-two group holding the strand.
 uint32_t batch_lanes(uint32_t P, bool noise, uint32_t ppt) {
     nxg_tile t{};
     nxg_get_tile(P, noise ? 1u : 0u, &t);
+    if (t.lanes_per_strand == 1u && !noise && P <= static_cast<uint32_t>(dev::kWalkMaxCvs)) { return 1u; }
     if (t.cvs_per_lane == ppt && t.lanes_per_strand * ppt >= P) { return t.lanes_per_strand; }
     uint32_t l = 2u;
     while (l * ppt < P) { l *= 2u; }
@@ -460,6 +515,7 @@ uint32_t generate_batched(const nxg_device_asset_desc *assets, const nxg_deforme
             bd.g.classic_width = classic[d].apply_width != 0u;
         }
         bd.offsets = reinterpret_cast<const float4 *>(w + layout.offsets[d]);
+        bd.g.guide_frames = bd.offsets + uint64_t{assets[d].header.guide_count} * params[d].cvs_per_strand;
         bd.keys = reinterpret_cast<uint32_t *>(w + layout.keys[d]);
         bd.bins = reinterpret_cast<uint32_t *>(w + layout.bins[d]);
         bd.noise = bd.g.p.noise;
@@ -469,7 +525,7 @@ uint32_t generate_batched(const nxg_device_asset_desc *assets, const nxg_deforme
         bd.offset_begin = offsets;
         strands += params[d].strand_count;
         items += (params[d].strand_count + 32u * warps_per_cta - 1u) / (32u * warps_per_cta);
-        offsets += uint64_t{assets[d].header.guide_count} * params[d].cvs_per_strand;
+        offsets += uint64_t{assets[d].header.guide_count} * (params[d].cvs_per_strand + 1u);
     }
     b.total_strands = strands;
     b.total_items = items;

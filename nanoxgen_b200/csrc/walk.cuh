@@ -129,13 +129,13 @@ __device__ __forceinline__ Root walk_root(const AssetArgs &a, const FrameArgs &f
 
 // Setup step for this lane's strand.  The stencil slots follow eval_slot and
 // the loop of generate.h:214-244 with the frame's guide roots, normals and
-// support radii read from the per-frame guide records.  Also writes the
-// strand's root UV and point count, and stages its twelve RootSample words
-// at root_words[lane * 12] for walk_store_roots.
+// support radii read from the per-frame guide records.  With `outputs`,
+// also writes the strand's root UV and point count and stages its twelve
+// RootSample words at root_words[lane * 12] for walk_store_roots.
 template <bool NOISE>
 __device__ __forceinline__ WalkRoot walk_setup(const LaunchArgs &g, float4 *records, uint32_t *locals,
                                                uint32_t *root_words, int lane, uint32_t pick, bool valid,
-                                               uint32_t P) {
+                                               uint32_t P, bool outputs = true) {
     const AssetArgs &a = g.a;
     const FrameArgs &f = g.f;
     const ParamArgs &p = g.p;
@@ -148,11 +148,11 @@ __device__ __forceinline__ WalkRoot walk_setup(const LaunchArgs &g, float4 *reco
     r.surface_u = F3{0.0f, 0.0f, 0.0f};
     F3 rest_position = {0.0f, 0.0f, 0.0f};
     const Root root = walk_root<NOISE>(a, f, p.seed, g.first_strand + local, r.surface_u, rest_position);
-    if (g.roots) {
+    if (outputs && g.roots) {
 #pragma unroll
         for (int w = 0; w < 12; ++w) { root_words[lane * 12 + w] = root_word(root, w); }
     }
-    if (valid) {  // generate.h:621-623
+    if (outputs && valid) {  // generate.h:621-623
         if (g.root_uvs) { g.root_uvs[local] = make_float2(root.u, root.v); }
         if (g.point_counts) { g.point_counts[local] = P; }
     }
