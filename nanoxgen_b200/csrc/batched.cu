@@ -53,6 +53,7 @@ struct BatchDesc {
 
 struct BatchArgs {
     uint32_t count;
+    uint32_t warp_bytes;       // shared memory per warp of batched_generate
     uint32_t total_strands;
     uint32_t total_items;
     uint32_t *item_counter;
@@ -229,6 +230,47 @@ static_assert(kBatchRecordBytes >= kWalkRecordBytes, "lane-walk records fit the 
 static_assert(kBatchStageBytes >= sizeof(float4) * kWalkMaxCvs, "spline scratch fits the stage area");
 static_assert(kBatchLatticeBytes >= kWalkLocalBytes, "output words fit the lattice area");
 
+// Per-warp shared memory when some description takes noisy lane-walk items:
+// table | t values and radii | stage | records aliased by the lattice |
+// output words.
+constexpr size_t kBatchWalkWarpBytes =
+    kBatchTableBytes + kBatchTvalBytes + kWalkStageBytes + kWalkLatticeBytes + kWalkLocalBytes;
+static_assert(kWalkLatticeBytes >= kWalkRecordBytes, "records fit the lattice area");
+
+// A noisy description on the lane-walk tile (2..32 CVs): setup, base into the
+// stage, the frame walk and the store step (walk.cuh), with the Classic
+// application when the description has scalars.
+template <bool CLASSIC>
+__device__ __noinline__ void batched_noise_walk_item(const BatchDesc &d, uint32_t batch, uint32_t end, int lane,
+                                                     unsigned char *mine) {
+    const float4 *table = reinterpret_cast<const float4 *>(mine);
+    const float *tvals = reinterpret_cast<const float *>(mine + kBatchTableBytes);
+    const float *rvals = tvals + 2 * kWalkMaxCvs;
+    float4 *stage = reinterpret_cast<float4 *>(mine + kBatchTableBytes + kBatchTvalBytes);
+    unsigned char *after_stage = mine + kBatchTableBytes + kBatchTvalBytes + kWalkStageBytes;
+    float4 *records = reinterpret_cast<float4 *>(after_stage);
+    float2 *lattice = reinterpret_cast<float2 *>(after_stage);
+    uint32_t *locals = reinterpret_cast<uint32_t *>(after_stage + kWalkLatticeBytes);
+    const int P = static_cast<int>(d.g.p.cvs_per_strand);
+    const uint32_t item = batch + static_cast<uint32_t>(lane);
+    const bool valid = item < end;
+    const int in_batch = static_cast<int>(end - batch);
+    const float inv_p = 1.0f / static_cast<float>(P);
+    const WalkRoot wr = walk_setup<true>(d.g, records, locals, nullptr, lane, valid ? item : batch, valid,
+                                         static_cast<uint32_t>(P), false);
+    __syncwarp();
+    walk_base<false>(d.g, records, stage, locals, tvals, rvals, d.offsets, lane, in_batch, P, inv_p);
+    __syncwarp();
+    walk_frame(d.g.p, wr, lane < in_batch, stage + lane * kWalkStride, lattice + lane, tvals, rvals, table, P);
+    __syncwarp();
+    if (CLASSIC && d.g.scalars != nullptr) {
+        walk_store<true>(d.g, stage, locals, lane, in_batch, P, inv_p);
+    } else {
+        walk_store<false>(d.g, stage, locals, lane, in_batch, P, inv_p);
+    }
+    __syncwarp();
+}
+
 // A noise-free description on the lane-walk tile (2..32 CVs): setup and the
 // lane-parallel base step writing the output directly (walk.cuh), with the
 // Classic application when the description has scalars.  Roots, root UVs
@@ -307,7 +349,7 @@ __global__ void batched_generate_kernel(const __grid_constant__ BatchArgs b) {
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const uint32_t warps = blockDim.x >> 5;
-    unsigned char *mine = reinterpret_cast<unsigned char *>(smem) + kBatchWarpBytes * warp;
+    unsigned char *mine = reinterpret_cast<unsigned char *>(smem) + b.warp_bytes * warp;
     float4 *table = reinterpret_cast<float4 *>(mine);
     float *tvals = reinterpret_cast<float *>(mine + kBatchTableBytes);
     int current = -1;
@@ -343,7 +385,11 @@ __global__ void batched_generate_kernel(const __grid_constant__ BatchArgs b) {
         }
         const uint32_t end = min(batch + 32u, d.g.count);
         if (d.lanes == 1u) {
-            batched_walk_item<CLASSIC>(d, batch, end, lane, mine);
+            if (d.noise) {
+                batched_noise_walk_item<CLASSIC>(d, batch, end, lane, mine);
+            } else {
+                batched_walk_item<CLASSIC>(d, batch, end, lane, mine);
+            }
         } else if (CLASSIC && d.g.scalars != nullptr) {
             if (d.noise) {
                 batched_dispatch_lanes<PPT, true, CLASSIC>(d, batch, end, lane, mine);
@@ -391,13 +437,12 @@ BatchLayout batch_layout(const nxg_device_asset_desc *assets, const nxg_generati
 }
 
 // Lanes per strand of a description in a batched launch whose CVs per lane
-// are `ppt`: 1 (a lane-walk item) for a noise-free description on the
-// lane-walk tile; the registered tile's lanes when it uses the same CVs per
+// are `ppt`: 1 (lane-walk items) for a description on the lane-walk tile; the registered tile's lanes when it uses the same CVs per
 // lane; else the narrowest power-of-two group holding the strand.
 uint32_t batch_lanes(uint32_t P, bool noise, uint32_t ppt) {
     nxg_tile t{};
     nxg_get_tile(P, noise ? 1u : 0u, &t);
-    if (t.lanes_per_strand == 1u && !noise && P <= static_cast<uint32_t>(dev::kWalkMaxCvs)) { return 1u; }
+    if (t.lanes_per_strand == 1u && P <= static_cast<uint32_t>(dev::kWalkMaxCvs)) { return 1u; }
     if (t.cvs_per_lane == ppt && t.lanes_per_strand * ppt >= P) { return t.lanes_per_strand; }
     uint32_t l = 2u;
     while (l * ppt < P) { l *= 2u; }
@@ -474,14 +519,25 @@ uint32_t generate_batched(const nxg_device_asset_desc *assets, const nxg_deforme
     if (cudaGetDevice(&device) == cudaSuccess) {
         cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
     }
-    uint32_t block = std::min(static_cast<uint32_t>(attr.maxThreadsPerBlock) / 32u * 32u,
-                              std::max<uint32_t>(32u, (cfg.block_size + 31u) / 32u * 32u));
-    while (block > 32u && dev::kBatchWarpBytes * (block / 32u) + 64u > static_cast<size_t>(smem_optin)) { block -= 32u; }
+    // Noisy descriptions on the lane-walk tile need the walk's stage and
+    // lattice per warp; CTAs are then one warp each, so the SM holds as many
+    // of those warps as its shared memory allows.
+    bool noise_walk = false;
+    for (uint32_t d = 0; d < count; ++d) {
+        const bool noise = params[d].noise_amplitude != 0.0f && params[d].noise_mask != 0.0f;
+        noise_walk = noise_walk || (noise && batch_lanes(params[d].cvs_per_strand, true, ppt) == 1u);
+    }
+    const size_t warp_bytes = noise_walk ? dev::kBatchWalkWarpBytes : dev::kBatchWarpBytes;
+    uint32_t block = noise_walk ? 32u
+                                : std::min(static_cast<uint32_t>(attr.maxThreadsPerBlock) / 32u * 32u,
+                                           std::max<uint32_t>(32u, (cfg.block_size + 31u) / 32u * 32u));
+    while (block > 32u && warp_bytes * (block / 32u) + 64u > static_cast<size_t>(smem_optin)) { block -= 32u; }
     const uint32_t warps_per_cta = block / 32u;
 
     auto *w = static_cast<unsigned char *>(workspace);
     dev::BatchArgs b{};
     b.count = count;
+    b.warp_bytes = static_cast<uint32_t>(warp_bytes);
     b.item_counter = reinterpret_cast<uint32_t *>(w + layout.counter);
     // Costliest descriptions first (CVs per strand, tripled with noise), so the
     // longest work items start early and the tail is made of cheap ones.
@@ -558,7 +614,7 @@ uint32_t generate_batched(const nxg_device_asset_desc *assets, const nxg_deforme
     dev::batched_offsets_kernel<<<std::max(1u, offset_blocks), 256, 0, s>>>(b);
     if ((status = record_cuda(cudaGetLastError()))) { return status; }
 
-    const size_t shm = dev::kBatchWarpBytes * (block / 32u);
+    const size_t shm = warp_bytes * (block / 32u);
     if ((status = record_cuda(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                    static_cast<int>(shm))))) {
         return status;
