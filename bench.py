@@ -32,7 +32,11 @@ STRANDS_PER_GPU = 1_000_000
 FALLBACK_HBM_GBS = 6650.0
 # strand_keys, exclusive_scan, scatter_order (the strand order), guide_offsets,
 # strand_roots, generate
-KERNELS_PER_STEP = 6
+# Launches per step of the large workload: strand keys, bin scan, scatter,
+# guide offsets, then the lane-walk generator (tile lanes 1) or strand roots
+# plus the lane-group generator.
+def kernels_per_step(tile) -> int:
+    return 5 if tile[0] == 1 else 6
 
 
 def parse_args():
@@ -66,10 +70,12 @@ def measured_peak():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def profile_traffic_per_point():
-    """DRAM bytes per generated point of the generate kernel, from the ncu
-    summary committed under profiles/ (None until one exists)."""
-    path = os.path.join(ROOT, "profiles", "generate_kernel_large_sphere.md")
+def profile_traffic_per_point(walk: bool = True):
+    """DRAM bytes per generated point of the generate kernel (the lane-walk
+    kernel, or the lane-group kernel), from the ncu summary committed under
+    profiles/ (None until one exists)."""
+    name = "generate_walk_kernel_large_sphere.md" if walk else "generate_kernel_large_sphere.md"
+    path = os.path.join(ROOT, "profiles", name)
     try:
         with open(path) as fh:
             m = re.search(r"traffic_bytes_per_point:\s*([0-9.eE+-]+)", fh.read())
@@ -326,7 +332,13 @@ def run_gpu_arm(args):
     alg_bytes = out_bytes + asset.nbytes
     peak, peak_kind = measured_peak()
     achieved = alg_bytes / (kernel_ms / 1e3) / 1e9
-    tpp = profile_traffic_per_point()
+    tpp = profile_traffic_per_point(tile[0] == 1)
+    if tile[0] != 1:
+        kernel_name = "generate_kernel<%d,%d,%s>" % (tile[0], tile[1], "noise" if noise else "plain")
+    elif noise and tile[2] <= 64:
+        kernel_name = "generate_pipe_kernel"
+    else:
+        kernel_name = "generate_walk_kernel<%s>" % ("noise" if noise else "plain")
     line = {
         "metric": "points/sec", "value": points_total / (ms_per_step / 1e3), "unit": "points/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
@@ -341,13 +353,13 @@ def run_gpu_arm(args):
         "hbm_gbs": world * alg_bytes / (ms_per_step / 1e3) / 1e9,
         "tile": {"lanes_per_strand": tile[0], "cvs_per_lane": tile[1], "block_size": tile[2],
                  "chosen_by": "--tile" if args.tile else "nxg_autotune_packed in warm-up"},
-        "roofline": {"bound": "hbm", "kernel": "generate_kernel<%d,%d,%s>" % (tile[0], tile[1], "noise" if noise else "plain"),
+        "roofline": {"bound": "hbm", "kernel": kernel_name,
                      "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
                      "traffic": (tpp * S * P) if tpp else None,
                      "algorithmic_bytes": alg_bytes, "kernel_ms": kernel_ms,
                      "note": "algorithmic bytes = 16 B/point + 60 B/strand (roots, root UVs, counts) + asset"},
-        "clocks": clocks, "gpu_launches": KERNELS_PER_STEP * args.steps,
+        "clocks": clocks, "gpu_launches": kernels_per_step(tile) * args.steps,
     }
     if e2e:
         line["e2e"] = e2e
