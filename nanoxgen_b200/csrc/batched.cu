@@ -246,7 +246,7 @@ __device__ __noinline__ void batched_noise_walk_item(const BatchDesc &d, uint32_
     const float4 *table = reinterpret_cast<const float4 *>(mine);
     const float *tvals = reinterpret_cast<const float *>(mine + kBatchTableBytes);
     const float *rvals = tvals + 2 * kWalkMaxCvs;
-    float4 *stage = reinterpret_cast<float4 *>(mine + kBatchTableBytes + kBatchTvalBytes);
+    float *stage = reinterpret_cast<float *>(mine + kBatchTableBytes + kBatchTvalBytes);
     unsigned char *after_stage = mine + kBatchTableBytes + kBatchTvalBytes + kWalkStageBytes;
     float4 *records = reinterpret_cast<float4 *>(after_stage);
     float2 *lattice = reinterpret_cast<float2 *>(after_stage);
@@ -261,12 +261,12 @@ __device__ __noinline__ void batched_noise_walk_item(const BatchDesc &d, uint32_
     __syncwarp();
     walk_base<false>(d.g, records, stage, locals, tvals, rvals, d.offsets, lane, in_batch, P, inv_p);
     __syncwarp();
-    walk_frame(d.g.p, wr, lane < in_batch, stage + lane * kWalkStride, lattice + lane, tvals, rvals, table, P);
+    walk_frame(d.g.p, wr, lane < in_batch, stage + lane * kWalkRowFloats, lattice + lane, tvals, table, P);
     __syncwarp();
     if (CLASSIC && d.g.scalars != nullptr) {
-        walk_store<true>(d.g, stage, locals, lane, in_batch, P, inv_p);
+        walk_store<true>(d.g, stage, locals, rvals, lane, in_batch, P, inv_p);
     } else {
-        walk_store<false>(d.g, stage, locals, lane, in_batch, P, inv_p);
+        walk_store<false>(d.g, stage, locals, rvals, lane, in_batch, P, inv_p);
     }
     __syncwarp();
 }

@@ -100,7 +100,7 @@ __global__ void generate_kernel(LaunchArgs g, const float4 *offsets) {
 // store.  Without noise the base step writes the output directly (no
 // stage), applying Classic scalars itself when given.
 template <bool NOISE, bool CLASSIC>
-__global__ void __launch_bounds__(256, 1) generate_walk_kernel(LaunchArgs g, const float4 *offsets) {
+__global__ void __launch_bounds__(384, 1) generate_walk_kernel(LaunchArgs g, const float4 *offsets) {
     constexpr bool kStaged = NOISE;
     constexpr bool kWalk = NOISE;  // noise walk inside this kernel
     extern __shared__ float4 smem[];
@@ -126,7 +126,7 @@ __global__ void __launch_bounds__(256, 1) generate_walk_kernel(LaunchArgs g, con
     const int warp = threadIdx.x >> 5;
     constexpr size_t kWarpBytes = walk_warp_bytes(kWalk, kStaged);
     unsigned char *mine = warp_base + kWarpBytes * warp;
-    float4 *stage = reinterpret_cast<float4 *>(mine);  // staged variants only
+    float *stage = reinterpret_cast<float *>(mine);  // staged variants only
     float4 *records = reinterpret_cast<float4 *>(kStaged ? mine + kWalkStageBytes : mine);
     float2 *lattice = reinterpret_cast<float2 *>(mine + kWalkStageBytes);
     uint32_t *root_words = reinterpret_cast<uint32_t *>(kStaged ? mine : mine + kWalkRecordBytes);
@@ -157,11 +157,11 @@ __global__ void __launch_bounds__(256, 1) generate_walk_kernel(LaunchArgs g, con
                                                inv_p);
         __syncwarp();
         if constexpr (kWalk) {
-            walk_frame(g.p, wr, lane < in_batch, stage + lane * kWalkStride, lattice + lane, tvals, rvals, table, P);
+            walk_frame(g.p, wr, lane < in_batch, stage + lane * kWalkRowFloats, lattice + lane, tvals, table, P);
             __syncwarp();
         }
         if constexpr (kStaged) {
-            walk_store<CLASSIC>(g, stage, locals, lane, in_batch, P, inv_p);
+            walk_store<CLASSIC>(g, stage, locals, rvals, lane, in_batch, P, inv_p);
             __syncwarp();
         }
     }
@@ -213,7 +213,7 @@ __global__ void __launch_bounds__(64, 1) generate_pipe_kernel(LaunchArgs g, cons
         const int in_batch = static_cast<int>(min(32u, end - batch));
         const int b = static_cast<int>(it & 1u);
         unsigned char *buf = base + b * kPipeBufferBytes;
-        float4 *stage = reinterpret_cast<float4 *>(buf);
+        float *stage = reinterpret_cast<float *>(buf);
         float *fr = reinterpret_cast<float *>(buf + kWalkStageBytes);  // 12 x 32: root position, normal, surface_u, domain
         uint32_t *locals = reinterpret_cast<uint32_t *>(buf + kWalkStageBytes + kPipeFrameBytes);
         if (producer) {
@@ -249,9 +249,9 @@ __global__ void __launch_bounds__(64, 1) generate_pipe_kernel(LaunchArgs g, cons
             wr.normal = F3{fr[3 * 32 + lane], fr[4 * 32 + lane], fr[5 * 32 + lane]};
             wr.surface_u = F3{fr[6 * 32 + lane], fr[7 * 32 + lane], fr[8 * 32 + lane]};
             wr.domain = F3{fr[9 * 32 + lane], fr[10 * 32 + lane], fr[11 * 32 + lane]};
-            walk_frame(g.p, wr, lane < in_batch, stage + lane * kWalkStride, lattice + lane, tvals, rvals, table, P);
+            walk_frame(g.p, wr, lane < in_batch, stage + lane * kWalkRowFloats, lattice + lane, tvals, table, P);
             __syncwarp();
-            walk_store<false>(g, stage, locals, lane, in_batch, P, inv_p);
+            walk_store<false>(g, stage, locals, rvals, lane, in_batch, P, inv_p);
             if (it + 2u < iterations) { named_arrive(3u + b); }
         }
     }
@@ -771,8 +771,9 @@ bool valid_tile(uint32_t P, uint32_t lanes, uint32_t ppt) {
 }
 
 // Tile shape for P CVs: the registered one, else the lane-walk generator for
-// 2..32 CVs (lanes_per_strand 1, 128-thread CTAs), else four CVs per lane on
-// the narrowest power-of-two group that holds the strand.
+// 2..32 CVs (lanes_per_strand 1; CTAs of 320 threads with noise, 256
+// without), else four CVs per lane on the narrowest power-of-two group that
+// holds the strand.
 void default_tile(uint32_t P, bool noise, int *lanes, int *ppt, uint32_t *block) {
     const uint32_t packed = P <= kMaxParallelCvs ? g_tiles[P][noise ? 1 : 0].load(std::memory_order_relaxed) : 0u;
     if (packed) {
@@ -784,7 +785,7 @@ void default_tile(uint32_t P, bool noise, int *lanes, int *ppt, uint32_t *block)
     if (P >= 2u && P <= static_cast<uint32_t>(dev::kWalkMaxCvs)) {  // the lane-walk generator
         *lanes = 1;
         *ppt = 1;
-        *block = 128u;
+        *block = noise ? 320u : 256u;  // with noise: ten 22 KB warps fill the SM's shared memory
         return;
     }
     *ppt = 4;
@@ -1179,7 +1180,7 @@ uint32_t nxg_autotune_packed(const nxg_device_asset_desc *asset, const nxg_defor
     nxg_tile winner{0u, 0u, 0u};
     float winner_ms = 0.0f;
     const uint32_t reps = std::max(1u, repeats);
-    const uint32_t blocks[3] = {64u, 128u, 256u};
+    const uint32_t blocks[4] = {64u, 128u, 256u, 320u};
     for (uint32_t lanes = 1u; lanes <= 32u && !error; lanes *= 2u) {
         for (uint32_t ppt = 1u; ppt <= 4u && !error; ppt *= 2u) {
             // tiles that hold the strand without idling half of their lanes

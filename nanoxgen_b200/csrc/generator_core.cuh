@@ -233,9 +233,11 @@ __device__ __forceinline__ float2 lattice_column(const float4 *table, int axis, 
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ F3 xyz(float4 v) { return {v.x, v.y, v.z}; }
 
-__device__ inline F3 classic_curve_eval(const float4 *pts, int P, float t) {
-    if (t < 1.0e-7f) { return xyz(pts[0]); }
-    if (t > 1.0f - 1.0e-7f) { return xyz(pts[P - 1]); }
+// pt(i) returns CV i of the strand.
+template <class Pts>
+__device__ inline F3 classic_curve_eval_by(Pts pt, int P, float t) {
+    if (t < 1.0e-7f) { return pt(0); }
+    if (t > 1.0f - 1.0e-7f) { return pt(P - 1); }
     const float scaled = __fmul_rn(t, static_cast<float>(P - 1));
     const int span = static_cast<int>(static_cast<uint32_t>(scaled));
     const float f = __fsub_rn(scaled, static_cast<float>(span));
@@ -246,26 +248,31 @@ __device__ inline F3 classic_curve_eval(const float4 *pts, int P, float t) {
     const float b1 = __fadd_rn(__fsub_rn(__fmul_rn(3.0f, f3), __fmul_rn(6.0f, f2)), 4.0f);
     const float b2 =
         __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(-3.0f, f3), __fmul_rn(3.0f, f2)), __fmul_rn(3.0f, f)), 1.0f);
-    const F3 p0 = span == 0 ? xsub(xmul(xyz(pts[0]), 2.0f), xyz(pts[1])) : xyz(pts[span - 1]);
-    const F3 p1 = xyz(pts[span]);
-    const F3 p2 = xyz(pts[span + 1]);
-    const F3 p3 = span + 2 == P ? xsub(xmul(xyz(pts[P - 1]), 2.0f), xyz(pts[P - 2])) : xyz(pts[span + 2]);
+    const F3 p0 = span == 0 ? xsub(xmul(pt(0), 2.0f), pt(1)) : pt(span - 1);
+    const F3 p1 = pt(span);
+    const F3 p2 = pt(span + 1);
+    const F3 p3 = span + 2 == P ? xsub(xmul(pt(P - 1), 2.0f), pt(P - 2)) : pt(span + 2);
     return xmul(xadd(xadd(xadd(xmul(p0, b0), xmul(p1, b1)), xmul(p2, b2)), xmul(p3, f3)), 1.0f / 6.0f);
 }
 
-__device__ inline float classic_spline_length(const float4 *pts, int P) {
+template <class Pts>
+__device__ inline float classic_spline_length_by(Pts pt, int P) {
     const int intervals = 2 * P + 4;
     const float step = __fdiv_rn(1.0f, static_cast<float>(intervals));
-    F3 previous = xyz(pts[0]);
+    F3 previous = pt(0);
     float length = 0.0f;
     for (int k = 1; k < intervals; ++k) {
-        const F3 current = classic_curve_eval(pts, P, __fmul_rn(step, static_cast<float>(k)));
+        const F3 current = classic_curve_eval_by(pt, P, __fmul_rn(step, static_cast<float>(k)));
         const F3 d = xsub(current, previous);
         length = __fadd_rn(length, __fsqrt_rn(xdot(d, d)));
         previous = current;
     }
-    const F3 d = xsub(xyz(pts[P - 1]), previous);
+    const F3 d = xsub(pt(P - 1), previous);
     return __fadd_rn(length, __fsqrt_rn(xdot(d, d)));
+}
+
+__device__ inline float classic_spline_length(const float4 *pts, int P) {
+    return classic_spline_length_by([pts](int i) { return xyz(pts[i]); }, P);
 }
 
 // Phase B: strand b of the batch on an L-lane group; lane gl owns the

@@ -7,7 +7,7 @@
 //   base   (lane = CV)      the base curve from the guide-offset table, read
 //                           as coalesced rows (consecutive lanes on
 //                           consecutive CVs of one guide), into a stage in
-//                           shared memory, one 33-float4 row per strand;
+//                           shared memory, one row of 33 xyz slots per strand;
 //   frame  (lane = strand)  with noise: the arc-length prefix, the strand's
 //                           noise lattice, then the reference's cursor walk
 //                           (generate.h:445-502) over the staged row -- the
@@ -19,9 +19,9 @@
 //                           stores, with the Classic application when
 //                           per-root scalars are given.
 //
-// Stage rows are 33 float4 apart, so a warp reading column c of 32 rows
-// (frame step) and a warp reading one row (base/store steps) are both free of
-// shared-memory bank conflicts.
+// Stage rows are 99 words apart and a CV takes 3 words; both strides are odd,
+// so a warp reading column c of 32 rows (frame step) and a warp reading one
+// row (base/store steps) are both free of shared-memory bank conflicts.
 #pragma once
 
 #include "generator_core.cuh"
@@ -30,7 +30,8 @@ namespace nxg {
 namespace dev {
 
 constexpr int kWalkMaxCvs = 32;
-constexpr int kWalkStride = kWalkMaxCvs + 1;   // float4 per staged strand row
+constexpr int kWalkStride = kWalkMaxCvs + 1;   // CV slots per staged strand row
+constexpr int kWalkRowFloats = 3 * kWalkStride; // a row holds x, y, z per CV (99 words: an odd stride)
 constexpr int kWalkAxisColumns = 12;           // noise lattice columns per axis and strand
 constexpr int kWalkRecords = 8;                // float4 setup records per strand
 
@@ -39,7 +40,7 @@ constexpr int kWalkRecords = 8;                // float4 setup records per stran
 // output words; the RootSample words use the stage.  The plain variant has no
 // stage -- its base step writes the output directly -- so: records | RootSample
 // words | output words.
-constexpr size_t kWalkStageBytes = sizeof(float4) * 32u * kWalkStride;
+constexpr size_t kWalkStageBytes = sizeof(float) * 32u * kWalkRowFloats;
 constexpr size_t kWalkRecordBytes = sizeof(float4) * kWalkRecords * 32u;
 constexpr size_t kWalkLatticeBytes = sizeof(float2) * 3u * kWalkAxisColumns * 32u;
 constexpr size_t kWalkRootWordBytes = sizeof(uint32_t) * 12u * 32u;
@@ -251,6 +252,16 @@ __device__ __forceinline__ void walk_emit(const LaunchArgs &g, uint32_t word, in
     }
 }
 
+// CV c of a staged row.
+__device__ __forceinline__ F3 stage_get(const float *row, int c) {
+    return F3{row[3 * c], row[3 * c + 1], row[3 * c + 2]};
+}
+__device__ __forceinline__ void stage_put(float *row, int c, F3 v) {
+    row[3 * c] = v.x;
+    row[3 * c + 1] = v.y;
+    row[3 * c + 2] = v.z;
+}
+
 // Strand of a flattened (strand, CV) item: floor((item + 0.5) / P), exact for
 // item < 32 * 32 (the quotient is at least 0.5 / P from an integer).
 __device__ __forceinline__ int walk_strand(int item, float inv_p) {
@@ -320,7 +331,7 @@ __device__ __forceinline__ void walk_classic_setup(const LaunchArgs &g, float4 *
 // into the stage or (DIRECT) straight to the output; CLASSIC (with DIRECT)
 // applies records 6 and 7: scale about the first point, width override.
 template <bool DIRECT, bool CLASSIC = false>
-__device__ __forceinline__ void walk_base(const LaunchArgs &g, const float4 *records, float4 *stage,
+__device__ __forceinline__ void walk_base(const LaunchArgs &g, const float4 *records, float *stage,
                                           const uint32_t *locals, const float *tvals, const float *rvals,
                                           const float4 *offsets, int lane, int in_batch, int P, float inv_p) {
     const int items = in_batch * P;
@@ -340,7 +351,7 @@ __device__ __forceinline__ void walk_base(const LaunchArgs &g, const float4 *rec
         if constexpr (DIRECT) {
             walk_emit(g, locals[s], P, c, make_float4(base.x, base.y, base.z, radius));
         } else {
-            stage[s * kWalkStride + c] = make_float4(base.x, base.y, base.z, radius);
+            stage_put(stage + s * kWalkRowFloats, c, base);  // radii come from the t table at the store
         }
     }
 }
@@ -539,20 +550,19 @@ __device__ __forceinline__ float walk_preserve_scale(const ParamArgs &p, float o
 
 // Frame step for the strand whose staged row is `row` (this lane's strand):
 // the base curve's length, the lattice, then the cursor walk, leaving the
-// noisy points (with radii) in the row.  The walk reads CV c + 3 after
+// noisy points in the row.  The walk reads CV c + 3 after
 // writing CV c, so it never reads a point it has replaced.  Every lane of the
 // warp calls it; lanes whose strand does not count (past the batch) work on
 // whatever their row holds and are ignored.
-__device__ __forceinline__ void walk_frame(const ParamArgs &p, const WalkRoot &wr, bool counts, float4 *row,
-                                           float2 *lat, const float *tvals, const float *rvals, const float4 *table,
-                                           int P) {
+__device__ __forceinline__ void walk_frame(const ParamArgs &p, const WalkRoot &wr, bool counts, float *row,
+                                           float2 *lat, const float *tvals, const float4 *table, int P) {
     // Length of the base curve (generate.h:420-433); the walk accumulates the
     // same prefix again as its arc length.
     float original_length = 0.0f;
     {
-        F3 prev = xyz(row[0]);
+        F3 prev = stage_get(row, 0);
         for (int c = 1; c < P; ++c) {
-            const F3 cur = xyz(row[c]);
+            const F3 cur = stage_get(row, c);
             const F3 d = cur - prev;
             original_length += sqrt_approx(dot(d, d));
             prev = cur;
@@ -561,17 +571,12 @@ __device__ __forceinline__ void walk_frame(const ParamArgs &p, const WalkRoot &w
     const float f_eff = walk_effective_frequency(p, original_length);
     const WalkLattice wl = walk_fill_lattice(wr.domain, original_length * f_eff, lat, table);
     const float noisy = walk_cursor_any(
-        p, wr, f_eff, wl, counts, lat, tvals, table, P, [&](int c) { return xyz(row[c]); },
-        [&](int c, F3 q) { row[c] = make_float4(q.x, q.y, q.z, rvals[c]); });
+        p, wr, f_eff, wl, counts, lat, tvals, table, P, [&](int c) { return stage_get(row, c); },
+        [&](int c, F3 q) { stage_put(row, c, q); });
     const float scale = walk_preserve_scale(p, original_length, noisy);
     if (scale != 1.0f) {
         const F3 root = wr.position;
-        for (int c = 0; c < P; ++c) {
-            const F3 q = root + (xyz(row[c]) - root) * scale;
-            row[c].x = q.x;
-            row[c].y = q.y;
-            row[c].z = q.z;
-        }
+        for (int c = 0; c < P; ++c) { stage_put(row, c, root + (stage_get(row, c) - root) * scale); }
     }
 }
 
@@ -586,8 +591,8 @@ constexpr size_t kPipeSmemBytes = sizeof(float4) * kTableFloat4 + 2u * sizeof(fl
 // Store step: item = s * P + c; the Classic application (scale about the
 // first point, width override, drop rule) as in emit_strand.
 template <bool CLASSIC>
-__device__ __forceinline__ void walk_store(const LaunchArgs &g, const float4 *stage, const uint32_t *locals, int lane,
-                                           int in_batch, int P, float inv_p) {
+__device__ __forceinline__ void walk_store(const LaunchArgs &g, const float *stage, const uint32_t *locals,
+                                           const float *rvals, int lane, int in_batch, int P, float inv_p) {
     const ParamArgs &p = g.p;
     const int items = in_batch * P;
     for (int item = lane; item < items; item += 32) {
@@ -595,19 +600,21 @@ __device__ __forceinline__ void walk_store(const LaunchArgs &g, const float4 *st
         const int c = item - s * P;
         const uint32_t word = locals[s];
         if (word >> 31) { continue; }
-        const float4 *row = stage + s * kWalkStride;
-        float4 q = row[c];
+        const float *row = stage + s * kWalkRowFloats;
+        const F3 point = stage_get(row, c);
+        float4 q = make_float4(point.x, point.y, point.z, rvals[c]);
         if constexpr (CLASSIC) {
             const float2 sc = __ldg(g.scalars + word);
-            const F3 front = xyz(row[0]);
-            const F3 back = xyz(row[P - 1]);
+            const F3 front = stage_get(row, 0);
+            const F3 back = stage_get(row, P - 1);
             const float scale = g.classic_length ? sc.x : 1.0f;
             const float raw_width = g.classic_width ? sc.y
                 : (p.radius_scale > 0.0f ? __fdiv_rn(__fmul_rn(2.0f, strand_radius(p, 0.0f)), p.radius_scale) : 0.0f);
             bool keep = !(raw_width < 1.0e-4f);
             const F3 chord = back - front;
             if (keep && !(sqrtf(dot(chord, chord)) * scale > 1.01e-4f)) {
-                keep = !(__fmul_rn(classic_spline_length(row, P), scale) < 1.0e-4f);
+                keep = !(__fmul_rn(classic_spline_length_by([row](int i) { return stage_get(row, i); }, P), scale) <
+                         1.0e-4f);
             }
             if (g.classic_length) {
                 const F3 v = xadd(front, xmul(xsub(xyz(q), front), scale));
