@@ -66,6 +66,15 @@ __host__ __device__ constexpr size_t walk_head_bytes(bool noise) {
 // Nearest mode becomes one slot of weight 1 and normal mode zero slots, so
 // the base step evaluates every strand as
 //   base = root + (inv * sum_j w_j offsets[row_j + c] + normal' * t_c) * length_scale.
+// Square root by the PTX approximate instruction (one MUFU operation, no
+// special-case branch); its relative error (below 2^-22) is far inside the
+// position tolerance where it is used (arc lengths, sin(acos x), blend weights).
+__device__ __forceinline__ float sqrt_approx(float x) {
+    float r;
+    asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 struct WalkRoot {
     F3 position, normal, surface_u, domain;
 };
@@ -171,29 +180,51 @@ __device__ __forceinline__ WalkRoot walk_setup(const LaunchArgs &g, float4 *reco
         for (uint32_t j = 0; j < kSlots; ++j) { stencil[j] = __ldg(row + j); }
     }
     float *slot_words = reinterpret_cast<float *>(records);
+    // Guide frame record of slot j (an out-of-range slot reads as a corrupt
+    // record: no slot).  With noise (fewer warps per SM to hide latency) all
+    // eight are requested before any is used; without, one at a time, which
+    // keeps the register count and the occupancy of the plain kernel.
+    float4 gr[kSlots], gn[kSlots];
+    auto load_slot = [&](uint32_t j) {
+        const bool in_range = stencil[j] != kInvalid && stencil[j] < a.guide_count;
+        const uint32_t gi = in_range ? stencil[j] : 0u;
+        gr[j] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        gn[j] = gr[j];
+        if (a.guide_count != 0u) {
+            gr[j] = __ldg(g.guide_frames + 2u * gi);
+            gn[j] = __ldg(g.guide_frames + 2u * gi + 1u);
+        }
+        if (!in_range) { gn[j].w = 0.0f; }
+    };
+    if constexpr (NOISE) {
+#pragma unroll
+        for (uint32_t j = 0; j < kSlots; ++j) { load_slot(j); }
+    }
+    // Blend weights (1 - d / r)^power in fast arithmetic (they feed positions
+    // only); d^2, the rejection test and the radius test that decide which
+    // slots count stay in the reference's exact rounding.
+    const bool square = p.weight_power == 2.0f;
     float wsum = 0.0f;
     float nearest_d2 = FLT_MAX;
     uint32_t nearest = kInvalid;
     uint32_t blended = 0u;
 #pragma unroll
     for (uint32_t j = 0; j < kSlots; ++j) {
-        const uint32_t gi = stencil[j];
-        if (gi == kInvalid || gi >= a.guide_count) { continue; }
-        const float4 gr = __ldg(g.guide_frames + 2u * gi);
-        const float4 gn = __ldg(g.guide_frames + 2u * gi + 1u);
-        if (__float_as_uint(gn.w) == 0u) { continue; }  // corrupt record
-        const F3 delta = xsub(root.position, F3{gr.x, gr.y, gr.z});
+        if constexpr (!NOISE) { load_slot(j); }
+        if (__float_as_uint(gn[j].w) == 0u) { continue; }  // out of range or corrupt record
+        const F3 delta = xsub(root.position, F3{gr[j].x, gr[j].y, gr[j].z});
         const float d2 = xdot(delta, delta);
-        if (xdot(root.normal, F3{gn.x, gn.y, gn.z}) < p.rejection_cos) { continue; }
+        if (xdot(root.normal, F3{gn[j].x, gn[j].y, gn[j].z}) < p.rejection_cos) { continue; }
         if (d2 < nearest_d2) {  // strict first minimum over eligible slots (generate.h:234)
             nearest_d2 = d2;
-            nearest = gi;
+            nearest = stencil[j];
         }
-        const float radius = gr.w;
+        const float radius = gr[j].w;
         if (radius <= 0.0f || d2 >= __fmul_rn(radius, radius)) { continue; }
-        const float w = powf(__fsub_rn(1.0f, __fdiv_rn(__fsqrt_rn(d2), radius)), p.weight_power);
+        const float x = 1.0f - __fdividef(sqrt_approx(d2), radius);
+        const float w = square ? x * x : __powf(x, p.weight_power);
         float *dst = slot_words + ((blended >> 1) * 32u + lane) * 4u + (blended & 1u) * 2u;
-        dst[0] = __uint_as_float(gi * P);
+        dst[0] = __uint_as_float(stencil[j] * P);
         dst[1] = w;
         ++blended;
         wsum = __fadd_rn(wsum, w);
@@ -423,6 +454,7 @@ __device__ __forceinline__ WalkLattice walk_fill_lattice(F3 dom, float span, flo
             wdb[corner] = wgt[corner] * (wb - static_cast<float>(ob));
             wdc[corner] = wgt[corner] * (wc - static_cast<float>(oc));
         }
+#pragma unroll 2
         for (int k = 0; k < wl.n[ax]; ++k) {
             float A = 0.0f, B = 0.0f;
 #pragma unroll
@@ -439,15 +471,6 @@ __device__ __forceinline__ WalkLattice walk_fill_lattice(F3 dom, float span, flo
 
 __device__ __forceinline__ float walk_effective_frequency(const ParamArgs &p, float original_length) {
     return original_length > 0.0f ? fmaxf(0.5f / original_length, p.noise_frequency) : p.noise_frequency;
-}
-
-// Square root by the PTX approximate instruction (one MUFU operation, no
-// special-case branch); its relative error (below 2^-22) is far inside the
-// position tolerance where it is used (arc lengths and sin(acos x)).
-__device__ __forceinline__ float sqrt_approx(float x) {
-    float r;
-    asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
-    return r;
 }
 
 // The cursor walk (generate.h:465-502) over base points base(0..P-1),
@@ -561,6 +584,7 @@ __device__ __forceinline__ void walk_frame(const ParamArgs &p, const WalkRoot &w
     float original_length = 0.0f;
     {
         F3 prev = stage_get(row, 0);
+#pragma unroll 8
         for (int c = 1; c < P; ++c) {
             const F3 cur = stage_get(row, c);
             const F3 d = cur - prev;
