@@ -255,6 +255,22 @@ def test_launch_block_sizes(torch_cuda, sphere, block):
     assert all(np.array_equal(x, y) for x, y in zip(ref, out))
 
 
+@pytest.mark.parametrize("block", [64, 96, 320])
+def test_lane_walk_ctas_match_oracle(torch_cuda, oracle, sphere, block):
+    """The lane-walk generator with noise as producer/consumer warp pairs
+    (64 threads) and as three- and ten-warp CTAs, over CV counts that do and
+    do not fill a warp, with and without preserveLength."""
+    from nanoxgen_b200.generator import set_tile
+    w, asset = sphere
+    for cvs, preserve in ((7, 0.0), (17, 0.3), (32, 0.0), (32, 0.6)):
+        params = w.params.copy(strand_count=2500, cvs_per_strand=cvs, noise_preserve_length=preserve)
+        try:
+            set_tile(cvs, True, 1, 1, block)
+            _compare(asset, params, _gen(torch_cuda, asset, params), oracle.generate(asset.buffer, params, threads=8))
+        finally:
+            set_tile(cvs, True)
+
+
 def test_every_tile_matches_oracle_and_autotuner(torch_cuda, oracle, sphere):
     """Each admissible tile (lanes per strand x CVs per lane) is a different
     lane layout of the same arithmetic: all stay within tolerance of the
@@ -267,6 +283,11 @@ def test_every_tile_matches_oracle_and_autotuner(torch_cuda, oracle, sphere):
     try:
         for lanes, ppt in ((1, 1), (4, 4), (8, 2), (8, 4), (16, 1), (16, 2), (32, 1)):
             set_tile(P, True, lanes, ppt, 128)
+            _compare(asset, w.params, _gen(torch_cuda, d, w.params), theirs)
+        # the lane walk as producer/consumer warp pairs (64-thread CTAs) and
+        # as ten-warp CTAs
+        for block in (64, 320):
+            set_tile(P, True, 1, 1, block)
             _compare(asset, w.params, _gen(torch_cuda, d, w.params), theirs)
         pts, *_ = allocate_outputs(w.params.strand_count, P, "cuda")
         (lanes, ppt, block), ms = autotune(d, w.params, pts, repeats=2)
