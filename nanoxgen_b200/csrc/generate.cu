@@ -8,7 +8,9 @@
 //                        (a counting sort's histogram pass);
 //   2. exclusive_scan  : bin offsets;
 //   3. scatter_order   : the permutation that groups strands sharing guides,
-//                        so one CTA's strands read the same guide CVs from L1;
+//                        so one CTA's strands read the same guide CVs from L1
+//                        (ranks in shared memory per block, one global atomic
+//                        per block and bin);
 //   4. generate        : persistent CTAs walk contiguous ranges of the
 //                        permutation; a group of L lanes owns one strand and
 //                        each lane owns CVs c*L + lane.  Stencil slots are
@@ -578,6 +580,32 @@ __global__ void scatter_order_kernel(const uint32_t *keys, uint32_t *offsets, ui
     }
 }
 
+// The same scatter with one global atomic per (block, non-empty bin): block
+// b owns strands [b * chunk, (b + 1) * chunk); it counts its keys in shared
+// memory, reserves each bin's range of the order with one atomicAdd on the
+// bin offset, then places each strand at that range plus its shared-memory
+// rank.  For up to kPrivateBins bins (the count array is in shared memory).
+__global__ void __launch_bounds__(1024) scatter_order_blocked_kernel(const uint32_t *keys, uint32_t *offsets,
+                                                                     uint32_t count, uint32_t bins, uint32_t chunk,
+                                                                     uint32_t *order) {
+    extern __shared__ uint32_t slots[];  // per bin: count, then the next free position
+    const uint32_t begin = blockIdx.x * chunk;
+    const uint32_t end = min(count, begin + chunk);
+    for (uint32_t b = threadIdx.x; b < bins; b += blockDim.x) { slots[b] = 0u; }
+    __syncthreads();
+    for (uint32_t i = begin + threadIdx.x; i < end; i += blockDim.x) { atomicAdd(&slots[min(keys[i], bins - 1u)], 1u); }
+    __syncthreads();
+    for (uint32_t b = threadIdx.x; b < bins; b += blockDim.x) {
+        const uint32_t n = slots[b];
+        slots[b] = n ? atomicAdd(&offsets[b], n) : 0u;
+    }
+    __syncthreads();
+    for (uint32_t i = begin + threadIdx.x; i < end; i += blockDim.x) {
+        const uint32_t pos = atomicAdd(&slots[min(keys[i], bins - 1u)], 1u);
+        if (pos < count) { order[pos] = i; }
+    }
+}
+
 // Per-strand state for stencil/root parity checks (generate.h:568-575).
 struct StrandStateOut {
     uint32_t root[12];
@@ -877,7 +905,21 @@ uint32_t launch_order(const nxg_device_asset_desc &asset, uint32_t seed, uint32_
     if ((status = record_cuda(cudaGetLastError()))) { return status; }
     dev::exclusive_scan_kernel<<<1, 1024, 0, stream>>>(hist, bins);
     if ((status = record_cuda(cudaGetLastError()))) { return status; }
-    dev::scatter_order_kernel<<<blocks, threads, 0, stream>>>(keys, hist, count, bins, order);
+    if (bins <= dev::kPrivateBins) {  // one block per SM, shared-memory ranks
+        const uint32_t scatter_blocks = static_cast<uint32_t>(std::max(1, sms));
+        const uint32_t chunk = (count + scatter_blocks - 1u) / scatter_blocks;
+        const uint32_t used = (count + chunk - 1u) / chunk;
+        if (bins * 4u > 48u * 1024u) {
+            if ((status = record_cuda(cudaFuncSetAttribute(dev::scatter_order_blocked_kernel,
+                                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                           static_cast<int>(bins * 4u))))) {
+                return status;
+            }
+        }
+        dev::scatter_order_blocked_kernel<<<used, 1024, bins * 4u, stream>>>(keys, hist, count, bins, chunk, order);
+    } else {
+        dev::scatter_order_kernel<<<blocks, threads, 0, stream>>>(keys, hist, count, bins, order);
+    }
     return record_cuda(cudaGetLastError());
 }
 

@@ -480,9 +480,12 @@ __device__ __forceinline__ float walk_effective_frequency(const ParamArgs &p, fl
 // tip; the transported normal rotates by rotate_by(axis, acos(cos)) with
 // cos(acos x) = x and sin(acos x) = sqrt(1 - x^2):
 //   M v = cos v + (1 - cos)(axis . v) axis + sin (axis x v),
-// and is left unchanged when the axis is zero.  The body has no per-lane
-// branches (each decision is a select), so the compiler can overlap the
-// noise, tangent and frame chains of neighbouring CVs; noise at CV 0 is
+// and is left unchanged when the axis is zero (the axis and that test in
+// ordinary arithmetic: where the reference's rounded cross product vanishes
+// for nearly parallel tangents, the rotation left here is within rounding of
+// the identity).  The body has no per-lane branches (each decision is a
+// select), so the compiler can overlap the noise, tangent and frame chains of
+// neighbouring CVs; noise at CV 0 is
 // multiplied by t_0 = 0.  LATTICE: every lane of the warp reads lattice
 // noise (else every lane evaluates gradient_noise).  Base points are
 // requested three CVs before they are used.
@@ -501,21 +504,21 @@ __device__ __forceinline__ float walk_cursor(const ParamArgs &p, const WalkRoot 
     F3 previous_point = cur;
     float noisy = 0.0f;
     float arc = 0.0f;
-#pragma unroll 2
+#pragma unroll 4
     for (int c = 0; c < P; ++c) {
         const F3 further = c + 3 < P ? base(c + 3) : ahead;
         const F3 d = cur - previous_base;
         arc += sqrt_approx(dot(d, d));
         const F3 seg = xsub(nxt, cur);
         const F3 ntan = (c + 1 < P && xdot(seg, seg) > 0.0f) ? normalize(seg) : tan;
-        const F3 axis = xcross(tan, ntan);
+        const F3 axis = cross(tan, ntan);
         const float cs = fminf(fmaxf(dot(tan, ntan), -1.0f), 1.0f);
         const float sn = sqrt_approx(fmaf(-cs, cs, 1.0f));
         const float k = (1.0f - cs) * dot(axis, v);
         const F3 axv = cross(axis, v);
         const F3 rotated = normalize(F3{v.x * cs + axis.x * k + axv.x * sn, v.y * cs + axis.y * k + axv.y * sn,
                                         v.z * cs + axis.z * k + axv.z * sn});
-        v = xdot(axis, axis) > 0.0f ? rotated : v;
+        v = dot(axis, axis) > 0.0f ? rotated : v;
         const F3 bn = cross(v, ntan);
         const F3 tt = cross(bn, v);
         const float distance = arc * f_eff;
