@@ -53,7 +53,7 @@ struct BatchDesc {
 
 struct BatchArgs {
     uint32_t count;
-    uint32_t warp_bytes;       // shared memory per warp of batched_generate
+    uint32_t warp_bytes;       // shared memory per warp of batched_generate (after the CTA's head)
     uint32_t total_strands;
     uint32_t total_items;
     uint32_t *item_counter;
@@ -218,23 +218,24 @@ __global__ void __launch_bounds__(256) batched_prepare_kernel(const __grid_const
 }
 
 // Per-warp shared memory of the batched kernel.
+// Shared memory of batched_generate: a head per CTA (the current
+// description's gradient table, t values and, for 2..32 CVs, radii -- every
+// warp of a CTA works on the same description), then one region per warp.
 constexpr size_t kBatchTableBytes = sizeof(float4) * kTableFloat4;              // 4096
 constexpr size_t kBatchTvalBytes = sizeof(float) * 128u;                        // P <= 128
-constexpr size_t kBatchRecordBytes = sizeof(uint32_t) * kRecFields * 32u;       // 4096
+constexpr size_t kBatchHeadBytes = kBatchTableBytes + kBatchTvalBytes;
+constexpr size_t kBatchRecordBytes = sizeof(uint32_t) * kRecFields * 32u;       // 4480
 constexpr size_t kBatchStageBytes = sizeof(float4) * 32u * 4u;                  // 32 lanes x 4 CVs
 constexpr size_t kBatchLatticeBytes = sizeof(float2) * 384u;
-constexpr size_t kBatchWarpBytes =
-    kBatchTableBytes + kBatchTvalBytes + kBatchRecordBytes + kBatchStageBytes + kBatchLatticeBytes;
+constexpr size_t kBatchWarpBytes = kBatchRecordBytes + kBatchStageBytes + kBatchLatticeBytes;
 
 static_assert(kBatchRecordBytes >= kWalkRecordBytes, "lane-walk records fit the record area");
 static_assert(kBatchStageBytes >= sizeof(float4) * kWalkMaxCvs, "spline scratch fits the stage area");
 static_assert(kBatchLatticeBytes >= kWalkLocalBytes, "output words fit the lattice area");
 
 // Per-warp shared memory when some description takes noisy lane-walk items:
-// table | t values and radii | stage | records aliased by the lattice |
-// output words.
-constexpr size_t kBatchWalkWarpBytes =
-    kBatchTableBytes + kBatchTvalBytes + kWalkStageBytes + kWalkLatticeBytes + kWalkLocalBytes;
+// stage | records aliased by the lattice | output words.
+constexpr size_t kBatchWalkWarpBytes = kWalkStageBytes + kWalkLatticeBytes + kWalkLocalBytes;
 static_assert(kWalkLatticeBytes >= kWalkRecordBytes, "records fit the lattice area");
 
 // A noisy description on the lane-walk tile (2..32 CVs): setup, base into the
@@ -242,12 +243,10 @@ static_assert(kWalkLatticeBytes >= kWalkRecordBytes, "records fit the lattice ar
 // application when the description has scalars.
 template <bool CLASSIC>
 __device__ __noinline__ void batched_noise_walk_item(const BatchDesc &d, uint32_t batch, uint32_t end, int lane,
-                                                     unsigned char *mine) {
-    const float4 *table = reinterpret_cast<const float4 *>(mine);
-    const float *tvals = reinterpret_cast<const float *>(mine + kBatchTableBytes);
+                                                     unsigned char *mine, const float4 *table, const float *tvals) {
     const float *rvals = tvals + 2 * kWalkMaxCvs;
-    float *stage = reinterpret_cast<float *>(mine + kBatchTableBytes + kBatchTvalBytes);
-    unsigned char *after_stage = mine + kBatchTableBytes + kBatchTvalBytes + kWalkStageBytes;
+    float *stage = reinterpret_cast<float *>(mine);
+    unsigned char *after_stage = mine + kWalkStageBytes;
     float4 *records = reinterpret_cast<float4 *>(after_stage);
     float2 *lattice = reinterpret_cast<float2 *>(after_stage);
     uint32_t *locals = reinterpret_cast<uint32_t *>(after_stage + kWalkLatticeBytes);
@@ -277,13 +276,11 @@ __device__ __noinline__ void batched_noise_walk_item(const BatchDesc &d, uint32_
 // and point counts come from batched_prepare.
 template <bool CLASSIC>
 __device__ __noinline__ void batched_walk_item(const BatchDesc &d, uint32_t batch, uint32_t end, int lane,
-                                               unsigned char *mine) {
-    const float *tvals = reinterpret_cast<const float *>(mine + kBatchTableBytes);
+                                               unsigned char *mine, const float *tvals) {
     const float *rvals = tvals + 2 * kWalkMaxCvs;
-    float4 *records = reinterpret_cast<float4 *>(mine + kBatchTableBytes + kBatchTvalBytes);
-    float4 *scratch = reinterpret_cast<float4 *>(mine + kBatchTableBytes + kBatchTvalBytes + kBatchRecordBytes);
-    uint32_t *locals = reinterpret_cast<uint32_t *>(mine + kBatchTableBytes + kBatchTvalBytes + kBatchRecordBytes +
-                                                    kBatchStageBytes);
+    float4 *records = reinterpret_cast<float4 *>(mine);
+    float4 *scratch = reinterpret_cast<float4 *>(mine + kBatchRecordBytes);
+    uint32_t *locals = reinterpret_cast<uint32_t *>(mine + kBatchRecordBytes + kBatchStageBytes);
     const int P = static_cast<int>(d.g.p.cvs_per_strand);
     const uint32_t item = batch + static_cast<uint32_t>(lane);
     const bool valid = item < end;
@@ -304,13 +301,10 @@ __device__ __noinline__ void batched_walk_item(const BatchDesc &d, uint32_t batc
 
 template <int L, int PPT, bool NOISE, bool CLASSIC>
 __device__ __noinline__ void batched_item(const BatchDesc &d, uint32_t batch, uint32_t end, int lane,
-                                             unsigned char *mine) {
-    const float4 *table = reinterpret_cast<const float4 *>(mine);
-    const float *tvals = reinterpret_cast<const float *>(mine + kBatchTableBytes);
-    const Records rec{reinterpret_cast<uint32_t *>(mine + kBatchTableBytes + kBatchTvalBytes)};
-    float4 *stage_base = reinterpret_cast<float4 *>(mine + kBatchTableBytes + kBatchTvalBytes + kBatchRecordBytes);
-    float2 *lattice_base = reinterpret_cast<float2 *>(mine + kBatchTableBytes + kBatchTvalBytes + kBatchRecordBytes +
-                                                      kBatchStageBytes);
+                                             unsigned char *mine, const float4 *table, const float *tvals) {
+    const Records rec{reinterpret_cast<uint32_t *>(mine)};
+    float4 *stage_base = reinterpret_cast<float4 *>(mine + kBatchRecordBytes);
+    float2 *lattice_base = reinterpret_cast<float2 *>(mine + kBatchRecordBytes + kBatchStageBytes);
     constexpr int kGroups = 32 / L;
     const int group = lane / L;
     const int gl = lane % L;
@@ -330,13 +324,13 @@ __device__ __noinline__ void batched_item(const BatchDesc &d, uint32_t batch, ui
 
 template <int PPT, bool NOISE, bool CLASSIC>
 __device__ __forceinline__ void batched_dispatch_lanes(const BatchDesc &d, uint32_t batch, uint32_t end, int lane,
-                                                       unsigned char *mine) {
+                                                       unsigned char *mine, const float4 *table, const float *tvals) {
     switch (d.lanes) {
-        case 2: batched_item<2, PPT, NOISE, CLASSIC>(d, batch, end, lane, mine); break;
-        case 4: batched_item<4, PPT, NOISE, CLASSIC>(d, batch, end, lane, mine); break;
-        case 8: batched_item<8, PPT, NOISE, CLASSIC>(d, batch, end, lane, mine); break;
-        case 16: batched_item<16, PPT, NOISE, CLASSIC>(d, batch, end, lane, mine); break;
-        default: batched_item<32, PPT, NOISE, CLASSIC>(d, batch, end, lane, mine); break;
+        case 2: batched_item<2, PPT, NOISE, CLASSIC>(d, batch, end, lane, mine, table, tvals); break;
+        case 4: batched_item<4, PPT, NOISE, CLASSIC>(d, batch, end, lane, mine, table, tvals); break;
+        case 8: batched_item<8, PPT, NOISE, CLASSIC>(d, batch, end, lane, mine, table, tvals); break;
+        case 16: batched_item<16, PPT, NOISE, CLASSIC>(d, batch, end, lane, mine, table, tvals); break;
+        default: batched_item<32, PPT, NOISE, CLASSIC>(d, batch, end, lane, mine, table, tvals); break;
     }
 }
 
@@ -349,9 +343,9 @@ __global__ void batched_generate_kernel(const __grid_constant__ BatchArgs b) {
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const uint32_t warps = blockDim.x >> 5;
-    unsigned char *mine = reinterpret_cast<unsigned char *>(smem) + b.warp_bytes * warp;
-    float4 *table = reinterpret_cast<float4 *>(mine);
-    float *tvals = reinterpret_cast<float *>(mine + kBatchTableBytes);
+    float4 *table = smem;
+    float *tvals = reinterpret_cast<float *>(reinterpret_cast<unsigned char *>(smem) + kBatchTableBytes);
+    unsigned char *mine = reinterpret_cast<unsigned char *>(smem) + kBatchHeadBytes + b.warp_bytes * warp;
     int current = -1;
     // A work item is a contiguous slice of one description's strand order,
     // one 32-strand batch per warp of the CTA, so the CTA's strands share
@@ -365,41 +359,40 @@ __global__ void batched_generate_kernel(const __grid_constant__ BatchArgs b) {
         int di = 0;
         while (di + 1 < static_cast<int>(b.count) && b.d[di + 1].item_begin <= item) { ++di; }
         const BatchDesc &d = b.d[di];
-        const uint32_t batch = ((item - d.item_begin) * warps + static_cast<uint32_t>(warp)) * 32u;
-        if (batch >= d.g.count) { continue; }
-        if (di != current) {
-            __syncwarp();
+        if (di != current) {  // the whole CTA: every warp works on the item's description
             const int P = static_cast<int>(d.g.p.cvs_per_strand);
             if (d.noise) {
-                for (int i = lane; i < kTableFloat4; i += 32) {
+                for (int i = threadIdx.x; i < kTableFloat4; i += blockDim.x) {
                     table[i] = make_float4(__ldg(d.g.a.gradients + 3 * i), __ldg(d.g.a.gradients + 3 * i + 1),
                                            __ldg(d.g.a.gradients + 3 * i + 2), 0.0f);
                 }
             }
-            for (int i = lane; i < P; i += 32) {
+            for (int i = threadIdx.x; i < P; i += blockDim.x) {
                 tvals[i] = __fdiv_rn(static_cast<float>(i), static_cast<float>(P - 1));
                 if (P <= kWalkMaxCvs) { tvals[2 * kWalkMaxCvs + i] = strand_radius(d.g.p, tvals[i]); }
             }
-            __syncwarp();
+            __syncthreads();
             current = di;
         }
+        const uint32_t batch = ((item - d.item_begin) * warps + static_cast<uint32_t>(warp)) * 32u;
+        if (batch >= d.g.count) { continue; }
         const uint32_t end = min(batch + 32u, d.g.count);
         if (d.lanes == 1u) {
             if (d.noise) {
-                batched_noise_walk_item<CLASSIC>(d, batch, end, lane, mine);
+                batched_noise_walk_item<CLASSIC>(d, batch, end, lane, mine, table, tvals);
             } else {
-                batched_walk_item<CLASSIC>(d, batch, end, lane, mine);
+                batched_walk_item<CLASSIC>(d, batch, end, lane, mine, tvals);
             }
         } else if (CLASSIC && d.g.scalars != nullptr) {
             if (d.noise) {
-                batched_dispatch_lanes<PPT, true, CLASSIC>(d, batch, end, lane, mine);
+                batched_dispatch_lanes<PPT, true, CLASSIC>(d, batch, end, lane, mine, table, tvals);
             } else {
-                batched_dispatch_lanes<PPT, false, CLASSIC>(d, batch, end, lane, mine);
+                batched_dispatch_lanes<PPT, false, CLASSIC>(d, batch, end, lane, mine, table, tvals);
             }
         } else if (d.noise) {
-            batched_dispatch_lanes<PPT, true, false>(d, batch, end, lane, mine);
+            batched_dispatch_lanes<PPT, true, false>(d, batch, end, lane, mine, table, tvals);
         } else {
-            batched_dispatch_lanes<PPT, false, false>(d, batch, end, lane, mine);
+            batched_dispatch_lanes<PPT, false, false>(d, batch, end, lane, mine, table, tvals);
         }
     }
 }
@@ -520,18 +513,19 @@ uint32_t generate_batched(const nxg_device_asset_desc *assets, const nxg_deforme
         cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
     }
     // Noisy descriptions on the lane-walk tile need the walk's stage and
-    // lattice per warp; CTAs are then one warp each, so the SM holds as many
-    // of those warps as its shared memory allows.
+    // lattice per warp; CTAs are then ten warps, as many as the SM's shared
+    // memory holds.
     bool noise_walk = false;
     for (uint32_t d = 0; d < count; ++d) {
         const bool noise = params[d].noise_amplitude != 0.0f && params[d].noise_mask != 0.0f;
         noise_walk = noise_walk || (noise && batch_lanes(params[d].cvs_per_strand, true, ppt) == 1u);
     }
     const size_t warp_bytes = noise_walk ? dev::kBatchWalkWarpBytes : dev::kBatchWarpBytes;
-    uint32_t block = noise_walk ? 32u
-                                : std::min(static_cast<uint32_t>(attr.maxThreadsPerBlock) / 32u * 32u,
-                                           std::max<uint32_t>(32u, (cfg.block_size + 31u) / 32u * 32u));
-    while (block > 32u && warp_bytes * (block / 32u) + 64u > static_cast<size_t>(smem_optin)) { block -= 32u; }
+    uint32_t block = std::min(static_cast<uint32_t>(attr.maxThreadsPerBlock) / 32u * 32u,
+                              noise_walk ? 320u : std::max<uint32_t>(32u, (cfg.block_size + 31u) / 32u * 32u));
+    while (block > 32u && dev::kBatchHeadBytes + warp_bytes * (block / 32u) + 64u > static_cast<size_t>(smem_optin)) {
+        block -= 32u;
+    }
     const uint32_t warps_per_cta = block / 32u;
 
     auto *w = static_cast<unsigned char *>(workspace);
@@ -614,7 +608,7 @@ uint32_t generate_batched(const nxg_device_asset_desc *assets, const nxg_deforme
     dev::batched_offsets_kernel<<<std::max(1u, offset_blocks), 256, 0, s>>>(b);
     if ((status = record_cuda(cudaGetLastError()))) { return status; }
 
-    const size_t shm = warp_bytes * (block / 32u);
+    const size_t shm = dev::kBatchHeadBytes + warp_bytes * (block / 32u);
     if ((status = record_cuda(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                    static_cast<int>(shm))))) {
         return status;
