@@ -4,10 +4,13 @@
 // CV count, stencil and noise settings) is generated by:
 //   batched_clear      zero the per-description bins and the work counter;
 //   batched_prepare    one pass over every strand of every description:
-//                      root sample, sort key (first stencil guide) with its
-//                      histogram, RootSample / root UV / point count outputs;
+//                      root triangle, sort key (first stencil guide) with its
+//                      histogram, and for lane-group descriptions the
+//                      RootSample / root UV / point count outputs (lane-walk
+//                      items write theirs in batched_generate);
 //   batched_scan       one CTA per description: bin offsets;
-//   batched_scatter    per-description strand-locality orders;
+//   batched_scatter    per-description strand-locality orders (ranks in
+//                      shared memory, one global atomic per block and bin);
 //   batched_offsets    every description's guide-offset table and guide
 //                      frame records;
 //   batched_generate   persistent warps pull (description, 32-strand batch)
@@ -115,19 +118,47 @@ __global__ void __launch_bounds__(1024) batched_scan_kernel(const __grid_constan
     }
 }
 
-__global__ void batched_scatter_kernel(const __grid_constant__ BatchArgs b) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < b.total_strands; i += gridDim.x * blockDim.x) {
-        const BatchDesc &d = b.d[desc_of_strand(b, i)];
-        const uint32_t local = i - d.strand_begin;
-        const uint32_t bins = d.g.a.guide_count + 1u;
-        const uint32_t pos = atomicAdd(&d.bins[min(d.keys[local], bins - 1u)], 1u);
-        if (pos < d.g.count) { const_cast<uint32_t *>(d.g.order)[pos] = local; }
+// Block-aggregated scatter (see scatter_order_blocked_kernel): a block whose
+// flat range lies in one description with up to kBatchScatterBins bins
+// ranks its strands in shared memory and takes one global atomic per
+// non-empty bin; a block straddling descriptions takes one per strand.
+constexpr uint32_t kBatchScatterBins = 8192u;
+
+__global__ void __launch_bounds__(1024) batched_scatter_blocked_kernel(const __grid_constant__ BatchArgs b,
+                                                                       uint32_t chunk) {
+    extern __shared__ uint32_t slots[];
+    const uint32_t begin = blockIdx.x * chunk;
+    const uint32_t end = min(b.total_strands, begin + chunk);
+    if (begin >= end) { return; }
+    const int home = desc_of_strand(b, begin);
+    const BatchDesc &d = b.d[home];
+    const uint32_t bins = d.g.a.guide_count + 1u;
+    uint32_t *order = const_cast<uint32_t *>(d.g.order);
+    if (desc_of_strand(b, end - 1u) != home || bins > kBatchScatterBins) {
+        for (uint32_t i = begin + threadIdx.x; i < end; i += blockDim.x) {
+            const BatchDesc &e = b.d[desc_of_strand(b, i)];
+            const uint32_t local = i - e.strand_begin;
+            const uint32_t pos = atomicAdd(&e.bins[min(e.keys[local], e.g.a.guide_count)], 1u);
+            if (pos < e.g.count) { const_cast<uint32_t *>(e.g.order)[pos] = local; }
+        }
+        return;
+    }
+    const uint32_t lo = begin - d.strand_begin, hi = end - d.strand_begin;
+    for (uint32_t k = threadIdx.x; k < bins; k += blockDim.x) { slots[k] = 0u; }
+    __syncthreads();
+    for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) { atomicAdd(&slots[min(d.keys[i], bins - 1u)], 1u); }
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < bins; k += blockDim.x) {
+        const uint32_t n = slots[k];
+        slots[k] = n ? atomicAdd(&d.bins[k], n) : 0u;
+    }
+    __syncthreads();
+    for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+        const uint32_t pos = atomicAdd(&slots[min(d.keys[i], bins - 1u)], 1u);
+        if (pos < d.g.count) { order[pos] = i; }
     }
 }
 
-// Every description's guide-offset table (G x P float4) and guide frame
-// records (2 float4 per guide, after the table): G x P + G flat entries per
-// description.
 __global__ void batched_offsets_kernel(const __grid_constant__ BatchArgs b) {
     for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < b.total_offsets;
          i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
@@ -149,8 +180,9 @@ __global__ void batched_offsets_kernel(const __grid_constant__ BatchArgs b) {
     }
 }
 
-// Per flat strand: the root sample, its sort key (first stencil guide)
-// with the description's key histogram, and the RootSample / root UV /
+// Per flat strand: the root triangle, its sort key (first stencil guide)
+// with the description's key histogram, and -- for descriptions on
+// lane-group tiles -- the full root sample and the RootSample / root UV /
 // point count outputs.  Block b owns the contiguous flat range
 // [b*chunk, (b+1)*chunk), so its strands are mostly one description's and
 // that description's histogram is kept in shared memory.  Roots of a warp
@@ -179,11 +211,21 @@ __global__ void __launch_bounds__(256) batched_prepare_kernel(const __grid_const
         const int di = desc_of_strand(b, fi);
         const BatchDesc &d = b.d[di];
         const uint32_t local = fi - d.strand_begin;
-        const Root r = sample_root(d.g.a, d.g.f, d.g.p.seed, d.g.first_strand + local);
+        // Lane-walk descriptions write their root outputs in the generate
+        // kernel; here they need only the root triangle.
+        const bool outputs = d.lanes != 1u;
         uint32_t *rec = staged[warp] + lane * 12;
-        for (int w = 0; w < 12; ++w) { rec[w] = root_word(r, w); }
+        uint32_t triangle;
+        Root r{};
+        if (outputs) {
+            r = sample_root(d.g.a, d.g.f, d.g.p.seed, d.g.first_strand + local);
+            for (int w = 0; w < 12; ++w) { rec[w] = root_word(r, w); }
+            triangle = r.triangle;
+        } else {
+            triangle = sample_triangle(d.g.a, d.g.p.seed, d.g.first_strand + local);
+        }
         if (valid) {
-            const uint32_t gi = __ldg(d.g.a.stencil + static_cast<uint64_t>(r.triangle) * kSlots);
+            const uint32_t gi = __ldg(d.g.a.stencil + static_cast<uint64_t>(triangle) * kSlots);
             const uint32_t key = gi < d.g.a.guide_count ? gi : d.g.a.guide_count;
             d.keys[local] = key;
             if (priv && di == home) {
@@ -191,20 +233,20 @@ __global__ void __launch_bounds__(256) batched_prepare_kernel(const __grid_const
             } else {
                 atomicAdd(&d.bins[key], 1u);
             }
-            if (d.g.root_uvs) { d.g.root_uvs[local] = make_float2(r.u, r.v); }
-            if (d.g.point_counts) { d.g.point_counts[local] = d.g.p.cvs_per_strand; }
+            if (outputs && d.g.root_uvs) { d.g.root_uvs[local] = make_float2(r.u, r.v); }
+            if (outputs && d.g.point_counts) { d.g.point_counts[local] = d.g.p.cvs_per_strand; }
         }
         __syncwarp();
         const int d0 = __shfl_sync(kFull, di, 0);
         if (__all_sync(kFull, di == d0)) {
             const BatchDesc &dd = b.d[d0];
-            if (dd.g.roots) {
+            if (dd.g.roots && dd.lanes != 1u) {
                 const uint32_t local0 = __shfl_sync(kFull, local, 0);
                 const uint32_t n = min(32u, end - base);
                 uint32_t *dst = dd.g.roots + static_cast<uint64_t>(local0) * 12u;
                 for (uint32_t w = lane; w < n * 12u; w += 32u) { dst[w] = staged[warp][w]; }
             }
-        } else if (valid && d.g.roots) {  // the warp straddles two descriptions
+        } else if (valid && outputs && d.g.roots) {  // the warp straddles two descriptions
             for (int w = 0; w < 12; ++w) { d.g.roots[static_cast<uint64_t>(local) * 12u + w] = rec[w]; }
         }
         __syncwarp();
@@ -231,6 +273,7 @@ constexpr size_t kBatchWarpBytes = kBatchRecordBytes + kBatchStageBytes + kBatch
 
 static_assert(kBatchRecordBytes >= kWalkRecordBytes, "lane-walk records fit the record area");
 static_assert(kBatchStageBytes >= sizeof(float4) * kWalkMaxCvs, "spline scratch fits the stage area");
+static_assert(kBatchStageBytes >= kWalkRootWordBytes, "RootSample words fit the stage area");
 static_assert(kBatchLatticeBytes >= kWalkLocalBytes, "output words fit the lattice area");
 
 // Per-warp shared memory when some description takes noisy lane-walk items:
@@ -238,9 +281,9 @@ static_assert(kBatchLatticeBytes >= kWalkLocalBytes, "output words fit the latti
 constexpr size_t kBatchWalkWarpBytes = kWalkStageBytes + kWalkLatticeBytes + kWalkLocalBytes;
 static_assert(kWalkLatticeBytes >= kWalkRecordBytes, "records fit the lattice area");
 
-// A noisy description on the lane-walk tile (2..32 CVs): setup, base into the
-// stage, the frame walk and the store step (walk.cuh), with the Classic
-// application when the description has scalars.
+// A noisy description on the lane-walk tile (2..32 CVs): setup (with the
+// root outputs), base into the stage, the frame walk and the store step
+// (walk.cuh), with the Classic application when the description has scalars.
 template <bool CLASSIC>
 __device__ __noinline__ void batched_noise_walk_item(const BatchDesc &d, uint32_t batch, uint32_t end, int lane,
                                                      unsigned char *mine, const float4 *table, const float *tvals) {
@@ -255,9 +298,14 @@ __device__ __noinline__ void batched_noise_walk_item(const BatchDesc &d, uint32_
     const bool valid = item < end;
     const int in_batch = static_cast<int>(end - batch);
     const float inv_p = 1.0f / static_cast<float>(P);
-    const WalkRoot wr = walk_setup<true>(d.g, records, locals, nullptr, lane, valid ? item : batch, valid,
-                                         static_cast<uint32_t>(P), false);
+    uint32_t *root_words = reinterpret_cast<uint32_t *>(stage);  // free until the base step
+    const WalkRoot wr = walk_setup<true>(d.g, records, locals, root_words, lane, valid ? item : batch, valid,
+                                         static_cast<uint32_t>(P));
     __syncwarp();
+    if (d.g.roots) {
+        walk_store_roots(d.g, root_words, locals, lane, in_batch);
+        __syncwarp();
+    }
     walk_base<false>(d.g, records, stage, locals, tvals, rvals, d.offsets, lane, in_batch, P, inv_p);
     __syncwarp();
     walk_frame(d.g.p, wr, lane < in_batch, stage + lane * kWalkRowFloats, lattice + lane, tvals, table, P);
@@ -272,8 +320,8 @@ __device__ __noinline__ void batched_noise_walk_item(const BatchDesc &d, uint32_
 
 // A noise-free description on the lane-walk tile (2..32 CVs): setup and the
 // lane-parallel base step writing the output directly (walk.cuh), with the
-// Classic application when the description has scalars.  Roots, root UVs
-// and point counts come from batched_prepare.
+// Classic application when the description has scalars; setup writes the
+// root outputs.
 template <bool CLASSIC>
 __device__ __noinline__ void batched_walk_item(const BatchDesc &d, uint32_t batch, uint32_t end, int lane,
                                                unsigned char *mine, const float *tvals) {
@@ -286,9 +334,13 @@ __device__ __noinline__ void batched_walk_item(const BatchDesc &d, uint32_t batc
     const bool valid = item < end;
     const int in_batch = static_cast<int>(end - batch);
     const float inv_p = 1.0f / static_cast<float>(P);
-    walk_setup<false>(d.g, records, locals, nullptr, lane, valid ? item : batch, valid, static_cast<uint32_t>(P),
-                      false);
+    uint32_t *root_words = reinterpret_cast<uint32_t *>(scratch);  // free until the Classic setup
+    walk_setup<false>(d.g, records, locals, root_words, lane, valid ? item : batch, valid, static_cast<uint32_t>(P));
     __syncwarp();
+    if (d.g.roots) {
+        walk_store_roots(d.g, root_words, locals, lane, in_batch);
+        __syncwarp();
+    }
     if (CLASSIC && d.g.scalars != nullptr) {
         walk_classic_setup(d.g, records, lane, valid, locals[lane] & 0x7fffffffu, tvals, d.offsets, scratch, P);
         __syncwarp();
@@ -590,7 +642,6 @@ uint32_t generate_batched(const nxg_device_asset_desc *assets, const nxg_deforme
     const auto s = static_cast<cudaStream_t>(stream);
     const int sms = sm_count();
     set_last_cuda_error(0);
-    const uint32_t flat_blocks = static_cast<uint32_t>(std::min<uint64_t>((strands + 255u) / 256u, uint64_t(sms) * 8u));
     dev::batched_clear_kernel<<<std::max(1, sms), 256, 0, s>>>(b);
     if ((status = record_cuda(cudaGetLastError()))) { return status; }
     {
@@ -602,7 +653,12 @@ uint32_t generate_batched(const nxg_device_asset_desc *assets, const nxg_deforme
     }
     dev::batched_scan_kernel<<<count, 1024, 0, s>>>(b);
     if ((status = record_cuda(cudaGetLastError()))) { return status; }
-    dev::batched_scatter_kernel<<<flat_blocks, 256, 0, s>>>(b);
+    {
+        const uint32_t scatter_blocks = static_cast<uint32_t>(std::max(1, sms));
+        const uint32_t chunk = (strands + scatter_blocks - 1u) / scatter_blocks;
+        dev::batched_scatter_blocked_kernel<<<(strands + chunk - 1u) / chunk, 1024,
+                                              dev::kBatchScatterBins * sizeof(uint32_t), s>>>(b, chunk);
+    }
     if ((status = record_cuda(cudaGetLastError()))) { return status; }
     const uint32_t offset_blocks = static_cast<uint32_t>(std::min<uint64_t>((offsets + 255u) / 256u, uint64_t(sms) * 16u));
     dev::batched_offsets_kernel<<<std::max(1u, offset_blocks), 256, 0, s>>>(b);
