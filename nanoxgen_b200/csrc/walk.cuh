@@ -504,7 +504,7 @@ __device__ __forceinline__ float walk_cursor(const ParamArgs &p, const WalkRoot 
     F3 previous_point = cur;
     float noisy = 0.0f;
     float arc = 0.0f;
-#pragma unroll 4
+#pragma unroll 2
     for (int c = 0; c < P; ++c) {
         const F3 further = c + 3 < P ? base(c + 3) : ahead;
         const F3 d = cur - previous_base;
