@@ -271,6 +271,16 @@ def test_lane_walk_ctas_match_oracle(torch_cuda, oracle, sphere, block):
             set_tile(cvs, True)
 
 
+def test_lane_walk_direct_noise_when_the_lattice_overflows(torch_cuda, oracle, sphere):
+    """At a high noise frequency a strand spans more lattice columns than the
+    lane walk keeps (12 per axis); its warp then evaluates gradient noise
+    directly.  Also a frequency just inside the limit."""
+    w, asset = sphere
+    for frequency in (60.0, 14.0):
+        params = w.params.copy(strand_count=3000, cvs_per_strand=32, noise_frequency=frequency)
+        _compare(asset, params, _gen(torch_cuda, asset, params), oracle.generate(asset.buffer, params, threads=8))
+
+
 def test_every_tile_matches_oracle_and_autotuner(torch_cuda, oracle, sphere):
     """Each admissible tile (lanes per strand x CVs per lane) is a different
     lane layout of the same arithmetic: all stay within tolerance of the
