@@ -11,15 +11,18 @@
 //                        so one CTA's strands read the same guide CVs from L1
 //                        (ranks in shared memory per block, one global atomic
 //                        per block and bin);
-//   4. generate        : persistent CTAs walk contiguous ranges of the
-//                        permutation; a group of L lanes owns one strand and
-//                        each lane owns CVs c*L + lane.  Stencil slots are
-//                        evaluated one per lane and staged in shared memory,
-//                        the base curve, arc length, transported frame and
-//                        gradient noise are computed lane-parallel (prefix
-//                        scans over shuffles replace the reference's serial
-//                        cursor), and float4 points leave as coalesced
-//                        streaming stores.
+//   4. guide_offsets   : the frame's guide-offset table and guide frame
+//                        records;
+//   5. generate        : persistent CTAs walk contiguous ranges of the
+//                        permutation.  For 2..32 CVs (the built-in tile) the
+//                        lane-walk generator (walk.cuh): setup one lane per
+//                        strand, the base curve one lane per CV, the noise
+//                        frame one lane per strand walking the reference's
+//                        cursor, coalesced streaming stores.  Otherwise the
+//                        lane-group generator: a group of L lanes owns one
+//                        strand, the transported frame as prefix scans over
+//                        shuffles (generator_core.cuh), with a separate
+//                        roots kernel.
 // Strands longer than 128 CVs take a serial per-thread kernel that walks the
 // reference's cursor directly.
 #include "generator_core.cuh"
