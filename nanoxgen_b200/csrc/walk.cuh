@@ -95,6 +95,14 @@ __device__ __forceinline__ Root walk_root(const AssetArgs &a, const FrameArgs &f
     r.b2 = __fmul_rn(s, r2);
     const uint3 t = load_triangle(a, r.triangle);
     const F3 p0 = ld3(f.positions, t.x), p1 = ld3(f.positions, t.y), p2 = ld3(f.positions, t.z);
+    // A deformed frame's noise domain needs the rest-pose vertices too:
+    // requested with the frame's, before any arithmetic waits on them.
+    F3 q0 = p0, q1 = p1, q2 = p2;
+    if (NOISE && f.positions != a.positions) {
+        q0 = ld3(a.positions, t.x);
+        q1 = ld3(a.positions, t.y);
+        q2 = ld3(a.positions, t.z);
+    }
     r.position = xbary(p0, p1, p2, b0, r.b1, r.b2);
     r.normal = xnormalize(xcross(xsub(p1, p0), xsub(p2, p0)));
     if (a.flags & NXG_ASSET_HAS_NORMALS) {
@@ -130,9 +138,7 @@ __device__ __forceinline__ Root walk_root(const AssetArgs &a, const FrameArgs &f
         }
         surface_u = dot(tangent, tangent) > 1.0e-20f ? normalize(tangent) : fallback_surface_u(r.normal);
         const float rb0 = __fsub_rn(__fsub_rn(1.0f, r.b1), r.b2);
-        rest_position = f.positions == a.positions
-            ? xbary(p0, p1, p2, rb0, r.b1, r.b2)
-            : xbary(ld3(a.positions, t.x), ld3(a.positions, t.y), ld3(a.positions, t.z), rb0, r.b1, r.b2);
+        rest_position = xbary(q0, q1, q2, rb0, r.b1, r.b2);
     }
     return r;
 }
