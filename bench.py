@@ -45,7 +45,8 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["nxg", "reference"], default="nxg")
-    ap.add_argument("--workload", choices=["large", "batched", "motion", "classic", "batched_classic"],
+    ap.add_argument("--workload", choices=["large", "batched", "motion", "classic", "batched_classic",
+                                           "asset_build"],
                     default="large",
                     help="large: the single large description (headline); batched: nine descriptions in one "
                          "persistent launch vs. one launch per description; motion: five shutter samples of the "
@@ -695,6 +696,76 @@ def run_batched_classic(args):
     print(json.dumps(line), flush=True)
 
 
+def run_asset_build(args):
+    """The asset build of the large description's mesh (200,000 triangles,
+    4,096 guides): the per-triangle stencil search (stencil.cu) timed alone
+    on resident device inputs (`value`, candidates/s), the whole
+    nxg_build_asset_device call from host arrays (`e2e`), and the host
+    builders beside it (this library's threaded nxg_build_asset, and the
+    reference's own single-threaded build_asset when its library is built)."""
+    import numpy as np
+    import torch
+
+    from nanoxgen_b200.asset import build_asset, build_asset_device
+    from nanoxgen_b200.generator import build_stencils
+    device = torch.device("cuda", 0)
+    torch.cuda.set_device(device)
+    src = workload(args.strands).build_input
+    host = build_asset(src, 8)
+    guides = host.guides()
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(device)
+    positions = dev(np.asarray(src.positions, np.float32))
+    triangles = dev(np.asarray(src.triangles, np.uint32).view(np.int32))
+    roots = dev(guides["root_position"].astype(np.float32))
+    normals = dev(guides["root_normal"].astype(np.float32))
+    out = torch.empty((triangles.shape[0], 8), dtype=torch.int32, device=device)
+    tris, count = int(triangles.shape[0]), int(roots.shape[0])
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=device)
+    sampler = ClockSampler(0)
+    sampler.start()
+    times = _graph_time(device, lambda s: build_stencils(positions, triangles, roots, normals, 8, out=out, stream=s),
+                        args.steps, args.warmup, flush)
+    clocks = sampler.stop()
+    same_rows = bool(np.array_equal(out.cpu().numpy().view(np.uint32), host.stencil().reshape(tris, 8)))
+    ms = statistics.mean(times)
+    build_asset_device(src, 8)  # warm
+    e2e = []
+    for _ in range(max(3, min(args.steps, 10))):
+        t0 = time.perf_counter()
+        blob = build_asset_device(src, 8)
+        e2e.append((time.perf_counter() - t0) * 1e3)
+    same_blob = bool(np.array_equal(blob.buffer, host.buffer))
+    t0 = time.perf_counter()
+    build_asset(src, 8)
+    host_ms = (time.perf_counter() - t0) * 1e3
+    cpu = {"value": host_ms, "unit": "ms per build", "cores": os.cpu_count(), "kind": "port",
+           "sample": "this library's nxg_build_asset (host threads), one full build"}
+    ref = None
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "oracle"))
+        import checker
+        if checker.reference_available():
+            r = checker.Reference()
+            t0 = time.perf_counter()
+            ref_blob = r.build_asset(src)
+            ref = {"value": (time.perf_counter() - t0) * 1e3, "unit": "ms per build", "cores": 1,
+                   "kind": "reference", "sample": "the reference's build_asset, one full build",
+                   "same_bytes": bool(np.array_equal(ref_blob, host.buffer))}
+    em = statistics.mean(e2e)
+    line = {"metric": "stencil candidates/sec", "value": tris * count / (ms / 1e3), "unit": "candidates/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (IEEE-rounded, uncontracted)", "data": "synthetic",
+            "config": {"workload": "asset-build/displaced-sphere-%dk-tris/%d-guides" % (tris // 1000, count),
+                       "triangles": tris, "guides": count, "stencil_slots": 8,
+                       "l2": "flushed between timed replays (256 MiB write)"},
+            "rows_equal_host_build": same_rows,
+            "e2e": {"value": em, "unit": "ms per nxg_build_asset_device call",
+                    "h2d_bytes_per_step": int(positions.numel() * 4 + triangles.numel() * 4 + 2 * roots.numel() * 4),
+                    "d2h_bytes_per_step": int(out.numel() * 4), "blob_equal_host_build": same_blob},
+            "cpu_baseline": cpu, "reference_build": ref, "clocks": clocks, "gpu_launches": args.steps}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
@@ -707,6 +778,8 @@ def main():
         run_batched(args)
     elif args.workload == "motion":
         run_motion(args)
+    elif args.workload == "asset_build":
+        run_asset_build(args)
     else:
         run_gpu_arm(args)
 

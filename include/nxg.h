@@ -293,6 +293,36 @@ int nxg_build_asset(const nxg_asset_build_input *input, void **out_bytes, uint64
                     char *message, uint64_t message_capacity);
 void nxg_free(void *pointer);
 
+/* nxg_build_asset with its two all-pairs searches run on the current CUDA
+ * device: the per-triangle stencil search (asset.cpp:252-269, triangle_count
+ * x guide_count candidates) and the nearest other root of each guide behind
+ * the automatic support radius (asset.cpp:88-97, guide_count^2 distances);
+ * worker_count is ignored.  The blob
+ * is byte-identical to nxg_build_asset's for the same input.  Copies the
+ * mesh and guide roots to the device, copies the rows back and synchronizes
+ * `stream` (a cudaStream_t as void *, NULL = legacy default stream) before
+ * returning.  A CUDA failure returns 1 with the CUDA error text in
+ * `message` (and the code in nxg_last_cuda_error). */
+int nxg_build_asset_device(const nxg_asset_build_input *input, void *stream, void **out_bytes,
+                           uint64_t *out_size, char *message, uint64_t message_capacity);
+
+/* The stencil search alone on device buffers; enqueues one kernel on
+ * `stream`.  positions [vertex_count] and triangles [triangle_count] are the
+ * mesh; guide_roots [guide_count] are the guides' first CVs and
+ * guide_normals their root normals normalized as the asset's guide records
+ * hold them (nxg_guide_record.root_normal).  Writes stencil [triangle_count
+ * x 8] (16-byte aligned): per triangle the min(8, guide_count) guides of
+ * smallest |centroid - root|^2 (+1e20 where dot(face normal, root normal) <
+ * -0.25), ascending by (score, guide index), slots >= stencil_slots (1..8;
+ * 0 = 8) NXG_INVALID_INDEX.  A triangle with a vertex index >= vertex_count
+ * gets an all-invalid row.  Returns INVALID_ARGUMENT (NULL pointer, zero
+ * count, stencil_slots > 8), MISALIGNED_OUTPUT, CUDA or NONE. */
+uint32_t nxg_build_stencils_device(const nxg_vec3 *positions, uint32_t vertex_count,
+                                   const nxg_uint3 *triangles, uint32_t triangle_count,
+                                   const nxg_vec3 *guide_roots, const nxg_vec3 *guide_normals,
+                                   uint32_t guide_count, uint32_t stencil_slots, uint32_t *stencil,
+                                   void *stream);
+
 /* FNV-1a 64 over a byte range (asset.cpp:34-41). */
 uint64_t nxg_fnv1a(const void *bytes, uint64_t size);
 

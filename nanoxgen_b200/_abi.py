@@ -268,6 +268,10 @@ _SIGNATURES = {
     "nxg_build_asset": (ctypes.c_int, [ctypes.POINTER(AssetBuildInput), ctypes.POINTER(ctypes.c_void_p),
                                        ctypes.POINTER(ctypes.c_uint64), ctypes.c_char_p,
                                        ctypes.c_uint64]),
+    "nxg_build_asset_device": (ctypes.c_int, [ctypes.POINTER(AssetBuildInput), _P, ctypes.POINTER(ctypes.c_void_p),
+                                              ctypes.POINTER(ctypes.c_uint64), ctypes.c_char_p, ctypes.c_uint64]),
+    "nxg_build_stencils_device": (ctypes.c_uint32, [_P, ctypes.c_uint32, _P, ctypes.c_uint32, _P, _P,
+                                                    ctypes.c_uint32, ctypes.c_uint32, _P, _P]),
     "nxg_free": (None, [_P]),
     "nxg_fnv1a": (ctypes.c_uint64, [_P, ctypes.c_uint64]),
     "nxg_validate_generation_request": (ctypes.c_uint32, [ctypes.POINTER(DeviceAssetDesc),

@@ -150,6 +150,20 @@ def load_asset(path: str) -> Asset:
 def build_asset(source: AssetBuildInput, stencil_slots: int = 8, workers: int = 0) -> Asset:
     """asset.cpp:229-293 build_asset.  `stencil_slots` < 8 writes the slots
     beyond it as INVALID_INDEX (a K-guide stencil in the 8-slot format)."""
+    return _build(source, stencil_slots, workers, None)
+
+
+def build_asset_device(source: AssetBuildInput, stencil_slots: int = 8, stream=None) -> Asset:
+    """build_asset with its all-pairs searches on the current CUDA device:
+    the per-triangle stencil (asset.cpp:252-269, triangles x guides
+    candidates) and the automatic support radius's nearest roots
+    (asset.cpp:88-97); the blob is byte-identical to build_asset's.  `stream` is a torch.cuda.Stream, a raw
+    cudaStream_t handle or None (the legacy default stream)."""
+    handle = getattr(stream, "cuda_stream", stream) or 0
+    return _build(source, stencil_slots, 0, int(handle))
+
+
+def _build(source: AssetBuildInput, stencil_slots: int, workers: int, stream: Optional[int]) -> Asset:
     g = source.guides
     keep = []
 
@@ -184,11 +198,18 @@ def build_asset(source: AssetBuildInput, stencil_slots: int = 8, workers: int = 
     out = ctypes.c_void_p()
     size = ctypes.c_uint64()
     msg = ctypes.create_string_buffer(256)
-    if lib().nxg_build_asset(ctypes.byref(cin), ctypes.byref(out), ctypes.byref(size), msg, 256) != 0:
+    if stream is None:
+        failed = lib().nxg_build_asset(ctypes.byref(cin), ctypes.byref(out), ctypes.byref(size), msg, 256)
+    else:
+        failed = lib().nxg_build_asset_device(ctypes.byref(cin), stream or None, ctypes.byref(out),
+                                              ctypes.byref(size), msg, 256)
+    if failed:
         raise ValueError(msg.value.decode())
     try:
         blob = np.ctypeslib.as_array(ctypes.cast(out, ctypes.POINTER(ctypes.c_uint8)), shape=(size.value,))
-        return Asset(blob.copy(), validate=True)
+        # The builder wrote the header and content hash itself; validating
+        # would hash the whole blob a second time.
+        return Asset(blob.copy(), validate=False)
     finally:
         lib().nxg_free(out)
 

@@ -27,7 +27,7 @@ NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-
                      "-Xptxas", "-warn-spills"]
 CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-ffp-contract=off", "-Wall", "-Wextra", "-I" + INCLUDE]
 
-CUDA_SOURCES = ["generate.cu", "batched.cu", "classic.cu", "surrogate.cu"]
+CUDA_SOURCES = ["generate.cu", "batched.cu", "classic.cu", "surrogate.cu", "stencil.cu"]
 HOST_SOURCES = ["host.cpp", "expression.cpp"]
 HEADERS = ["nxg_internal.h", "strand_math.cuh", "generator_core.cuh", "seexpr_gradients.inc", "expression.h",
            "seexpr_permutation.inc", "classic_eval.cuh", "umma.cuh", "walk.cuh"]

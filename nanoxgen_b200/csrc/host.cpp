@@ -207,6 +207,10 @@ std::vector<nxg_vec3> make_normals(const nxg_asset_build_input &in) {
 }
 
 // asset.cpp:88-97 (std::min keeps the first argument unless the second is smaller).
+float radius_from_nearest(float nearest) {
+    return std::isfinite(nearest) ? std::max(nearest * 1.75f, 1.0e-4f) : 1.0f;
+}
+
 float automatic_support_radius(const nxg_asset_build_input &in, const std::vector<uint64_t> &first,
                                uint32_t index) {
     if (in.guide_support_radii[index] > 0.0f) { return in.guide_support_radii[index]; }
@@ -217,7 +221,7 @@ float automatic_support_radius(const nxg_asset_build_input &in, const std::vecto
         const float d = std::sqrt(len2(sub(root, in.guide_cvs[first[j]])));
         nearest = (d < nearest) ? d : nearest;
     }
-    return std::isfinite(nearest) ? std::max(nearest * 1.75f, 1.0e-4f) : 1.0f;
+    return radius_from_nearest(nearest);
 }
 
 // asset.cpp:99-150 (the Classic-metadata checks have no fields in this input).
@@ -480,8 +484,12 @@ uint32_t nxg_make_device_asset_descriptor(const void *host_bytes, uint64_t host_
     return NXG_ERROR_NONE;
 }
 
-int nxg_build_asset(const nxg_asset_build_input *input, void **out_bytes, uint64_t *out_size,
-                    char *message, uint64_t message_capacity) {
+namespace {
+
+// asset.cpp:229-293 build_asset; `device` runs the stencil search on the
+// current CUDA device (stencil.cu) instead of the host threads.
+int build_asset_blob(const nxg_asset_build_input *input, bool device, void *stream, void **out_bytes,
+                     uint64_t *out_size, char *message, uint64_t message_capacity) {
     if (!input || !out_bytes || !out_size) {
         copy_message("null argument", message, message_capacity);
         return 1;
@@ -506,7 +514,8 @@ int nxg_build_asset(const nxg_asset_build_input *input, void **out_bytes, uint64
             r.cv_count = static_cast<uint16_t>(in.guide_cv_counts[g]);
             r.flags = 0u;
             r.triangle_index = in.guide_triangles[g];
-            r.support_radius = automatic_support_radius(in, first, g);
+            // The device build finds the nearest roots on the GPU below.
+            r.support_radius = device ? in.guide_support_radii[g] : automatic_support_radius(in, first, g);
             r.barycentric = in.guide_barycentrics[g];
             r.root_uv = in.guide_root_uvs[g];
             r.root_position = in.guide_cvs[first[g]];
@@ -515,7 +524,25 @@ int nxg_build_asset(const nxg_asset_build_input *input, void **out_bytes, uint64
         }
         std::vector<uint32_t> stencil(static_cast<std::size_t>(in.triangle_count) * NXG_GUIDE_STENCIL_SIZE,
                                       NXG_INVALID_INDEX);
-        build_stencils(in, guides, stencil);
+        if (device) {
+            std::vector<nxg_vec3> roots(in.guide_count), root_normals(in.guide_count);
+            for (uint32_t g = 0; g < in.guide_count; ++g) {
+                roots[g] = guides[g].root_position;
+                root_normals[g] = guides[g].root_normal;
+            }
+            std::vector<float> nearest(in.guide_count);
+            const char *what = "";
+            if (nxg::device_guide_search(in.positions, in.vertex_count, in.triangles, in.triangle_count,
+                                         roots.data(), root_normals.data(), in.guide_cv_counts, in.guide_count,
+                                         in.stencil_slots, stencil.data(), nearest.data(), stream, &what) != 0) {
+                throw BuildError(std::string("device stencil search: ") + what);
+            }
+            for (uint32_t g = 0; g < in.guide_count; ++g) {
+                if (!(in.guide_support_radii[g] > 0.0f)) { guides[g].support_radius = radius_from_nearest(nearest[g]); }
+            }
+        } else {
+            build_stencils(in, guides, stencil);
+        }
         // asset.cpp:271-291
         Blob blob;
         blob.resize(sizeof(nxg_asset_header));
@@ -552,6 +579,18 @@ int nxg_build_asset(const nxg_asset_build_input *input, void **out_bytes, uint64
         copy_message(error.what(), message, message_capacity);
         return 1;
     }
+}
+
+} // namespace
+
+int nxg_build_asset(const nxg_asset_build_input *input, void **out_bytes, uint64_t *out_size,
+                    char *message, uint64_t message_capacity) {
+    return build_asset_blob(input, false, nullptr, out_bytes, out_size, message, message_capacity);
+}
+
+int nxg_build_asset_device(const nxg_asset_build_input *input, void *stream, void **out_bytes,
+                           uint64_t *out_size, char *message, uint64_t message_capacity) {
+    return build_asset_blob(input, true, stream, out_bytes, out_size, message, message_capacity);
 }
 
 void nxg_free(void *pointer) { std::free(pointer); }

@@ -31,4 +31,17 @@ uint32_t validate_common(const nxg_device_asset_desc &asset, const nxg_deformed_
 // the asset allocation.
 bool sections_in_bounds(const nxg_asset_header &header) noexcept;
 
+// The two all-pairs searches of build_asset on the current CUDA device
+// (stencil.cu): the per-triangle stencil rows (src/asset.cpp:252-269) and
+// each guide's nearest other root (the automatic support radius, before its
+// 1.75 scale).  Copies the mesh and guide roots/normals/CV counts from host
+// memory, runs both kernels, copies the triangle_count x 8 rows into the host
+// array `stencil` and the guide_count distances into `nearest`, and
+// synchronizes `stream`.  Returns 0 or the CUDA error code, with its text in
+// `what`.
+int device_guide_search(const nxg_vec3 *positions, uint32_t vertex_count, const nxg_uint3 *triangles,
+                        uint32_t triangle_count, const nxg_vec3 *guide_roots, const nxg_vec3 *guide_normals,
+                        const uint32_t *guide_cv_counts, uint32_t guide_count, uint32_t stencil_slots,
+                        uint32_t *stencil, float *nearest, void *stream, const char **what) noexcept;
+
 } // namespace nxg

@@ -32,6 +32,32 @@ def _ptr(t: Optional[torch.Tensor]) -> Optional[int]:
     return None if t is None else int(t.data_ptr())
 
 
+def build_stencils(positions: torch.Tensor, triangles: torch.Tensor, guide_roots: torch.Tensor,
+                   guide_normals: torch.Tensor, stencil_slots: int = 8,
+                   out: Optional[torch.Tensor] = None, stream: Optional[torch.cuda.Stream] = None) -> torch.Tensor:
+    """The stencil search of build_asset (asset.cpp:252-269) on CUDA tensors:
+    positions [V, 3] float32, triangles [T, 3] int32 (vertex indices),
+    guide_roots / guide_normals [G, 3] float32 (first CVs, normalized root
+    normals).  Returns `out` or a new [T, 8] int32 tensor whose bits are the
+    uint32 guide indices (INVALID_INDEX reads as -1)."""
+    for t in (positions, triangles, guide_roots, guide_normals):
+        if not t.is_cuda or not t.is_contiguous() or t.dim() != 2 or t.shape[1] != 3:
+            raise ValueError("expected contiguous [n, 3] CUDA tensors")
+    if positions.dtype != torch.float32 or guide_roots.dtype != torch.float32 or \
+            guide_normals.dtype != torch.float32 or triangles.dtype != torch.int32:
+        raise ValueError("positions, guide_roots, guide_normals float32; triangles int32")
+    if guide_roots.shape != guide_normals.shape:
+        raise ValueError("guide_roots and guide_normals differ in shape")
+    tris = triangles.shape[0]
+    if out is None:
+        out = torch.empty((tris, 8), dtype=torch.int32, device=positions.device)
+    check(lib().nxg_build_stencils_device(positions.data_ptr(), positions.shape[0], triangles.data_ptr(), tris,
+                                          guide_roots.data_ptr(), guide_normals.data_ptr(), guide_roots.shape[0],
+                                          stencil_slots, out.data_ptr(), _stream_handle(stream)),
+          "build_stencils_device")
+    return out
+
+
 class DeviceAsset:
     """A validated asset copied to device memory, with its checked descriptor."""
 

@@ -113,3 +113,26 @@ def test_asset_save_load_round_trip(nxg_lib, tmp_path):
         load_asset(path)
     assert hashlib.sha256(a.bytes()).hexdigest()
     assert Asset(a.bytes()).nbytes == a.nbytes
+
+
+def test_device_stencil_entry_rejects_bad_arguments(nxg_lib):
+    """nxg_build_stencils_device checks its arguments before any CUDA call."""
+    from nanoxgen_b200._abi import ERRORS
+    f = nxg_lib.nxg_build_stencils_device
+    p = 256  # never dereferenced: every call below fails its argument check
+    assert f(p, 3, p, 1, p, p, 1, 9, p, None) == ERRORS["InvalidArgument"]      # stencil_slots > 8
+    assert f(None, 3, p, 1, p, p, 1, 8, p, None) == ERRORS["InvalidArgument"]   # NULL positions
+    assert f(p, 3, p, 0, p, p, 1, 8, p, None) == ERRORS["InvalidArgument"]      # no triangles
+    assert f(p, 3, p, 1, p, p, 0, 8, p, None) == ERRORS["InvalidArgument"]      # no guides
+    assert f(p, 3, p, 1, p, p, 1, 8, p + 4, None) == ERRORS["MisalignedOutput"]  # stencil not 16-byte aligned
+
+
+def test_device_build_without_a_device_fails_loudly(nxg_lib):
+    """With no usable CUDA device the device build raises with the CUDA error
+    text instead of falling back to the host search."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    from nanoxgen_b200.asset import build_asset_device
+    with pytest.raises(ValueError, match="device stencil search"):
+        build_asset_device(fixtures.reference_unit_fixture(), 8)
