@@ -22,7 +22,7 @@
 // issued instructions per candidate instead of twenty-three) and scores the
 // rare group that passes exactly.
 //
-// guide_nearest_kernel, one thread per guide, finds each guide's nearest
+// guide_nearest_kernel, one warp per guide, finds each guide's nearest
 // other root for the automatic support radius (guide_count^2 distances).
 #include "generator_core.cuh"
 #include "nxg_internal.h"
@@ -182,8 +182,13 @@ __device__ __forceinline__ void consider_group(TriangleSearch &t, const GuideTil
     const float2 b = unpair(add2(add2(mul2(dx1, dx1), mul2(dy1, dy1)), mul2(dz1, dz1)));
     const float low = fminf(fminf(a.x, a.y), fminf(b.x, b.y));
     if (t.best[kSlots - 1].key < low * kFilterMargin) { return; }
+    // The group passed: each guide is checked on its own packed value before
+    // its exact score (a warp runs a guide's exact path only when one of its
+    // lanes needs it).
+    const float packed[4] = {a.x, a.y, b.x, b.y};
 #pragma unroll
     for (uint32_t k = 0; k < 4u; ++k) {
+        if (t.best[kSlots - 1].key < packed[k] * kFilterMargin) { continue; }
         consider(t.best, root_distance2(t.centroid, tile, j + k), gi + k, count, t.face, tile.normal[j + k]);
     }
 }
@@ -269,38 +274,28 @@ stencil_kernel(const nxg_vec3 *__restrict__ positions, uint32_t vertex_count, co
 
 // Distance from every guide root to its nearest other root (the automatic
 // support radius, src/asset.cpp automatic_support_radius): |root_i - root_j|
-// with IEEE sqrt, minimum over j != i with a CV count > 0.  Every distance is
-// >= +0 and a NaN one never wins, so the minimum does not depend on order.
+// with IEEE sqrt, minimum over j != i with a CV count > 0.  One warp per
+// guide, lanes striding over j, then a warp minimum: every distance is >= +0,
+// a NaN one never replaces a lane's running value (which starts at FLT_MAX,
+// as the host's), so the minimum is the host's whatever the order.
 __global__ void __launch_bounds__(kStencilThreads)
 guide_nearest_kernel(const nxg_vec3 *__restrict__ roots, const uint32_t *__restrict__ cv_counts, uint32_t guide_count,
                      float *__restrict__ nearest) {
-    __shared__ float sx[kStencilTile], sy[kStencilTile], sz[kStencilTile];
-    __shared__ uint32_t sc[kStencilTile];
-    const uint32_t gi = blockIdx.x * kStencilThreads + threadIdx.x;
-    const bool live = gi < guide_count;
-    F3 root{0.0f, 0.0f, 0.0f};
-    if (live) { root = F3{roots[gi].x, roots[gi].y, roots[gi].z}; }
-    float best = 3.402823466e38f;  // FLT_MAX, as the host starts
-    for (uint32_t base = 0; base < guide_count; base += kStencilTile) {
-        const uint32_t n = guide_count - base < kStencilTile ? guide_count - base : kStencilTile;
-        __syncthreads();
-        for (uint32_t i = threadIdx.x; i < n; i += kStencilThreads) {
-            const nxg_vec3 r = roots[base + i];
-            sx[i] = r.x;
-            sy[i] = r.y;
-            sz[i] = r.z;
-            sc[i] = cv_counts[base + i];
-        }
-        __syncthreads();
-        if (!live) { continue; }
-        for (uint32_t j = 0; j < n; ++j) {
-            if (base + j == gi || sc[j] == 0u) { continue; }
-            const F3 d = xsub(root, F3{sx[j], sy[j], sz[j]});
-            const float dist = __fsqrt_rn(xdot(d, d));
-            best = dist < best ? dist : best;
-        }
+    const uint32_t gi = (blockIdx.x * kStencilThreads + threadIdx.x) >> 5, lane = threadIdx.x & 31u;
+    if (gi >= guide_count) { return; }  // whole warps
+    const nxg_vec3 r = roots[gi];
+    const F3 root{r.x, r.y, r.z};
+    float best = 3.402823466e38f;  // FLT_MAX
+    for (uint32_t j = lane; j < guide_count; j += 32u) {
+        if (j == gi || cv_counts[j] == 0u) { continue; }
+        const nxg_vec3 o = roots[j];
+        const F3 d = xsub(root, F3{o.x, o.y, o.z});
+        const float dist = __fsqrt_rn(xdot(d, d));
+        best = dist < best ? dist : best;
     }
-    if (live) { nearest[gi] = best; }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) { best = fminf(best, __shfl_xor_sync(kFull, best, o)); }
+    if (lane == 0u) { nearest[gi] = best; }
 }
 
 uint32_t slots_kept(uint32_t guide_count, uint32_t stencil_slots) {
@@ -355,7 +350,8 @@ int device_guide_search(const nxg_vec3 *positions, uint32_t vertex_count, const 
         (e = cudaMemcpyAsync(d_root, guide_roots, gb, cudaMemcpyHostToDevice, s)) == cudaSuccess &&
         (e = cudaMemcpyAsync(d_normal, guide_normals, gb, cudaMemcpyHostToDevice, s)) == cudaSuccess &&
         (e = cudaMemcpyAsync(d_counts, guide_cv_counts, cb, cudaMemcpyHostToDevice, s)) == cudaSuccess) {
-        const uint32_t blocks = (guide_count + dev::kStencilThreads - 1u) / dev::kStencilThreads;
+        const uint64_t threads = uint64_t{guide_count} * 32u;
+        const uint32_t blocks = static_cast<uint32_t>((threads + dev::kStencilThreads - 1u) / dev::kStencilThreads);
         dev::guide_nearest_kernel<<<blocks, dev::kStencilThreads, 0, s>>>(d_root, d_counts, guide_count, d_nearest);
         if ((e = cudaGetLastError()) == cudaSuccess &&
             (e = dev::launch_stencils(d_pos, vertex_count, d_tri, triangle_count, d_root, d_normal, guide_count,
