@@ -85,6 +85,41 @@ def profile_traffic_per_point(walk: bool = True):
         return None
 
 
+def profile_instructions_per_strand(walk: bool, noise: bool):
+    """Warp instructions per generated strand of the generate kernel, from the
+    ncu summary committed under profiles/ (None until one exists)."""
+    if not walk:
+        return None, None
+    name = "generate_walk_kernel_large_sphere.md" if noise else "generate_walk_kernel_plain_large_sphere.md"
+    try:
+        with open(os.path.join(ROOT, "profiles", name)) as fh:
+            m = re.search(r"warp_instructions_per_strand:\s*([0-9.eE+-]+)", fh.read())
+            return (float(m.group(1)), "profiles/" + name) if m else (None, None)
+    except OSError:
+        return None, None
+
+
+def issue_ceiling(walk: bool, noise: bool, strands: int, alg_bytes: int, peak: float, sm_mhz):
+    """The HBM fraction the generate kernel would reach if every SM issued one
+    warp instruction per scheduler per cycle: instructions per strand (ncu) x
+    strands / (148 SMs x 4 schedulers x clock)."""
+    per, source = profile_instructions_per_strand(walk, noise)
+    if per is None:
+        return None
+    mhz = sm_mhz or 1965.0
+    ms = per * strands / (148 * 4 * mhz * 1e6) * 1e3
+    return {"warp_instructions_per_strand": per, "ms_at_full_issue": ms,
+            "frac_at_full_issue": alg_bytes / (ms / 1e3) / 1e9 / peak, "sm_mhz": mhz, "source": source}
+
+
+def limiter(frac: float, issue) -> str:
+    if frac >= 0.6:
+        return "hbm"
+    if issue is not None and issue["frac_at_full_issue"] < 1.0:
+        return "instruction issue and latency (frac_at_full_issue < 1)"
+    return "latency"
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
 
@@ -137,79 +172,123 @@ def workload(strands_total: int):
     return w
 
 
-def cpu_baseline(asset, params, seconds: float):
-    """The reference's generate_packed_cpu (oracle/_ref) on all host cores over
-    a bounded prefix sample of the workload's strands; the C restatement of
-    the oracle when the reference library is absent."""
-    cores = os.cpu_count() or 1
+def cpu_model() -> str:
     try:
-        from oracle.checker import Reference, reference_available
-        if not reference_available():
-            raise FileNotFoundError
-        ref = Reference()
-        handle = ref.handle(asset.buffer)
-        kind = "reference"
-
-        def run(n):
-            p = params.copy(strand_count=n)
-            t0 = time.perf_counter()
-            ref.generate(handle, p, 1.0, workers=cores, want_output=False)
-            return time.perf_counter() - t0
-    except (FileNotFoundError, OSError):
-        from oracle.checker import Oracle
-        orc = Oracle()
-        kind = "port"
-
-        def run(n):
-            t0 = time.perf_counter()
-            orc.generate(asset.buffer, params.copy(strand_count=n), 1.0, count=n, threads=cores)
-            return time.perf_counter() - t0
-    P = int(params.cvs_per_strand)
-    probe = 20_000
-    t = run(probe)
-    per_strand = t / probe
-    reps = 3
-    n = int(min(params.strand_count, max(probe, seconds / reps / max(per_strand, 1e-9))))
-    times = [run(n) for _ in range(reps)]
-    med = statistics.median(times)
-    return {"value": n * P / med, "unit": "points/s", "cores": cores, "kind": kind,
-            "sample": "first %d strands x %d CVs of the workload (median of %d calls, %.2f s each; "
-                      "includes the reference's per-call asset validation)" % (n, P, reps, med)}
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
-def run_reference_arm(args):
-    rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
-        return
-    from nanoxgen_b200.asset import build_asset
-    w = workload(args.strands)
-    asset = build_asset(w.build_input, w.stencil_slots)
-    cores = os.cpu_count() or 1
-    P = int(w.params.cvs_per_strand)
+def _percentile(values, q: float) -> float:
+    v = sorted(values)
+    return v[min(len(v) - 1, int(round(q * (len(v) - 1))))]
+
+
+def _reference_runner(blob):
+    """run(n, workers, want_output) -> (seconds, outputs) over the first n
+    strands: the reference's generate_packed_cpu (oracle/_ref) where it is
+    built, else the oracle's C restatement; plus the kind and the
+    validation-only timer (the reference hashes the asset inside every call)."""
     from oracle.checker import Oracle, Reference, reference_available
     if reference_available():
         ref = Reference()
-        handle = ref.handle(asset.buffer)
-        kind = "reference"
+        handle = ref.handle(blob)
 
-        def run(n):
+        def run(params, n, workers, want_output=False):
             t0 = time.perf_counter()
-            ref.generate(handle, w.params.copy(strand_count=n), 1.0, workers=cores, want_output=False)
-            return time.perf_counter() - t0
-    else:
-        orc = Oracle()
-        kind = "port"
+            out = ref.generate(handle, params.copy(strand_count=n), 1.0, workers=workers, want_output=want_output)
+            return time.perf_counter() - t0, out
 
-        def run(n):
+        def validate():
             t0 = time.perf_counter()
-            orc.generate(asset.buffer, w.params.copy(strand_count=n), 1.0, count=n, threads=cores)
+            ref.validate_asset(blob)
             return time.perf_counter() - t0
-    per = run(20_000) / 20_000
+        return run, validate, "reference"
+    orc = Oracle()
+
+    def run(params, n, workers, want_output=False):
+        t0 = time.perf_counter()
+        out = orc.generate(blob, params.copy(strand_count=n), 1.0, count=n, threads=workers)
+        return time.perf_counter() - t0, out
+
+    def validate():
+        t0 = time.perf_counter()
+        orc.validate_asset(blob)
+        return time.perf_counter() - t0
+    return run, validate, "port"
+
+
+def cpu_baseline(blob, params, seconds: float, diag: float, gpu_points=None, gpu_triangles=None):
+    """The reference's generate_packed_cpu (oracle/_ref) on all host cores over
+    a bounded prefix sample of the workload's strands: one warm-up, then
+    median and p90 of 7 calls (the reference's tools/benchmark.cpp:62-80
+    pattern), one single-thread sample, the per-call asset validation timed
+    on its own; and, when the GPU's output is given, the largest distance
+    between the GPU's points and the reference's over the first strands."""
+    import numpy as np
+    cores = os.cpu_count() or 1
+    run, validate, kind = _reference_runner(blob)
+    P = int(params.cvs_per_strand)
+    probe = 20_000
+    per_strand = run(params, probe, cores)[0] / probe
+    reps = 7
+    n = int(min(params.strand_count, max(probe, seconds / (reps + 1) / max(per_strand, 1e-9))))
+    run(params, n, cores)
+    times = [run(params, n, cores)[0] for _ in range(reps)]
+    med, p90 = statistics.median(times), _percentile(times, 0.9)
+    val = statistics.median([validate() for _ in range(3)])
+    n1 = max(2_000, n // cores)
+    single = statistics.median([run(params, n1, 1)[0] for _ in range(3)])
+    out = {"value": n * P / med, "unit": "points/s", "cores": cores, "kind": kind, "cpu_model": cpu_model(),
+           "sample": "first %d strands x %d CVs of the workload; median of %d calls after one warm-up "
+                     "(%.3f s; p90 %.3f s), including the per-call asset validation" % (n, P, reps, med, p90),
+           "median_s": med, "p90_s": p90,
+           "value_p90": n * P / p90,
+           "value_without_validation": n * P / max(med - val, 1e-9), "validation_s": val,
+           "single_thread": {"value": n1 * P / single, "strands": n1, "median_s": single, "calls": 3}}
+    if gpu_points is not None:
+        m = min(n, 20_000)
+        _, ref_out = run(params, m, cores, want_output=True)
+        rpts, rroots = ref_out[0], ref_out[1]
+        d = gpu_points[:m * P, :3].astype(np.float64) - rpts[:m * P, :3].astype(np.float64)
+        err = float(np.sqrt((d * d).sum(-1)).max())
+        rerr = float(np.abs(gpu_points[:m * P, 3].astype(np.float64) - rpts[:m * P, 3]).max())
+        out["parity"] = {"strands_checked": m, "max_error_rel_diag": err / diag,
+                         "max_radius_error_rel_diag": rerr / diag, "tolerance_rel_diag": 1e-5,
+                         "root_triangles_equal": bool(gpu_triangles is not None and
+                                                      np.array_equal(gpu_triangles[:m], rroots["triangle_index"]))}
+    return out
+
+
+def run_reference_arm(args):
+    """The reference's own generate_packed_cpu on the host cores, on the asset
+    its own build_asset makes from the workload (nothing of this library is
+    loaded on this arm)."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle.checker import Reference, reference_available
+    w = workload(args.strands)
+    if not reference_available():
+        print(json.dumps({"impl": "reference", "unavailable": "the reference library oracle/_ref/libnxg_ref.so is "
+                          "not built and the reference sources are absent"}), flush=True)
+        return
+    blob = Reference().build_asset(w.build_input)
+    if w.stencil_slots != 8:
+        raise SystemExit("the headline workload uses 8-guide stencils")
+    cores = os.cpu_count() or 1
+    P = int(w.params.cvs_per_strand)
+    run, validate, kind = _reference_runner(blob)
+    per = run(w.params, 20_000, cores)[0] / 20_000
     budget = 90.0 / max(1, args.steps + args.warmup)
     n = int(min(w.params.strand_count, max(20_000, min(2.0, budget) / max(per, 1e-9))))
     for _ in range(args.warmup):
-        run(n)
-    times = [run(n) for _ in range(args.steps)]
+        run(w.params, n, cores)
+    times = [run(w.params, n, cores)[0] for _ in range(args.steps)]
     total = sum(times)
     value = args.steps * n * P / total
     line = {"metric": "points/sec", "value": value, "unit": "points/s", "n_gpus": args.gpus, "steps": args.steps,
@@ -217,9 +296,12 @@ def run_reference_arm(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "impl": "reference",
             "config": {"workload": w.name, "strands_per_step": n, "cvs_per_strand": P,
-                       "note": "generate_packed_cpu on the host cores over a prefix sample of the workload"},
+                       "note": "generate_packed_cpu on the host cores over a prefix sample of the workload; "
+                               "asset made by the reference's build_asset"},
             "cpu_baseline": {"value": value, "unit": "points/s", "cores": cores, "kind": kind,
-                             "sample": "first %d strands x %d CVs per step" % (n, P)},
+                             "cpu_model": cpu_model(),
+                             "sample": "first %d strands x %d CVs per step (median %.3f s, p90 %.3f s)"
+                                       % (n, P, statistics.median(times), _percentile(times, 0.9))},
             "e2e": {"value": value, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -321,7 +403,11 @@ def run_gpu_arm(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(asset, params.copy(strand_count=S), args.cpu_seconds)
+        m = min(S, 20_000)
+        gpu_pts = points[:m * P].cpu().numpy()
+        gpu_tris = roots.view(-1, 12)[:m, 8].cpu().numpy().view("uint32")
+        cpu = cpu_baseline(asset.buffer, params.copy(strand_count=S), args.cpu_seconds, asset.bbox_diagonal(),
+                           gpu_pts, gpu_tris)
 
     distributed.finalize()
     if rank != 0:
@@ -334,6 +420,7 @@ def run_gpu_arm(args):
     peak, peak_kind = measured_peak()
     achieved = alg_bytes / (kernel_ms / 1e3) / 1e9
     tpp = profile_traffic_per_point(tile[0] == 1)
+    issue = issue_ceiling(tile[0] == 1, noise, S, alg_bytes, peak, clocks.get("sm_mhz"))
     if tile[0] != 1:
         kernel_name = "generate_kernel<%d,%d,%s>" % (tile[0], tile[1], "noise" if noise else "plain")
     elif noise and tile[2] <= 64:
@@ -359,9 +446,15 @@ def run_gpu_arm(args):
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
                      "traffic": (tpp * S * P) if tpp else None,
                      "algorithmic_bytes": alg_bytes, "kernel_ms": kernel_ms,
-                     "note": "algorithmic bytes = 16 B/point + 60 B/strand (roots, root UVs, counts) + asset"},
+                     "limiter": limiter(achieved / peak, issue),
+                     "issue_ceiling": issue,
+                     "note": "algorithmic bytes = 16 B/point + 60 B/strand (roots, root UVs, counts) + asset; "
+                             "'bound' names the roofline the fraction is taken against, 'limiter' what the "
+                             "profile shows limiting the kernel"},
         "clocks": clocks, "gpu_launches": kernels_per_step(tile) * args.steps,
     }
+    if cpu and "parity" in cpu:
+        line["max_error_rel_diag"] = cpu["parity"]["max_error_rel_diag"]
     if e2e:
         line["e2e"] = e2e
     if cpu:

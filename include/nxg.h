@@ -501,9 +501,10 @@ uint32_t nxg_generate_batched(const nxg_device_asset_desc *assets, const nxg_def
  * exceeds NXG_STATIC_SCRATCH_BYTES (for a 4,096-guide description at 32
  * CVs, about 240,000 strands fit and a million do not).  Allocates
  * nothing.  The first call on each device looks up the scratch's device
- * address (once per device), so make that first call before any stream
- * capture.  Every call shares the one scratch: calls that can overlap on
- * the GPU (different streams without ordering between them) race on it. */
+ * address (once per device, and again after a device reset gives the device
+ * a new context), so make that first call before any stream capture.  Every
+ * call shares the one scratch: calls that can overlap on the GPU (different
+ * streams without ordering between them) race on it. */
 uint32_t nxg_generate_packed_static_scratch(const nxg_device_asset_desc *asset,
                                             const nxg_deformed_desc *deformed,
                                             const nxg_generation_params *params,
@@ -524,11 +525,35 @@ typedef struct nxg_strand_state {
 } nxg_strand_state;
 
 /* Evaluates the state above for `count` global strand ids (device array)
- * into `out` (device array), on `stream`.  Uses the generator's own device
- * functions, so its indices are the ones the generator blends. */
+ * into `out` (device array), on `stream`.  Uses the device functions of the
+ * lane-group and serial generators (strands of more than 32 CVs), so its
+ * indices are the ones those generators blend; the lane walk's own choices
+ * are reported by nxg_query_walk_states. */
 uint32_t nxg_query_strand_states(const nxg_device_asset_desc *asset, const nxg_deformed_desc *deformed,
                                  const nxg_generation_params *params, const uint32_t *strands,
                                  uint32_t count, nxg_strand_state *out, void *stream);
+
+/* The lane-walk generator's own per-strand stencil decisions (the walk
+ * generates every strand of 2..32 CVs).  No reference counterpart as an
+ * entry point: it exposes, for parity checks, the choices the reference makes
+ * inside make_guide_blend_state and interpolate_offset (generate.h:214-266).
+ * mode: 0 blend (weight_sum > 1e-12), 1 nearest guide, 2 root normal. */
+typedef struct nxg_walk_state {
+    uint32_t mode;
+    uint32_t nearest;       /* nearest non-rejected guide, else NXG_INVALID_INDEX */
+    float weight_sum;       /* the sum the mode was decided on */
+    uint32_t slot_count;    /* weighted slots the base step reads */
+    uint32_t guides[8];     /* their guides in stencil-slot order, else NXG_INVALID_INDEX */
+    float weights[8];       /* their weights (1 for the nearest guide), else 0 */
+} nxg_walk_state;
+
+/* Runs the lane walk's setup step for `count` global strand ids (device
+ * array) into `out` (device array), on `stream`.  `workspace` (256-byte
+ * aligned, at least nxg_packed_workspace_size(asset, params, count) bytes)
+ * receives the frame's guide records first, as in generation. */
+uint32_t nxg_query_walk_states(const nxg_device_asset_desc *asset, const nxg_deformed_desc *deformed,
+                               const nxg_generation_params *params, const uint32_t *strands, uint32_t count,
+                               nxg_walk_state *out, void *workspace, uint64_t workspace_bytes, void *stream);
 
 #ifdef __cplusplus
 } /* extern "C" */

@@ -237,6 +237,10 @@ GUIDE_DTYPE = np.dtype([("first_cv", "<u4"), ("cv_count", "<u2"), ("flags", "<u2
                         ("barycentric", "<f4", 2), ("root_uv", "<f4", 2),
                         ("root_position", "<f4", 3), ("root_normal", "<f4", 3)])
 assert ROOT_DTYPE.itemsize == 48 and STATE_DTYPE.itemsize == 144 and GUIDE_DTYPE.itemsize == 56
+# nxg_walk_state: the lane walk's own stencil decisions (80 bytes).
+WALK_STATE_DTYPE = np.dtype([("mode", "<u4"), ("nearest", "<u4"), ("weight_sum", "<f4"), ("slot_count", "<u4"),
+                             ("guides", "<u4", 8), ("weights", "<f4", 8)])
+assert WALK_STATE_DTYPE.itemsize == 80
 
 # nxg_error (device_contract.h:58-80 plus additions).
 ERROR_NAMES = [
@@ -337,6 +341,9 @@ _SIGNATURES = {
                                                   ctypes.POINTER(DeformedDesc),
                                                   ctypes.POINTER(GenerationParams), _P, ctypes.c_uint32,
                                                   _P, _P]),
+    "nxg_query_walk_states": (ctypes.c_uint32, [ctypes.POINTER(DeviceAssetDesc), ctypes.POINTER(DeformedDesc),
+                                                ctypes.POINTER(GenerationParams), _P, ctypes.c_uint32, _P, _P,
+                                                ctypes.c_uint64, _P]),
     # nxg_classic.h
     "nxg_expression_compile": (ctypes.c_uint32, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_uint32,
                                                  ctypes.POINTER(ctypes.c_void_p), ctypes.c_char_p, ctypes.c_size_t]),

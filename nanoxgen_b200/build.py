@@ -8,9 +8,11 @@ under oracle/ (see oracle/Makefile).
 from __future__ import annotations
 
 import os
+import re
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
@@ -29,8 +31,6 @@ CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-ffp-contract=off", "-Wall", "-Wextr
 
 CUDA_SOURCES = ["generate.cu", "batched.cu", "classic.cu", "surrogate.cu", "stencil.cu"]
 HOST_SOURCES = ["host.cpp", "expression.cpp"]
-HEADERS = ["nxg_internal.h", "strand_math.cuh", "generator_core.cuh", "seexpr_gradients.inc", "expression.h",
-           "seexpr_permutation.inc", "classic_eval.cuh", "umma.cuh", "walk.cuh"]
 
 
 def _stale(target: str, deps: list[str]) -> bool:
@@ -46,33 +46,55 @@ def _run(cmd: list[str], verbose: bool) -> None:
     subprocess.check_call(cmd)
 
 
+def _includes(path: str, seen: set) -> list[str]:
+    """`path` and every header it includes by a quoted name, found next to it
+    or under include/, recursively."""
+    if path in seen:
+        return []
+    seen.add(path)
+    out = [path]
+    with open(path) as fh:
+        for name in re.findall(r'^\s*#\s*include\s+"([^"]+)"', fh.read(), re.M):
+            for d in (os.path.dirname(path), INCLUDE):
+                cand = os.path.join(d, name)
+                if os.path.exists(cand):
+                    out += _includes(cand, seen)
+                    break
+    return out
+
+
 def build_library(verbose: bool = False, force: bool = False) -> str:
-    """Compiles and links libnxg_b200.so when any source is newer than it."""
+    """Compiles (in parallel) the translation units whose source or included
+    headers are newer than their object, then links libnxg_b200.so."""
     os.makedirs(OBJ, exist_ok=True)
-    common = [os.path.join(INCLUDE, "nxg.h"), os.path.join(INCLUDE, "nxg_classic.h")] + [os.path.join(CSRC, h) for h in HEADERS]
-    objects = []
-    for src in CUDA_SOURCES:
+    jobs, objects = [], []
+    for src in CUDA_SOURCES + HOST_SOURCES:
         path = os.path.join(CSRC, src)
         obj = os.path.join(OBJ, src + ".o")
-        if force or _stale(obj, [path] + common):
-            _run([NVCC] + NVCC_FLAGS + ["-c", path, "-o", obj], verbose)
         objects.append(obj)
-    for src in HOST_SOURCES:
-        path = os.path.join(CSRC, src)
-        obj = os.path.join(OBJ, src + ".o")
-        if force or _stale(obj, [path] + common):
-            _run([CXX] + CXX_FLAGS + ["-c", path, "-o", obj], verbose)
-        objects.append(obj)
+        if force or _stale(obj, _includes(path, set())):
+            tool = [NVCC] + NVCC_FLAGS if src.endswith(".cu") else [CXX] + CXX_FLAGS
+            jobs.append(tool + ["-c", path, "-o", obj])
+    if jobs:
+        with ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 1)) as pool:
+            for f in [pool.submit(_run, cmd, verbose) for cmd in jobs]:
+                f.result()
     if force or _stale(LIB, objects):
         _run([NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", LIB] + objects + ["-lpthread"], verbose)
     return LIB
+
+
+def reference_root() -> str:
+    """The reference checkout: $NXG_REFERENCE_ROOT, else a `reference`
+    directory beside this repository."""
+    return os.environ.get("NXG_REFERENCE_ROOT", os.path.join(os.path.dirname(ROOT), "reference"))
 
 
 def build_oracle(verbose: bool = False) -> None:
     """Builds oracle/liboracle.so, and oracle/_ref/libnxg_ref.so where the
     reference checkout exists (test-only checkers, never product code)."""
     targets = ["oracle"]
-    ref = os.environ.get("NXG_REFERENCE_ROOT", "/root/reference")
+    ref = reference_root()
     if os.path.isfile(os.path.join(ref, "src", "asset.cpp")):
         targets.append("ref")
     _run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "REF=" + ref] + targets, verbose)

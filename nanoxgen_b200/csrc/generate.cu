@@ -655,6 +655,20 @@ __global__ void query_states_kernel(AssetArgs a, FrameArgs f, ParamArgs p, const
     out[i] = s;
 }
 
+// The lane walk's own setup decisions for listed strands (one warp per CTA,
+// g.order = the strand ids, first_strand 0): walk_setup itself, with the
+// frame's guide records already in g.guide_frames, outputs off.
+__global__ void __launch_bounds__(32) walk_states_kernel(LaunchArgs g, uint32_t count, WalkDecision *out) {
+    __shared__ float4 records[kWalkRecords * 32];
+    __shared__ uint32_t locals[32];
+    const int lane = threadIdx.x & 31;
+    const uint32_t i = blockIdx.x * 32u + static_cast<uint32_t>(lane);
+    const bool valid = i < count;
+    WalkDecision d;
+    walk_setup<false>(g, records, locals, nullptr, lane, valid ? i : 0u, valid, g.p.cvs_per_strand, false, &d);
+    if (valid) { out[i] = d; }
+}
+
 } // namespace dev
 
 using dev::LaunchArgs;
@@ -1170,6 +1184,46 @@ uint32_t nxg_query_strand_states(const nxg_device_asset_desc *asset, const nxg_d
     return nxg::record_cuda(cudaGetLastError());
 }
 
+uint32_t nxg_query_walk_states(const nxg_device_asset_desc *asset, const nxg_deformed_desc *deformed,
+                               const nxg_generation_params *params, const uint32_t *strands, uint32_t count,
+                               nxg_walk_state *out, void *workspace, uint64_t workspace_bytes, void *stream) {
+    static_assert(sizeof(nxg_walk_state) == sizeof(nxg::dev::WalkDecision), "nxg_walk_state layout");
+    if (!asset || !params || (count && (!strands || !out))) { return NXG_ERROR_INVALID_ARGUMENT; }
+    const nxg_deformed_desc none{};
+    const nxg_launch_config default_config{128u};
+    const nxg_deformed_desc &frame = deformed ? *deformed : none;
+    uint32_t error = nxg::validate_common(*asset, frame, *params, default_config);
+    if (error != NXG_ERROR_NONE) { return error; }
+    if ((error = nxg::check_launch_inputs(*asset, nullptr)) != NXG_ERROR_NONE) { return error; }
+    if (count == 0u) { return NXG_ERROR_NONE; }
+    const uint32_t P = params->cvs_per_strand;
+    if (!nxg::parallel_path(asset->header.guide_count, P)) { return NXG_ERROR_INVALID_ARGUMENT; }
+    if ((error = nxg::check_workspace(*asset, count, P, workspace, workspace_bytes)) != NXG_ERROR_NONE) {
+        return error;
+    }
+    const auto s = static_cast<cudaStream_t>(stream);
+    const nxg::WorkspaceLayout ws = nxg::workspace_layout(asset->header.guide_count, count, P);
+    auto *offsets = reinterpret_cast<float4 *>(static_cast<unsigned char *>(workspace) + ws.offsets);
+    nxg::LaunchArgs g{};
+    g.a = nxg::resolve_asset(*asset);
+    g.f = nxg::resolve_frame(g.a, frame);
+    g.p = nxg::resolve_params(*params, 1.0f);
+    g.first_strand = 0u;
+    g.count = 0xffffffffu;  // strand ids are global: every id is a valid order entry
+    g.order = strands;
+    g.guide_frames = offsets + uint64_t{asset->header.guide_count} * P;
+    nxg::set_last_cuda_error(0);
+    const uint64_t n = uint64_t{asset->header.guide_count} * P;
+    const uint32_t threads = 256u;
+    const uint32_t blocks = static_cast<uint32_t>(std::max<uint64_t>(1u, std::min<uint64_t>(
+        (n + threads - 1u) / threads, static_cast<uint64_t>(nxg::device_sm_count()) * 16u)));
+    nxg::dev::guide_offsets_kernel<<<blocks, threads, 0, s>>>(g.a, g.f, P, g.p.support_scale, offsets);
+    if ((error = nxg::record_cuda(cudaGetLastError()))) { return error; }
+    nxg::dev::walk_states_kernel<<<(count + 31u) / 32u, 32, 0, s>>>(g, count,
+                                                                  reinterpret_cast<nxg::dev::WalkDecision *>(out));
+    return nxg::record_cuda(cudaGetLastError());
+}
+
 uint32_t nxg_set_tile(uint32_t cvs_per_strand, uint32_t noise, const nxg_tile *tile) {
     if (cvs_per_strand < 2u || cvs_per_strand > nxg::kMaxParallelCvs) { return NXG_ERROR_INVALID_ARGUMENT; }
     std::atomic<uint32_t> &slot = nxg::g_tiles[cvs_per_strand][noise ? 1 : 0];
@@ -1373,28 +1427,67 @@ namespace {
 __device__ __align__(256) unsigned char g_static_scratch[NXG_STATIC_SCRATCH_BYTES];
 
 constexpr int kMaxScratchDevices = 64;
-std::atomic<void *> g_static_scratch_address[kMaxScratchDevices];
+
+// Driver entry points for the identity of the current context, so that an
+// address looked up before a device reset (which destroys the context and
+// unloads this module's device memory) is never handed out after it.
+using CtxGetCurrentFn = int (*)(void **context);
+using CtxGetIdFn = int (*)(void *context, unsigned long long *id);
+
+struct ScratchSlot {
+    unsigned long long context_id;  // 0: not looked up on this device yet
+    void *address;
+};
+ScratchSlot g_static_scratch_slots[kMaxScratchDevices];
 std::mutex g_static_scratch_mutex;
 
-// The device address of g_static_scratch on the current device, looked up
-// once per device with cudaGetSymbolAddress (host code may not use the
-// array's name as a device pointer).
+// The id of the context current on this thread, or 0 when none is current or
+// the driver cannot say.
+unsigned long long current_context_id() {
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult found{};
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &found) == cudaSuccess &&
+            found == cudaDriverEntryPointSuccess) {
+            get_current = reinterpret_cast<CtxGetCurrentFn>(fn);
+        }
+        fn = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &fn, cudaEnableDefault, &found) == cudaSuccess &&
+            found == cudaDriverEntryPointSuccess) {
+            get_id = reinterpret_cast<CtxGetIdFn>(fn);
+        }
+    });
+    void *context = nullptr;
+    unsigned long long id = 0u;
+    if (!get_current || !get_id || get_current(&context) != 0 || context == nullptr || get_id(context, &id) != 0) {
+        return 0u;
+    }
+    return id;
+}
+
+// The device address of g_static_scratch on the current device (host code
+// may not use the array's name as a device pointer).  Looked up with
+// cudaGetSymbolAddress once per device and context: again after a device
+// reset, or whenever the current context's id cannot be read.
 uint32_t static_scratch_address(void **out) {
     int device = 0;
     if (const uint32_t status = record_cuda(cudaGetDevice(&device))) { return status; }
     if (device < 0 || device >= kMaxScratchDevices) { return NXG_ERROR_INVALID_ARGUMENT; }
-    void *address = g_static_scratch_address[device].load(std::memory_order_acquire);
-    if (!address) {
-        std::lock_guard<std::mutex> lock(g_static_scratch_mutex);
-        address = g_static_scratch_address[device].load(std::memory_order_acquire);
-        if (!address) {
-            if (const uint32_t status = record_cuda(cudaGetSymbolAddress(&address, g_static_scratch))) {
-                return status;
-            }
-            g_static_scratch_address[device].store(address, std::memory_order_release);
+    std::lock_guard<std::mutex> lock(g_static_scratch_mutex);
+    ScratchSlot &slot = g_static_scratch_slots[device];
+    const unsigned long long id = current_context_id();
+    if (id == 0u || id != slot.context_id || slot.address == nullptr) {
+        void *address = nullptr;
+        if (const uint32_t status = record_cuda(cudaGetSymbolAddress(&address, g_static_scratch))) {
+            return status;
         }
+        slot.address = address;
+        slot.context_id = current_context_id();  // the lookup makes the device's context current
     }
-    *out = address;
+    *out = slot.address;
     return NXG_ERROR_NONE;
 }
 

@@ -143,15 +143,70 @@ __device__ __forceinline__ Root walk_root(const AssetArgs &a, const FrameArgs &f
     return r;
 }
 
+// The blend weight sum of generate.h:226-241 in the reference's rounding:
+// every value IEEE-rounded and uncontracted, the weights summed in slot order.
+// The setup step's weights use fast arithmetic; it calls this only when its
+// sum may lie on the other side of the 1e-12 threshold that chooses between
+// blending and the nearest-guide fallback (generate.h:261), so that choice is
+// the reference's (for powers other than 2, to the last-bit agreement of
+// CUDA's powf with the host's).  Not inlined: the hot path never takes it.
+static __device__ __noinline__ float walk_exact_weight_sum(const LaunchArgs &g, uint32_t triangle, F3 position, F3 normal) {
+    const AssetArgs &a = g.a;
+    const ParamArgs &p = g.p;
+    float wsum = 0.0f;
+    for (uint32_t j = 0; j < kSlots; ++j) {
+        const uint32_t gi = __ldg(a.stencil + static_cast<uint64_t>(triangle) * kSlots + j);
+        if (gi == kInvalid || gi >= a.guide_count) { continue; }
+        const float4 gr = __ldg(g.guide_frames + 2u * gi);
+        const float4 gn = __ldg(g.guide_frames + 2u * gi + 1u);
+        if (__float_as_uint(gn.w) == 0u) { continue; }
+        const F3 delta = xsub(position, F3{gr.x, gr.y, gr.z});
+        const float d2 = xdot(delta, delta);
+        if (xdot(normal, F3{gn.x, gn.y, gn.z}) < p.rejection_cos) { continue; }
+        const float radius = gr.w;
+        if (radius <= 0.0f || d2 >= __fmul_rn(radius, radius)) { continue; }
+        const float x = __fsub_rn(1.0f, __fdiv_rn(__fsqrt_rn(d2), radius));
+        wsum = __fadd_rn(wsum, p.weight_power == 2.0f ? __fmul_rn(x, x) : powf(x, p.weight_power));
+    }
+    return wsum;
+}
+
+// Whether the fast weight sum `wsum` can lie on the other side of the
+// 1e-12 blend threshold from the reference's.  Each fast base
+// x = 1 - sqrt(d2) / r is within 4e-7 (absolute) of the IEEE one, so a
+// weight x^p is within a relative p * 4e-7 / x of it, plus the fast power's
+// own error (below p * 4e-7 + 1e-5 relative for __powf); the sum's relative
+// error is at most the largest of its terms', taken at the smallest base
+// `xmin`.  Twice that bound is used.
+__device__ __forceinline__ bool walk_blend_uncertain(float wsum, float xmin, float power) {
+    const float rel = 2.0f * (__fdividef(power * 4.0e-7f, xmin) + power * 4.0e-7f + 1.0e-5f);
+    return fabsf(wsum - 1.0e-12f) <= rel * fmaxf(wsum, 1.0e-12f);
+}
+
+// The lane walk's own per-strand decisions, for inspection
+// (nxg_query_walk_states): the blend mode (0 blend, 1 nearest guide,
+// 2 root normal), the nearest eligible guide, the weight sum the decision
+// was taken on, and the weighted slots in the order the base step reads
+// them (guide index and weight; one slot of weight 1 in nearest mode).
+struct WalkDecision {
+    uint32_t mode;
+    uint32_t nearest;
+    float weight_sum;
+    uint32_t slot_count;
+    uint32_t guides[kSlots];
+    float weights[kSlots];
+};
+
 // Setup step for this lane's strand.  The stencil slots follow eval_slot and
 // the loop of generate.h:214-244 with the frame's guide roots, normals and
 // support radii read from the per-frame guide records.  With `outputs`,
 // also writes the strand's root UV and point count and stages its twelve
-// RootSample words at root_words[lane * 12] for walk_store_roots.
+// RootSample words at root_words[lane * 12] for walk_store_roots.  With
+// `decision` (inspection only), also reports the choices made.
 template <bool NOISE>
 __device__ __forceinline__ WalkRoot walk_setup(const LaunchArgs &g, float4 *records, uint32_t *locals,
                                                uint32_t *root_words, int lane, uint32_t pick, bool valid,
-                                               uint32_t P, bool outputs = true) {
+                                               uint32_t P, bool outputs = true, WalkDecision *decision = nullptr) {
     const AssetArgs &a = g.a;
     const FrameArgs &f = g.f;
     const ParamArgs &p = g.p;
@@ -211,6 +266,7 @@ __device__ __forceinline__ WalkRoot walk_setup(const LaunchArgs &g, float4 *reco
     // slots count stay in the reference's exact rounding.
     const bool square = p.weight_power == 2.0f;
     float wsum = 0.0f;
+    float xmin = FLT_MAX;
     float nearest_d2 = FLT_MAX;
     uint32_t nearest = kInvalid;
     uint32_t blended = 0u;
@@ -227,7 +283,10 @@ __device__ __forceinline__ WalkRoot walk_setup(const LaunchArgs &g, float4 *reco
         }
         const float radius = gr[j].w;
         if (radius <= 0.0f || d2 >= __fmul_rn(radius, radius)) { continue; }
-        const float x = 1.0f - __fdividef(sqrt_approx(d2), radius);
+        // Clamped positive: a fast quotient can round to 1 or above at the
+        // radius, and __powf of zero or a negative base is not a weight.
+        const float x = fmaxf(1.0f - __fdividef(sqrt_approx(d2), radius), 1.0e-30f);
+        xmin = fminf(xmin, x);
         const float w = square ? x * x : __powf(x, p.weight_power);
         float *dst = slot_words + ((blended >> 1) * 32u + lane) * 4u + (blended & 1u) * 2u;
         dst[0] = __uint_as_float(stencil[j] * P);
@@ -235,18 +294,35 @@ __device__ __forceinline__ WalkRoot walk_setup(const LaunchArgs &g, float4 *reco
         ++blended;
         wsum = __fadd_rn(wsum, w);
     }
+    if (blended != 0u && walk_blend_uncertain(wsum, xmin, p.weight_power)) {
+        wsum = walk_exact_weight_sum(g, root.triangle, root.position, root.normal);
+    }
     float inv = 0.0f;
     F3 normal_term = {0.0f, 0.0f, 0.0f};
     uint32_t nb = blended;
+    uint32_t mode = 0u;
     if (wsum > 1.0e-12f) {
         inv = 1.0f / wsum;
     } else if (nearest != kInvalid) {
         records[lane] = make_float4(__uint_as_float(nearest * P), 1.0f, 0.0f, 0.0f);
         nb = 1u;
         inv = 1.0f;
+        mode = 1u;
     } else {
         nb = 0u;
         normal_term = root.normal;
+        mode = 2u;
+    }
+    if (decision != nullptr) {
+        decision->mode = mode;
+        decision->nearest = nearest;
+        decision->weight_sum = wsum;
+        decision->slot_count = nb;
+        for (uint32_t j = 0; j < kSlots; ++j) {
+            const float *src = slot_words + (((j >> 1) * 32u + lane) * 4u + (j & 1u) * 2u);
+            decision->guides[j] = j < nb ? __float_as_uint(src[0]) / P : kInvalid;
+            decision->weights[j] = j < nb ? src[1] : 0.0f;
+        }
     }
     records[4 * 32 + lane] = make_float4(root.position.x, root.position.y, root.position.z, inv);
     records[5 * 32 + lane] = make_float4(normal_term.x, normal_term.y, normal_term.z, __uint_as_float(nb));

@@ -132,14 +132,16 @@ def displaced_sphere_radius(theta, phi):
 
 
 def large_sphere(strands: int = 1_000_000, cvs: int = 32, guides: int = 4096, seed: int = 2025,
-                 n_lon: int = 400, n_rings: int = 251) -> Workload:
+                 n_lon: int = 400, n_rings: int = 251, jitter: float = GUIDE_JITTER_32) -> Workload:
     """Single large description: displaced sphere (200,000 triangles, radial
     displacement 0.05 sin(7 theta) sin(5 phi)), 4,096 guides of 32 CVs,
     8-guide stencils, 1,000,000 strands x 32 points, taper 0.02 -> 0.002,
-    noise 0.2 at frequency 12 (output 32M float4 = 512 MiB)."""
+    noise 0.2 at frequency 12 (output 32M float4 = 512 MiB).  `jitter` is the
+    guides' per-CV N(0, jitter) (the plain sphere's 0.02 is 1.4 CV spacings
+    here; the default is a tenth of one)."""
     rng = np.random.default_rng(seed)
     pos, uv, tris = sphere_mesh(n_lon, n_rings, displaced_sphere_radius)
-    gs = surface_guides(pos, tris, guides, 32, rng, texcoords=uv, jitter=GUIDE_JITTER_32)
+    gs = surface_guides(pos, tris, guides, 32, rng, texcoords=uv, jitter=jitter)
     params = GenerationParams(strand_count=strands, cvs_per_strand=cvs, seed=11, root_width=0.02,
                               tip_width=0.002, noise_amplitude=0.2, noise_frequency=12.0)
     name = "displaced-sphere-%dk-tris/%d-guides/k8/%d-strands-x%d" % (tris.shape[0] // 1000, guides, strands, cvs)

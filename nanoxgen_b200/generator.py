@@ -212,6 +212,24 @@ def query_strand_states(dasset: DeviceAsset, params: GenerationParams, strands: 
     return out.cpu().numpy().view(_abi.STATE_DTYPE).reshape(-1)
 
 
+def query_walk_states(dasset: DeviceAsset, params: GenerationParams, strands: Sequence[int] | np.ndarray,
+                      deformed: Optional[DeformedGeometry] = None,
+                      stream: Optional[torch.cuda.Stream] = None) -> np.ndarray:
+    """The lane-walk generator's own stencil decisions per strand
+    (nxg_walk_state records: blend mode, nearest guide, the weight sum the
+    mode was decided on, the weighted slots), for global strand ids."""
+    ids = torch.as_tensor(np.asarray(strands, np.uint32).view(np.int32), device=dasset.device)
+    out = torch.empty((ids.numel(), _abi.WALK_STATE_DTYPE.itemsize // 4), dtype=torch.int32, device=dasset.device)
+    ddesc = deformed.descriptor() if deformed is not None else DeformedDesc()
+    ws = dasset.workspace(params, max(1, ids.numel()))
+    code = lib().nxg_query_walk_states(ctypes.byref(dasset.desc), ctypes.byref(ddesc), ctypes.byref(params),
+                                       ids.data_ptr(), ids.numel(), out.data_ptr(), ws.data_ptr(),
+                                       ws.numel() * ws.element_size(), _stream_handle(stream))
+    check(code, "nxg_query_walk_states")
+    torch.cuda.synchronize(dasset.device)
+    return out.cpu().numpy().view(_abi.WALK_STATE_DTYPE).reshape(-1)
+
+
 def validate_packed_request(dasset_desc: DeviceAssetDesc, params: GenerationParams, output: PackedOutputDesc,
                             deformed: Optional[DeformedDesc] = None, block_size: int = 128) -> int:
     """nxg_validate_packed_request (device_contract.h:221-254); pure host."""

@@ -129,7 +129,7 @@ class Oracle:
 def reference_available() -> bool:
     if os.path.exists(REF_PATH):
         return True
-    ref = os.environ.get("NXG_REFERENCE_ROOT", "/root/reference")
+    ref = os.environ.get("NXG_REFERENCE_ROOT", os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference"))
     if os.path.isfile(os.path.join(ref, "src", "asset.cpp")):
         subprocess.check_call(["make", "-s", "-C", HERE, "ref", "REF=" + ref])
         return os.path.exists(REF_PATH)

@@ -85,6 +85,98 @@ def test_stencil_indices_bit_exact(torch_cuda, oracle, sphere):
             np.testing.assert_allclose(st["weights"], ref["weights"], rtol=1e-5, atol=1e-7)
 
 
+INVALID = 0xFFFFFFFF
+
+
+def _reference_mode(ref) -> int:
+    """interpolate_offset's choice (generate.h:261-266): 0 blend, 1 nearest
+    guide, 2 root normal."""
+    if ref["weight_sum"] > np.float32(1e-12):
+        return 0
+    return 1 if ref["nearest"] != INVALID else 2
+
+
+def _check_walk_state(st, ref, strand):
+    mode = _reference_mode(ref)
+    assert st["mode"] == mode, strand
+    assert st["nearest"] == ref["nearest"], strand
+    if mode == 0:
+        used = ref["indices"] != INVALID
+        n = int(used.sum())
+        assert st["slot_count"] == n, strand
+        assert np.array_equal(st["guides"][:n], ref["indices"][used]), strand          # slot order kept
+        np.testing.assert_allclose(st["weights"][:n], ref["weights"][used], rtol=2e-5, atol=1e-30)
+    elif mode == 1:
+        assert st["slot_count"] == 1 and st["guides"][0] == ref["nearest"] and st["weights"][0] == 1.0, strand
+    else:
+        assert st["slot_count"] == 0, strand
+    return mode
+
+
+def test_walk_stencil_decisions_bit_exact(torch_cuda, oracle, sphere):
+    """The lane walk's own setup step (nxg_query_walk_states), which is what
+    generates every strand of 2..32 CVs: its blended guides in slot order, its
+    nearest guide and its blend / nearest / normal choice against the
+    reference's make_guide_blend_state and interpolate_offset
+    (generate.h:214-266).  The parameter sets include rejection-heavy,
+    narrow-support and high-power cases, where many strands fall back to the
+    nearest guide or sit near the 1e-12 weight-sum threshold."""
+    from nanoxgen_b200.generator import DeviceAsset, query_walk_states
+    w, asset = sphere
+    d = DeviceAsset(asset)
+    ids = np.arange(0, w.params.strand_count, 3, dtype=np.uint32)
+    modes = np.zeros(3, np.int64)
+    for params in (w.params, w.params.copy(normal_rejection_cos=0.5, guide_support_scale=0.4),
+                   w.params.copy(guide_weight_power=40.0, guide_support_scale=0.7),
+                   w.params.copy(guide_weight_power=0.5, guide_support_scale=0.15),
+                   w.params.copy(normal_rejection_cos=0.999, guide_support_scale=0.3)):
+        states = query_walk_states(d, params, ids)
+        for s, st in zip(ids, states):
+            modes[_check_walk_state(st, oracle.strand_state(asset.buffer, params, int(s)), int(s))] += 1
+    assert modes.min() > 0, modes  # every mode was exercised
+
+
+def test_walk_blend_threshold_decision(torch_cuda, oracle, nxg_lib):
+    """Weight sums within a few parts per million of the 1e-12 threshold.
+    One guide, so the sum is its weight (1 - d/r)^p; the power is stepped one
+    float at a time across the value that puts a strand's weight at 1e-12.
+    The fast weights the walk blends with are further than that from the
+    reference's, so the walk must take the decision on exactly rounded
+    weights.  The only allowed disagreement is where the reference's own sum
+    is within 4 ulp of 1e-12 (CUDA's powf and the host's may differ in the
+    last bit)."""
+    from nanoxgen_b200 import fixtures
+    from nanoxgen_b200._abi import GenerationParams
+    from nanoxgen_b200.asset import build_asset
+    from nanoxgen_b200.generator import DeviceAsset, query_walk_states
+    asset = build_asset(fixtures.reference_unit_fixture())
+    d = DeviceAsset(asset)
+    base = GenerationParams(strand_count=64, cvs_per_strand=8, seed=5, guide_weight_power=1.0)
+    threshold = np.float32(1e-12)
+    checked = flips_possible = 0
+    for strand in range(0, 64, 8):
+        x = float(oracle.strand_state(asset.buffer, base, strand)["weights"][0])
+        if not 0.05 < x < 0.9999:
+            continue
+        p_star = np.float32(np.log(1e-12) / np.log(x))
+        powers = [p_star]
+        for _ in range(24):
+            powers.append(np.nextafter(powers[-1], np.float32(np.inf)))
+            powers.insert(0, np.nextafter(powers[0], np.float32(-np.inf)))
+        for pw in powers:
+            params = base.copy(guide_weight_power=float(pw))
+            st = query_walk_states(d, params, [strand])[0]
+            ref = oracle.strand_state(asset.buffer, params, strand)
+            near = abs(int(np.float32(ref["weight_sum"]).view(np.int32)) - int(threshold.view(np.int32))) <= 4
+            if near:
+                flips_possible += 1
+                continue
+            _check_walk_state(st, ref, strand)
+            checked += 1
+    assert checked >= 300, checked
+    print("threshold scan: %d decisions checked, %d within 4 ulp skipped" % (checked, flips_possible))
+
+
 @pytest.mark.parametrize("name", ["unit_fixture.npz", "plain_sphere.npz"])
 def test_golden_outputs(torch_cuda, name):
     """Against the reference's own outputs committed under tests/golden."""

@@ -17,7 +17,7 @@ from helpers import max_position_error
 pytestmark = pytest.mark.gpu
 
 
-def test_static_scratch_matches_workspace_path_on_two_calls(cuda, nxg_lib):
+def test_static_scratch_matches_workspace_path_on_two_calls(cuda, nxg_lib, oracle):
     import torch
 
     from nanoxgen_b200 import _abi, fixtures
@@ -39,6 +39,7 @@ def test_static_scratch_matches_workspace_path_on_two_calls(cuda, nxg_lib):
     ref_roots = reference.roots.cpu().numpy()
     ref_counts = reference.point_counts.cpu().numpy()
     tol = 1e-5 * asset.bbox_diagonal()
+    orc_points, orc_roots, _, orc_counts = oracle.generate(asset.buffer, params, 1.5, threads=8)
 
     stream = torch.cuda.current_stream().cuda_stream
     for call in range(2):                                      # the scratch keeps the last call's contents
@@ -54,6 +55,10 @@ def test_static_scratch_matches_workspace_path_on_two_calls(cuda, nxg_lib):
         assert max_position_error(got, ref_points) <= tol, call
         assert float(np.abs(got[:, 3] - ref_points[:, 3]).max()) <= tol, call
         assert np.array_equal(roots.cpu().numpy(), ref_roots) and np.array_equal(counts.cpu().numpy(), ref_counts)
+        # and against the oracle directly: roots bit-exact, positions within 1e-5 x diagonal
+        assert roots.cpu().numpy().tobytes() == orc_roots.tobytes(), call
+        assert np.array_equal(counts.cpu().numpy().view(np.uint32), orc_counts), call
+        assert max_position_error(got, orc_points) <= tol, call
 
 
 def test_static_scratch_rejects_requests_beyond_its_size(cuda, nxg_lib):
