@@ -143,17 +143,22 @@ __device__ __forceinline__ Root walk_root(const AssetArgs &a, const FrameArgs &f
     return r;
 }
 
-// The blend weight sum of generate.h:226-241 in the reference's rounding:
-// every value IEEE-rounded and uncontracted, the weights summed in slot order.
-// The setup step's weights use fast arithmetic; it calls this only when its
-// sum may lie on the other side of the 1e-12 threshold that chooses between
-// blending and the nearest-guide fallback (generate.h:261), so that choice is
-// the reference's (for powers other than 2, to the last-bit agreement of
-// CUDA's powf with the host's).  Not inlined: the hot path never takes it.
-static __device__ __noinline__ float walk_exact_weight_sum(const LaunchArgs &g, uint32_t triangle, F3 position, F3 normal) {
+// The blend weights of generate.h:226-241 in the reference's rounding: every
+// value IEEE-rounded and uncontracted.  Rewrites the weights of the strand's
+// blended slots (records in slot order, as the setup step staged them) and
+// returns their sum in slot order.  The setup step's weights use fast
+// arithmetic; it calls this only for strands where those may be inaccurate
+// (a slot near the edge of its support radius) or where the sum may lie on
+// the other side of the 1e-12 threshold that chooses between blending and the
+// nearest-guide fallback (generate.h:261), so both the blend and that choice
+// are the reference's (for powers other than 2, to the last-bit agreement of
+// CUDA's powf with the host's).  Not inlined: the hot path rarely takes it.
+static __device__ __noinline__ float walk_exact_weights(const LaunchArgs &g, uint32_t triangle, F3 position,
+                                                        F3 normal, float *slot_words, int lane) {
     const AssetArgs &a = g.a;
     const ParamArgs &p = g.p;
     float wsum = 0.0f;
+    uint32_t blended = 0u;
     for (uint32_t j = 0; j < kSlots; ++j) {
         const uint32_t gi = __ldg(a.stencil + static_cast<uint64_t>(triangle) * kSlots + j);
         if (gi == kInvalid || gi >= a.guide_count) { continue; }
@@ -166,21 +171,26 @@ static __device__ __noinline__ float walk_exact_weight_sum(const LaunchArgs &g, 
         const float radius = gr.w;
         if (radius <= 0.0f || d2 >= __fmul_rn(radius, radius)) { continue; }
         const float x = __fsub_rn(1.0f, __fdiv_rn(__fsqrt_rn(d2), radius));
-        wsum = __fadd_rn(wsum, p.weight_power == 2.0f ? __fmul_rn(x, x) : powf(x, p.weight_power));
+        const float w = p.weight_power == 2.0f ? __fmul_rn(x, x) : powf(x, p.weight_power);
+        slot_words[((blended >> 1) * 32u + static_cast<uint32_t>(lane)) * 4u + (blended & 1u) * 2u + 1u] = w;
+        ++blended;
+        wsum = __fadd_rn(wsum, w);
     }
     return wsum;
 }
 
-// Whether the fast weight sum `wsum` can lie on the other side of the
-// 1e-12 blend threshold from the reference's.  Each fast base
-// x = 1 - sqrt(d2) / r is within 4e-7 (absolute) of the IEEE one, so a
-// weight x^p is within a relative p * 4e-7 / x of it, plus the fast power's
-// own error (below p * 4e-7 + 1e-5 relative for __powf); the sum's relative
-// error is at most the largest of its terms', taken at the smallest base
-// `xmin`.  Twice that bound is used.
-__device__ __forceinline__ bool walk_blend_uncertain(float wsum, float xmin, float power) {
-    const float rel = 2.0f * (__fdividef(power * 4.0e-7f, xmin) + power * 4.0e-7f + 1.0e-5f);
-    return fabsf(wsum - 1.0e-12f) <= rel * fmaxf(wsum, 1.0e-12f);
+// Whether the setup step must take exact weights.  A fast base
+// x = 1 - sqrt(d2) / r is within 4e-7 (absolute) of the IEEE one, so a weight
+// x^p is off by at most a relative p * 4e-7 / x from it (`edge` = the sum of
+// w * p * 4e-7 / x over the slots), plus the fast power's own error, below
+// p * 4e-7 + 1e-5 relative for __powf (one rounding for the square).  Exact
+// weights are taken when the first part exceeds 1e-5 of the sum (the blend
+// itself could move by that fraction of an offset), when a base was clamped
+// (`clamped`), or when twice the whole bound reaches across 1e-12.
+__device__ __forceinline__ bool walk_needs_exact_weights(float wsum, float edge, bool clamped, bool square,
+                                                         float power) {
+    const float bound = edge + (square ? 1.2e-7f : power * 4.0e-7f + 1.0e-5f) * wsum;
+    return clamped || edge > 1.0e-5f * wsum || fabsf(wsum - 1.0e-12f) <= 2.0f * bound;
 }
 
 // The lane walk's own per-strand decisions, for inspection
@@ -266,7 +276,8 @@ __device__ __forceinline__ WalkRoot walk_setup(const LaunchArgs &g, float4 *reco
     // slots count stay in the reference's exact rounding.
     const bool square = p.weight_power == 2.0f;
     float wsum = 0.0f;
-    float xmin = FLT_MAX;
+    float edge = 0.0f;      // sum of w * p * 4e-7 / x (walk_needs_exact_weights)
+    bool clamped = false;
     float nearest_d2 = FLT_MAX;
     uint32_t nearest = kInvalid;
     uint32_t blended = 0u;
@@ -285,17 +296,19 @@ __device__ __forceinline__ WalkRoot walk_setup(const LaunchArgs &g, float4 *reco
         if (radius <= 0.0f || d2 >= __fmul_rn(radius, radius)) { continue; }
         // Clamped positive: a fast quotient can round to 1 or above at the
         // radius, and __powf of zero or a negative base is not a weight.
-        const float x = fmaxf(1.0f - __fdividef(sqrt_approx(d2), radius), 1.0e-30f);
-        xmin = fminf(xmin, x);
+        const float raw = 1.0f - __fdividef(sqrt_approx(d2), radius);
+        const float x = fmaxf(raw, 1.0e-30f);
+        clamped = clamped || !(raw > 1.0e-30f);
         const float w = square ? x * x : __powf(x, p.weight_power);
+        edge += __fdividef(w, x) * (p.weight_power * 4.0e-7f);
         float *dst = slot_words + ((blended >> 1) * 32u + lane) * 4u + (blended & 1u) * 2u;
         dst[0] = __uint_as_float(stencil[j] * P);
         dst[1] = w;
         ++blended;
         wsum = __fadd_rn(wsum, w);
     }
-    if (blended != 0u && walk_blend_uncertain(wsum, xmin, p.weight_power)) {
-        wsum = walk_exact_weight_sum(g, root.triangle, root.position, root.normal);
+    if (blended != 0u && walk_needs_exact_weights(wsum, edge, clamped, square, p.weight_power)) {
+        wsum = walk_exact_weights(g, root.triangle, root.position, root.normal, slot_words, lane);
     }
     float inv = 0.0f;
     F3 normal_term = {0.0f, 0.0f, 0.0f};
