@@ -1,9 +1,12 @@
 // expression.cpp -- host compiler for XGen scalar expressions.
 //
 // Produces the SSA program that the device evaluator (classic.cu) runs for
-// every root.  The language, the compiled program and the error texts follow
-// the reference compiler:
-//   source normalisation        src/xgen_expression.cpp:50-118
+// every root.  The language, the compiled program (instruction numbering,
+// operand order, emission order) and the error texts are the reference
+// compiler's; the code is a reader that rewrites comments and line breaks on
+// the fly, a one-pass scanner and a precedence-climbing parser.  Behaviour
+// followed:
+//   source rewriting (comments, "\n", line joining)  src/xgen_expression.cpp:50-118
 //   tokens                      src/xgen_expression.cpp:120-223
 //   grammar / SSA emission      src/xgen_expression.cpp:225-557
 //   float program conversion    src/xgen_expression.cpp:783-818
@@ -15,6 +18,7 @@
 #include "nxg_classic.h"
 #include "expression.h"
 
+#include <algorithm>
 #include <charconv>
 #include <cmath>
 #include <cstdlib>
@@ -118,69 +122,123 @@ constexpr size_t kMaxInstructions = 100000u;
 constexpr size_t kMaxLocals = 4096u;
 constexpr size_t kMaxRampPoints = 4096u;
 
-// ------------------------------------------------------------ normalising
-
-bool continues_line(char c) {
-    switch (c) {
-        case '+': case '-': case '*': case '/': case '<': case '>': case '=': case '!':
-        case '&': case '|': case '?': case ':': case ',': case '(':
-            return true;
-        default:
-            return false;
+// --------------------------------------------------------------- reading
+//
+// The language is defined on a rewritten form of the source: the two
+// characters "\n" stand for a newline, '#' comments run to the end of their
+// line and become a statement break (';'), and every remaining newline joins
+// the two lines (a space) when the text before it ends, or the text after it
+// starts, with an operator, and separates statements (';') otherwise.  Error
+// offsets count bytes of that rewritten form.  Reader produces it one
+// character at a time, so the scanner below never sees a rewritten copy of
+// the source; it also reports, for each character it hands out, where the
+// character sits in the source (numbers are parsed in place there).
+class Reader {
+public:
+    explicit Reader(const std::string &source) : src_(source) {
+        if (src_.size() > kMaxSourceBytes) { fail("XGen scalar expression source byte limit exceeded"); }
+        if (src_.find('\0') != std::string::npos) { fail("XGen scalar expression contains a NUL byte"); }
     }
-}
 
-// '#' comments end at a newline, which becomes ';'.  A newline then joins the
-// lines (a space) when the text before it ends, or the text after it starts,
-// with an operator; otherwise it separates statements (';').
-std::string normalise(const std::string &source) {
-    if (source.size() > kMaxSourceBytes) { fail("XGen scalar expression source byte limit exceeded"); }
-    if (source.find('\0') != std::string::npos) { fail("XGen scalar expression contains a NUL byte"); }
-    std::string stripped;
-    stripped.reserve(source.size());
-    bool in_comment = false;
-    for (size_t i = 0; i < source.size(); ++i) {
-        char c = source[i];
-        if (c == '\\' && i + 1 < source.size() && source[i + 1] == 'n') {
-            c = '\n';
-            ++i;
+    // The character `ahead` positions on (0 = the next one), or -1 past the end.
+    int peek(size_t ahead = 0) {
+        while (pending_.size() <= ahead) {
+            if (!produce()) { return -1; }
         }
-        if (in_comment) {
-            if (c == '\n' || c == '\r') {
-                in_comment = false;
-                stripped.push_back(';');
+        return static_cast<unsigned char>(pending_[ahead].c);
+    }
+    int next() {
+        const int c = peek();
+        if (c >= 0) {
+            pending_.erase(pending_.begin());
+            ++offset_;
+        }
+        return c;
+    }
+    // Rewritten-form offset of the next character.
+    size_t offset() const { return offset_; }
+    // Source position of the next character; the source itself.
+    size_t source_position() {
+        peek();
+        return pending_.empty() ? src_.size() : pending_.front().at;
+    }
+    const std::string &source() const { return src_; }
+
+private:
+    struct Pending {
+        char c;
+        size_t at;
+    };
+
+    // Operators that carry an expression over a line break.
+    static bool joins(char c) { return std::strchr("+-*/<>=!&|?:,(", c) != nullptr; }
+    static bool line_end(char c) { return c == '\n' || c == '\r'; }
+
+    // The source character at `pos`, with the "\n" escape read as a newline;
+    // `width` is how many source bytes it spans.
+    char logical(size_t pos, size_t &width) const {
+        if (src_[pos] == '\\' && pos + 1 < src_.size() && src_[pos + 1] == 'n') {
+            width = 2;
+            return '\n';
+        }
+        width = 1;
+        return src_[pos];
+    }
+
+    // Whether the first character after a line break (blanks and further
+    // line breaks skipped) starts with a joining operator or ')'.  A comment
+    // there counts as a statement break.
+    bool next_line_joins(size_t pos) const {
+        while (pos < src_.size()) {
+            size_t width = 0;
+            const char c = logical(pos, width);
+            if (c != ' ' && c != '\t' && !line_end(c)) { return c != '#' && (joins(c) || c == ')'); }
+            pos += width;
+        }
+        return false;
+    }
+
+    void emit(char c, size_t at) {
+        pending_.push_back(Pending{c, at});
+        if (c != ' ' && c != '\t') { last_solid_ = c; }
+    }
+
+    // Appends the next rewritten character(s); false at the end of the source.
+    bool produce() {
+        while (pos_ < src_.size()) {
+            size_t width = 0;
+            const size_t at = pos_;
+            const char c = logical(pos_, width);
+            pos_ += width;
+            if (c == '#') {  // skip to the line end, which the comment consumes
+                while (pos_ < src_.size()) {
+                    const char d = logical(pos_, width);
+                    pos_ += width;
+                    if (line_end(d)) {
+                        emit(';', at);
+                        return true;
+                    }
+                }
+                return false;
             }
-        } else if (c == '#') {
-            in_comment = true;
-        } else {
-            stripped.push_back(c);
+            if (line_end(c)) {
+                emit((last_solid_ != 0 && joins(last_solid_)) || next_line_joins(pos_) ? ' ' : ';', at);
+                return true;
+            }
+            emit(c, at);
+            return true;
         }
+        return false;
     }
-    std::string joined;
-    joined.reserve(stripped.size());
-    for (size_t i = 0; i < stripped.size(); ++i) {
-        const char c = stripped[i];
-        if (c != '\n' && c != '\r') {
-            joined.push_back(c);
-            continue;
-        }
-        size_t before = joined.size();
-        while (before > 0 && (joined[before - 1] == ' ' || joined[before - 1] == '\t')) { --before; }
-        size_t after = i + 1;
-        while (after < stripped.size() &&
-               (stripped[after] == ' ' || stripped[after] == '\t' || stripped[after] == '\n' ||
-                stripped[after] == '\r')) {
-            ++after;
-        }
-        const bool with_previous = before > 0 && continues_line(joined[before - 1]);
-        const bool with_next =
-            after < stripped.size() && (continues_line(stripped[after]) || stripped[after] == ')');
-        joined.push_back(with_previous || with_next ? ' ' : ';');
-    }
-    return joined;
-}
 
-// ------------------------------------------------------------------ tokens
+    const std::string &src_;
+    size_t pos_ = 0;
+    size_t offset_ = 0;
+    char last_solid_ = 0;  // the last character handed on other than a blank
+    std::vector<Pending> pending_;
+};
+
+// -------------------------------------------------------------- scanning
 
 enum class Tok : uint8_t {
     End, Number, Variable, Identifier, String, Semicolon, Comma, LParen, RParen, Question, Colon,
@@ -195,387 +253,352 @@ struct Token {
     size_t offset = 0;
 };
 
-bool ident_start(char c) { return (c >= 'a' && c <= 'z') || (c >= 'A' && c <= 'Z') || c == '_'; }
-bool ident_part(char c) { return ident_start(c) || (c >= '0' && c <= '9'); }
+bool ident_start(int c) { return (c >= 'a' && c <= 'z') || (c >= 'A' && c <= 'Z') || c == '_'; }
+bool ident_part(int c) { return ident_start(c) || (c >= '0' && c <= '9'); }
+bool is_digit(int c) { return c >= '0' && c <= '9'; }
 
-std::vector<Token> lex(const std::string &s) {
-    std::vector<Token> out;
-    const auto push = [&out](Tok kind, size_t offset, std::string text = {}, double number = 0.0) {
-        if (out.size() >= kMaxTokens) { fail("XGen scalar expression token limit exceeded"); }
-        out.push_back(Token{kind, std::move(text), number, offset});
+// Punctuation: a character, optionally followed by a second one that makes a
+// different token (`pair`), else `single` -- or, where the character has no
+// meaning alone, the error text `alone`.
+struct Punct {
+    char first, second;
+    Tok pair, single;
+    const char *alone;
+};
+constexpr Punct kPunctuation[] = {
+    {';', 0, Tok::End, Tok::Semicolon, nullptr}, {',', 0, Tok::End, Tok::Comma, nullptr},
+    {'(', 0, Tok::End, Tok::LParen, nullptr},    {')', 0, Tok::End, Tok::RParen, nullptr},
+    {'?', 0, Tok::End, Tok::Question, nullptr},  {':', 0, Tok::End, Tok::Colon, nullptr},
+    {'+', 0, Tok::End, Tok::Plus, nullptr},      {'*', 0, Tok::End, Tok::Star, nullptr},
+    {'/', 0, Tok::End, Tok::Slash, nullptr},     {'-', '>', Tok::Arrow, Tok::Minus, nullptr},
+    {'=', '=', Tok::Equal, Tok::Assign, nullptr}, {'!', '=', Tok::NotEqual, Tok::Bang, nullptr},
+    {'<', '=', Tok::LessEqual, Tok::Less, nullptr}, {'>', '=', Tok::GreaterEqual, Tok::Greater, nullptr},
+    {'&', '&', Tok::And, Tok::End, "single '&' is unsupported; use '&&'"},
+    {'|', '|', Tok::Or, Tok::End, "single '|' is unsupported; use '||'"},
+};
+
+// The whole token list of a source (the parser looks two tokens ahead).
+std::vector<Token> scan(const std::string &source) {
+    Reader in(source);
+    std::vector<Token> tokens;
+    const auto add = [&tokens](Token t) {
+        if (tokens.size() >= kMaxTokens) { fail("XGen scalar expression token limit exceeded"); }
+        tokens.push_back(std::move(t));
     };
-    size_t i = 0;
-    while (i < s.size()) {
-        const char c = s[i];
+    for (;;) {
+        const int c = in.peek();
+        const size_t at = in.offset();
+        if (c < 0) { break; }
         if (c == ' ' || c == '\t' || c == '\f' || c == '\v') {
-            ++i;
+            in.next();
             continue;
         }
-        const bool digit = c >= '0' && c <= '9';
-        if (digit || (c == '.' && i + 1 < s.size() && s[i + 1] >= '0' && s[i + 1] <= '9')) {
-            const char *begin = s.c_str() + i;
-            char *end = nullptr;
-            const double value = std::strtod(begin, &end);
-            const size_t used = static_cast<size_t>(end - begin);
-            if (used == 0 || !std::isfinite(value)) { syntax(i, "invalid or non-finite numeric literal"); }
-            push(Tok::Number, i, {}, value);
-            i += used;
-            continue;
-        }
-        if (c == '$') {
-            const size_t at = i++;
-            if (i >= s.size() || !ident_start(s[i])) { syntax(at, "expected a variable name after '$'"); }
-            const size_t name = i++;
-            while (i < s.size() && ident_part(s[i])) { ++i; }
-            push(Tok::Variable, at, s.substr(name, i - name));
-            continue;
-        }
-        if (ident_start(c)) {
-            const size_t at = i++;
-            while (i < s.size() && ident_part(s[i])) { ++i; }
-            push(Tok::Identifier, at, s.substr(at, i - at));
-            continue;
-        }
-        if (c == '\'' || c == '"') {
-            const size_t at = i++;
-            std::string text;
-            while (i < s.size() && s[i] != c) {
-                if (s[i] == '\\' && i + 1 < s.size()) { ++i; }
-                text.push_back(s[i++]);
+        Token t;
+        t.offset = at;
+        if (is_digit(c) || (c == '.' && is_digit(in.peek(1)))) {
+            // strtod in place: a literal never spans a rewritten character.
+            const char *first = in.source().c_str() + in.source_position();
+            char *last = nullptr;
+            t.number = std::strtod(first, &last);
+            const size_t length = static_cast<size_t>(last - first);
+            if (length == 0 || !std::isfinite(t.number)) { syntax(at, "invalid or non-finite numeric literal"); }
+            for (size_t k = 0; k < length; ++k) { in.next(); }
+            t.kind = Tok::Number;
+        } else if (c == '$' || ident_start(c)) {
+            t.kind = c == '$' ? Tok::Variable : Tok::Identifier;
+            if (c == '$') {
+                in.next();
+                if (!ident_start(in.peek())) { syntax(at, "expected a variable name after '$'"); }
             }
-            if (i == s.size()) { syntax(at, "unterminated string literal"); }
-            ++i;
-            push(Tok::String, at, std::move(text));
-            continue;
-        }
-        const auto pair = [&](char second, Tok both, Tok single) {
-            if (i + 1 < s.size() && s[i + 1] == second) {
-                push(both, i);
-                i += 2;
+            while (ident_part(in.peek())) { t.text.push_back(static_cast<char>(in.next())); }
+        } else if (c == '\'' || c == '"') {
+            in.next();
+            for (int d = in.next();; d = in.next()) {
+                if (d < 0) { syntax(at, "unterminated string literal"); }
+                if (d == c) { break; }
+                if (d == '\\' && in.peek() >= 0) { d = in.next(); }
+                t.text.push_back(static_cast<char>(d));
+            }
+            t.kind = Tok::String;
+        } else {
+            const Punct *p = nullptr;
+            for (const Punct &q : kPunctuation) {
+                if (q.first == c) { p = &q; }
+            }
+            if (p == nullptr) { syntax(at, "unsupported character"); }
+            in.next();
+            if (p->second != 0 && in.peek() == p->second) {
+                in.next();
+                t.kind = p->pair;
+            } else if (p->alone != nullptr) {
+                syntax(at, p->alone);
             } else {
-                push(single, i);
-                ++i;
+                t.kind = p->single;
             }
-        };
-        switch (c) {
-            case ';': push(Tok::Semicolon, i++); break;
-            case ',': push(Tok::Comma, i++); break;
-            case '(': push(Tok::LParen, i++); break;
-            case ')': push(Tok::RParen, i++); break;
-            case '?': push(Tok::Question, i++); break;
-            case ':': push(Tok::Colon, i++); break;
-            case '+': push(Tok::Plus, i++); break;
-            case '*': push(Tok::Star, i++); break;
-            case '/': push(Tok::Slash, i++); break;
-            case '-': pair('>', Tok::Arrow, Tok::Minus); break;
-            case '=': pair('=', Tok::Equal, Tok::Assign); break;
-            case '!': pair('=', Tok::NotEqual, Tok::Bang); break;
-            case '<': pair('=', Tok::LessEqual, Tok::Less); break;
-            case '>': pair('=', Tok::GreaterEqual, Tok::Greater); break;
-            case '&':
-                if (i + 1 >= s.size() || s[i + 1] != '&') { syntax(i, "single '&' is unsupported; use '&&'"); }
-                push(Tok::And, i);
-                i += 2;
-                break;
-            case '|':
-                if (i + 1 >= s.size() || s[i + 1] != '|') { syntax(i, "single '|' is unsupported; use '||'"); }
-                push(Tok::Or, i);
-                i += 2;
-                break;
-            default:
-                syntax(i, "unsupported character");
         }
+        add(std::move(t));
     }
-    push(Tok::End, s.size());
-    return out;
+    Token end;
+    end.offset = in.offset();
+    add(std::move(end));
+    return tokens;
 }
 
-// ------------------------------------------------------------------ parser
+// --------------------------------------------------------------- parsing
+//
+// Precedence climbing over a binding-power table.  Binary operators bind
+// tighter the higher their power and associate to the left; the conditional
+// a ? b : c binds loosest and associates to the right; prefix + - ! apply to
+// an operand, which is a primary value followed by any ->method(...) calls.
+// Operands are emitted before the instruction that uses them, so every value
+// is an SSA index into the instruction list; locals alias earlier values.
 
-// Recursive descent, lowest precedence first: ?: (right associative), ||,
-// &&, == !=, < <= > >=, + -, * /, prefix + - !, postfix ->method(...).
-// Every value is an SSA instruction index; locals alias earlier values.
-class Parser {
+struct Binary {
+    Tok token;
+    int power;
+    ExprOp op;
+};
+constexpr Binary kBinary[] = {
+    {Tok::Or, 1, kOpLogicalOr},        {Tok::And, 2, kOpLogicalAnd},
+    {Tok::Equal, 3, kOpEqual},          {Tok::NotEqual, 3, kOpNotEqual},
+    {Tok::Less, 4, kOpLess},            {Tok::LessEqual, 4, kOpLessEqual},
+    {Tok::Greater, 4, kOpGreater},      {Tok::GreaterEqual, 4, kOpGreaterEqual},
+    {Tok::Plus, 5, kOpAdd},             {Tok::Minus, 5, kOpSubtract},
+    {Tok::Star, 6, kOpMultiply},        {Tok::Slash, 6, kOpDivide},
+};
+
+const Binary *binary_of(Tok t) {
+    for (const Binary &b : kBinary) {
+        if (b.token == t) { return &b; }
+    }
+    return nullptr;
+}
+
+// Intrinsics by name: the op and the argument count (-1: any count from 1).
+struct Intrinsic {
+    const char *name;
+    ExprOp op;
+    int arity;
+};
+constexpr Intrinsic kIntrinsics[] = {
+    {"hash", kOpHash, -1},    {"min", kOpMinimum, 2},      {"max", kOpMaximum, 2},
+    {"clamp", kOpClamp, 3},   {"fit", kOpFit, 5},          {"gamma", kOpGamma, 2},
+    {"contrast", kOpContrast, 2}, {"smoothstep", kOpSmoothstep, 3},
+};
+
+class Compiler {
 public:
-    Parser(std::vector<Token> tokens, const std::string &name, const std::string &type)
+    Compiler(std::vector<Token> tokens, const std::string &name, const std::string &type)
         : tokens_(std::move(tokens)) {
         program_.expression_seed = string_seed(name + type);
     }
 
-    Program run() {
+    // statements := statement (';' statement)*, where a statement is
+    // `name = value` (with or without '$') or a value; the last statement's
+    // value is the result.
+    Program compile() {
         bool any = false;
-        while (peek().kind != Tok::End) {
-            while (accept(Tok::Semicolon)) {}
-            if (peek().kind == Tok::End) { break; }
-            if ((peek().kind == Tok::Variable || peek().kind == Tok::Identifier) && peek(1).kind == Tok::Assign) {
-                const Token target = take();
-                take();
-                const uint32_t value = expression();
-                if (locals_.find(target.text) == locals_.end() && locals_.size() >= kMaxLocals) {
+        for (;;) {
+            while (at(Tok::Semicolon)) { ++cursor_; }
+            if (at(Tok::End)) { break; }
+            const bool assignment = (at(Tok::Variable) || at(Tok::Identifier)) && ahead(1).kind == Tok::Assign;
+            std::string target;
+            if (assignment) {
+                target = ahead(0).text;
+                cursor_ += 2;
+            }
+            const uint32_t value = value_of(0);
+            if (assignment) {
+                if (!locals_.count(target) && locals_.size() >= kMaxLocals) {
                     fail("XGen scalar expression local limit exceeded");
                 }
-                locals_[target.text] = value;
-                program_.result = value;
-            } else {
-                program_.result = expression();
+                locals_[target] = value;
             }
+            program_.result = value;
             any = true;
-            if (peek().kind != Tok::Semicolon && peek().kind != Tok::End) {
-                syntax(peek().offset, "expected ';' after expression");
-            }
+            if (!at(Tok::Semicolon) && !at(Tok::End)) { syntax(ahead(0).offset, "expected ';' after expression"); }
         }
         if (!any) { syntax(0, "expression is empty"); }
         return std::move(program_);
     }
 
 private:
-    const Token &peek(size_t ahead = 0) const {
-        const size_t at = cursor_ + ahead;
-        return tokens_[at < tokens_.size() ? at : tokens_.size() - 1];
-    }
-    Token take() { return tokens_[cursor_++]; }
-    bool accept(Tok kind) {
-        if (peek().kind != kind) { return false; }
+    const Token &ahead(size_t k) const { return tokens_[std::min(cursor_ + k, tokens_.size() - 1)]; }
+    bool at(Tok t) const { return ahead(0).kind == t; }
+    bool eat(Tok t) {
+        if (!at(t)) { return false; }
         ++cursor_;
         return true;
     }
-    void expect(Tok kind, const char *what) {
-        if (!accept(kind)) { syntax(peek().offset, what); }
+    void need(Tok t, const char *message) {
+        if (!eat(t)) { syntax(ahead(0).offset, message); }
     }
 
-    uint32_t emit(ExprOp op, const std::vector<uint32_t> &args = {}, double immediate = 0.0, uint32_t aux = 0) {
+    uint32_t emit(ExprOp op, const std::vector<uint32_t> &operands = {}, double immediate = 0.0,
+                  uint32_t auxiliary = 0) {
         if (program_.instructions.size() >= kMaxInstructions) {
             fail("XGen scalar expression instruction limit exceeded");
         }
-        if (args.size() > std::numeric_limits<uint16_t>::max()) {
+        if (operands.size() > std::numeric_limits<uint16_t>::max()) {
             fail("XGen scalar expression operand limit exceeded");
         }
-        const size_t offset = program_.operands.size();
-        if (offset > std::numeric_limits<uint32_t>::max()) {
-            fail("XGen scalar expression operand storage exceeded");
-        }
-        program_.operands.insert(program_.operands.end(), args.begin(), args.end());
-        program_.instructions.push_back(Instruction{static_cast<uint8_t>(op), static_cast<uint32_t>(offset),
-                                                    static_cast<uint16_t>(args.size()), aux, immediate});
+        const size_t first = program_.operands.size();
+        if (first > std::numeric_limits<uint32_t>::max()) { fail("XGen scalar expression operand storage exceeded"); }
+        program_.operands.insert(program_.operands.end(), operands.begin(), operands.end());
+        program_.instructions.push_back(Instruction{static_cast<uint8_t>(op), static_cast<uint32_t>(first),
+                                                    static_cast<uint16_t>(operands.size()), auxiliary, immediate});
         return static_cast<uint32_t>(program_.instructions.size() - 1);
     }
 
-    uint32_t expression() { return conditional(); }
-
-    uint32_t conditional() {
-        const uint32_t test = either();
-        if (!accept(Tok::Question)) { return test; }
-        const uint32_t yes = expression();
-        expect(Tok::Colon, "expected ':' in conditional expression");
-        const uint32_t no = conditional();
-        return emit(kOpSelect, {test, yes, no});
-    }
-
-    uint32_t either() {
-        uint32_t v = both();
-        while (accept(Tok::Or)) { v = emit(kOpLogicalOr, {v, both()}); }
-        return v;
-    }
-
-    uint32_t both() {
-        uint32_t v = equality();
-        while (accept(Tok::And)) { v = emit(kOpLogicalAnd, {v, equality()}); }
-        return v;
-    }
-
-    uint32_t equality() {
-        uint32_t v = relation();
+    // A value whose binary operators all bind tighter than `floor`; at floor
+    // 0 a trailing conditional is taken as well.
+    uint32_t value_of(int floor) {
+        uint32_t left = operand();
         for (;;) {
-            if (accept(Tok::Equal)) {
-                v = emit(kOpEqual, {v, relation()});
-            } else if (accept(Tok::NotEqual)) {
-                v = emit(kOpNotEqual, {v, relation()});
-            } else {
-                return v;
+            if (floor == 0 && eat(Tok::Question)) {
+                const uint32_t yes = value_of(0);
+                need(Tok::Colon, "expected ':' in conditional expression");
+                const uint32_t no = value_of(0);
+                left = emit(kOpSelect, {left, yes, no});
+                continue;
             }
+            const Binary *b = binary_of(ahead(0).kind);
+            if (b == nullptr || b->power <= floor) { return left; }
+            ++cursor_;
+            const uint32_t right = value_of(b->power);
+            left = emit(b->op, {left, right});
         }
     }
 
-    uint32_t relation() {
-        uint32_t v = sum();
-        for (;;) {
-            ExprOp op;
-            if (accept(Tok::Less)) {
-                op = kOpLess;
-            } else if (accept(Tok::LessEqual)) {
-                op = kOpLessEqual;
-            } else if (accept(Tok::Greater)) {
-                op = kOpGreater;
-            } else if (accept(Tok::GreaterEqual)) {
-                op = kOpGreaterEqual;
-            } else {
-                return v;
-            }
-            v = emit(op, {v, sum()});
-        }
-    }
-
-    uint32_t sum() {
-        uint32_t v = product();
-        for (;;) {
-            if (accept(Tok::Plus)) {
-                v = emit(kOpAdd, {v, product()});
-            } else if (accept(Tok::Minus)) {
-                v = emit(kOpSubtract, {v, product()});
-            } else {
-                return v;
-            }
-        }
-    }
-
-    uint32_t product() {
-        uint32_t v = unary();
-        for (;;) {
-            if (accept(Tok::Star)) {
-                v = emit(kOpMultiply, {v, unary()});
-            } else if (accept(Tok::Slash)) {
-                v = emit(kOpDivide, {v, unary()});
-            } else {
-                return v;
-            }
-        }
-    }
-
-    uint32_t unary() {
-        if (accept(Tok::Plus)) { return unary(); }
-        if (accept(Tok::Minus)) { return emit(kOpNegate, {unary()}); }
-        if (accept(Tok::Bang)) { return emit(kOpLogicalNot, {unary()}); }
-        return methods();
-    }
-
-    uint32_t methods() {
+    // Prefix operators, then a primary value and its method calls.
+    uint32_t operand() {
+        if (eat(Tok::Plus)) { return operand(); }
+        if (eat(Tok::Minus)) { return emit(kOpNegate, {operand()}); }
+        if (eat(Tok::Bang)) { return emit(kOpLogicalNot, {operand()}); }
         uint32_t v = primary();
-        while (accept(Tok::Arrow)) {
-            if (peek().kind != Tok::Identifier) { syntax(peek().offset, "expected a method name after '->'"); }
-            const Token name = take();
-            expect(Tok::LParen, "expected '(' after expression method name");
-            std::vector<uint32_t> args{v};
-            if (!accept(Tok::RParen)) {
-                do {
-                    args.push_back(expression());
-                } while (accept(Tok::Comma));
-                expect(Tok::RParen, "expected ')' after expression method arguments");
-            }
-            v = call(name, args);
+        while (eat(Tok::Arrow)) {
+            if (!at(Tok::Identifier)) { syntax(ahead(0).offset, "expected a method name after '->'"); }
+            const Token name = tokens_[cursor_++];
+            need(Tok::LParen, "expected '(' after expression method name");
+            std::vector<uint32_t> arguments{v};
+            arguments_until_paren(arguments, "expected ')' after expression method arguments");
+            v = intrinsic(name, arguments);
         }
         return v;
     }
 
-    double ramp_number(const char *what) {
-        double sign = 1.0;
-        if (!accept(Tok::Plus) && accept(Tok::Minus)) { sign = -1.0; }
-        if (peek().kind != Tok::Number) { syntax(peek().offset, std::string("expected a numeric ramp ") + what); }
-        return sign * take().number;
-    }
-
-    // rampUI(position, value, interpolation : position, value, interpolation ...)
-    uint32_t ramp(const Token &name) {
-        const size_t first = program_.ramp_points.size();
-        for (;;) {
-            const double position = ramp_number("position");
-            expect(Tok::Comma, "expected ',' after ramp position");
-            const double value = ramp_number("value");
-            expect(Tok::Comma, "expected ',' after ramp value");
-            const double interpolation = ramp_number("interpolation");
-            if (interpolation != std::floor(interpolation) || interpolation < 0.0 || interpolation > 3.0) {
-                syntax(name.offset, "ramp interpolation must be an integer in [0, 3]");
-            }
-            if (position < 0.0 || position > 1.0) { syntax(name.offset, "ramp positions must be in [0, 1]"); }
-            if (program_.ramp_points.size() >= kMaxRampPoints) {
-                fail("XGen scalar expression ramp point limit exceeded");
-            }
-            if (program_.ramp_points.size() != first && position <= program_.ramp_points.back().position) {
-                syntax(name.offset, "ramp positions must be strictly increasing");
-            }
-            program_.ramp_points.push_back(RampPoint{position, value, static_cast<uint8_t>(interpolation)});
-            if (!accept(Tok::Colon)) { break; }
-        }
-        expect(Tok::RParen, "expected ')' after rampUI points");
-        const size_t count = program_.ramp_points.size() - first;
-        if (count == 0 || count > std::numeric_limits<uint16_t>::max() ||
-            first > std::numeric_limits<uint32_t>::max()) {
-            syntax(name.offset, "ramp point storage limit exceeded");
-        }
-        const uint32_t index = static_cast<uint32_t>(program_.ramps.size());
-        program_.ramps.push_back(ExprRamp{static_cast<uint32_t>(first), static_cast<uint32_t>(count)});
-        return emit(kOpRamp, {}, 0.0, index);
+    // Comma-separated values up to ')', appended to `out` (the '(' is taken).
+    void arguments_until_paren(std::vector<uint32_t> &out, const char *unclosed) {
+        if (eat(Tok::RParen)) { return; }
+        do {
+            out.push_back(value_of(0));
+        } while (eat(Tok::Comma));
+        need(Tok::RParen, unclosed);
     }
 
     uint32_t primary() {
-        if (peek().kind == Tok::Number) { return emit(kOpConstant, {}, take().number); }
-        if (peek().kind == Tok::Variable) {
-            const Token v = take();
-            const auto local = locals_.find(v.text);
-            if (local != locals_.end()) { return local->second; }
-            uint32_t index = 0;
-            while (index < program_.inputs.size() && program_.inputs[index] != v.text) { ++index; }
-            if (index == program_.inputs.size()) { program_.inputs.push_back(v.text); }
-            return emit(kOpInput, {}, 0.0, index);
+        const Token &t = ahead(0);
+        switch (t.kind) {
+            case Tok::Number:
+                ++cursor_;
+                return emit(kOpConstant, {}, t.number);
+            case Tok::Variable: {
+                ++cursor_;
+                const auto local = locals_.find(t.text);
+                if (local != locals_.end()) { return local->second; }
+                const auto known = std::find(program_.inputs.begin(), program_.inputs.end(), t.text);
+                const uint32_t index = static_cast<uint32_t>(known - program_.inputs.begin());
+                if (known == program_.inputs.end()) { program_.inputs.push_back(t.text); }
+                return emit(kOpInput, {}, 0.0, index);
+            }
+            case Tok::LParen: {
+                ++cursor_;
+                const uint32_t v = value_of(0);
+                need(Tok::RParen, "expected ')'");
+                return v;
+            }
+            case Tok::String:
+                syntax(t.offset, "string values require an explicit PTEX binding such as map()");
+            case Tok::Identifier:
+                break;
+            default:
+                syntax(t.offset, "expected a scalar value");
         }
-        if (accept(Tok::LParen)) {
-            const uint32_t v = expression();
-            expect(Tok::RParen, "expected ')'");
-            return v;
-        }
-        if (peek().kind == Tok::String) {
-            syntax(peek().offset, "string values require an explicit PTEX binding such as map()");
-        }
-        if (peek().kind != Tok::Identifier) { syntax(peek().offset, "expected a scalar value"); }
-        const Token name = take();
-        if (name.text == "true") { return emit(kOpConstant, {}, 1.0); }
-        if (name.text == "false") { return emit(kOpConstant, {}, 0.0); }
-        if (!accept(Tok::LParen)) {
+        const Token name = tokens_[cursor_++];
+        if (name.text == "true" || name.text == "false") { return emit(kOpConstant, {}, name.text == "true"); }
+        if (!eat(Tok::LParen)) {
             const auto local = locals_.find(name.text);
-            if (local != locals_.end()) { return local->second; }
-            syntax(name.offset, "bare identifier is unsupported: " + name.text);
+            if (local == locals_.end()) { syntax(name.offset, "bare identifier is unsupported: " + name.text); }
+            return local->second;
         }
-        if (name.text == "rampUI") { return ramp(name); }
-        std::vector<uint32_t> args;
-        if (!accept(Tok::RParen)) {
-            do {
-                args.push_back(expression());
-            } while (accept(Tok::Comma));
-            expect(Tok::RParen, "expected ')' after function arguments");
-        }
-        return call(name, args);
+        if (name.text == "rampUI") { return ramp(name.offset); }
+        std::vector<uint32_t> arguments;
+        arguments_until_paren(arguments, "expected ')' after function arguments");
+        return intrinsic(name, arguments);
     }
 
-    uint32_t call(const Token &name, const std::vector<uint32_t> &args) {
-        const auto arity = [&](size_t n) {
-            if (args.size() != n) {
-                syntax(name.offset, name.text + " expects " + std::to_string(n) + " argument(s)");
-            }
-        };
+    uint32_t intrinsic(const Token &name, const std::vector<uint32_t> &arguments) {
         const std::string &f = name.text;
-        if (f == "hash") {
-            if (args.empty()) { syntax(name.offset, "hash expects at least one argument"); }
-            return emit(kOpHash, args);
-        }
         if (f == "rand") {
-            if (args.size() > 3) { syntax(name.offset, "rand expects zero to three arguments"); }
+            if (arguments.size() > 3) { syntax(name.offset, "rand expects zero to three arguments"); }
             // Each call site draws its own seed from (expression seed, call number).
             const double site[2] = {static_cast<double>(program_.expression_seed),
-                                    static_cast<double>(program_.random_call_count)};
-            const double seed = seexpr_hash(site, 2);
-            ++program_.random_call_count;
-            return emit(kOpRandom, args, seed);
+                                    static_cast<double>(program_.random_call_count++)};
+            return emit(kOpRandom, arguments, seexpr_hash(site, 2));
         }
-        if (f == "min") { arity(2); return emit(kOpMinimum, args); }
-        if (f == "max") { arity(2); return emit(kOpMaximum, args); }
-        if (f == "clamp") { arity(3); return emit(kOpClamp, args); }
-        if (f == "fit") { arity(5); return emit(kOpFit, args); }
-        if (f == "gamma") { arity(2); return emit(kOpGamma, args); }
-        if (f == "contrast") { arity(2); return emit(kOpContrast, args); }
-        if (f == "smoothstep") { arity(3); return emit(kOpSmoothstep, args); }
         if (f == "map") {
             syntax(name.offset, "map requires an explicit PTEX binding and is not a scalar intrinsic");
         }
+        for (const Intrinsic &in : kIntrinsics) {
+            if (f != in.name) { continue; }
+            if (in.arity < 0 && arguments.empty()) { syntax(name.offset, f + " expects at least one argument"); }
+            if (in.arity >= 0 && arguments.size() != static_cast<size_t>(in.arity)) {
+                syntax(name.offset, f + " expects " + std::to_string(in.arity) + " argument(s)");
+            }
+            return emit(in.op, arguments);
+        }
         syntax(name.offset, "unsupported function: " + f);
+    }
+
+    // One signed numeric field of a rampUI point.
+    double ramp_field(const char *what) {
+        const double sign = eat(Tok::Plus) ? 1.0 : (eat(Tok::Minus) ? -1.0 : 1.0);
+        if (!at(Tok::Number)) { syntax(ahead(0).offset, std::string("expected a numeric ramp ") + what); }
+        return sign * tokens_[cursor_++].number;
+    }
+
+    // rampUI(position, value, interpolation : ...) after its '('.  Points are
+    // checked as they are read; errors point at the rampUI name.
+    uint32_t ramp(size_t where) {
+        const size_t first = program_.ramp_points.size();
+        do {
+            RampPoint point{};
+            point.position = ramp_field("position");
+            need(Tok::Comma, "expected ',' after ramp position");
+            point.value = ramp_field("value");
+            need(Tok::Comma, "expected ',' after ramp value");
+            const double kind = ramp_field("interpolation");
+            if (kind < 0.0 || kind > 3.0 || kind != std::floor(kind)) {
+                syntax(where, "ramp interpolation must be an integer in [0, 3]");
+            }
+            if (!(point.position >= 0.0 && point.position <= 1.0)) {
+                syntax(where, "ramp positions must be in [0, 1]");
+            }
+            if (program_.ramp_points.size() >= kMaxRampPoints) { fail("XGen scalar expression ramp point limit exceeded"); }
+            if (program_.ramp_points.size() > first && !(point.position > program_.ramp_points.back().position)) {
+                syntax(where, "ramp positions must be strictly increasing");
+            }
+            point.interpolation = static_cast<uint8_t>(kind);
+            program_.ramp_points.push_back(point);
+        } while (eat(Tok::Colon));
+        need(Tok::RParen, "expected ')' after rampUI points");
+        const size_t count = program_.ramp_points.size() - first;
+        if (count == 0 || count > std::numeric_limits<uint16_t>::max() ||
+            first > std::numeric_limits<uint32_t>::max()) {
+            syntax(where, "ramp point storage limit exceeded");
+        }
+        program_.ramps.push_back(ExprRamp{static_cast<uint32_t>(first), static_cast<uint32_t>(count)});
+        return emit(kOpRamp, {}, 0.0, static_cast<uint32_t>(program_.ramps.size() - 1));
     }
 
     std::vector<Token> tokens_;
@@ -905,9 +928,9 @@ uint32_t nxg_expression_compile(const char *source, const char *expression_name,
         if ((flags & NXG_EXPRESSION_CLASSIC) != 0u) {
             text = nxg::classic_rewrite(nxg::classic_strip(text), frequencies);
         }
-        nxg::Parser parser(nxg::lex(nxg::normalise(text)), expression_name ? expression_name : "",
-                           object_type ? object_type : "");
-        const nxg::Program program = parser.run();
+        nxg::Compiler compiler(nxg::scan(text), expression_name ? expression_name : "",
+                               object_type ? object_type : "");
+        const nxg::Program program = compiler.compile();
         auto *handle = new (std::nothrow) nxg_expression;
         if (handle == nullptr) { return NXG_ERROR_INVALID_ARGUMENT; }
         static_cast<Expression &>(*handle) = nxg::to_float_program(program, std::move(frequencies));

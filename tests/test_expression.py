@@ -22,6 +22,11 @@ PROGRAMS = [
     "contrast($u, 0.3)", "min($u,$v)==max($u,$v)", "1e3 + .5 + 0x10", "$a=2;\n(\n$a\n+\n1)",
     "1 <= 2 >= 0 != 1 < 3 > 2", "$u / $v * $id - $cLength", "2 *\n 3\n - 1", "1\n2", "#only a comment\n5",
     "3 \\n 4", "a = 1\nb = 2\na + b",
+    # the source rewriting: CR/LF, blank lines, tabs, comments next to operators,
+    # escapes inside literals and strings, a comment at the very end
+    "1 +\r\n2", "1\r\n\r\n+ 2", "1\t\n\t* 3", "(\n1\n)\n", "1 # a\n# b\n+ 2",
+    "$a = 1 #\n$a", "1\f+\v2", "1.e2 + 2.5E-1 + 0x1p3", "2\\n\\n* 3", "4 # tail",
+    "-\n1", "!\n0", "$u\n->clamp(0,1)", "min(\n1,\n2\n)", "1 ?\n2 :\n3", "x = 2 ; ; x",
 ]
 
 ERRORS = [
@@ -29,6 +34,10 @@ ERRORS = [
     "rampUI(0,0,1.5)", "clamp(1,2)", "min(1)", "fit(1,2,3,4)", "(1", "1 2", "1e999", "a", "rand(1,2,3,4)",
     "hash()", "@", "rampUI(0.5,0,1:0.2,0,1)", "$u->(1)", "$u->clamp 1", "$u->clamp(0,1", "rampUI(2,0,1)",
     "rampUI(x)", "rampUI(0 0 1)", "rampUI(0,0,1", "1 ? 2", "$1", "noise($Prefg*6)", "max(1,2,3)",
+    # offsets counted in the rewritten text (after comments, escapes, joined lines)
+    "1 # c\n @", "a\\n@", "'x#y'", "\"a\\\"b\"", "1 +\n\n @", "2 \\n\\n \\n ~", "(1\n", "1\r\n2 3",
+    "'a\\nb'", "caf\xe9", "rampUI(0,0,1 : 1,1)", "rampUI(-0.5,0,1)", "$u->", "1 ==", "x = ", "hash(1,)",
+    "2 *# c\n3", "1e\\n5",
 ]
 
 CLASSIC = [
@@ -96,3 +105,49 @@ def test_expression_info_and_inputs(nxg_lib):
     assert e.inputs == ["__nxg_pref_noise_0", "v"]
     assert info.pref_noise_count == 1 and info.pref_noise_frequencies[0] == 6.0
     assert info.instruction_count == 14 and info.result == 13
+
+
+def _random_source(rng) -> str:
+    """A random expression over the whole grammar, with random blanks, line
+    breaks, comments and escapes between tokens (some inputs are invalid on
+    purpose)."""
+    atoms = ["1", "2.5", ".5", "3e2", "0x10", "$u", "$v", "$id", "$a", "a", "true", "false", "'s'",
+             "rand()", "rand(1, 2)", "hash($id, 3)", "min($u, 0.3)", "fit($v, 0, 1, 2, 3)",
+             "rampUI(0, 0, 1 : 1, 1, 2)", "clamp($u, 0, 1)", "$u->gamma(2)"]
+    binary = ["+", "-", "*", "/", "<", "<=", ">", ">=", "==", "!=", "&&", "||"]
+    gaps = [" ", "", "  ", "\t", "\n", "\\n", " # note\n", "\r\n", "\n\n"]
+
+    def value(depth):
+        r = rng.random()
+        if depth > 3 or r < 0.3:
+            return str(rng.choice(atoms))
+        if r < 0.6:
+            return value(depth + 1) + rng.choice(gaps) + str(rng.choice(binary)) + rng.choice(gaps) + value(depth + 1)
+        if r < 0.7:
+            return str(rng.choice(["-", "!", "+"])) + value(depth + 1)
+        if r < 0.8:
+            return "(" + rng.choice(gaps) + value(depth + 1) + rng.choice(gaps) + ")"
+        return value(depth + 1) + " ?" + rng.choice(gaps) + value(depth + 1) + " :" + rng.choice(gaps) + value(depth + 1)
+
+    statements = []
+    if rng.random() < 0.5:
+        statements.append("$a = " + value(1))
+    statements.append(value(0))
+    return str(rng.choice([";", "\n", "; "])).join(statements)
+
+
+def test_random_sources_match_reference(nxg_lib, reference):
+    """400 seeded random sources: the same program or the same error text."""
+    rng = np.random.default_rng(20261204)
+    compiled = 0
+    for _ in range(400):
+        source = _random_source(rng)
+        theirs, message = reference.compile_expression(source, "width", "SplinePrimitive")
+        if theirs is None:
+            with pytest.raises(ExpressionError) as err:
+                Expression(source, "width", "SplinePrimitive")
+            assert str(err.value) == message, source
+        else:
+            assert Expression(source, "width", "SplinePrimitive").describe() == theirs.describe(), source
+            compiled += 1
+    assert 100 < compiled < 400, compiled
