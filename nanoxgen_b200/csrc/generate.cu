@@ -103,9 +103,13 @@ __global__ void generate_kernel(LaunchArgs g, const float4 *offsets) {
 // range_end); each warp takes 32 strands at a time through setup (which also
 // writes the roots, root UVs and point counts), base, frame (with noise) and
 // store.  Without noise the base step writes the output directly (no
-// stage), applying Classic scalars itself when given.
+// stage), applying Classic scalars itself when given.  Register budgets:
+// the noise variant runs one CTA of up to twelve warps per SM (its shared
+// memory allows no more); the plain one three CTAs of eight warps (at most 80
+// registers), the plain Classic one two.
 template <bool NOISE, bool CLASSIC>
-__global__ void __launch_bounds__(384, 1) generate_walk_kernel(LaunchArgs g, const float4 *offsets) {
+__global__ void __launch_bounds__(NOISE ? 384 : 256, NOISE ? 1 : (CLASSIC ? 2 : 3))
+    generate_walk_kernel(LaunchArgs g, const float4 *offsets) {
     constexpr bool kStaged = NOISE;
     constexpr bool kWalk = NOISE;  // noise walk inside this kernel
     extern __shared__ float4 smem[];

@@ -146,13 +146,12 @@ __device__ __forceinline__ Root walk_root(const AssetArgs &a, const FrameArgs &f
 // The blend weights of generate.h:226-241 in the reference's rounding: every
 // value IEEE-rounded and uncontracted.  Rewrites the weights of the strand's
 // blended slots (records in slot order, as the setup step staged them) and
-// returns their sum in slot order.  The setup step's weights use fast
-// arithmetic; it calls this only for strands where those may be inaccurate
-// (a slot near the edge of its support radius) or where the sum may lie on
+// returns their sum in slot order.  For powers other than 2 the setup step
+// takes the fast power; it calls this only for strands whose sum may lie on
 // the other side of the 1e-12 threshold that chooses between blending and the
-// nearest-guide fallback (generate.h:261), so both the blend and that choice
-// are the reference's (for powers other than 2, to the last-bit agreement of
-// CUDA's powf with the host's).  Not inlined: the hot path rarely takes it.
+// nearest-guide fallback (generate.h:261), so that choice is the reference's
+// (to the last-bit agreement of CUDA's powf with the host's).  Not inlined:
+// the hot path rarely takes it.
 static __device__ __noinline__ float walk_exact_weights(const LaunchArgs &g, uint32_t triangle, F3 position,
                                                         F3 normal, float *slot_words, int lane) {
     const AssetArgs &a = g.a;
@@ -179,18 +178,11 @@ static __device__ __noinline__ float walk_exact_weights(const LaunchArgs &g, uin
     return wsum;
 }
 
-// Whether the setup step must take exact weights.  A fast base
-// x = 1 - sqrt(d2) / r is within 4e-7 (absolute) of the IEEE one, so a weight
-// x^p is off by at most a relative p * 4e-7 / x from it (`edge` = the sum of
-// w * p * 4e-7 / x over the slots), plus the fast power's own error, below
-// p * 4e-7 + 1e-5 relative for __powf (one rounding for the square).  Exact
-// weights are taken when the first part exceeds 1e-5 of the sum (the blend
-// itself could move by that fraction of an offset), when a base was clamped
-// (`clamped`), or when twice the whole bound reaches across 1e-12.
-__device__ __forceinline__ bool walk_needs_exact_weights(float wsum, float edge, bool clamped, bool square,
-                                                         float power) {
-    const float bound = edge + (square ? 1.2e-7f : power * 4.0e-7f + 1.0e-5f) * wsum;
-    return clamped || edge > 1.0e-5f * wsum || fabsf(wsum - 1.0e-12f) <= 2.0f * bound;
+// Whether a weight sum from the fast power (__powf, within p * 4e-7 + 1e-5
+// relative of powf for exact bases) may lie on the other side of the 1e-12
+// blend threshold from the reference's; twice that bound is used.
+__device__ __forceinline__ bool walk_blend_uncertain(float wsum, float power) {
+    return fabsf(wsum - 1.0e-12f) <= 2.0f * (power * 4.0e-7f + 1.0e-5f) * wsum;
 }
 
 // The lane walk's own per-strand decisions, for inspection
@@ -276,8 +268,6 @@ __device__ __forceinline__ WalkRoot walk_setup(const LaunchArgs &g, float4 *reco
     // slots count stay in the reference's exact rounding.
     const bool square = p.weight_power == 2.0f;
     float wsum = 0.0f;
-    float edge = 0.0f;      // sum of w * p * 4e-7 / x (walk_needs_exact_weights)
-    bool clamped = false;
     float nearest_d2 = FLT_MAX;
     uint32_t nearest = kInvalid;
     uint32_t blended = 0u;
@@ -294,20 +284,20 @@ __device__ __forceinline__ WalkRoot walk_setup(const LaunchArgs &g, float4 *reco
         }
         const float radius = gr[j].w;
         if (radius <= 0.0f || d2 >= __fmul_rn(radius, radius)) { continue; }
-        // Clamped positive: a fast quotient can round to 1 or above at the
-        // radius, and __powf of zero or a negative base is not a weight.
-        const float raw = 1.0f - __fdividef(sqrt_approx(d2), radius);
-        const float x = fmaxf(raw, 1.0e-30f);
-        clamped = clamped || !(raw > 1.0e-30f);
-        const float w = square ? x * x : __powf(x, p.weight_power);
-        edge += __fdividef(w, x) * (p.weight_power * 4.0e-7f);
+        // The base 1 - sqrt(d2) / r in the reference's rounding: near the
+        // edge of the support radius it cancels, and a fast quotient would
+        // change the weight there by a large fraction.  The square is then
+        // the reference's weight bit for bit; other powers take __powf.
+        const float x = __fsub_rn(1.0f, __fdiv_rn(__fsqrt_rn(d2), radius));
+        const float w = square ? __fmul_rn(x, x)
+                               : (x > 0.0f ? __powf(x, p.weight_power) : (p.weight_power > 0.0f ? 0.0f : 1.0f));
         float *dst = slot_words + ((blended >> 1) * 32u + lane) * 4u + (blended & 1u) * 2u;
         dst[0] = __uint_as_float(stencil[j] * P);
         dst[1] = w;
         ++blended;
         wsum = __fadd_rn(wsum, w);
     }
-    if (blended != 0u && walk_needs_exact_weights(wsum, edge, clamped, square, p.weight_power)) {
+    if (!square && blended != 0u && walk_blend_uncertain(wsum, p.weight_power)) {
         wsum = walk_exact_weights(g, root.triangle, root.position, root.normal, slot_words, lane);
     }
     float inv = 0.0f;
