@@ -360,7 +360,8 @@ uint32_t nxg_validate_motion_request(const nxg_device_asset_desc *asset,
 /* Bytes of device workspace nxg_generate_packed needs for `strand_count`
  * strands of this asset at params->cvs_per_strand CVs: the strand-locality
  * sort (keys, permutation, per-guide bins) and the per-frame guide-offset
- * table (guide_count x cvs_per_strand float4).  The workspace must be
+ * table (guide_count x cvs_per_strand float4, then 2 guide records per guide
+ * and 32 zero entries).  The workspace must be
  * 256-byte aligned; its contents need no initialisation. */
 uint64_t nxg_packed_workspace_size(const nxg_device_asset_desc *asset, const nxg_generation_params *params,
                                    uint32_t strand_count);

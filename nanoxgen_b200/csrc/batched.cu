@@ -172,10 +172,13 @@ __global__ void batched_offsets_kernel(const __grid_constant__ BatchArgs b) {
             const_cast<float4 *>(d.offsets)[local] = guide_offset_entry(d.g.a, d.g.f, P,
                                                                         static_cast<uint32_t>(local / P),
                                                                         static_cast<uint32_t>(local % P));
-        } else {
+        } else if (local < table + d.g.a.guide_count) {
             const uint64_t gi = local - table;
             guide_frame_entry(d.g.a, d.g.f, d.g.p.support_scale, static_cast<uint32_t>(gi),
                               const_cast<float4 *>(d.offsets) + table + 2u * gi);
+        } else {  // the zero row after the frame records
+            const_cast<float4 *>(d.offsets)[d.g.zero_row + (local - table - d.g.a.guide_count)] =
+                make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         }
     }
 }
@@ -298,14 +301,9 @@ __device__ __noinline__ void batched_noise_walk_item(const BatchDesc &d, uint32_
     const bool valid = item < end;
     const int in_batch = static_cast<int>(end - batch);
     const float inv_p = 1.0f / static_cast<float>(P);
-    uint32_t *root_words = reinterpret_cast<uint32_t *>(stage);  // free until the base step
-    const WalkRoot wr = walk_setup<true>(d.g, records, locals, root_words, lane, valid ? item : batch, valid,
+    const WalkRoot wr = walk_setup<true>(d.g, records, locals, lane, valid ? item : batch, valid,
                                          static_cast<uint32_t>(P));
     __syncwarp();
-    if (d.g.roots) {
-        walk_store_roots(d.g, root_words, locals, lane, in_batch);
-        __syncwarp();
-    }
     walk_base<false>(d.g, records, stage, locals, tvals, rvals, d.offsets, lane, in_batch, P, inv_p);
     __syncwarp();
     walk_frame(d.g.p, wr, lane < in_batch, stage + lane * kWalkRowFloats, lattice + lane, tvals, table, P);
@@ -333,20 +331,14 @@ __device__ __noinline__ void batched_walk_item(const BatchDesc &d, uint32_t batc
     const uint32_t item = batch + static_cast<uint32_t>(lane);
     const bool valid = item < end;
     const int in_batch = static_cast<int>(end - batch);
-    const float inv_p = 1.0f / static_cast<float>(P);
-    uint32_t *root_words = reinterpret_cast<uint32_t *>(scratch);  // free until the Classic setup
-    walk_setup<false>(d.g, records, locals, root_words, lane, valid ? item : batch, valid, static_cast<uint32_t>(P));
+    walk_setup<false>(d.g, records, locals, lane, valid ? item : batch, valid, static_cast<uint32_t>(P));
     __syncwarp();
-    if (d.g.roots) {
-        walk_store_roots(d.g, root_words, locals, lane, in_batch);
-        __syncwarp();
-    }
     if (CLASSIC && d.g.scalars != nullptr) {
         walk_classic_setup(d.g, records, lane, valid, locals[lane] & 0x7fffffffu, tvals, d.offsets, scratch, P);
         __syncwarp();
-        walk_base<true, true>(d.g, records, nullptr, locals, tvals, rvals, d.offsets, lane, in_batch, P, inv_p);
+        walk_base_direct<true>(d.g, records, locals, tvals, rvals, d.offsets, lane, in_batch, P);
     } else {
-        walk_base<true, false>(d.g, records, nullptr, locals, tvals, rvals, d.offsets, lane, in_batch, P, inv_p);
+        walk_base_direct<false>(d.g, records, locals, tvals, rvals, d.offsets, lane, in_batch, P);
     }
     __syncwarp();
 }
@@ -475,7 +467,7 @@ BatchLayout batch_layout(const nxg_device_asset_desc *assets, const nxg_generati
         l.bins.push_back(at);
         at += up((G + 1u) * 4u);
         l.offsets.push_back(at);
-        at += up(G * (P + 2u) * 16u);  // offset table, then 2 guide frame records per guide
+        at += up((G * (P + 2u) + dev::kWalkMaxCvs) * 16u);  // offset table, 2 guide frame records per guide, zero row
     }
     l.total = at;
     return l;
@@ -618,6 +610,7 @@ uint32_t generate_batched(const nxg_device_asset_desc *assets, const nxg_deforme
         }
         bd.offsets = reinterpret_cast<const float4 *>(w + layout.offsets[d]);
         bd.g.guide_frames = bd.offsets + uint64_t{assets[d].header.guide_count} * params[d].cvs_per_strand;
+        bd.g.zero_row = assets[d].header.guide_count * (params[d].cvs_per_strand + 2u);
         bd.keys = reinterpret_cast<uint32_t *>(w + layout.keys[d]);
         bd.bins = reinterpret_cast<uint32_t *>(w + layout.bins[d]);
         bd.noise = bd.g.p.noise;
@@ -627,7 +620,7 @@ uint32_t generate_batched(const nxg_device_asset_desc *assets, const nxg_deforme
         bd.offset_begin = offsets;
         strands += params[d].strand_count;
         items += (params[d].strand_count + 32u * warps_per_cta - 1u) / (32u * warps_per_cta);
-        offsets += uint64_t{assets[d].header.guide_count} * (params[d].cvs_per_strand + 1u);
+        offsets += uint64_t{assets[d].header.guide_count} * (params[d].cvs_per_strand + 1u) + dev::kWalkMaxCvs;
     }
     b.total_strands = strands;
     b.total_items = items;

@@ -138,7 +138,7 @@ __global__ void __launch_bounds__(NOISE ? 384 : 256, NOISE ? 1 : (CLASSIC ? 2 : 
     float *stage = reinterpret_cast<float *>(mine);  // staged variants only
     float4 *records = reinterpret_cast<float4 *>(kStaged ? mine + kWalkStageBytes : mine);
     float2 *lattice = reinterpret_cast<float2 *>(mine + kWalkStageBytes);
-    uint32_t *root_words = reinterpret_cast<uint32_t *>(kStaged ? mine : mine + kWalkRecordBytes);
+    float4 *scratch = reinterpret_cast<float4 *>(mine + kWalkRecordBytes);  // plain Classic variant only
     uint32_t *locals = reinterpret_cast<uint32_t *>(mine + kWarpBytes - kWalkLocalBytes);
     const float inv_p = 1.0f / static_cast<float>(P);
     const uint32_t span = g.range_end - g.range_begin;
@@ -150,20 +150,18 @@ __global__ void __launch_bounds__(NOISE ? 384 : 256, NOISE ? 1 : (CLASSIC ? 2 : 
         const uint32_t item = batch + static_cast<uint32_t>(lane);
         const bool valid = item < end;
         const int in_batch = static_cast<int>(min(32u, end - batch));
-        const WalkRoot wr = walk_setup<NOISE>(g, records, locals, root_words, lane, valid ? item : batch, valid,
+        const WalkRoot wr = walk_setup<NOISE>(g, records, locals, lane, valid ? item : batch, valid,
                                               static_cast<uint32_t>(P));
         __syncwarp();
-        if (g.roots) {
-            walk_store_roots(g, root_words, locals, lane, in_batch);
-            __syncwarp();
-        }
         if constexpr (CLASSIC && !NOISE) {
-            walk_classic_setup(g, records, lane, valid, locals[lane] & 0x7fffffffu, tvals, offsets,
-                               reinterpret_cast<float4 *>(root_words), P);
+            walk_classic_setup(g, records, lane, valid, locals[lane] & 0x7fffffffu, tvals, offsets, scratch, P);
             __syncwarp();
         }
-        walk_base<!kStaged, CLASSIC && !NOISE>(g, records, stage, locals, tvals, rvals, offsets, lane, in_batch, P,
-                                               inv_p);
+        if constexpr (kStaged) {
+            walk_base<false>(g, records, stage, locals, tvals, rvals, offsets, lane, in_batch, P, inv_p);
+        } else {
+            walk_base_direct<CLASSIC>(g, records, locals, tvals, rvals, offsets, lane, in_batch, P);
+        }
         __syncwarp();
         if constexpr (kWalk) {
             walk_frame(g.p, wr, lane < in_batch, stage + lane * kWalkRowFloats, lattice + lane, tvals, table, P);
@@ -229,9 +227,8 @@ __global__ void __launch_bounds__(64, 1) generate_pipe_kernel(LaunchArgs g, cons
             if (it >= 2u) { named_sync(3u + b); }
             const uint32_t item = batch + static_cast<uint32_t>(lane);
             const bool valid = item < end;
-            uint32_t *root_words = reinterpret_cast<uint32_t *>(stage);  // free until the base step
-            const WalkRoot wr = walk_setup<true>(g, records, locals, root_words, lane, valid ? item : batch,
-                                                 valid, static_cast<uint32_t>(P));
+            const WalkRoot wr = walk_setup<true>(g, records, locals, lane, valid ? item : batch, valid,
+                                                 static_cast<uint32_t>(P));
             fr[0 * 32 + lane] = wr.position.x;
             fr[1 * 32 + lane] = wr.position.y;
             fr[2 * 32 + lane] = wr.position.z;
@@ -245,10 +242,6 @@ __global__ void __launch_bounds__(64, 1) generate_pipe_kernel(LaunchArgs g, cons
             fr[10 * 32 + lane] = wr.domain.y;
             fr[11 * 32 + lane] = wr.domain.z;
             __syncwarp();
-            if (g.roots) {
-                walk_store_roots(g, root_words, locals, lane, in_batch);
-                __syncwarp();
-            }
             walk_base<false>(g, records, stage, locals, tvals, rvals, offsets, lane, in_batch, P, inv_p);
             named_arrive(1u + b);
         } else {
@@ -336,11 +329,15 @@ __global__ void strand_roots_kernel(LaunchArgs g) {
 }
 
 // The frame's guide-offset table (G x P float4) and, after it, the guide
-// frame records (2 float4 per guide) the lane-walk generator reads.
+// frame records (2 float4 per guide) the lane-walk generator reads, then the
+// zero row (kWalkMaxCvs zero entries) its unused stencil slots point at.
 __global__ void guide_offsets_kernel(AssetArgs a, FrameArgs f, uint32_t P, float support_scale, float4 *offsets) {
     const uint64_t n = static_cast<uint64_t>(a.guide_count) * P;
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
     const uint64_t first = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    for (uint64_t k = first; k < static_cast<uint64_t>(kWalkMaxCvs); k += stride) {
+        offsets[n + 2u * a.guide_count + k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
     for (uint64_t idx = first; idx < n; idx += stride) {
         offsets[idx] = guide_offset_entry(a, f, P, static_cast<uint32_t>(idx / P), static_cast<uint32_t>(idx % P));
     }
@@ -669,7 +666,7 @@ __global__ void __launch_bounds__(32) walk_states_kernel(LaunchArgs g, uint32_t 
     const uint32_t i = blockIdx.x * 32u + static_cast<uint32_t>(lane);
     const bool valid = i < count;
     WalkDecision d;
-    walk_setup<false>(g, records, locals, nullptr, lane, valid ? i : 0u, valid, g.p.cvs_per_strand, false, &d);
+    walk_setup<false>(g, records, locals, lane, valid ? i : 0u, valid, g.p.cvs_per_strand, false, &d);
     if (valid) { out[i] = d; }
 }
 
@@ -696,14 +693,15 @@ bool parallel_path(uint32_t guide_count, uint32_t P) {
 }
 
 // keys[count] | order[count] | bins[guides + 1] | offsets[guides * P] (float4)
-// followed by the guide frame records [guides * 2] (float4)
+// followed by the guide frame records [guides * 2] and the zero row
+// [kWalkMaxCvs] (float4)
 WorkspaceLayout workspace_layout(uint32_t guide_count, uint32_t count, uint32_t P) {
     WorkspaceLayout w{};
     w.keys = 0u;
     w.order = align_up(uint64_t{count} * 4u, kWorkspaceAlign);
     w.hist = w.order + align_up(uint64_t{count} * 4u, kWorkspaceAlign);
     w.offsets = w.hist + align_up((uint64_t{guide_count} + 1u) * 4u, kWorkspaceAlign);
-    w.offset_bytes = parallel_path(guide_count, P) ? uint64_t{guide_count} * (P + 2u) * 16u : 0u;
+    w.offset_bytes = parallel_path(guide_count, P) ? (uint64_t{guide_count} * (P + 2u) + dev::kWalkMaxCvs) * 16u : 0u;
     w.total = w.offsets + align_up(w.offset_bytes, kWorkspaceAlign);
     return w;
 }
@@ -984,6 +982,7 @@ uint32_t launch_generate(const nxg_device_asset_desc &asset, const nxg_deformed_
     }
     auto *offsets = reinterpret_cast<float4 *>(wbase + ws.offsets);
     g.guide_frames = offsets + uint64_t{asset.header.guide_count} * P;
+    g.zero_row = asset.header.guide_count * (P + 2u);
     {
         const uint64_t n = uint64_t{asset.header.guide_count} * P;
         const uint32_t threads = 256u;
@@ -1216,6 +1215,7 @@ uint32_t nxg_query_walk_states(const nxg_device_asset_desc *asset, const nxg_def
     g.count = 0xffffffffu;  // strand ids are global: every id is a valid order entry
     g.order = strands;
     g.guide_frames = offsets + uint64_t{asset->header.guide_count} * P;
+    g.zero_row = asset->header.guide_count * (P + 2u);
     nxg::set_last_cuda_error(0);
     const uint64_t n = uint64_t{asset->header.guide_count} * P;
     const uint32_t threads = 256u;

@@ -36,6 +36,7 @@ struct LaunchArgs {
     uint32_t *point_counts;
     const uint32_t *order;   // permutation of [0, count), or nullptr for identity
     const float4 *guide_frames;  // 2 per guide (guide_frame_entry), or nullptr
+    uint32_t zero_row;           // offset-table index of kWalkMaxCvs zero entries (unused lane-walk slots)
     const float2 *scalars;   // Classic per-root (length scale, width), or nullptr
     uint32_t classic_length; // scale each strand about its first point by scalars.x
     uint32_t classic_width;  // radius = 0.5 * max(scalars.y, 0) * radius_scale

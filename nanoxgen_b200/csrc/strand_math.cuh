@@ -169,10 +169,11 @@ __device__ __forceinline__ Root sample_root(const AssetArgs &a, const FrameArgs 
     const uint3 t = load_triangle(a, r.triangle);
     const F3 p0 = ld3(f.positions, t.x), p1 = ld3(f.positions, t.y), p2 = ld3(f.positions, t.z);
     r.position = xbary(p0, p1, p2, b0, r.b1, r.b2);
-    r.normal = xnormalize(xcross(xsub(p1, p0), xsub(p2, p0)));
-    if (a.flags & NXG_ASSET_HAS_NORMALS) {
+    if (a.flags & NXG_ASSET_HAS_NORMALS) {  // the face normal is replaced by the vertex normals' blend
         r.normal = xnormalize(xbary(ld3(f.normals, t.x), ld3(f.normals, t.y), ld3(f.normals, t.z),
                                     b0, r.b1, r.b2));
+    } else {
+        r.normal = xnormalize(xcross(xsub(p1, p0), xsub(p2, p0)));
     }
     r.u = 0.0f;
     r.v = 0.0f;

@@ -104,10 +104,13 @@ __device__ __forceinline__ Root walk_root(const AssetArgs &a, const FrameArgs &f
         q2 = ld3(a.positions, t.z);
     }
     r.position = xbary(p0, p1, p2, b0, r.b1, r.b2);
-    r.normal = xnormalize(xcross(xsub(p1, p0), xsub(p2, p0)));
+    // The face normal only where the asset has no vertex normals (the
+    // reference computes it first and then replaces it).
     if (a.flags & NXG_ASSET_HAS_NORMALS) {
         r.normal = xnormalize(xbary(ld3(f.normals, t.x), ld3(f.normals, t.y), ld3(f.normals, t.z),
                                     b0, r.b1, r.b2));
+    } else {
+        r.normal = xnormalize(xcross(xsub(p1, p0), xsub(p2, p0)));
     }
     r.u = 0.0f;
     r.v = 0.0f;
@@ -199,16 +202,32 @@ struct WalkDecision {
     float weights[kSlots];
 };
 
+// The strand's RootSample (types.h:126-136) at roots[local]: three 16-byte
+// stores when the array is 16-byte aligned, else twelve word stores.
+__device__ __forceinline__ void walk_store_root(uint32_t *roots, uint32_t local, const Root &r) {
+    uint32_t *dst = roots + static_cast<uint64_t>(local) * 12u;
+    if ((reinterpret_cast<std::uintptr_t>(roots) & 15u) == 0u) {
+        uint4 *v = reinterpret_cast<uint4 *>(dst);
+        v[0] = make_uint4(root_word(r, 0), root_word(r, 1), root_word(r, 2), root_word(r, 3));
+        v[1] = make_uint4(root_word(r, 4), root_word(r, 5), root_word(r, 6), root_word(r, 7));
+        v[2] = make_uint4(root_word(r, 8), root_word(r, 9), root_word(r, 10), root_word(r, 11));
+    } else {
+#pragma unroll
+        for (int w = 0; w < 12; ++w) { dst[w] = root_word(r, w); }
+    }
+}
+
 // Setup step for this lane's strand.  The stencil slots follow eval_slot and
 // the loop of generate.h:214-244 with the frame's guide roots, normals and
 // support radii read from the per-frame guide records.  With `outputs`,
-// also writes the strand's root UV and point count and stages its twelve
-// RootSample words at root_words[lane * 12] for walk_store_roots.  With
-// `decision` (inspection only), also reports the choices made.
+// also writes the strand's RootSample, root UV and point count.  With
+// `decision` (inspection only), also reports the choices made.  Slots past
+// the strand's count point at the frame's zero row with weight 0, so the
+// base step may read any slot of the four records.
 template <bool NOISE>
-__device__ __forceinline__ WalkRoot walk_setup(const LaunchArgs &g, float4 *records, uint32_t *locals,
-                                               uint32_t *root_words, int lane, uint32_t pick, bool valid,
-                                               uint32_t P, bool outputs = true, WalkDecision *decision = nullptr) {
+__device__ __forceinline__ WalkRoot walk_setup(const LaunchArgs &g, float4 *records, uint32_t *locals, int lane,
+                                               uint32_t pick, bool valid, uint32_t P, bool outputs = true,
+                                               WalkDecision *decision = nullptr) {
     const AssetArgs &a = g.a;
     const FrameArgs &f = g.f;
     const ParamArgs &p = g.p;
@@ -221,16 +240,14 @@ __device__ __forceinline__ WalkRoot walk_setup(const LaunchArgs &g, float4 *reco
     r.surface_u = F3{0.0f, 0.0f, 0.0f};
     F3 rest_position = {0.0f, 0.0f, 0.0f};
     const Root root = walk_root<NOISE>(a, f, p.seed, g.first_strand + local, r.surface_u, rest_position);
-    if (outputs && g.roots) {
-#pragma unroll
-        for (int w = 0; w < 12; ++w) { root_words[lane * 12 + w] = root_word(root, w); }
-    }
     if (outputs && valid) {  // generate.h:621-623
+        if (g.roots) { walk_store_root(g.roots, local, root); }
         if (g.root_uvs) { g.root_uvs[local] = make_float2(root.u, root.v); }
         if (g.point_counts) { g.point_counts[local] = P; }
     }
+    const float zero_row = __uint_as_float(g.zero_row);
 #pragma unroll
-    for (int q = 0; q < 4; ++q) { records[q * 32 + lane] = make_float4(0.0f, 0.0f, 0.0f, 0.0f); }
+    for (int q = 0; q < 4; ++q) { records[q * 32 + lane] = make_float4(zero_row, 0.0f, zero_row, 0.0f); }
     uint32_t stencil[kSlots];
     const uint32_t *row = a.stencil + static_cast<uint64_t>(root.triangle) * kSlots;
     if ((reinterpret_cast<std::uintptr_t>(a.stencil) & 15u) == 0u) {
@@ -307,7 +324,7 @@ __device__ __forceinline__ WalkRoot walk_setup(const LaunchArgs &g, float4 *reco
     if (wsum > 1.0e-12f) {
         inv = 1.0f / wsum;
     } else if (nearest != kInvalid) {
-        records[lane] = make_float4(__uint_as_float(nearest * P), 1.0f, 0.0f, 0.0f);
+        records[lane] = make_float4(__uint_as_float(nearest * P), 1.0f, zero_row, 0.0f);
         nb = 1u;
         inv = 1.0f;
         mode = 1u;
@@ -339,17 +356,6 @@ __device__ __forceinline__ WalkRoot walk_setup(const LaunchArgs &g, float4 *reco
         r.domain = (rest_position + F3{0.419276f, 0.184247f, 0.805721f}) * domain_scale;
     }
     return r;
-}
-
-// The staged RootSample words of the batch, twelve consecutive words per
-// strand (lanes over words, so a warp store covers whole records).
-__device__ __forceinline__ void walk_store_roots(const LaunchArgs &g, const uint32_t *root_words,
-                                                 const uint32_t *locals, int lane, int in_batch) {
-    for (int i = lane; i < in_batch * 12; i += 32) {
-        const int s = i / 12;
-        const uint32_t word = locals[s];
-        if ((word >> 31) == 0u) { g.roots[static_cast<uint64_t>(word) * 12u + static_cast<uint32_t>(i - s * 12)] = root_words[i]; }
-    }
 }
 
 // One output point of the strand whose output word is `word` (skipped when
@@ -468,6 +474,84 @@ __device__ __forceinline__ void walk_base(const LaunchArgs &g, const float4 *rec
             walk_emit(g, locals[s], P, c, make_float4(base.x, base.y, base.z, radius));
         } else {
             stage_put(stage + s * kWalkRowFloats, c, base);  // radii come from the t table at the store
+        }
+    }
+}
+
+// Base step straight to the output (no noise).  Eight lanes per strand and
+// four strands per pass: lane (s = pass * 4 + lane / 8, c = lane % 8)
+// computes CVs c + 8m, m < ceil(P / 8).  One address per slot serves the
+// lane's loads (the other CVs sit at fixed distances along the guide's
+// offset row), every load of a warp instruction stays within one 128-byte
+// line per strand, and a lane's t values are fixed for the whole kernel.  A
+// pass runs as many slot pairs as its strands' largest count; a strand's
+// loads past its own count are predicated off (no memory request), and its
+// records there hold the zero row with weight 0, so the accumulation needs
+// no predicate.  CLASSIC applies records 6 and 7 as walk_base does.  Every
+// lane of the warp calls it.
+template <bool CLASSIC>
+__device__ __forceinline__ void walk_base_direct(const LaunchArgs &g, const float4 *records, const uint32_t *locals,
+                                                 const float *tvals, const float *rvals, const float4 *offsets,
+                                                 int lane, int in_batch, int P) {
+    constexpr int kPerLane = kWalkMaxCvs / 8;
+    const int c = lane & 7;
+    const int cpl = (P + 7) >> 3;
+    float tv[kPerLane];
+#pragma unroll
+    for (int m = 0; m < kPerLane; ++m) { tv[m] = tvals[min(c + 8 * m, P - 1)]; }
+    const float ls = g.p.length_scale;
+    const float4 *column = offsets + c;
+    for (int first = 0; first < in_batch; first += 4) {
+        const int s = first + (lane >> 3);
+        const bool live = s < in_batch;
+        const float4 head = records[4 * 32 + s];
+        const float4 tail = records[5 * 32 + s];
+        const uint32_t nb = live ? __float_as_uint(tail.w) : 0u;
+        const uint32_t pairs = __reduce_max_sync(kFull, (nb + 1u) >> 1);
+        F3 acc[kPerLane];
+        float4 da[kPerLane], db[kPerLane];
+#pragma unroll
+        for (int m = 0; m < kPerLane; ++m) {
+            acc[m] = F3{0.0f, 0.0f, 0.0f};
+            da[m] = db[m] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
+        for (uint32_t q = 0; q < pairs; ++q) {
+            // A strand loads only its own slots: past its count the registers
+            // keep the last (finite) entries and the weights are zero.
+            const float4 gw = records[q * 32 + s];
+            const float4 *ra = column + __float_as_uint(gw.x);
+            const float4 *rb = column + __float_as_uint(gw.z);
+            const bool la = 2u * q < nb, lb = 2u * q + 1u < nb;
+#pragma unroll
+            for (int m = 0; m < kPerLane; ++m) {
+                if (m < cpl) {
+                    if (la) { da[m] = __ldg(ra + 8 * m); }
+                    if (lb) { db[m] = __ldg(rb + 8 * m); }
+                }
+            }
+#pragma unroll
+            for (int m = 0; m < kPerLane; ++m) {
+                if (m < cpl) { acc[m] = acc[m] + xyz(da[m]) * gw.y + xyz(db[m]) * gw.w; }
+            }
+        }
+        const uint32_t word = live ? locals[s] : 0x80000000u;
+        float4 front = {0.0f, 0.0f, 0.0f, 1.0f}, width = {0.0f, 0.0f, 0.0f, 0.0f};
+        if constexpr (CLASSIC) {
+            front = records[6 * 32 + s];
+            width = records[7 * 32 + s];
+        }
+#pragma unroll
+        for (int m = 0; m < kPerLane; ++m) {
+            const int cm = c + 8 * m;
+            if (m < cpl && cm < P) {
+                F3 base = F3{head.x, head.y, head.z} + (acc[m] * head.w + F3{tail.x, tail.y, tail.z} * tv[m]) * ls;
+                float radius = rvals[cm];
+                if constexpr (CLASSIC) {
+                    if (g.classic_length) { base = xadd(xyz(front), xmul(xsub(base, xyz(front)), front.w)); }
+                    if (width.y != 0.0f) { radius = width.x; }
+                }
+                walk_emit(g, word, P, cm, make_float4(base.x, base.y, base.z, radius));
+            }
         }
     }
 }
