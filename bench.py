@@ -59,6 +59,8 @@ def parse_args():
                     help="lanes,cvs_per_lane,block_size of the generate kernel (default: autotuned in warm-up)")
     ap.add_argument("--noise-amplitude", type=float, default=None,
                     help="override the workload's noise magnitude (0 = the noise-free path)")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="batched workloads: keep the library's default tiles instead of timing tiles in warm-up")
     return ap.parse_args()
 
 
@@ -512,7 +514,7 @@ def run_batched(args):
     for w, d, o in zip(batch.workloads, dassets, runner.outputs):
         key = (int(w.params.cvs_per_strand), w.params.noise_amplitude != 0.0)
         if key not in tuned:
-            tuned[key] = autotune(d, w.params, o[0], repeats=2)[0]
+            tuned[key] = "default" if args.no_autotune else autotune(d, w.params, o[0], repeats=2)[0]
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=device)
     sampler = ClockSampler(0)
     sampler.start()

@@ -13,14 +13,17 @@
 //                      shared memory, one global atomic per block and bin);
 //   batched_offsets    every description's guide-offset table and guide
 //                      frame records;
-//   batched_generate   persistent warps pull (description, 32-strand batch)
-//                      items from an atomic counter -- items of the costliest
+//   batched_generate   one launch per class of work item -- noisy
+//                      lane-walk items, noise-free items, noisy lane-group
+//                      items -- each with the CTA shape, shared memory and
+//                      register budget of its variants; persistent warps pull
+//                      (description, 32-strand batch) items of their class
+//                      from an atomic counter -- items of the costliest
 //                      descriptions first -- and run each item with its
 //                      description's tile (lanes per strand x CVs per lane,
-//                      or the lane walk for noise-free strands of up to 32
-//                      CVs) and noise setting.
-// Six launches per frame whatever the description count, all enqueue-only
-// and capturable in one CUDA graph.
+//                      or the lane walk for strands of up to 32 CVs).
+// Six to eight launches per frame whatever the description count, all
+// enqueue-only and capturable in one CUDA graph.
 #include "generator_core.cuh"
 #include "walk.cuh"
 #include "nxg_classic.h"
@@ -56,10 +59,15 @@ struct BatchDesc {
 
 struct BatchArgs {
     uint32_t count;
-    uint32_t warp_bytes;       // shared memory per warp of batched_generate (after the CTA's head)
+    uint32_t warp_bytes[3];    // shared memory per warp of each class's generate launch (after the CTA's head)
     uint32_t total_strands;
-    uint32_t total_items;
-    uint32_t *item_counter;
+    // Work-item classes, each its own generate launch: 0 = noisy
+    // descriptions on lane-walk items, 1 = noise-free descriptions, 2 = noisy
+    // descriptions on lane-group items.  Descriptions d[k] of class c are k
+    // in [desc_first[c], desc_end[c]).
+    uint32_t total_items[3];
+    uint32_t desc_first[3], desc_end[3];
+    uint32_t *item_counter;    // one counter per class
     uint64_t total_offsets;
     BatchDesc d[kMaxBatch];
 };
@@ -71,7 +79,7 @@ __device__ __forceinline__ int desc_of_strand(const BatchArgs &b, uint32_t i) {
 }
 
 __global__ void batched_clear_kernel(const __grid_constant__ BatchArgs b) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) { *b.item_counter = 0u; }
+    if (blockIdx.x == 0 && threadIdx.x < 3) { b.item_counter[threadIdx.x] = 0u; }
     for (uint32_t d = 0; d < b.count; ++d) {
         const uint32_t bins = b.d[d].g.a.guide_count + 1u;
         for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < bins; i += gridDim.x * blockDim.x) {
@@ -273,6 +281,10 @@ constexpr size_t kBatchRecordBytes = sizeof(uint32_t) * kRecFields * 32u;       
 constexpr size_t kBatchStageBytes = sizeof(float4) * 32u * 4u;                  // 32 lanes x 4 CVs
 constexpr size_t kBatchLatticeBytes = sizeof(float2) * 384u;
 constexpr size_t kBatchWarpBytes = kBatchRecordBytes + kBatchStageBytes + kBatchLatticeBytes;
+// 32-strand batches per warp in one work item of each class: four for the
+// noisy classes (fewer CTA-wide claims between long batches), one for the
+// noise-free class (its descriptions are small; finer items balance better).
+__host__ __device__ constexpr uint32_t batches_per_warp(int cls) { return cls == 1 ? 1u : 4u; }
 
 static_assert(kBatchRecordBytes >= kWalkRecordBytes, "lane-walk records fit the record area");
 static_assert(kBatchStageBytes >= sizeof(float4) * kWalkMaxCvs, "spline scratch fits the stage area");
@@ -379,29 +391,43 @@ __device__ __forceinline__ void batched_dispatch_lanes(const BatchDesc &d, uint3
 }
 
 // CLASSIC: some description applies Classic per-root scalars; descriptions
-// without scalars still take the plain item.
-template <int PPT, bool CLASSIC>
-__global__ void batched_generate_kernel(const __grid_constant__ BatchArgs b) {
+// without scalars still take the plain item.  CLS: the work-item class this
+// launch runs (0: noisy lane-walk items, 1: noise-free items, 2: noisy
+// lane-group items), so each launch holds only its variants' code and runs
+// at their register and shared-memory footprint.
+template <int PPT, bool CLASSIC, int CLS>
+__global__ void __launch_bounds__(CLS == 1 ? 256 : 320, CLS == 1 ? 3 : 1)
+    batched_generate_kernel(const __grid_constant__ BatchArgs b) {
     extern __shared__ float4 smem[];
     __shared__ uint32_t claimed;
+    __shared__ uint32_t next_batch;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const uint32_t warps = blockDim.x >> 5;
+    const uint32_t per_item = warps * batches_per_warp(CLS);
     float4 *table = smem;
     float *tvals = reinterpret_cast<float *>(reinterpret_cast<unsigned char *>(smem) + kBatchTableBytes);
-    unsigned char *mine = reinterpret_cast<unsigned char *>(smem) + kBatchHeadBytes + b.warp_bytes * warp;
+    unsigned char *mine = reinterpret_cast<unsigned char *>(smem) + kBatchHeadBytes + b.warp_bytes[CLS] * warp;
+    const uint32_t total = b.total_items[CLS];
+    const int first = static_cast<int>(b.desc_first[CLS]);
+    const int last = static_cast<int>(b.desc_end[CLS]) - 1;
     int current = -1;
     // A work item is a contiguous slice of one description's strand order,
-    // one 32-strand batch per warp of the CTA, so the CTA's strands share
-    // guide-offset rows in L1.  Each pass of the loop consumes one item.
-    for (uint32_t guard = 0; guard <= b.total_items; ++guard) {
-        if (threadIdx.x == 0) { claimed = atomicAdd(b.item_counter, 1u); }
+    // batches_per_warp(CLS) 32-strand batches per warp of the CTA, so the CTA's
+    // strands share guide-offset rows in L1; its warps take the item's
+    // batches from a shared counter, so a slow batch holds up only its own
+    // warp until the item ends.  Each pass of the loop consumes one item.
+    for (uint32_t guard = 0; guard <= total; ++guard) {
+        if (threadIdx.x == 0) {
+            claimed = atomicAdd(b.item_counter + CLS, 1u);
+            next_batch = 0u;
+        }
         __syncthreads();
         const uint32_t item = claimed;
         __syncthreads();
-        if (item >= b.total_items) { break; }
-        int di = 0;
-        while (di + 1 < static_cast<int>(b.count) && b.d[di + 1].item_begin <= item) { ++di; }
+        if (item >= total) { break; }
+        int di = first;
+        while (di < last && b.d[di + 1].item_begin <= item) { ++di; }
         const BatchDesc &d = b.d[di];
         if (di != current) {  // the whole CTA: every warp works on the item's description
             const int P = static_cast<int>(d.g.p.cvs_per_strand);
@@ -418,26 +444,31 @@ __global__ void batched_generate_kernel(const __grid_constant__ BatchArgs b) {
             __syncthreads();
             current = di;
         }
-        const uint32_t batch = ((item - d.item_begin) * warps + static_cast<uint32_t>(warp)) * 32u;
-        if (batch >= d.g.count) { continue; }
+        for (;;) {
+        uint32_t k = 0u;
+        if (lane == 0) { k = atomicAdd(&next_batch, 1u); }
+        k = __shfl_sync(kFull, k, 0);
+        if (k >= per_item) { break; }
+        const uint32_t batch = ((item - d.item_begin) * per_item + k) * 32u;
+        if (batch >= d.g.count) { break; }
         const uint32_t end = min(batch + 32u, d.g.count);
-        if (d.lanes == 1u) {
-            if (d.noise) {
-                batched_noise_walk_item<CLASSIC>(d, batch, end, lane, mine, table, tvals);
-            } else {
+        if constexpr (CLS == 0) {
+            batched_noise_walk_item<CLASSIC>(d, batch, end, lane, mine, table, tvals);
+        } else if constexpr (CLS == 1) {
+            if (d.lanes == 1u) {
                 batched_walk_item<CLASSIC>(d, batch, end, lane, mine, tvals);
+            } else if (CLASSIC && d.g.scalars != nullptr) {
+                batched_dispatch_lanes<PPT, false, CLASSIC>(d, batch, end, lane, mine, table, tvals);
+            } else {
+                batched_dispatch_lanes<PPT, false, false>(d, batch, end, lane, mine, table, tvals);
             }
         } else if (CLASSIC && d.g.scalars != nullptr) {
-            if (d.noise) {
-                batched_dispatch_lanes<PPT, true, CLASSIC>(d, batch, end, lane, mine, table, tvals);
-            } else {
-                batched_dispatch_lanes<PPT, false, CLASSIC>(d, batch, end, lane, mine, table, tvals);
-            }
-        } else if (d.noise) {
-            batched_dispatch_lanes<PPT, true, false>(d, batch, end, lane, mine, table, tvals);
+            batched_dispatch_lanes<PPT, true, CLASSIC>(d, batch, end, lane, mine, table, tvals);
         } else {
-            batched_dispatch_lanes<PPT, false, false>(d, batch, end, lane, mine, table, tvals);
+            batched_dispatch_lanes<PPT, true, false>(d, batch, end, lane, mine, table, tvals);
         }
+        }
+        __syncthreads();  // the item's batches are done before the next claim resets the counter
     }
 }
 
@@ -540,42 +571,66 @@ uint32_t generate_batched(const nxg_device_asset_desc *assets, const nxg_deforme
     if (!workspace || workspace_bytes < layout.total) { return NXG_ERROR_WORKSPACE_TOO_SMALL; }
     if (reinterpret_cast<std::uintptr_t>(workspace) % kAlign != 0u) { return NXG_ERROR_MISALIGNED_OUTPUT; }
 
-    // CTA size of the generate kernel (work items are one 32-strand batch per warp).
+    // Tile family of the launch: two CVs per lane when every strand fits 32 x 2.
     uint32_t max_cvs = 0u;
     for (uint32_t d = 0; d < count; ++d) { max_cvs = std::max(max_cvs, params[d].cvs_per_strand); }
     const uint32_t ppt = max_cvs <= 64u ? 2u : 4u;
-    const void *fn = any_classic
-        ? (ppt == 2u ? reinterpret_cast<const void *>(dev::batched_generate_kernel<2, true>)
-                     : reinterpret_cast<const void *>(dev::batched_generate_kernel<4, true>))
-        : (ppt == 2u ? reinterpret_cast<const void *>(dev::batched_generate_kernel<2, false>)
-                     : reinterpret_cast<const void *>(dev::batched_generate_kernel<4, false>));
+    // Work-item class of each description, one generate launch per class at
+    // its own occupancy: 0 for noisy descriptions on the lane-walk tile, whose
+    // warps need the walk's stage and lattice (ten-warp CTAs fill the SM's
+    // shared memory); 1 for noise-free descriptions; 2 for noisy descriptions
+    // on lane-group tiles.
+    constexpr uint32_t kClasses = 3u;
+    std::vector<uint32_t> cls(count);
+    for (uint32_t d = 0; d < count; ++d) {
+        const bool noise = params[d].noise_amplitude != 0.0f && params[d].noise_mask != 0.0f;
+        cls[d] = !noise ? 1u : (batch_lanes(params[d].cvs_per_strand, true, ppt) == 1u ? 0u : 2u);
+    }
+    const auto kernel = [&](uint32_t c) -> const void * {
+        if (c == 0u) {
+            return any_classic ? reinterpret_cast<const void *>(dev::batched_generate_kernel<2, true, 0>)
+                               : reinterpret_cast<const void *>(dev::batched_generate_kernel<2, false, 0>);
+        }
+        if (c == 1u) {
+            if (any_classic) {
+                return ppt == 2u ? reinterpret_cast<const void *>(dev::batched_generate_kernel<2, true, 1>)
+                                 : reinterpret_cast<const void *>(dev::batched_generate_kernel<4, true, 1>);
+            }
+            return ppt == 2u ? reinterpret_cast<const void *>(dev::batched_generate_kernel<2, false, 1>)
+                             : reinterpret_cast<const void *>(dev::batched_generate_kernel<4, false, 1>);
+        }
+        if (any_classic) {
+            return ppt == 2u ? reinterpret_cast<const void *>(dev::batched_generate_kernel<2, true, 2>)
+                             : reinterpret_cast<const void *>(dev::batched_generate_kernel<4, true, 2>);
+        }
+        return ppt == 2u ? reinterpret_cast<const void *>(dev::batched_generate_kernel<2, false, 2>)
+                         : reinterpret_cast<const void *>(dev::batched_generate_kernel<4, false, 2>);
+    };
     uint32_t status = NXG_ERROR_NONE;
-    cudaFuncAttributes attr{};
-    if ((status = record_cuda(cudaFuncGetAttributes(&attr, fn)))) { return status; }
     int device = 0, smem_optin = 48 * 1024;
     if (cudaGetDevice(&device) == cudaSuccess) {
         cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
     }
-    // Noisy descriptions on the lane-walk tile need the walk's stage and
-    // lattice per warp; CTAs are then ten warps, as many as the SM's shared
-    // memory holds.
-    bool noise_walk = false;
-    for (uint32_t d = 0; d < count; ++d) {
-        const bool noise = params[d].noise_amplitude != 0.0f && params[d].noise_mask != 0.0f;
-        noise_walk = noise_walk || (noise && batch_lanes(params[d].cvs_per_strand, true, ppt) == 1u);
+    // CTA size per class (work items are one 32-strand batch per warp).
+    const size_t class_warp_bytes[kClasses] = {dev::kBatchWalkWarpBytes, dev::kBatchWarpBytes,
+                                               dev::kBatchWarpBytes};
+    uint32_t class_block[kClasses] = {0u, 0u, 0u};
+    for (uint32_t c = 0; c < kClasses; ++c) {
+        cudaFuncAttributes attr{};
+        if ((status = record_cuda(cudaFuncGetAttributes(&attr, kernel(c))))) { return status; }
+        uint32_t block = std::min(static_cast<uint32_t>(attr.maxThreadsPerBlock) / 32u * 32u,
+                                  c == 0u ? 320u : std::max<uint32_t>(32u, (cfg.block_size + 31u) / 32u * 32u));
+        while (block > 32u &&
+               dev::kBatchHeadBytes + class_warp_bytes[c] * (block / 32u) + 64u > static_cast<size_t>(smem_optin)) {
+            block -= 32u;
+        }
+        class_block[c] = block;
     }
-    const size_t warp_bytes = noise_walk ? dev::kBatchWalkWarpBytes : dev::kBatchWarpBytes;
-    uint32_t block = std::min(static_cast<uint32_t>(attr.maxThreadsPerBlock) / 32u * 32u,
-                              noise_walk ? 320u : std::max<uint32_t>(32u, (cfg.block_size + 31u) / 32u * 32u));
-    while (block > 32u && dev::kBatchHeadBytes + warp_bytes * (block / 32u) + 64u > static_cast<size_t>(smem_optin)) {
-        block -= 32u;
-    }
-    const uint32_t warps_per_cta = block / 32u;
 
     auto *w = static_cast<unsigned char *>(workspace);
     dev::BatchArgs b{};
     b.count = count;
-    b.warp_bytes = static_cast<uint32_t>(warp_bytes);
+    for (uint32_t c = 0; c < kClasses; ++c) { b.warp_bytes[c] = static_cast<uint32_t>(class_warp_bytes[c]); }
     b.item_counter = reinterpret_cast<uint32_t *>(w + layout.counter);
     // Costliest descriptions first (CVs per strand, tripled with noise), so the
     // longest work items start early and the tail is made of cheap ones.
@@ -585,8 +640,11 @@ uint32_t generate_batched(const nxg_device_asset_desc *assets, const nxg_deforme
         const bool noise = params[d].noise_amplitude != 0.0f && params[d].noise_mask != 0.0f;
         return uint64_t{params[d].cvs_per_strand} * (noise ? 3u : 1u);
     };
-    std::stable_sort(rank.begin(), rank.end(), [&](uint32_t x, uint32_t y) { return cost(x) > cost(y); });
-    uint32_t strands = 0u, items = 0u;
+    std::stable_sort(rank.begin(), rank.end(), [&](uint32_t x, uint32_t y) {
+        return cls[x] != cls[y] ? cls[x] < cls[y] : cost(x) > cost(y);
+    });
+    uint32_t strands = 0u, items[kClasses] = {0u, 0u, 0u};
+    for (uint32_t c = 0; c < kClasses; ++c) { b.desc_first[c] = b.desc_end[c] = count; }
     uint64_t offsets = 0u;
     for (uint32_t k = 0; k < count; ++k) {
         const uint32_t d = rank[k];
@@ -616,14 +674,18 @@ uint32_t generate_batched(const nxg_device_asset_desc *assets, const nxg_deforme
         bd.noise = bd.g.p.noise;
         bd.want_roots = (outputs[d].roots || outputs[d].root_uvs || outputs[d].point_counts) ? 1u : 0u;
         bd.strand_begin = strands;
-        bd.item_begin = items;
+        const uint32_t c = cls[d];
+        if (b.desc_first[c] == count) { b.desc_first[c] = k; }
+        b.desc_end[c] = k + 1u;
+        bd.item_begin = items[c];
         bd.offset_begin = offsets;
         strands += params[d].strand_count;
-        items += (params[d].strand_count + 32u * warps_per_cta - 1u) / (32u * warps_per_cta);
+        const uint32_t per_item = 32u * (class_block[c] / 32u) * dev::batches_per_warp(static_cast<int>(c));
+        items[c] += (params[d].strand_count + per_item - 1u) / per_item;
         offsets += uint64_t{assets[d].header.guide_count} * (params[d].cvs_per_strand + 1u) + dev::kWalkMaxCvs;
     }
     b.total_strands = strands;
-    b.total_items = items;
+    for (uint32_t c = 0; c < kClasses; ++c) { b.total_items[c] = items[c]; }
     b.total_offsets = offsets;
     // One CVs-per-lane value per launch keeps the kernel's register footprint
     // that of a single tile family: two when every strand fits 32 lanes x 2.
@@ -657,27 +719,26 @@ uint32_t generate_batched(const nxg_device_asset_desc *assets, const nxg_deforme
     dev::batched_offsets_kernel<<<std::max(1u, offset_blocks), 256, 0, s>>>(b);
     if ((status = record_cuda(cudaGetLastError()))) { return status; }
 
-    const size_t shm = dev::kBatchHeadBytes + warp_bytes * (block / 32u);
-    if ((status = record_cuda(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                   static_cast<int>(shm))))) {
-        return status;
-    }
-    int per_sm = 0;
-    if ((status = record_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, static_cast<int>(block),
-                                                                            shm)))) {
-        return status;
-    }
-    const uint32_t grid = static_cast<uint32_t>(std::max(1, sms * std::max(per_sm, 1)));
-    if (any_classic) {
-        if (ppt == 2u) {
-            dev::batched_generate_kernel<2, true><<<grid, block, shm, s>>>(b);
-        } else {
-            dev::batched_generate_kernel<4, true><<<grid, block, shm, s>>>(b);
+    // One generate launch per class with work, in stream order; each runs
+    // persistent CTAs at its own occupancy.
+    for (uint32_t c = 0; c < kClasses; ++c) {
+        if (items[c] == 0u) { continue; }
+        const void *fn = kernel(c);
+        const uint32_t block = class_block[c];
+        const size_t shm = dev::kBatchHeadBytes + class_warp_bytes[c] * (block / 32u);
+        if ((status = record_cuda(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                       static_cast<int>(shm))))) {
+            return status;
         }
-    } else if (ppt == 2u) {
-        dev::batched_generate_kernel<2, false><<<grid, block, shm, s>>>(b);
-    } else {
-        dev::batched_generate_kernel<4, false><<<grid, block, shm, s>>>(b);
+        int per_sm = 0;
+        if ((status = record_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, static_cast<int>(block),
+                                                                                shm)))) {
+            return status;
+        }
+        const uint32_t grid = static_cast<uint32_t>(
+            std::min<uint64_t>(items[c], static_cast<uint64_t>(std::max(1, sms * std::max(per_sm, 1)))));
+        void *args[] = {&b};
+        if ((status = record_cuda(cudaLaunchKernel(fn, dim3(grid), dim3(block), args, shm, s)))) { return status; }
     }
     return record_cuda(cudaGetLastError());
 }
