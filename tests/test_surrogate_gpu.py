@@ -3,11 +3,13 @@ oracle (oracle/mlp_reference.py) and the exact Classic runtime.
 
 Bars: forward outputs and full-batch gradients match the oracle evaluated on
 the same BF16-rounded weights, inputs and activations (the remaining
-difference is FP32 accumulation order: outputs within 1e-2 of the output
-scale, every layer's gradient within 2e-2 relative L2 and cosine >= 0.999);
-training lowers the loss; exact mode reproduces nxg_classic_root_scalars
-bit for bit; a fully checked batch never returns a root outside the
-tolerance.
+difference is FP32 accumulation order: outputs within 2e-5 of the output
+scale, every layer's gradient within 3.5e-5 relative L2 and cosine >=
+0.999999, about ten times the agreement measured on a B200); training lowers
+the loss; exact mode reproduces nxg_classic_root_scalars bit for bit; a fully
+checked batch never returns a root outside the tolerance; and the measured
+gain (or loss) of the judged surrogate against the exact runtime alone is
+reported.
 """
 import numpy as np
 import pytest
@@ -76,7 +78,7 @@ def test_forward_matches_oracle(sphere):
     scale = np.asarray(h["output_scale"], np.float64)
     err = np.abs(out - theirs) / scale
     print("forward: max %.3g mean %.3g (output-scale units)" % (err.max(), err.mean()))
-    assert err.max() <= 1e-2 and err.mean() <= 1e-3
+    assert err.max() <= 2e-5 and err.mean() <= 5e-6
 
 
 def test_gradients_match_oracle(sphere):
@@ -85,14 +87,14 @@ def test_gradients_match_oracle(sphere):
     m.fit_outputs(targets)
     loss, grad = m.gradients(feats, targets)
     rloss, rgrad = ref.loss_and_gradients(m.parameters(), feats.cpu().numpy(), targets.cpu().numpy(), m.header())
-    assert abs(loss - rloss) <= 1e-3 * abs(rloss)
+    assert abs(loss - rloss) <= 1e-4 * abs(rloss)
     bounds = [(ref.P1, ref.P2), (ref.P2, ref.P3), (ref.P3, ref.P4), (ref.P4, ref.PARAMETERS)]
     for layer, (a, b) in enumerate(bounds, 1):
         g, r = grad[a:b].astype(np.float64), rgrad[a:b]
         rel = np.linalg.norm(g - r) / np.linalg.norm(r)
         cos = float(g @ r / (np.linalg.norm(g) * np.linalg.norm(r)))
         print("layer %d: relative L2 %.3g, cosine %.6f" % (layer, rel, cos))
-        assert rel <= 2e-2 and cos >= 0.999, layer
+        assert rel <= 3.5e-5 and cos >= 0.999999, layer
     assert np.all(grad[~ref.used_mask()] == 0.0)
 
 
@@ -178,3 +180,62 @@ def test_adaptive_judge_routes_distrusted_batches_to_the_exact_kernel(sphere):
         assert st == [0, 0, checked, checked], (launch, st)
         np.testing.assert_array_equal(got[:30000].cpu().numpy().view(np.uint32),
                                       exact[:30000].cpu().numpy().view(np.uint32))
+
+
+def _time_ms(fn, repeats=10):
+    import torch
+    fn()
+    torch.cuda.synchronize()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    for _ in range(repeats):
+        fn()
+    stop.record()
+    torch.cuda.synchronize()
+    return start.elapsed_time(stop) / repeats
+
+
+def test_measured_gain_against_exact_runtime(sphere):
+    """What the trained network gains over the exact runtime alone on the
+    cfg5 expressions (1M roots): the fallback rate and the time of the judged
+    scalar stage (adaptive mode, 4 checks per 128-root batch) at 1e-3 and at
+    5e-2, against the exact stage.  The expressions are hash-lattice noise at
+    frequencies 6 and 20, which the 3 x 64 network reproduces to a few percent
+    only, so at 1e-3 every checked batch fails and the exact runtime serves
+    the frame: a loss, measured and printed.  Asserted: every root the judge
+    returns at 1e-3 is the exact runtime's value (bit for bit), and each
+    measurement is a finite time."""
+    import torch
+    from nanoxgen_b200.classic import root_scalars
+    w, _, dasset = sphere
+    m = _model(sphere, seed=21)
+    _, feats, targets = _data(sphere, 262144, seed=303)
+    m.fit_outputs(targets)
+    m.train(feats, targets, epochs=6, batch=16384, learning_rate=3e-3, lr_decay=0.85)
+    n = 1_000_000
+    params = _params(w, n)
+    exact = torch.empty((n, 2), dtype=torch.float32, device="cuda")
+    judged = torch.empty_like(exact)
+    status = torch.zeros(4, dtype=torch.int32, device="cuda")
+    exact_ms = _time_ms(lambda: root_scalars(dasset, params, _plan(), out=exact))
+    tiles = (n + 127) // 128
+    report = {}
+    for tol in (1e-3, 5e-2):
+        run = lambda: m.root_scalars(dasset, params, _plan(), length_tolerance=tol, width_tolerance=tol,
+                                     checks_per_batch=4, mode=3, out=judged, status=status)
+        run()  # the first adaptive launch checks every batch and sets the model's trust
+        ms = _time_ms(run)
+        status.zero_()
+        run()
+        torch.cuda.synchronize()
+        st = status.cpu().tolist()
+        assert st[0] == 0
+        by_network = st[3] - st[2]  # checked batches whose network values were kept
+        report[tol] = (ms, by_network / tiles)
+        print("tolerance %g: judged stage %.3f ms vs exact %.3f ms (gain %.2fx); %d of %d batches served by the "
+              "network, %d checked batches re-run exactly, %d left to the exact kernel"
+              % (tol, ms, exact_ms, exact_ms / ms, by_network, tiles, st[2], tiles - st[3]))
+        assert np.isfinite(ms) and ms > 0.0
+        if tol == 1e-3:
+            np.testing.assert_array_equal(judged.cpu().numpy().view(np.uint32), exact.cpu().numpy().view(np.uint32))
+    assert report[1e-3][1] == 0.0  # no batch passes 1e-3 on these expressions
