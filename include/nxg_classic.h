@@ -141,6 +141,72 @@ uint32_t nxg_generate_batched_classic(const nxg_device_asset_desc *assets, const
                                       const nxg_launch_config *config, void *workspace, uint64_t workspace_bytes,
                                       void *stream);
 
+/* -------------------------------------------------------------- FX passes */
+
+/* The Classic FX pipeline of apply_xgen_classic_float_runtime_plan_cpu
+ * (src/xgen_classic_runtime.cpp:1420-1919) on the GPU, as a pass over a
+ * generated packed curve set: per strand, the SplinePrimitive length and
+ * width with the drop rule, the description's FX modules in order -- NoiseFX
+ * mode 0 (apply_noise, :897-1040) and CutFX rebuild type 1
+ * (cut_from_tip_and_rebuild, :692-748) -- then the width profile (taper,
+ * taperStart, widthRamp).  ClumpingFX is not supported.  Expressions are
+ * compiled with NXG_EXPRESSION_CLASSIC and the attribute's own name and
+ * object type; they may read $id, $cLength, $cWidth, $u, $v and
+ * noise($Prefg*k) (evaluated at the root's position). */
+#define NXG_CLASSIC_MAX_FX 8u
+#define NXG_CLASSIC_MAX_FX_CVS 64u
+
+enum { NXG_CLASSIC_FX_NOISE = 0, NXG_CLASSIC_FX_CUT = 1 };
+
+typedef struct nxg_classic_fx {
+    uint32_t type;                         /* NXG_CLASSIC_FX_NOISE or NXG_CLASSIC_FX_CUT */
+    uint32_t reserved;
+    /* NoiseFXModule attributes (type NOISE), all required */
+    const nxg_expression *mask, *magnitude, *magnitude_scale, *frequency, *correlation, *preserve_length;
+    const nxg_expression *amount;          /* CutFXModule.amount (type CUT) */
+} nxg_classic_fx;
+
+typedef struct nxg_classic_fx_plan {
+    /* SplinePrimitive attributes, NULL when absent */
+    const nxg_expression *length, *width, *taper, *taper_start, *width_ramp;
+    const nxg_classic_fx *effects;         /* in the description's order */
+    uint32_t effect_count;                 /* <= NXG_CLASSIC_MAX_FX */
+    uint32_t description_id;               /* rand() face seed */
+    const char *description_name;          /* rand() face seed (text after its last ':'); NULL = "" */
+} nxg_classic_fx_plan;
+
+/* Device bytes of a plan's packed form (constant; 256-byte aligned buffer). */
+uint64_t nxg_classic_fx_plan_bytes(void);
+
+/* Packs `plan` and copies it into `device_plan` on `stream` (a host-to-device
+ * copy from library-owned host memory, complete when the call returns).
+ * Returns NXG_ERROR_EXPRESSION_LIMIT / _INPUT when a program does not fit
+ * the device form or reads an unbound variable, NXG_ERROR_INVALID_ARGUMENT
+ * for a malformed plan. */
+uint32_t nxg_classic_fx_plan_upload(const nxg_classic_fx_plan *plan, void *device_plan, uint64_t bytes,
+                                    void *stream);
+
+typedef struct nxg_classic_fx_curves {
+    float *points;                 /* strand_count x cvs_per_strand float4 (position, radius), in/out */
+    uint32_t *point_counts;        /* in/out; a strand whose count is not cvs_per_strand is skipped, a
+                                      dropped strand gets 0 (its points are left as they were) */
+    const void *roots;             /* nxg_root_sample[strand_count] of the curves */
+    const float *surface_tangents; /* strand_count x 3 (the frame's cU per strand); required with NoiseFX */
+    const float *noise_domains;    /* strand_count x 3 NoiseFX domain positions, or NULL (the curve's root) */
+    uint32_t strand_count;
+    uint32_t cvs_per_strand;       /* 2 .. NXG_CLASSIC_MAX_FX_CVS */
+    uint32_t first_id;             /* $id of strand 0 */
+    float radius_scale;
+} nxg_classic_fx_curves;
+
+/* Applies the uploaded plan to `curves` on `stream` (enqueue only).
+ * device_status (2 x uint32, zeroed by the caller) receives
+ * NXG_ERROR_EXPRESSION_DOMAIN and the number of failing strands where an
+ * expression yields a non-finite value or a negative length (the reference
+ * throws there). */
+uint32_t nxg_classic_fx_apply(const void *device_plan, const nxg_classic_fx_curves *curves,
+                              uint32_t *device_status, void *stream);
+
 /* ---------------------------------------------------------------- surrogate */
 
 /* The model is one caller-owned device buffer of nxg_surrogate_model_bytes()

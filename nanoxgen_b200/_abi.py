@@ -181,6 +181,34 @@ class ClassicApplyDesc(ctypes.Structure):
                 ("apply_width", ctypes.c_uint32)]
 
 
+class ClassicFx(ctypes.Structure):
+    """nxg_classic_fx (nxg_classic.h): one NoiseFX or CutFX module."""
+    _fields_ = [("type", ctypes.c_uint32), ("reserved", ctypes.c_uint32), ("mask", ctypes.c_void_p),
+                ("magnitude", ctypes.c_void_p), ("magnitude_scale", ctypes.c_void_p), ("frequency", ctypes.c_void_p),
+                ("correlation", ctypes.c_void_p), ("preserve_length", ctypes.c_void_p), ("amount", ctypes.c_void_p)]
+
+
+class ClassicFxPlan(ctypes.Structure):
+    """nxg_classic_fx_plan (nxg_classic.h)."""
+    _fields_ = [("length", ctypes.c_void_p), ("width", ctypes.c_void_p), ("taper", ctypes.c_void_p),
+                ("taper_start", ctypes.c_void_p), ("width_ramp", ctypes.c_void_p),
+                ("effects", ctypes.POINTER(ClassicFx)), ("effect_count", ctypes.c_uint32),
+                ("description_id", ctypes.c_uint32), ("description_name", ctypes.c_char_p)]
+
+
+class ClassicFxCurves(ctypes.Structure):
+    """nxg_classic_fx_curves (nxg_classic.h)."""
+    _fields_ = [("points", ctypes.c_void_p), ("point_counts", ctypes.c_void_p), ("roots", ctypes.c_void_p),
+                ("surface_tangents", ctypes.c_void_p), ("noise_domains", ctypes.c_void_p),
+                ("strand_count", ctypes.c_uint32), ("cvs_per_strand", ctypes.c_uint32),
+                ("first_id", ctypes.c_uint32), ("radius_scale", ctypes.c_float)]
+
+
+CLASSIC_FX_NOISE = 0
+CLASSIC_FX_CUT = 1
+CLASSIC_MAX_FX = 8
+CLASSIC_MAX_FX_CVS = 64
+
 SURROGATE_INPUTS = 8
 SURROGATE_PARAMETERS = 12544
 
@@ -354,6 +382,9 @@ _SIGNATURES = {
     "nxg_expression_get_ramp_point": (ctypes.c_uint32, [_P, ctypes.c_uint32, ctypes.POINTER(ExpressionRampPoint)]),
     "nxg_expression_input_name": (ctypes.c_char_p, [_P, ctypes.c_uint32]),
     "nxg_xgen_string_seed": (ctypes.c_uint32, [ctypes.c_char_p]),
+    "nxg_classic_fx_plan_bytes": (ctypes.c_uint64, []),
+    "nxg_classic_fx_plan_upload": (ctypes.c_uint32, [ctypes.POINTER(ClassicFxPlan), _P, ctypes.c_uint64, _P]),
+    "nxg_classic_fx_apply": (ctypes.c_uint32, [_P, ctypes.POINTER(ClassicFxCurves), _P, _P]),
     "nxg_classic_root_scalars": (ctypes.c_uint32, [ctypes.POINTER(DeviceAssetDesc), ctypes.POINTER(GenerationParams),
                                                    ctypes.POINTER(ClassicScalarPlan), ctypes.c_uint32,
                                                    ctypes.c_uint32, _P, _P, _P]),

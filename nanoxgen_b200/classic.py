@@ -172,3 +172,89 @@ def generate_packed_classic(dasset: DeviceAsset, params: GenerationParams, scala
                                             n, ws.data_ptr(), ws.numel(), _stream_handle(stream)),
           "nxg_generate_packed_classic")
     return PackedCurves(n, cvs, points, point_counts, roots, root_uvs)
+
+
+# ------------------------------------------------------------- FX passes
+
+NOISE_FX_ATTRIBUTES = ("mask", "magnitude", "magnitudeScale", "frequency", "correlation", "preserveLength")
+
+
+class FxPlan:
+    """A description's Classic runtime plan for nxg_classic_fx_apply: the
+    SplinePrimitive length, width, taper, taperStart and widthRamp
+    expressions (each optional) and its FX modules in order, each
+    ``("noise", {mask, magnitude, magnitudeScale, frequency, correlation,
+    preserveLength})`` or ``("cut", {"amount": ...})``; every attribute is
+    compiled as the Classic runtime compiles it (its own name and object
+    type).  ``upload`` packs the plan into a device buffer once."""
+
+    def __init__(self, primitive: dict, effects=(), description_id: int = 0, description_name: str = ""):
+        keys = ("length", "width", "taper", "taperStart", "widthRamp")
+        unknown = set(primitive) - set(keys)
+        if unknown:
+            raise ValueError("unknown SplinePrimitive attributes: %s" % sorted(unknown))
+        if len(effects) > _abi.CLASSIC_MAX_FX:
+            raise ValueError("at most %d FX modules" % _abi.CLASSIC_MAX_FX)
+        self.primitive = {k: Expression.classic(v, k) for k, v in primitive.items() if v is not None}
+        self.effects = []
+        for kind, values in effects:
+            if kind == "noise":
+                self.effects.append((kind, {n: Expression.classic(values[n], n, "NoiseFXModule")
+                                            for n in NOISE_FX_ATTRIBUTES}))
+            elif kind == "cut":
+                self.effects.append((kind, {"amount": Expression.classic(values["amount"], "amount", "CutFXModule")}))
+            else:
+                raise ValueError("FX module %r is not supported (NoiseFX and CutFX are)" % (kind,))
+        self.description_id = int(description_id)
+        self.description_name = description_name.encode()
+        self.device: Optional[torch.Tensor] = None
+
+    @property
+    def has_noise(self) -> bool:
+        return any(kind == "noise" for kind, _ in self.effects)
+
+    def descriptor(self) -> _abi.ClassicFxPlan:
+        h = lambda e: e.handle.value if e is not None else None
+        fx = (_abi.ClassicFx * max(1, len(self.effects)))()
+        for i, (kind, values) in enumerate(self.effects):
+            if kind == "noise":
+                fx[i] = _abi.ClassicFx(_abi.CLASSIC_FX_NOISE, 0, *(h(values[n]) for n in NOISE_FX_ATTRIBUTES), None)
+            else:
+                fx[i] = _abi.ClassicFx(_abi.CLASSIC_FX_CUT, 0, None, None, None, None, None, None,
+                                       h(values["amount"]))
+        self._fx = fx
+        p = self.primitive
+        return _abi.ClassicFxPlan(h(p.get("length")), h(p.get("width")), h(p.get("taper")), h(p.get("taperStart")),
+                                  h(p.get("widthRamp")), fx, len(self.effects), self.description_id,
+                                  self.description_name)
+
+    def upload(self, device="cuda", stream: Optional[torch.cuda.Stream] = None) -> torch.Tensor:
+        """Packs the plan into a device buffer (kept as ``self.device``)."""
+        nbytes = int(lib().nxg_classic_fx_plan_bytes())
+        buf = torch.empty(nbytes, dtype=torch.uint8, device=device)
+        assert buf.data_ptr() % 256 == 0
+        desc = self.descriptor()
+        check(lib().nxg_classic_fx_plan_upload(ctypes.byref(desc), buf.data_ptr(), nbytes, _stream_handle(stream)),
+              "nxg_classic_fx_plan_upload")
+        self.device = buf
+        return buf
+
+
+def classic_fx_apply(plan: FxPlan, curves: PackedCurves, surface_tangents: Optional[torch.Tensor] = None,
+                     radius_scale: float = 1.0, first_id: int = 0, noise_domains: Optional[torch.Tensor] = None,
+                     status: Optional[torch.Tensor] = None,
+                     stream: Optional[torch.cuda.Stream] = None) -> torch.Tensor:
+    """Applies the uploaded `plan` to generated curves in place (points,
+    point counts; dropped strands get count 0).  Returns the 2-word device
+    status (error code, failing strands).  Enqueue only."""
+    if plan.device is None:
+        plan.upload(curves.points.device, stream)
+    S, P = int(curves.strand_count), int(curves.cvs_per_strand)
+    if status is None:
+        status = torch.zeros(2, dtype=torch.int32, device=curves.points.device)
+    ptr = lambda t: None if t is None else t.data_ptr()
+    desc = _abi.ClassicFxCurves(curves.points.data_ptr(), curves.point_counts.data_ptr(), curves.roots.data_ptr(),
+                                ptr(surface_tangents), ptr(noise_domains), S, P, first_id, radius_scale)
+    check(lib().nxg_classic_fx_apply(plan.device.data_ptr(), ctypes.byref(desc), status.data_ptr(),
+                                     _stream_handle(stream)), "nxg_classic_fx_apply")
+    return status

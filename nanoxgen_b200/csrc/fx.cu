@@ -1,0 +1,507 @@
+// fx.cu -- the Classic FX passes on sm_100a (nxg_classic_fx_*).
+//
+// A pass over a generated packed curve set that applies a description's
+// Classic runtime plan per strand, in the order of
+// apply_xgen_classic_float_runtime_plan_cpu (src/xgen_classic_runtime.cpp:
+// 1420-1919): the SplinePrimitive length (scale about the root) and width,
+// the drop rule on cLength and the width, the FX modules in the
+// description's order -- NoiseFX mode 0 (apply_noise, :897-1040), CutFX
+// rebuild type 1 (cut_from_tip_and_rebuild, :692-748) -- then the width
+// profile (taper, taperStart, widthRamp).  One thread carries one strand
+// through every step, as the reference's per-strand loop does; the strand's
+// points live in the thread's local arrays (at most NXG_CLASSIC_MAX_FX_CVS).
+// Arithmetic keeps the reference's order and IEEE rounding (uncontracted
+// intrinsics), except the rotation's acos/cos/sin, which come from CUDA's
+// math library, so the frame matches to rounding rather than bit for bit.
+// The packed plan (every program in the device form the exact runtime uses)
+// lives in a caller-owned device buffer, uploaded once.
+#include "classic_eval.cuh"
+#include "expression.h"
+#include "generator_core.cuh"
+#include "nxg_classic.h"
+#include "nxg_internal.h"
+#include "strand_math.cuh"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+namespace nxg {
+namespace dev {
+
+constexpr int kFxMaxCvs = static_cast<int>(NXG_CLASSIC_MAX_FX_CVS);
+constexpr int kFxMaxEffects = static_cast<int>(NXG_CLASSIC_MAX_FX);
+
+// Programs of one effect: NoiseFX mask, magnitude, magnitudeScale,
+// frequency, correlation, preserveLength; CutFX amount in slot 0.
+enum : int { kFxMask = 0, kFxMagnitude, kFxMagnitudeScale, kFxFrequency, kFxCorrelation, kFxPreserve, kFxSlots };
+
+struct FxPlan {
+    uint32_t effect_count;
+    uint32_t effect_type[kFxMaxEffects];
+    uint32_t uses_random;
+    float description_id;   // rand() face seed inputs
+    float patch_seed;
+    DeviceExpression length, width, taper, taper_start, width_ramp;
+    DeviceExpression effect[kFxMaxEffects][kFxSlots];
+};
+
+struct FxArgs {
+    const FxPlan *plan;
+    float4 *points;
+    uint32_t *point_counts;
+    const uint32_t *roots;        // 12 words per strand
+    const float *surface_tangents;
+    const float *noise_domains;
+    uint32_t count, P, first_id;
+    float radius_scale;
+    uint32_t *status;
+};
+
+// The runtime context of one strand (ClassicFloatRuntimeContext,
+// xgen_classic_runtime.h:157-170) for the variables this runtime binds.
+struct FxContext {
+    F3 pref;            // noise($Prefg*k) is evaluated at the root's position
+    float id, u, v, face_seed, c_length, c_width, t;
+};
+
+// Inputs of one program (input_value, xgen_classic_runtime.cpp:503-556).
+__device__ inline void fx_bind(const DeviceExpression &e, const float4 *table, const FxContext &c, float *inputs) {
+    for (uint32_t i = 0; i < e.input_count; ++i) {
+        float x = 0.0f;
+        switch (e.input_binding[i]) {
+            case kBindPrefNoise: {
+                const float f = e.input_frequency[i];
+                x = classic_noise(table, __fmul_rn(c.pref.x, f), __fmul_rn(c.pref.y, f), __fmul_rn(c.pref.z, f));
+                break;
+            }
+            case kBindId: x = c.id; break;
+            case kBindU: x = c.u; break;
+            case kBindV: x = c.v; break;
+            case kBindCLength: x = c.c_length; break;
+            case kBindCWidth: x = c.c_width; break;
+            default: x = 0.0f;
+        }
+        inputs[i] = x;
+    }
+}
+
+// evaluate_runtime_expression for one strand's context; false where the
+// reference throws (non-finite value).
+__device__ inline bool fx_eval(const DeviceExpression &e, const float4 *table, const uint8_t *perm,
+                               const FxContext &c, float *value) {
+    float inputs[kExprMaxInputs];
+    fx_bind(e, table, c, inputs);
+    return evaluate(e, inputs, RootContext{c.u, c.v, c.face_seed, c.t}, perm, value);
+}
+
+// One strand's curve: positions in local arrays.
+struct FxCurve {
+    F3 p[kFxMaxCvs];
+};
+
+__device__ inline float fx_spline_length(const FxCurve &k, int P) {
+    return classic_spline_length_by([&k](int i) { return k.p[i]; }, P);
+}
+
+// curve_polyline_length (xgen_classic_runtime.cpp:681-690).
+__device__ inline float fx_polyline_length(const FxCurve &k, int P) {
+    float length = 0.0f;
+    for (int i = 1; i < P; ++i) {
+        const F3 d = xsub(k.p[i], k.p[i - 1]);
+        length = __fadd_rn(length, __fsqrt_rn(xdot(d, d)));
+    }
+    return length;
+}
+
+// scale_curve (xgen_classic_runtime.cpp:576-585): about the first point.
+__device__ inline void fx_scale(FxCurve &k, int P, float s) {
+    const F3 root = k.p[0];
+    for (int i = 0; i < P; ++i) { k.p[i] = xadd(root, xmul(xsub(k.p[i], root), s)); }
+}
+
+__device__ inline F3 fx_normalize_or(F3 v, F3 fallback) {
+    return xdot(v, v) >= 1.0e-12f ? xnormalize(v) : fallback;
+}
+
+// fallback_surface_u (generate.h:312-316) in the reference's rounding.
+__device__ inline F3 fx_fallback_surface_u(F3 n) {
+    const F3 axis = (n.z > -0.999f && n.z < 0.999f) ? F3{0.0f, 0.0f, 1.0f} : F3{0.0f, 1.0f, 0.0f};
+    return xnormalize(xcross(n, axis));
+}
+
+// apply_noise (xgen_classic_runtime.cpp:897-1040) on one strand: the
+// module's parameters, then the SgCurve frame transported from the surface
+// normal along the current curve with gradient-noise displacement of every
+// CV after the root, then preserveLength.  `c.t` is left at the last CV's t,
+// as the reference's context is.  False where the reference throws.
+__device__ inline bool fx_noise(FxCurve &k, int P, const DeviceExpression *m, const float4 *table,
+                                const uint8_t *perm, FxContext &c, F3 domain_position, F3 surface_normal,
+                                F3 surface_tangent) {
+    float raw = 0.0f;
+    if (!fx_eval(m[kFxMask], table, perm, c, &raw)) { return false; }
+    const float mask = std_clamp(raw, 0.0f, 1.0f);
+    if (!(mask > 1.0e-6f)) { return true; }
+    float frequency = 0.0f, correlation = 0.0f, preserve = 0.0f;
+    if (!fx_eval(m[kFxFrequency], table, perm, c, &raw)) { return false; }
+    frequency = std_max(raw, 0.0f);
+    if (!fx_eval(m[kFxCorrelation], table, perm, c, &raw)) { return false; }
+    correlation = std_clamp(__fmul_rn(raw, 0.01f), 0.0f, 1.0f);
+    if (!fx_eval(m[kFxPreserve], table, perm, c, &raw)) { return false; }
+    preserve = std_clamp(__fmul_rn(raw, 0.01f), 0.0f, 1.0f);
+    if (!isfinite(frequency) || !isfinite(correlation) || !isfinite(preserve)) { return false; }
+    const float original_length = fx_polyline_length(k, P);
+    const float effective_frequency =
+        original_length > 0.0f ? std_max(__fdiv_rn(0.5f, original_length), frequency) : frequency;
+    const float decorrelation = __fsub_rn(1.0f, correlation);
+    const float domain_scale = __fmul_rn(__fmul_rn(100.0f, decorrelation), decorrelation);
+    const F3 domain = xmul(xadd(domain_position, F3{0.419276f, 0.184247f, 0.805721f}), domain_scale);
+    constexpr float kMin = 1.0e-12f;
+    surface_tangent = xdot(surface_tangent, surface_tangent) >= kMin ? xnormalize(surface_tangent)
+                                                                    : fx_fallback_surface_u(surface_normal);
+    F3 previous_base = k.p[0], current_base = k.p[0], next_base = k.p[1];
+    F3 prior_tangent = fx_normalize_or(surface_normal, F3{0.0f, 1.0f, 0.0f});
+    F3 transported = surface_tangent;
+    float travelled = 0.0f;
+    const float last = static_cast<float>(P - 1);
+    for (int cv = 0; cv < P; ++cv) {
+        if (cv > 0) {
+            const F3 d = xsub(current_base, previous_base);
+            travelled = __fadd_rn(travelled, __fsqrt_rn(xdot(d, d)));
+        }
+        F3 next_tangent = prior_tangent;
+        if (cv + 1 < P) {
+            const F3 segment = xsub(next_base, current_base);
+            if (xdot(segment, segment) >= kMin) { next_tangent = xnormalize(segment); }
+        }
+        const F3 axis = xcross(prior_tangent, next_tangent);
+        const float axis_l2 = xdot(axis, axis);
+        const float tangent_dot = std_clamp(xdot(prior_tangent, next_tangent), -1.0f, 1.0f);
+        if (axis_l2 >= kMin) {
+            const F3 rotation_axis = xmul(axis, __fdiv_rn(1.0f, __fsqrt_rn(axis_l2)));
+            const float angle = acosf(tangent_dot);
+            const float cosine = cosf(angle);
+            const float sine = sinf(angle);
+            const F3 rotated = xadd(xadd(xmul(transported, cosine), xmul(xcross(rotation_axis, transported), sine)),
+                                    xmul(rotation_axis, __fmul_rn(xdot(rotation_axis, transported),
+                                                                  __fsub_rn(1.0f, cosine))));
+            transported = fx_normalize_or(rotated, F3{0.0f, 0.0f, 0.0f});
+        }
+        const F3 normal = transported;
+        const F3 binormal = fx_normalize_or(xcross(normal, next_tangent), F3{0.0f, 0.0f, 0.0f});
+        const F3 tangent = xcross(binormal, normal);
+        c.t = __fdiv_rn(static_cast<float>(cv), last);
+        float magnitude = 0.0f, scale = 0.0f;
+        if (!fx_eval(m[kFxMagnitude], table, perm, c, &magnitude)) { return false; }
+        if (!fx_eval(m[kFxMagnitudeScale], table, perm, c, &scale)) { return false; }
+        magnitude = __fmul_rn(__fmul_rn(std_max(magnitude, 0.0f), std_max(scale, 0.0f)), mask);
+        if (!isfinite(magnitude)) { return false; }
+        if (cv > 0) {
+            const float distance = __fmul_rn(travelled, effective_frequency);
+            const float lx = __fmul_rn(
+                __fsub_rn(classic_noise(table, __fadd_rn(domain.x, distance), domain.y, domain.z), 0.5f), magnitude);
+            const float ly = __fmul_rn(
+                __fsub_rn(classic_noise(table, domain.x, __fadd_rn(domain.y, distance), domain.z), 0.5f), magnitude);
+            const float lz = __fmul_rn(
+                __fsub_rn(classic_noise(table, domain.x, domain.y, __fadd_rn(domain.z, distance)), 0.5f), magnitude);
+            k.p[cv] = xadd(xadd(xadd(current_base, xmul(normal, lx)), xmul(binormal, ly)), xmul(tangent, lz));
+        }
+        prior_tangent = next_tangent;
+        previous_base = current_base;
+        if (cv + 1 < P) {
+            current_base = next_base;
+            if (cv + 2 < P) { next_base = k.p[cv + 2]; }
+        }
+    }
+    if (preserve > 0.001f) {
+        const float noisy = fx_polyline_length(k, P);
+        if (noisy > 0.0f) {
+            const float target = __fadd_rn(__fmul_rn(original_length, preserve),
+                                           __fmul_rn(noisy, __fsub_rn(1.0f, preserve)));
+            if (fabsf(__fsub_rn(noisy, target)) >= 0.0001f) { fx_scale(k, P, __fdiv_rn(target, noisy)); }
+        }
+    }
+    return true;
+}
+
+// cut_from_tip_and_rebuild (xgen_classic_runtime.cpp:692-748): walks the
+// curve's spline back from the tip in 2P + 4 steps until `amount` of length
+// is behind, then resamples the remaining span to P CVs.  Returns the cut
+// parameter (0 when the whole curve is cut).
+__device__ inline float fx_cut(FxCurve &k, FxCurve &scratch, int P, float amount) {
+    for (int i = 0; i < P; ++i) { scratch.p[i] = k.p[i]; }
+    const auto source = [&scratch](int i) { return scratch.p[i]; };
+    float cut_parameter = 1.0f;
+    bool collapsed = false;
+    if (amount >= 1.0e-10f) {
+        const float step = __fdiv_rn(1.0f, __fadd_rn(__fmul_rn(2.0f, static_cast<float>(P)), 4.0f));
+        float previous_parameter = 1.0f;
+        F3 previous = scratch.p[P - 1];
+        float accumulated = 0.0f;
+        // The walk ends within 2P + 5 steps (the parameter reaches 0).
+        for (int guard = 0; guard < 4 * kFxMaxCvs + 16; ++guard) {
+            const float parameter = std_max(__fsub_rn(previous_parameter, step), 0.0f);
+            const F3 current = classic_curve_eval_by(source, P, parameter);
+            const F3 d = xsub(previous, current);
+            const float segment = __fsqrt_rn(xdot(d, d));
+            accumulated = __fadd_rn(accumulated, segment);
+            if (accumulated >= amount && segment > 0.0f) {
+                cut_parameter = __fadd_rn(parameter, __fmul_rn(__fdiv_rn(__fsub_rn(accumulated, amount), segment),
+                                                               __fsub_rn(previous_parameter, parameter)));
+                break;
+            }
+            if (parameter <= 1.0e-10f) {
+                cut_parameter = 0.0f;
+                collapsed = true;
+                break;
+            }
+            previous_parameter = parameter;
+            previous = current;
+        }
+    }
+    if (collapsed) {
+        for (int i = 0; i < P; ++i) { k.p[i] = scratch.p[0]; }
+    } else if (cut_parameter > 0.0f) {
+        const float step = __fdiv_rn(cut_parameter, static_cast<float>(P - 1));
+        k.p[0] = scratch.p[0];
+        for (int i = 1; i < P; ++i) {
+            k.p[i] = classic_curve_eval_by(source, P, __fmul_rn(step, static_cast<float>(i)));
+        }
+    }
+    return cut_parameter;
+}
+
+__device__ inline void fx_fail(uint32_t *status, uint32_t code = NXG_ERROR_EXPRESSION_DOMAIN) {
+    atomicCAS(status, 0u, code);
+    atomicAdd(status + 1, 1u);
+}
+
+// One thread per strand (the per-strand body of
+// apply_xgen_classic_float_runtime_plan_cpu, xgen_classic_runtime.cpp:
+// 1614-1868).  A strand whose point count is not P is left alone; a dropped
+// strand's count becomes 0 and its points stay as they were.
+__global__ void __launch_bounds__(128) classic_fx_kernel(const FxArgs k) {
+    __shared__ float4 table[256];
+    __shared__ uint8_t perm[256];
+    stage_classic_tables(table, perm);
+    __syncthreads();
+    const FxPlan &plan = *k.plan;
+    const int P = static_cast<int>(k.P);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < k.count; i += gridDim.x * blockDim.x) {
+        if (k.point_counts[i] != k.P) { continue; }
+        const uint32_t *rw = k.roots + 12u * static_cast<uint64_t>(i);
+        const F3 root_position = {__uint_as_float(rw[0]), __uint_as_float(rw[1]), __uint_as_float(rw[2])};
+        const F3 root_normal = {__uint_as_float(rw[3]), __uint_as_float(rw[4]), __uint_as_float(rw[5])};
+        FxContext c;
+        c.pref = root_position;
+        c.id = static_cast<float>(k.first_id + i);
+        c.u = __uint_as_float(rw[6]);
+        c.v = __uint_as_float(rw[7]);
+        const uint32_t face = rw[11] == kInvalid ? rw[8] : rw[11];  // surface_face_id, else the triangle
+        c.face_seed = plan.uses_random ? classic_face_seed(plan.description_id, plan.patch_seed, face, perm) : 0.0f;
+        c.c_length = 0.0f;
+        c.c_width = 0.0f;
+        c.t = 0.0f;
+        float4 *pts = k.points + static_cast<uint64_t>(i) * k.P;
+        FxCurve curve, scratch;
+        for (int j = 0; j < P; ++j) { curve.p[j] = xyz(pts[j]); }
+        const float first_radius = pts[0].w;
+        c.c_length = fx_spline_length(curve, P);
+        bool ok = true;
+        if (plan.length.present) {
+            float s = 0.0f;
+            ok = fx_eval(plan.length, table, perm, c, &s) && s >= 0.0f;
+            if (ok) {
+                fx_scale(curve, P, s);
+                c.c_length = __fmul_rn(c.c_length, s);
+            }
+        }
+        float raw_width = 0.0f;
+        if (ok) {
+            if (plan.width.present) {
+                ok = fx_eval(plan.width, table, perm, c, &raw_width);
+            } else {
+                raw_width = k.radius_scale > 0.0f ? __fdiv_rn(__fmul_rn(2.0f, first_radius), k.radius_scale) : 0.0f;
+            }
+        }
+        if (!ok) {
+            fx_fail(k.status);
+            continue;
+        }
+        // XgSplinePrimitive::mkGeometry's rejection before any FX.
+        if (c.c_length < 1.0e-4f || raw_width < 1.0e-4f) {
+            k.point_counts[i] = 0u;
+            continue;
+        }
+        c.c_width = raw_width;
+        bool keep = true;
+        bool tangents = true;
+        for (uint32_t e = 0; ok && e < plan.effect_count; ++e) {
+            if (plan.effect_type[e] == NXG_CLASSIC_FX_NOISE && k.surface_tangents == nullptr) {
+                ok = tangents = false;  // NoiseFX needs the strand's surface tangent
+            } else if (plan.effect_type[e] == NXG_CLASSIC_FX_NOISE) {
+                const F3 domain = k.noise_domains
+                    ? F3{k.noise_domains[3u * i], k.noise_domains[3u * i + 1u], k.noise_domains[3u * i + 2u]}
+                    : curve.p[0];
+                const F3 tangent = {k.surface_tangents[3u * i], k.surface_tangents[3u * i + 1u],
+                                    k.surface_tangents[3u * i + 2u]};
+                ok = fx_noise(curve, P, plan.effect[e], table, perm, c, domain, root_normal, tangent);
+            } else {
+                float amount = 0.0f;
+                ok = fx_eval(plan.effect[e][0], table, perm, c, &amount);
+                if (ok && fx_cut(curve, scratch, P, std_max(amount, 0.0f)) < 1.0e-4f) { keep = false; }
+            }
+            if (ok) { c.c_length = fx_spline_length(curve, P); }
+        }
+        float taper = 0.0f, taper_start = 0.0f;
+        if (ok && plan.taper.present) { ok = fx_eval(plan.taper, table, perm, c, &taper); }
+        if (ok && plan.taper_start.present) { ok = fx_eval(plan.taper_start, table, perm, c, &taper_start); }
+        const bool profile = plan.width.present || plan.taper.present || plan.taper_start.present ||
+                             plan.width_ramp.present;
+        const float last = static_cast<float>(P - 1);
+        float radii[kFxMaxCvs];
+        for (int j = 0; ok && j < P; ++j) {
+            float radius = pts[j].w;
+            if (profile) {
+                c.t = __fdiv_rn(static_cast<float>(j), last);
+                float scale = 1.0f;
+                if (c.t > taper_start && taper_start < 1.0f) {
+                    scale = __fmul_rn(scale, __fsub_rn(1.0f, __fmul_rn(taper, __fdiv_rn(__fsub_rn(c.t, taper_start),
+                                                                                          __fsub_rn(1.0f, taper_start)))));
+                }
+                if (plan.width_ramp.present) {
+                    float ramp = 0.0f;
+                    ok = fx_eval(plan.width_ramp, table, perm, c, &ramp);
+                    scale = __fmul_rn(scale, ramp);
+                }
+                const float raw_diameter = __fmul_rn(c.c_width, scale);
+                ok = ok && isfinite(raw_diameter);
+                radius = __fmul_rn(__fmul_rn(0.5f, std_max(raw_diameter, 0.0f)), k.radius_scale);
+            }
+            radii[j] = radius;
+        }
+        if (!ok) {
+            fx_fail(k.status, tangents ? NXG_ERROR_EXPRESSION_DOMAIN : NXG_ERROR_INVALID_ARGUMENT);
+            continue;
+        }
+        for (int j = 0; j < P; ++j) { pts[j] = make_float4(curve.p[j].x, curve.p[j].y, curve.p[j].z, radii[j]); }
+        if (!keep) { k.point_counts[i] = 0u; }
+    }
+}
+
+} // namespace dev
+} // namespace nxg
+
+namespace nxg {
+namespace {
+
+uint32_t pack_optional(const nxg_expression *e, DeviceExpression &d) {
+    std::memset(&d, 0, sizeof d);
+    return e ? pack_device_expression(e, d) : NXG_ERROR_NONE;
+}
+
+// xgen_runtime_face_seed's name seed: the text after the last ':'.
+float name_seed(const char *name) {
+    const char *text = name ? name : "";
+    for (const char *p = text; *p; ++p) {
+        if (*p == ':') { text = p + 1; }
+    }
+    return static_cast<float>(nxg_xgen_string_seed(text));
+}
+
+} // namespace
+} // namespace nxg
+
+extern "C" {
+
+uint64_t nxg_classic_fx_plan_bytes(void) { return (sizeof(nxg::dev::FxPlan) + 255u) / 256u * 256u; }
+
+uint32_t nxg_classic_fx_plan_upload(const nxg_classic_fx_plan *plan, void *device_plan, uint64_t bytes,
+                                    void *stream) {
+    using nxg::dev::FxPlan;
+    if (!plan || !device_plan || bytes < sizeof(FxPlan) || plan->effect_count > NXG_CLASSIC_MAX_FX ||
+        (plan->effect_count && !plan->effects)) {
+        return NXG_ERROR_INVALID_ARGUMENT;
+    }
+    std::vector<unsigned char> storage(sizeof(FxPlan));
+    FxPlan &host = *reinterpret_cast<FxPlan *>(storage.data());
+    uint32_t error = NXG_ERROR_NONE;
+    if ((error = nxg::pack_optional(plan->length, host.length)) ||
+        (error = nxg::pack_optional(plan->width, host.width)) ||
+        (error = nxg::pack_optional(plan->taper, host.taper)) ||
+        (error = nxg::pack_optional(plan->taper_start, host.taper_start)) ||
+        (error = nxg::pack_optional(plan->width_ramp, host.width_ramp))) {
+        return error;
+    }
+    host.effect_count = plan->effect_count;
+    for (uint32_t e = 0; e < plan->effect_count; ++e) {
+        const nxg_classic_fx &fx = plan->effects[e];
+        host.effect_type[e] = fx.type;
+        if (fx.type == NXG_CLASSIC_FX_NOISE) {
+            const nxg_expression *programs[nxg::dev::kFxSlots] = {fx.mask, fx.magnitude, fx.magnitude_scale,
+                                                                 fx.frequency, fx.correlation, fx.preserve_length};
+            for (int k = 0; k < nxg::dev::kFxSlots; ++k) {
+                if (!programs[k]) { return NXG_ERROR_INVALID_ARGUMENT; }
+                if ((error = nxg::pack_optional(programs[k], host.effect[e][k]))) { return error; }
+            }
+        } else if (fx.type == NXG_CLASSIC_FX_CUT) {
+            if (!fx.amount) { return NXG_ERROR_INVALID_ARGUMENT; }
+            if ((error = nxg::pack_optional(fx.amount, host.effect[e][0]))) { return error; }
+        } else {
+            return NXG_ERROR_INVALID_ARGUMENT;
+        }
+    }
+    uint32_t random = host.length.uses_random | host.width.uses_random | host.taper.uses_random |
+                      host.taper_start.uses_random | host.width_ramp.uses_random;
+    for (uint32_t e = 0; e < plan->effect_count; ++e) {
+        for (int k = 0; k < nxg::dev::kFxSlots; ++k) { random |= host.effect[e][k].uses_random; }
+    }
+    host.uses_random = random;
+    host.description_id = static_cast<float>(plan->description_id);
+    host.patch_seed = nxg::name_seed(plan->description_name);
+    nxg::set_last_cuda_error(0);
+    // From pageable memory: the copy is staged before the call returns.
+    return nxg::record_cuda(cudaMemcpyAsync(device_plan, storage.data(), sizeof(FxPlan), cudaMemcpyHostToDevice,
+                                            static_cast<cudaStream_t>(stream)));
+}
+
+uint32_t nxg_classic_fx_apply(const void *device_plan, const nxg_classic_fx_curves *curves,
+                              uint32_t *device_status, void *stream) {
+    if (!device_plan || !curves || !device_status || !curves->points || !curves->point_counts || !curves->roots) {
+        return NXG_ERROR_INVALID_ARGUMENT;
+    }
+    if (curves->cvs_per_strand < 2u || curves->cvs_per_strand > NXG_CLASSIC_MAX_FX_CVS ||
+        !std::isfinite(curves->radius_scale) || curves->radius_scale < 0.0f) {
+        return NXG_ERROR_INVALID_ARGUMENT;
+    }
+    if (reinterpret_cast<std::uintptr_t>(curves->points) % 16u != 0u ||
+        reinterpret_cast<std::uintptr_t>(curves->roots) % 4u != 0u ||
+        reinterpret_cast<std::uintptr_t>(device_plan) % 256u != 0u) {
+        return NXG_ERROR_MISALIGNED_OUTPUT;
+    }
+    if (curves->strand_count == 0u) { return NXG_ERROR_NONE; }
+    nxg::dev::FxArgs k{};
+    k.plan = static_cast<const nxg::dev::FxPlan *>(device_plan);
+    k.points = reinterpret_cast<float4 *>(curves->points);
+    k.point_counts = curves->point_counts;
+    k.roots = static_cast<const uint32_t *>(curves->roots);
+    k.surface_tangents = curves->surface_tangents;
+    k.noise_domains = curves->noise_domains;
+    k.count = curves->strand_count;
+    k.P = curves->cvs_per_strand;
+    k.first_id = curves->first_id;
+    k.radius_scale = curves->radius_scale;
+    k.status = device_status;
+    nxg::set_last_cuda_error(0);
+    const uint32_t threads = 128u;
+    const uint32_t blocks = static_cast<uint32_t>(std::min<uint64_t>(
+        (uint64_t{k.count} + threads - 1u) / threads, static_cast<uint64_t>(nxg::device_sm_count()) * 16u));
+    nxg::dev::classic_fx_kernel<<<blocks, threads, 0, static_cast<cudaStream_t>(stream)>>>(k);
+    return nxg::record_cuda(cudaGetLastError());
+}
+
+} // extern "C"

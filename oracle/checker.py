@@ -409,3 +409,75 @@ class Reference:
             raise ValueError(msg.value.decode())
         k = kept.value
         return points[:k * cvs], counts[:k], roots[:k], uvs[:k]
+
+    # ------------------------------------------------ Classic FX passes
+
+    def classic_plan_fx(self, primitive: dict, effects: list, description_id: int = 0, name: str = "description"):
+        """compile_xgen_classic_float_runtime_plan for a description with the
+        SplinePrimitive attributes in `primitive` (length, width, taper,
+        taperStart, widthRamp) and FX modules `effects`, each ("noise", {mask,
+        magnitude, magnitudeScale, frequency, correlation, preserveLength}) or
+        ("cut", {amount}), in order."""
+        lib = self._expression_prototypes()
+        if not getattr(self, "_fx_ready", False):
+            lib.ref_classic_plan_fx.restype = _P
+            lib.ref_classic_plan_fx.argtypes = [_P, ctypes.c_uint32, _P, _P, ctypes.c_uint32, ctypes.c_char_p,
+                                                ctypes.c_char_p, ctypes.c_uint64]
+            lib.ref_classic_plan_effects.argtypes = [_P, _P]
+            lib.ref_classic_apply_fx.restype = ctypes.c_uint32
+            lib.ref_classic_apply_fx.argtypes = [_P, _P, _P, _P, _P, ctypes.c_uint32, ctypes.c_uint32,
+                                                 ctypes.c_float, _P, ctypes.c_uint64, _P, ctypes.c_uint32, _P,
+                                                 ctypes.c_char_p, ctypes.c_uint64]
+            self._fx_ready = True
+        keep = []
+
+        def text(v):
+            if v is None:
+                return None
+            b = ctypes.c_char_p(v.encode())
+            keep.append(b)
+            return b
+        prim = (ctypes.c_char_p * 5)(*[text(primitive.get(k)) for k in
+                                       ("length", "width", "taper", "taperStart", "widthRamp")])
+        types = np.array([0 if kind == "noise" else 1 for kind, _ in effects] or [0], np.uint32)
+        noise_names = ("mask", "magnitude", "magnitudeScale", "frequency", "correlation", "preserveLength")
+        attrs = []
+        for kind, values in effects:
+            attrs += [text(values.get(n)) for n in noise_names] if kind == "noise" else \
+                [text(values["amount"])] + [None] * 5
+        arr = (ctypes.c_char_p * max(1, len(attrs)))(*attrs)
+        msg = ctypes.create_string_buffer(4096)
+        ptr = lib.ref_classic_plan_fx(ctypes.cast(prim, _P), len(effects), types.ctypes.data, ctypes.cast(arr, _P),
+                                      description_id, name.encode(), msg, 4096)
+        if not ptr:
+            raise ValueError(msg.value.decode())
+        plan = Reference.Plan(self, ptr, [r for r in msg.value.decode().split("\n") if r])
+        counts = np.zeros(3, np.uint32)
+        lib.ref_classic_plan_effects(ptr, counts.ctypes.data)
+        plan.effect_counts = tuple(int(c) for c in counts)
+        return plan
+
+    def classic_apply_fx(self, plan, points, counts, roots, uvs, cvs: int, radius_scale: float, runtime_inputs=None,
+                         surface_tangents=None, workers: int = 1):
+        """apply_xgen_classic_float_runtime_plan_cpu with surface tangents;
+        returns the compacted (points, counts, roots, uvs)."""
+        lib = self.lib
+        points = np.ascontiguousarray(points, np.float32).copy()
+        counts = np.ascontiguousarray(counts, np.uint32).copy()
+        roots = np.ascontiguousarray(roots).copy()
+        uvs = np.ascontiguousarray(uvs, np.float32).copy()
+        S = counts.size
+        inputs = None if runtime_inputs is None else np.ascontiguousarray(runtime_inputs, np.float32)
+        tang = None if surface_tangents is None else np.ascontiguousarray(surface_tangents, np.float32)
+        kept = ctypes.c_uint32()
+        msg = ctypes.create_string_buffer(512)
+        rc = lib.ref_classic_apply_fx(plan.ptr, points.ctypes.data, counts.ctypes.data, roots.ctypes.data,
+                                      uvs.ctypes.data, S, cvs, radius_scale,
+                                      None if inputs is None else inputs.ctypes.data,
+                                      0 if inputs is None else inputs.size,
+                                      None if tang is None else tang.ctypes.data, workers, ctypes.byref(kept),
+                                      msg, 512)
+        if rc != 0:
+            raise ValueError(msg.value.decode())
+        k = kept.value
+        return points[:k * cvs], counts[:k], roots[:k], uvs[:k]

@@ -225,4 +225,101 @@ std::uint32_t ref_classic_apply(const void *plan, float *points, std::uint32_t *
     }
 }
 
+// compile_xgen_classic_float_runtime_plan for a description with the given
+// SplinePrimitive attributes (length, width, taper, taperStart, widthRamp;
+// NULL = absent) and FX modules in order: type 0 NoiseFXModule (mode 0;
+// attributes mask, magnitude, magnitudeScale, frequency, correlation,
+// preserveLength from six strings) or type 1 CutFXModule (rebuildType 1;
+// amount from the first string).  Fallback reasons go to msg.
+void *ref_classic_plan_fx(const char *const *primitive, std::uint32_t effect_count, const std::uint32_t *types,
+                          const char *const *effect_attributes, std::uint32_t description_id,
+                          const char *description_name, char *msg, std::uint64_t cap) {
+    try {
+        ClassicDescription description{};
+        description.name = description_name ? description_name : "description";
+        description.attributes.push_back({"descriptionId", std::to_string(description_id), 0u});
+        ClassicObject spline{};
+        spline.type = "SplinePrimitive";
+        const char *names[5] = {"length", "width", "taper", "taperStart", "widthRamp"};
+        for (int k = 0; k < 5; ++k) {
+            if (primitive[k]) { spline.attributes.push_back({names[k], primitive[k], 0u}); }
+        }
+        description.objects.push_back(spline);
+        const char *noise_names[6] = {"mask", "magnitude", "magnitudeScale", "frequency", "correlation",
+                                      "preserveLength"};
+        for (std::uint32_t e = 0; e < effect_count; ++e) {
+            ClassicObject fx{};
+            const char *const *a = effect_attributes + 6u * e;
+            fx.attributes.push_back({"name", "fx" + std::to_string(e), 0u});
+            if (types[e] == 0u) {
+                fx.type = "NoiseFXModule";
+                fx.attributes.push_back({"mode", "0", 0u});
+                for (int k = 0; k < 6; ++k) { fx.attributes.push_back({noise_names[k], a[k], 0u}); }
+            } else {
+                fx.type = "CutFXModule";
+                fx.attributes.push_back({"rebuildType", "1", 0u});
+                fx.attributes.push_back({"amount", a[0], 0u});
+            }
+            description.objects.push_back(fx);
+        }
+        auto *plan = new ClassicFloatRuntimePlan(compile_xgen_classic_float_runtime_plan(description, {}));
+        std::string reasons;
+        for (const std::string &r : plan->fallback_reasons) { reasons += r + "\n"; }
+        copy_text(reasons, msg, cap);
+        return plan;
+    } catch (const std::exception &e) {
+        copy_text(e.what(), msg, cap);
+        return nullptr;
+    }
+}
+
+// Effects compiled into a plan: count of NoiseFX, CutFX and of all effects.
+void ref_classic_plan_effects(const void *plan, std::uint32_t *out) {
+    const ClassicFloatRuntimePlan &p = *static_cast<const ClassicFloatRuntimePlan *>(plan);
+    out[0] = static_cast<std::uint32_t>(p.noises.size());
+    out[1] = static_cast<std::uint32_t>(p.cuts.size());
+    out[2] = static_cast<std::uint32_t>(p.effects.size());
+}
+
+// ref_classic_apply with one surface tangent per strand ([S] Vec3, may be
+// NULL when the plan has no NoiseFX).
+std::uint32_t ref_classic_apply_fx(const void *plan, float *points, std::uint32_t *counts, void *roots,
+                                   float *root_uvs, std::uint32_t strands, std::uint32_t cvs, float radius_scale,
+                                   const float *runtime_inputs, std::uint64_t runtime_input_count,
+                                   const float *surface_tangents, std::uint32_t workers, std::uint32_t *kept,
+                                   char *msg, std::uint64_t cap) {
+    try {
+        const ClassicFloatRuntimePlan &p = *static_cast<const ClassicFloatRuntimePlan *>(plan);
+        PackedGeneratedCurves curves{};
+        curves.strand_count = strands;
+        curves.cvs_per_strand = cvs;
+        const auto *pts = reinterpret_cast<const PackedCurvePoint *>(points);
+        curves.points.assign(pts, pts + static_cast<std::size_t>(strands) * cvs);
+        curves.point_counts.assign(counts, counts + strands);
+        const auto *rs = static_cast<const RootSample *>(roots);
+        curves.roots.assign(rs, rs + strands);
+        if (root_uvs) {
+            const auto *uv = reinterpret_cast<const Vec2 *>(root_uvs);
+            curves.root_uvs.assign(uv, uv + strands);
+        }
+        std::span<const Vec3> tangents;
+        if (surface_tangents) { tangents = std::span<const Vec3>(reinterpret_cast<const Vec3 *>(surface_tangents), strands); }
+        NanoXGenContext context(workers == 0u ? 1u : workers);
+        apply_xgen_classic_float_runtime_plan_cpu(
+            curves, p, radius_scale, tangents, {}, {}, {},
+            std::span<const float>(runtime_inputs, runtime_inputs ? runtime_input_count : 0u), {}, false,
+            &context);
+        std::memcpy(points, curves.points.data(), curves.points.size() * sizeof(PackedCurvePoint));
+        std::memcpy(counts, curves.point_counts.data(), curves.point_counts.size() * 4u);
+        std::memcpy(roots, curves.roots.data(), curves.roots.size() * sizeof(RootSample));
+        if (root_uvs) { std::memcpy(root_uvs, curves.root_uvs.data(), curves.root_uvs.size() * sizeof(Vec2)); }
+        *kept = curves.strand_count;
+        copy_text("", msg, cap);
+        return 0u;
+    } catch (const std::exception &e) {
+        copy_text(e.what(), msg, cap);
+        return 1u;
+    }
+}
+
 } // extern "C"
