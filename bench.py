@@ -46,7 +46,7 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["nxg", "reference"], default="nxg")
     ap.add_argument("--workload", choices=["large", "batched", "motion", "classic", "batched_classic",
-                                           "asset_build"],
+                                           "asset_build", "classic_fx"],
                     default="large",
                     help="large: the single large description (headline); batched: nine descriptions in one "
                          "persistent launch vs. one launch per description; motion: five shutter samples of the "
@@ -791,6 +791,147 @@ def run_batched_classic(args):
     print(json.dumps(line), flush=True)
 
 
+def _fx_workload():
+    """The Classic FX workload's plan: the cfg5 length and width expressions,
+    a NoiseFX pass, a CutFX pass on a share of cLength and a taper."""
+    from nanoxgen_b200 import fixtures
+    primitive = {"length": fixtures.CLASSIC_LENGTH.replace("*clamp(1-$v,0.2,1)", ""),
+                 "width": fixtures.CLASSIC_WIDTH, "taper": "0.6", "taperStart": "0.3"}
+    effects = [("noise", dict(mask="1", magnitude="0.03", magnitudeScale="1", frequency="8", correlation="30",
+                              preserveLength="40")),
+               ("cut", {"amount": "$cLength*0.1"})]
+    return primitive, effects
+
+
+def run_classic_fx(args):
+    """Classic FX passes over a generated frame: the large description's mesh
+    (200,000 triangles, 4,096 guides), 1,000,000 strands x 24 CVs generated
+    without generator noise, then nxg_classic_fx_apply with the plan of
+    _fx_workload.  A step is generation plus the FX pass (the pass works in
+    place, so each step regenerates its input); the FX kernel is also timed
+    alone.  The CPU baseline is the reference's
+    apply_xgen_classic_float_runtime_plan_cpu on a prefix sample."""
+    import numpy as np
+    import torch
+
+    from nanoxgen_b200 import fixtures
+    from nanoxgen_b200.asset import build_asset
+    from nanoxgen_b200.classic import FxPlan, classic_fx_apply
+    from nanoxgen_b200.generator import DeviceAsset, allocate_outputs, generate_packed, get_tile
+    device = torch.device("cuda", 0)
+    torch.cuda.set_device(device)
+    S = args.strands
+    w = fixtures.large_sphere(strands=S, cvs=24)
+    params = w.params.copy(noise_amplitude=0.0)
+    P = int(params.cvs_per_strand)
+    asset = build_asset(w.build_input, w.stencil_slots)
+    d = DeviceAsset(asset, device)
+    primitive, effects = _fx_workload()
+    plan = FxPlan(primitive, effects, 3, "description")
+    plan.upload(device)
+    points, roots, uvs, counts = allocate_outputs(S, P, device)
+    out = generate_packed(d, params, points=points, roots=roots, root_uvs=uvs, point_counts=counts)
+    torch.cuda.synchronize()
+    # One surface tangent per strand: the root normal crossed with the z axis
+    # (y near the poles), the NoiseFX frame's own fallback direction.
+    rn = out.roots_numpy()["normal"].astype(np.float64)
+    axis = np.where(np.abs(rn[:, 2:3]) < 0.999, [[0.0, 0.0, 1.0]], [[0.0, 1.0, 0.0]])
+    tan = np.cross(rn, axis)
+    tan /= np.maximum(np.linalg.norm(tan, axis=1, keepdims=True), 1e-30)
+    tangents = torch.from_numpy(tan.astype(np.float32)).to(device)
+    status = torch.zeros(2, dtype=torch.int32, device=device)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=device)
+    stream = torch.cuda.current_stream(device)
+    diag = asset.bbox_diagonal()
+
+    def step(ev=None):
+        generate_packed(d, params, points=points, roots=roots, root_uvs=uvs, point_counts=counts, stream=stream)
+        if ev is not None:
+            ev.record(stream)
+        classic_fx_apply(plan, out, tangents, status=status, stream=stream)
+
+    for _ in range(args.warmup):
+        flush.fill_(1)
+        step()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(0)
+    sampler.start()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+           torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for k in range(args.steps):
+        flush.fill_(k & 0xFF)
+        ev[k][0].record(stream)
+        step(ev[k][1])
+        ev[k][2].record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    step_ms = statistics.mean(a.elapsed_time(c) for a, b, c in ev)
+    fx_ms = statistics.mean(b.elapsed_time(c) for a, b, c in ev)
+    st = status.cpu().tolist()
+    kept = int((counts.cpu() != 0).sum())
+    line = {"metric": "points/sec", "value": S * P / (step_ms / 1e3), "unit": "points/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "classic-fx/displaced-sphere-200k-tris/%d-strands-x%d" % (S, P),
+                       "plan": {"primitive": primitive, "effects": [[k, v] for k, v in effects]},
+                       "l2": "flushed between timed steps (256 MiB write)"},
+            "fx_pass": {"ms": fx_ms, "points_per_s": S * P / (fx_ms / 1e3), "strands_kept": kept,
+                        "status": st},
+            "clocks": clocks, "gpu_launches": (kernels_per_step(get_tile(P, False)) + 1) * args.steps}
+    if not args.no_cpu_baseline:
+        from oracle.checker import Reference, reference_available
+        if reference_available():
+            # The reference's runtime on the same input curves: this library's
+            # generated frame (first n strands) before the FX pass.
+            n = min(S, 20_000)
+            generate_packed(d, params, points=points, roots=roots, root_uvs=uvs, point_counts=counts)
+            torch.cuda.synchronize()
+            in_pts = points[:n * P].cpu().numpy().copy()
+            in_roots = out.roots_numpy()[:n].copy()
+            in_uvs = uvs[:n].cpu().numpy().copy()
+            in_counts = counts[:n].cpu().numpy().view(np.uint32).copy()
+            classic_fx_apply(plan, out, tangents, status=status)
+            torch.cuda.synchronize()
+            ref = Reference()
+            rplan = ref.classic_plan_fx(primitive, effects, 3, "description")
+            freqs = rplan.info()["pref_noise"]
+            inputs = (np.stack([ref.classic_noise(in_roots["position"], f) for f in freqs], 1)
+                      if len(freqs) else None)
+            cores = os.cpu_count() or 1
+            apply = lambda: ref.classic_apply_fx(rplan, in_pts, in_counts, in_roots, in_uvs, P, 1.0, inputs,
+                                                 tan[:n].astype(np.float32), workers=cores)
+            got = apply()
+            times = []
+            for _ in range(7):
+                t0 = time.perf_counter()
+                apply()
+                times.append(time.perf_counter() - t0)
+            med, p90 = statistics.median(times), _percentile(times, 0.9)
+            t0 = time.perf_counter()
+            ref.classic_apply_fx(rplan, in_pts, in_counts, in_roots, in_uvs, P, 1.0, inputs,
+                                 tan[:n].astype(np.float32), workers=1)
+            single = time.perf_counter() - t0
+            mine_pts = points[:n * P].cpu().numpy()
+            keep = counts[:n].cpu().numpy() != 0
+            same = bool(keep.sum() == got[1].size)
+            parity = {"strands_checked": n, "same_survivors": same, "tolerance_rel_diag": 1e-5}
+            if same:
+                sel = np.repeat(keep, P)
+                dd = mine_pts[sel, :3].astype(np.float64) - got[0][:, :3]
+                parity["max_error_rel_diag"] = float(np.sqrt((dd * dd).sum(-1)).max(initial=0.0)) / diag
+                parity["max_radius_error_rel_diag"] = float(
+                    np.abs(mine_pts[sel, 3].astype(np.float64) - got[0][:, 3]).max(initial=0.0)) / diag
+            line["cpu_baseline"] = {"value": n * P / med, "unit": "points/s", "cores": cores, "kind": "reference",
+                                    "cpu_model": cpu_model(), "median_s": med, "p90_s": p90,
+                                    "value_p90": n * P / p90,
+                                    "single_thread": {"value": n * P / single, "strands": n, "seconds": single},
+                                    "sample": "the reference's apply_xgen_classic_float_runtime_plan_cpu on the "
+                                              "first %d strands x %d CVs of the generated frame (median of 7 "
+                                              "calls after one warm-up)" % (n, P),
+                                    "parity": parity}
+    print(json.dumps(line), flush=True)
+
+
 def run_asset_build(args):
     """The asset build of the large description's mesh (200,000 triangles,
     4,096 guides): the per-triangle stencil search (stencil.cu) timed alone
@@ -875,6 +1016,8 @@ def main():
         run_motion(args)
     elif args.workload == "asset_build":
         run_asset_build(args)
+    elif args.workload == "classic_fx":
+        run_classic_fx(args)
     else:
         run_gpu_arm(args)
 

@@ -43,6 +43,7 @@ enum : int { kFxMask = 0, kFxMagnitude, kFxMagnitudeScale, kFxFrequency, kFxCorr
 struct FxPlan {
     uint32_t effect_count;
     uint32_t effect_type[kFxMaxEffects];
+    uint32_t length_after[kFxMaxEffects];  // a later program binds cLength
     uint32_t uses_random;
     float description_id;   // rand() face seed inputs
     float patch_seed;
@@ -91,9 +92,10 @@ __device__ inline void fx_bind(const DeviceExpression &e, const float4 *table, c
 }
 
 // evaluate_runtime_expression for one strand's context; false where the
-// reference throws (non-finite value).
-__device__ inline bool fx_eval(const DeviceExpression &e, const float4 *table, const uint8_t *perm,
-                               const FxContext &c, float *value) {
+// reference throws (non-finite value).  One out-of-line copy: the
+// interpreter is large and is called from a dozen places.
+__device__ __noinline__ bool fx_eval(const DeviceExpression &e, const float4 *table, const uint8_t *perm,
+                                     const FxContext &c, float *value) {
     float inputs[kExprMaxInputs];
     fx_bind(e, table, c, inputs);
     return evaluate(e, inputs, RootContext{c.u, c.v, c.face_seed, c.t}, perm, value);
@@ -104,8 +106,85 @@ struct FxCurve {
     F3 p[kFxMaxCvs];
 };
 
-__device__ inline float fx_spline_length(const FxCurve &k, int P) {
-    return classic_spline_length_by([&k](int i) { return k.p[i]; }, P);
+// Strand-independent tables of one launch (P is uniform): the spline
+// length's sample weights, and t = cv / (P - 1) per CV.
+struct FxTables {
+    float4 length_weights[2 * kFxMaxCvs + 4];  // (b0, b1, b2, f^3) at t = k / (2P + 4)
+    int length_span[2 * kFxMaxCvs + 4];
+    float t[kFxMaxCvs];
+};
+
+// The cubic B-spline weights of curve_eval_classic at parameter t in the
+// reference's rounding (the arithmetic of classic_curve_eval_by).
+__device__ inline float4 fx_weights(float t, int P, int &span) {
+    const float scaled = __fmul_rn(t, static_cast<float>(P - 1));
+    span = static_cast<int>(static_cast<uint32_t>(scaled));
+    const float f = __fsub_rn(scaled, static_cast<float>(span));
+    const float f2 = __fmul_rn(f, f);
+    const float f3 = __fmul_rn(f2, f);
+    const float omf = __fsub_rn(1.0f, f);
+    return make_float4(
+        __fmul_rn(__fmul_rn(omf, omf), omf), __fadd_rn(__fsub_rn(__fmul_rn(3.0f, f3), __fmul_rn(6.0f, f2)), 4.0f),
+        __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(-3.0f, f3), __fmul_rn(3.0f, f2)), __fmul_rn(3.0f, f)), 1.0f), f3);
+}
+
+// Filled by the block before its first strand.  Every length sample has
+// 1/132 <= t <= 131/132, away from the end clamps of curve_eval_classic.
+__device__ inline void fx_fill_tables(FxTables &tb, int P) {
+    const int intervals = 2 * P + 4;
+    const float step = __fdiv_rn(1.0f, static_cast<float>(intervals));
+    for (int k = 1 + static_cast<int>(threadIdx.x); k < intervals; k += static_cast<int>(blockDim.x)) {
+        int span = 0;
+        tb.length_weights[k] = fx_weights(__fmul_rn(step, static_cast<float>(k)), P, span);
+        tb.length_span[k] = span;
+    }
+    for (int cv = static_cast<int>(threadIdx.x); cv < P; cv += static_cast<int>(blockDim.x)) {
+        tb.t[cv] = __fdiv_rn(static_cast<float>(cv), static_cast<float>(P - 1));
+    }
+}
+
+// The four control points of span s (the end spans extrapolated), moved
+// along the curve one span at a time as the parameter grows.
+struct FxWindow {
+    F3 p0, p1, p2, p3;
+    int s;
+    __device__ void start(const FxCurve &k, int P) {
+        s = 0;
+        p0 = xsub(xmul(k.p[0], 2.0f), k.p[1]);
+        p1 = k.p[0];
+        p2 = k.p[1];
+        p3 = P == 2 ? xsub(xmul(k.p[1], 2.0f), k.p[0]) : k.p[2];
+    }
+    __device__ void seek(const FxCurve &k, int P, int span) {
+        while (s < span) {
+            p0 = p1;
+            p1 = p2;
+            p2 = p3;
+            ++s;
+            p3 = s + 2 == P ? xsub(xmul(k.p[P - 1], 2.0f), k.p[P - 2]) : k.p[s + 2];
+        }
+    }
+    __device__ F3 at(float4 w) const {
+        return xmul(xadd(xadd(xadd(xmul(p0, w.x), xmul(p1, w.y)), xmul(p2, w.z)), xmul(p3, w.w)), 1.0f / 6.0f);
+    }
+};
+
+// spline_length_classic: 2P + 4 chords of the B-spline, summed in order.
+__device__ inline float fx_spline_length(const FxCurve &k, int P, const FxTables &tb) {
+    const int intervals = 2 * P + 4;
+    FxWindow w;
+    w.start(k, P);
+    F3 previous = k.p[0];
+    float length = 0.0f;
+    for (int j = 1; j < intervals; ++j) {
+        w.seek(k, P, tb.length_span[j]);
+        const F3 current = w.at(tb.length_weights[j]);
+        const F3 d = xsub(current, previous);
+        length = __fadd_rn(length, __fsqrt_rn(xdot(d, d)));
+        previous = current;
+    }
+    const F3 d = xsub(k.p[P - 1], previous);
+    return __fadd_rn(length, __fsqrt_rn(xdot(d, d)));
 }
 
 // curve_polyline_length (xgen_classic_runtime.cpp:681-690).
@@ -140,8 +219,8 @@ __device__ inline F3 fx_fallback_surface_u(F3 n) {
 // CV after the root, then preserveLength.  `c.t` is left at the last CV's t,
 // as the reference's context is.  False where the reference throws.
 __device__ inline bool fx_noise(FxCurve &k, int P, const DeviceExpression *m, const float4 *table,
-                                const uint8_t *perm, FxContext &c, F3 domain_position, F3 surface_normal,
-                                F3 surface_tangent) {
+                                const uint8_t *perm, const FxTables &tb, FxContext &c, F3 domain_position,
+                                F3 surface_normal, F3 surface_tangent) {
     float raw = 0.0f;
     if (!fx_eval(m[kFxMask], table, perm, c, &raw)) { return false; }
     const float mask = std_clamp(raw, 0.0f, 1.0f);
@@ -163,11 +242,22 @@ __device__ inline bool fx_noise(FxCurve &k, int P, const DeviceExpression *m, co
     constexpr float kMin = 1.0e-12f;
     surface_tangent = xdot(surface_tangent, surface_tangent) >= kMin ? xnormalize(surface_tangent)
                                                                     : fx_fallback_surface_u(surface_normal);
+    // magnitude and magnitudeScale depend on the CV only through a ramp of
+    // t; without one their value is the same at every CV and is taken once.
+    const bool per_cv = m[kFxMagnitude].ramp_count != 0u || m[kFxMagnitudeScale].ramp_count != 0u;
+    float magnitude = 0.0f;
+    if (!per_cv) {
+        float scale = 0.0f;
+        c.t = 0.0f;
+        if (!fx_eval(m[kFxMagnitude], table, perm, c, &magnitude)) { return false; }
+        if (!fx_eval(m[kFxMagnitudeScale], table, perm, c, &scale)) { return false; }
+        magnitude = __fmul_rn(__fmul_rn(std_max(magnitude, 0.0f), std_max(scale, 0.0f)), mask);
+        if (!isfinite(magnitude)) { return false; }
+    }
     F3 previous_base = k.p[0], current_base = k.p[0], next_base = k.p[1];
     F3 prior_tangent = fx_normalize_or(surface_normal, F3{0.0f, 1.0f, 0.0f});
     F3 transported = surface_tangent;
     float travelled = 0.0f;
-    const float last = static_cast<float>(P - 1);
     for (int cv = 0; cv < P; ++cv) {
         if (cv > 0) {
             const F3 d = xsub(current_base, previous_base);
@@ -194,12 +284,14 @@ __device__ inline bool fx_noise(FxCurve &k, int P, const DeviceExpression *m, co
         const F3 normal = transported;
         const F3 binormal = fx_normalize_or(xcross(normal, next_tangent), F3{0.0f, 0.0f, 0.0f});
         const F3 tangent = xcross(binormal, normal);
-        c.t = __fdiv_rn(static_cast<float>(cv), last);
-        float magnitude = 0.0f, scale = 0.0f;
-        if (!fx_eval(m[kFxMagnitude], table, perm, c, &magnitude)) { return false; }
-        if (!fx_eval(m[kFxMagnitudeScale], table, perm, c, &scale)) { return false; }
-        magnitude = __fmul_rn(__fmul_rn(std_max(magnitude, 0.0f), std_max(scale, 0.0f)), mask);
-        if (!isfinite(magnitude)) { return false; }
+        c.t = tb.t[cv];
+        if (per_cv) {
+            float scale = 0.0f;
+            if (!fx_eval(m[kFxMagnitude], table, perm, c, &magnitude)) { return false; }
+            if (!fx_eval(m[kFxMagnitudeScale], table, perm, c, &scale)) { return false; }
+            magnitude = __fmul_rn(__fmul_rn(std_max(magnitude, 0.0f), std_max(scale, 0.0f)), mask);
+            if (!isfinite(magnitude)) { return false; }
+        }
         if (cv > 0) {
             const float distance = __fmul_rn(travelled, effective_frequency);
             const float lx = __fmul_rn(
@@ -266,10 +358,23 @@ __device__ inline float fx_cut(FxCurve &k, FxCurve &scratch, int P, float amount
     if (collapsed) {
         for (int i = 0; i < P; ++i) { k.p[i] = scratch.p[0]; }
     } else if (cut_parameter > 0.0f) {
+        // Increasing parameters: the span window moves forward only.
         const float step = __fdiv_rn(cut_parameter, static_cast<float>(P - 1));
+        FxWindow w;
+        w.start(scratch, P);
         k.p[0] = scratch.p[0];
         for (int i = 1; i < P; ++i) {
-            k.p[i] = classic_curve_eval_by(source, P, __fmul_rn(step, static_cast<float>(i)));
+            const float t = __fmul_rn(step, static_cast<float>(i));
+            if (t < 1.0e-7f) {
+                k.p[i] = scratch.p[0];
+            } else if (t > 1.0f - 1.0e-7f) {
+                k.p[i] = scratch.p[P - 1];
+            } else {
+                int span = 0;
+                const float4 weights = fx_weights(t, P, span);
+                w.seek(scratch, P, span);
+                k.p[i] = w.at(weights);
+            }
         }
     }
     return cut_parameter;
@@ -284,13 +389,15 @@ __device__ inline void fx_fail(uint32_t *status, uint32_t code = NXG_ERROR_EXPRE
 // apply_xgen_classic_float_runtime_plan_cpu, xgen_classic_runtime.cpp:
 // 1614-1868).  A strand whose point count is not P is left alone; a dropped
 // strand's count becomes 0 and its points stay as they were.
-__global__ void __launch_bounds__(128) classic_fx_kernel(const FxArgs k) {
+__global__ void __launch_bounds__(128, 5) classic_fx_kernel(const FxArgs k) {
     __shared__ float4 table[256];
     __shared__ uint8_t perm[256];
+    __shared__ FxTables tb;
+    const int P = static_cast<int>(k.P);
     stage_classic_tables(table, perm);
+    fx_fill_tables(tb, P);
     __syncthreads();
     const FxPlan &plan = *k.plan;
-    const int P = static_cast<int>(k.P);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < k.count; i += gridDim.x * blockDim.x) {
         if (k.point_counts[i] != k.P) { continue; }
         const uint32_t *rw = k.roots + 12u * static_cast<uint64_t>(i);
@@ -310,7 +417,7 @@ __global__ void __launch_bounds__(128) classic_fx_kernel(const FxArgs k) {
         FxCurve curve, scratch;
         for (int j = 0; j < P; ++j) { curve.p[j] = xyz(pts[j]); }
         const float first_radius = pts[0].w;
-        c.c_length = fx_spline_length(curve, P);
+        c.c_length = fx_spline_length(curve, P, tb);
         bool ok = true;
         if (plan.length.present) {
             float s = 0.0f;
@@ -349,25 +456,25 @@ __global__ void __launch_bounds__(128) classic_fx_kernel(const FxArgs k) {
                     : curve.p[0];
                 const F3 tangent = {k.surface_tangents[3u * i], k.surface_tangents[3u * i + 1u],
                                     k.surface_tangents[3u * i + 2u]};
-                ok = fx_noise(curve, P, plan.effect[e], table, perm, c, domain, root_normal, tangent);
+                ok = fx_noise(curve, P, plan.effect[e], table, perm, tb, c, domain, root_normal, tangent);
             } else {
                 float amount = 0.0f;
                 ok = fx_eval(plan.effect[e][0], table, perm, c, &amount);
                 if (ok && fx_cut(curve, scratch, P, std_max(amount, 0.0f)) < 1.0e-4f) { keep = false; }
             }
-            if (ok) { c.c_length = fx_spline_length(curve, P); }
+            // cLength after this effect, where a later program reads it.
+            if (ok && plan.length_after[e]) { c.c_length = fx_spline_length(curve, P, tb); }
         }
         float taper = 0.0f, taper_start = 0.0f;
         if (ok && plan.taper.present) { ok = fx_eval(plan.taper, table, perm, c, &taper); }
         if (ok && plan.taper_start.present) { ok = fx_eval(plan.taper_start, table, perm, c, &taper_start); }
         const bool profile = plan.width.present || plan.taper.present || plan.taper_start.present ||
                              plan.width_ramp.present;
-        const float last = static_cast<float>(P - 1);
         float radii[kFxMaxCvs];
         for (int j = 0; ok && j < P; ++j) {
             float radius = pts[j].w;
             if (profile) {
-                c.t = __fdiv_rn(static_cast<float>(j), last);
+                c.t = tb.t[j];
                 float scale = 1.0f;
                 if (c.t > taper_start && taper_start < 1.0f) {
                     scale = __fmul_rn(scale, __fsub_rn(1.0f, __fmul_rn(taper, __fdiv_rn(__fsub_rn(c.t, taper_start),
@@ -454,6 +561,13 @@ uint32_t nxg_classic_fx_plan_upload(const nxg_classic_fx_plan *plan, void *devic
         } else {
             return NXG_ERROR_INVALID_ARGUMENT;
         }
+    }
+    // cLength is recomputed after an effect only for a program that follows
+    // it: a later effect's, or the width profile's.
+    uint32_t later = host.taper.uses_clength | host.taper_start.uses_clength | host.width_ramp.uses_clength;
+    for (uint32_t e = plan->effect_count; e-- > 0u;) {
+        host.length_after[e] = later;
+        for (int k = 0; k < nxg::dev::kFxSlots; ++k) { later |= host.effect[e][k].uses_clength; }
     }
     uint32_t random = host.length.uses_random | host.width.uses_random | host.taper.uses_random |
                       host.taper_start.uses_random | host.width_ramp.uses_random;
