@@ -156,14 +156,17 @@ uint32_t nxg_generate_batched_classic(const nxg_device_asset_desc *assets, const
 #define NXG_CLASSIC_MAX_FX 8u
 #define NXG_CLASSIC_MAX_FX_CVS 64u
 
-enum { NXG_CLASSIC_FX_NOISE = 0, NXG_CLASSIC_FX_CUT = 1 };
+enum { NXG_CLASSIC_FX_NOISE = 0, NXG_CLASSIC_FX_CUT = 1, NXG_CLASSIC_FX_CLUMP = 2 };
 
 typedef struct nxg_classic_fx {
-    uint32_t type;                         /* NXG_CLASSIC_FX_NOISE or NXG_CLASSIC_FX_CUT */
+    uint32_t type;                         /* NXG_CLASSIC_FX_NOISE, _CUT or _CLUMP */
     uint32_t reserved;
-    /* NoiseFXModule attributes (type NOISE), all required */
+    /* NoiseFXModule attributes (type NOISE), all required; `mask` is also
+       ClumpingFXModule.mask */
     const nxg_expression *mask, *magnitude, *magnitude_scale, *frequency, *correlation, *preserve_length;
     const nxg_expression *amount;          /* CutFXModule.amount (type CUT) */
+    /* ClumpingFXModule attributes (type CLUMP, with mask), all required */
+    const nxg_expression *clump, *clump_scale, *noise, *noise_scale, *noise_frequency, *noise_correlation;
 } nxg_classic_fx;
 
 typedef struct nxg_classic_fx_plan {
@@ -186,6 +189,29 @@ uint64_t nxg_classic_fx_plan_bytes(void);
 uint32_t nxg_classic_fx_plan_upload(const nxg_classic_fx_plan *plan, void *device_plan, uint64_t bytes,
                                     void *stream);
 
+/* The clump guides of one ClumpingFXModule (ClassicClumpRuntimeData,
+ * xgen_classic_runtime.h:59-88, without the root-relative copies), all
+ * device arrays.  Each guide has cvs_per_strand CVs. */
+typedef struct nxg_classic_clump_guides {
+    const float *axes;                /* guide_count x P x 3: the guide CVs (before the rebuild) */
+    const float *render_axes;         /* guide_count x P x 3: from nxg_classic_clump_prepare */
+    const float *spline_lengths;      /* guide_count: from nxg_classic_clump_prepare */
+    const float *normals;             /* guide_count x 3 */
+    const float *tangents;            /* guide_count x 3 */
+    const float *reference_positions; /* guide_count x 3 guide-noise domains, or NULL (the first CV) */
+    const float *uvs;                 /* guide_count x 2 */
+    const uint32_t *random_prefixes;  /* guide_count SeExpr prefixes (rand() in the guide noise) */
+    const uint32_t *strand_guides;    /* strand_count: the strand's guide, or NXG_INVALID_INDEX */
+    uint32_t guide_count;
+    uint32_t reserved;
+} nxg_classic_clump_guides;
+
+/* prepare_xgen_classic_clump_runtime_data (xgen_classic_runtime.cpp:839-892)
+ * on the device: each guide's CVs resampled at cv/(P-1) (the ends kept) into
+ * render_axes, and its spline length.  P >= 3; enqueue only. */
+uint32_t nxg_classic_clump_prepare(const float *axes, uint32_t guide_count, uint32_t cvs_per_guide,
+                                   float *render_axes, float *spline_lengths, void *stream);
+
 typedef struct nxg_classic_fx_curves {
     float *points;                 /* strand_count x cvs_per_strand float4 (position, radius), in/out */
     uint32_t *point_counts;        /* in/out; a strand whose count is not cvs_per_strand is skipped, a
@@ -197,13 +223,20 @@ typedef struct nxg_classic_fx_curves {
     uint32_t cvs_per_strand;       /* 2 .. NXG_CLASSIC_MAX_FX_CVS */
     uint32_t first_id;             /* $id of strand 0 */
     float radius_scale;
+    const uint32_t *random_prefixes;          /* strand_count SeExpr prefixes; required when a program
+                                                 calls rand() */
+    const nxg_classic_clump_guides *clumps;   /* host array, one per CLUMP effect in plan order */
+    uint32_t clump_count;
+    uint32_t reserved;
 } nxg_classic_fx_curves;
 
 /* Applies the uploaded plan to `curves` on `stream` (enqueue only).
  * device_status (2 x uint32, zeroed by the caller) receives
  * NXG_ERROR_EXPRESSION_DOMAIN and the number of failing strands where an
  * expression yields a non-finite value or a negative length (the reference
- * throws there). */
+ * throws there), or NXG_ERROR_INVALID_ARGUMENT where a strand needs an
+ * input that was not given (surface tangents for NoiseFX, random prefixes
+ * for rand(), a clump guide index beyond guide_count). */
 uint32_t nxg_classic_fx_apply(const void *device_plan, const nxg_classic_fx_curves *curves,
                               uint32_t *device_status, void *stream);
 

@@ -182,10 +182,22 @@ class ClassicApplyDesc(ctypes.Structure):
 
 
 class ClassicFx(ctypes.Structure):
-    """nxg_classic_fx (nxg_classic.h): one NoiseFX or CutFX module."""
+    """nxg_classic_fx (nxg_classic.h): one NoiseFX, CutFX or ClumpingFX module."""
     _fields_ = [("type", ctypes.c_uint32), ("reserved", ctypes.c_uint32), ("mask", ctypes.c_void_p),
                 ("magnitude", ctypes.c_void_p), ("magnitude_scale", ctypes.c_void_p), ("frequency", ctypes.c_void_p),
-                ("correlation", ctypes.c_void_p), ("preserve_length", ctypes.c_void_p), ("amount", ctypes.c_void_p)]
+                ("correlation", ctypes.c_void_p), ("preserve_length", ctypes.c_void_p), ("amount", ctypes.c_void_p),
+                ("clump", ctypes.c_void_p), ("clump_scale", ctypes.c_void_p), ("noise", ctypes.c_void_p),
+                ("noise_scale", ctypes.c_void_p), ("noise_frequency", ctypes.c_void_p),
+                ("noise_correlation", ctypes.c_void_p)]
+
+
+class ClassicClumpGuides(ctypes.Structure):
+    """nxg_classic_clump_guides (nxg_classic.h): one ClumpingFX module's guides (device arrays)."""
+    _fields_ = [("axes", ctypes.c_void_p), ("render_axes", ctypes.c_void_p), ("spline_lengths", ctypes.c_void_p),
+                ("normals", ctypes.c_void_p), ("tangents", ctypes.c_void_p),
+                ("reference_positions", ctypes.c_void_p), ("uvs", ctypes.c_void_p),
+                ("random_prefixes", ctypes.c_void_p), ("strand_guides", ctypes.c_void_p),
+                ("guide_count", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
 
 
 class ClassicFxPlan(ctypes.Structure):
@@ -201,11 +213,14 @@ class ClassicFxCurves(ctypes.Structure):
     _fields_ = [("points", ctypes.c_void_p), ("point_counts", ctypes.c_void_p), ("roots", ctypes.c_void_p),
                 ("surface_tangents", ctypes.c_void_p), ("noise_domains", ctypes.c_void_p),
                 ("strand_count", ctypes.c_uint32), ("cvs_per_strand", ctypes.c_uint32),
-                ("first_id", ctypes.c_uint32), ("radius_scale", ctypes.c_float)]
+                ("first_id", ctypes.c_uint32), ("radius_scale", ctypes.c_float),
+                ("random_prefixes", ctypes.c_void_p), ("clumps", ctypes.POINTER(ClassicClumpGuides)),
+                ("clump_count", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
 
 
 CLASSIC_FX_NOISE = 0
 CLASSIC_FX_CUT = 1
+CLASSIC_FX_CLUMP = 2
 CLASSIC_MAX_FX = 8
 CLASSIC_MAX_FX_CVS = 64
 
@@ -385,6 +400,7 @@ _SIGNATURES = {
     "nxg_classic_fx_plan_bytes": (ctypes.c_uint64, []),
     "nxg_classic_fx_plan_upload": (ctypes.c_uint32, [ctypes.POINTER(ClassicFxPlan), _P, ctypes.c_uint64, _P]),
     "nxg_classic_fx_apply": (ctypes.c_uint32, [_P, ctypes.POINTER(ClassicFxCurves), _P, _P]),
+    "nxg_classic_clump_prepare": (ctypes.c_uint32, [_P, ctypes.c_uint32, ctypes.c_uint32, _P, _P, _P]),
     "nxg_classic_root_scalars": (ctypes.c_uint32, [ctypes.POINTER(DeviceAssetDesc), ctypes.POINTER(GenerationParams),
                                                    ctypes.POINTER(ClassicScalarPlan), ctypes.c_uint32,
                                                    ctypes.c_uint32, _P, _P, _P]),

@@ -177,6 +177,7 @@ def generate_packed_classic(dasset: DeviceAsset, params: GenerationParams, scala
 # ------------------------------------------------------------- FX passes
 
 NOISE_FX_ATTRIBUTES = ("mask", "magnitude", "magnitudeScale", "frequency", "correlation", "preserveLength")
+CLUMP_FX_ATTRIBUTES = ("mask", "clump", "clumpScale", "noise", "noiseScale", "noiseFrequency", "noiseCorrelation")
 
 
 class FxPlan:
@@ -184,9 +185,11 @@ class FxPlan:
     SplinePrimitive length, width, taper, taperStart and widthRamp
     expressions (each optional) and its FX modules in order, each
     ``("noise", {mask, magnitude, magnitudeScale, frequency, correlation,
-    preserveLength})`` or ``("cut", {"amount": ...})``; every attribute is
-    compiled as the Classic runtime compiles it (its own name and object
-    type).  ``upload`` packs the plan into a device buffer once."""
+    preserveLength})``, ``("cut", {"amount": ...})`` or ``("clump", {mask,
+    clump, clumpScale, noise, noiseScale, noiseFrequency,
+    noiseCorrelation})``; every attribute is compiled as the Classic runtime
+    compiles it (its own name and object type).  ``upload`` packs the plan
+    into a device buffer once."""
 
     def __init__(self, primitive: dict, effects=(), description_id: int = 0, description_name: str = ""):
         keys = ("length", "width", "taper", "taperStart", "widthRamp")
@@ -203,8 +206,11 @@ class FxPlan:
                                             for n in NOISE_FX_ATTRIBUTES}))
             elif kind == "cut":
                 self.effects.append((kind, {"amount": Expression.classic(values["amount"], "amount", "CutFXModule")}))
+            elif kind == "clump":
+                self.effects.append((kind, {n: Expression.classic(values[n], n, "ClumpingFXModule")
+                                            for n in CLUMP_FX_ATTRIBUTES}))
             else:
-                raise ValueError("FX module %r is not supported (NoiseFX and CutFX are)" % (kind,))
+                raise ValueError("FX module %r is not supported (NoiseFX, CutFX and ClumpingFX are)" % (kind,))
         self.description_id = int(description_id)
         self.description_name = description_name.encode()
         self.device: Optional[torch.Tensor] = None
@@ -213,15 +219,27 @@ class FxPlan:
     def has_noise(self) -> bool:
         return any(kind == "noise" for kind, _ in self.effects)
 
+    @property
+    def clump_count(self) -> int:
+        return sum(kind == "clump" for kind, _ in self.effects)
+
+    @property
+    def uses_random(self) -> bool:
+        exprs = list(self.primitive.values()) + [e for _, v in self.effects for e in v.values()]
+        return any(e.info().random_call_count != 0 for e in exprs)
+
     def descriptor(self) -> _abi.ClassicFxPlan:
         h = lambda e: e.handle.value if e is not None else None
         fx = (_abi.ClassicFx * max(1, len(self.effects)))()
         for i, (kind, values) in enumerate(self.effects):
             if kind == "noise":
                 fx[i] = _abi.ClassicFx(_abi.CLASSIC_FX_NOISE, 0, *(h(values[n]) for n in NOISE_FX_ATTRIBUTES), None)
-            else:
+            elif kind == "cut":
                 fx[i] = _abi.ClassicFx(_abi.CLASSIC_FX_CUT, 0, None, None, None, None, None, None,
                                        h(values["amount"]))
+            else:
+                mask, *rest = (h(values[n]) for n in CLUMP_FX_ATTRIBUTES)
+                fx[i] = _abi.ClassicFx(_abi.CLASSIC_FX_CLUMP, 0, mask, None, None, None, None, None, None, *rest)
         self._fx = fx
         p = self.primitive
         return _abi.ClassicFxPlan(h(p.get("length")), h(p.get("width")), h(p.get("taper")), h(p.get("taperStart")),
@@ -240,21 +258,61 @@ class FxPlan:
         return buf
 
 
+class ClumpGuides:
+    """One ClumpingFX module's guides on the device (ClassicClumpRuntimeData,
+    xgen_classic_runtime.h:59-88, world space): guide CVs [G, P, 3] (before
+    the rebuild), normals and tangents [G, 3], uvs [G, 2], SeExpr prefixes
+    [G], the guide of every strand [S] (NXG_INVALID_INDEX = none) and,
+    optionally, the guide-noise domain positions [G, 3].  The render axes and
+    spline lengths are prepared on the device (nxg_classic_clump_prepare)."""
+
+    def __init__(self, axes, normals, tangents, uvs, random_prefixes, strand_guides, reference_positions=None,
+                 device="cuda", stream: Optional[torch.cuda.Stream] = None):
+        f32 = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.float32)).to(device)
+        u32 = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.uint32).view(np.int32)).to(device)
+        self.axes = f32(axes)
+        if self.axes.dim() != 3 or self.axes.shape[2] != 3:
+            raise ValueError("guide axes are [guides, cvs, 3]")
+        G, P = int(self.axes.shape[0]), int(self.axes.shape[1])
+        self.normals, self.tangents, self.uvs = f32(normals), f32(tangents), f32(uvs)
+        self.random_prefixes, self.strand_guides = u32(random_prefixes), u32(strand_guides)
+        self.reference_positions = None if reference_positions is None else f32(reference_positions)
+        self.render_axes = torch.empty_like(self.axes)
+        self.spline_lengths = torch.empty(G, dtype=torch.float32, device=self.axes.device)
+        check(lib().nxg_classic_clump_prepare(self.axes.data_ptr(), G, P, self.render_axes.data_ptr(),
+                                              self.spline_lengths.data_ptr(), _stream_handle(stream)),
+              "nxg_classic_clump_prepare")
+        self.guide_count = G
+
+    def descriptor(self) -> _abi.ClassicClumpGuides:
+        ptr = lambda t: None if t is None else t.data_ptr()
+        return _abi.ClassicClumpGuides(self.axes.data_ptr(), self.render_axes.data_ptr(),
+                                       self.spline_lengths.data_ptr(), self.normals.data_ptr(),
+                                       self.tangents.data_ptr(), ptr(self.reference_positions), self.uvs.data_ptr(),
+                                       self.random_prefixes.data_ptr(), self.strand_guides.data_ptr(),
+                                       self.guide_count, 0)
+
+
 def classic_fx_apply(plan: FxPlan, curves: PackedCurves, surface_tangents: Optional[torch.Tensor] = None,
                      radius_scale: float = 1.0, first_id: int = 0, noise_domains: Optional[torch.Tensor] = None,
-                     status: Optional[torch.Tensor] = None,
-                     stream: Optional[torch.cuda.Stream] = None) -> torch.Tensor:
+                     status: Optional[torch.Tensor] = None, stream: Optional[torch.cuda.Stream] = None,
+                     random_prefixes: Optional[torch.Tensor] = None, clumps=()) -> torch.Tensor:
     """Applies the uploaded `plan` to generated curves in place (points,
-    point counts; dropped strands get count 0).  Returns the 2-word device
-    status (error code, failing strands).  Enqueue only."""
+    point counts; dropped strands get count 0).  `random_prefixes` (one
+    SeExpr prefix per strand) is required when a program calls rand();
+    `clumps` holds one ClumpGuides per ClumpingFX module, in plan order.
+    Returns the 2-word device status (error code, failing strands).
+    Enqueue only."""
     if plan.device is None:
         plan.upload(curves.points.device, stream)
     S, P = int(curves.strand_count), int(curves.cvs_per_strand)
     if status is None:
         status = torch.zeros(2, dtype=torch.int32, device=curves.points.device)
     ptr = lambda t: None if t is None else t.data_ptr()
+    guides = (_abi.ClassicClumpGuides * max(1, len(clumps)))(*(c.descriptor() for c in clumps))
     desc = _abi.ClassicFxCurves(curves.points.data_ptr(), curves.point_counts.data_ptr(), curves.roots.data_ptr(),
-                                ptr(surface_tangents), ptr(noise_domains), S, P, first_id, radius_scale)
+                                ptr(surface_tangents), ptr(noise_domains), S, P, first_id, radius_scale,
+                                ptr(random_prefixes), guides, len(clumps), 0)
     check(lib().nxg_classic_fx_apply(plan.device.data_ptr(), ctypes.byref(desc), status.data_ptr(),
                                      _stream_handle(stream)), "nxg_classic_fx_apply")
     return status

@@ -152,8 +152,12 @@ __device__ inline float ramp_value(const ExprRampPoint *pts, uint32_t n, float t
     return std_clamp(value, 0.0f, 1.0f);
 }
 
+// has_prefix: rand() draws from a per-primitive SeExpr prefix (the Classic
+// runtime's random_prefixes) instead of (u, v, face seed).
 struct RootContext {
     float u, v, face_seed, t;
+    uint32_t prefix = 0u;
+    uint32_t has_prefix = 0u;
 };
 
 // One SSA program for one root.  Returns false where the reference throws
@@ -195,9 +199,13 @@ __device__ inline bool evaluate(const DeviceExpression &e, const float *inputs, 
                 break;
             }
             case kOpRandom: {
-                // Without a per-root SeExpr prefix: hash(u, v, face seed, site seed[, seed])
+                // With a SeExpr prefix: the LCG over (prefix, the site's
+                // component); without: hash(u, v, face seed, site seed)
+                // (xgen_expression.cpp:1063-1088); then the explicit seed.
                 const bool seeded = n == 1 || n == 3;
-                uint32_t state = hash_step(hash_step(hash_step(hash_step(0u, c.u), c.v), c.face_seed), in.immediate);
+                uint32_t state = c.has_prefix
+                    ? c.prefix * kLcgA + in.auxiliary + kLcgC
+                    : hash_step(hash_step(hash_step(hash_step(0u, c.u), c.v), c.face_seed), in.immediate);
                 if (seeded) { state = hash_step(state, vals[arg[n - 1]]); }
                 value = hash_finish(state, perm);
                 if (n >= 2) {

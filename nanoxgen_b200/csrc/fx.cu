@@ -37,8 +37,12 @@ constexpr int kFxMaxCvs = static_cast<int>(NXG_CLASSIC_MAX_FX_CVS);
 constexpr int kFxMaxEffects = static_cast<int>(NXG_CLASSIC_MAX_FX);
 
 // Programs of one effect: NoiseFX mask, magnitude, magnitudeScale,
-// frequency, correlation, preserveLength; CutFX amount in slot 0.
-enum : int { kFxMask = 0, kFxMagnitude, kFxMagnitudeScale, kFxFrequency, kFxCorrelation, kFxPreserve, kFxSlots };
+// frequency, correlation, preserveLength; CutFX amount in slot 0;
+// ClumpingFX mask, clump, clumpScale, noise, noiseScale, noiseFrequency,
+// noiseCorrelation.
+enum : int { kFxMask = 0, kFxMagnitude, kFxMagnitudeScale, kFxFrequency, kFxCorrelation, kFxPreserve };
+enum : int { kClumpMask = 0, kClumpAmount, kClumpScale, kClumpNoise, kClumpNoiseScale, kClumpNoiseFrequency,
+             kClumpNoiseCorrelation, kFxSlots };
 
 struct FxPlan {
     uint32_t effect_count;
@@ -61,6 +65,9 @@ struct FxArgs {
     uint32_t count, P, first_id;
     float radius_scale;
     uint32_t *status;
+    const uint32_t *random_prefixes;
+    uint32_t clump_count;
+    nxg_classic_clump_guides clumps[kFxMaxEffects];
 };
 
 // The runtime context of one strand (ClassicFloatRuntimeContext,
@@ -68,6 +75,7 @@ struct FxArgs {
 struct FxContext {
     F3 pref;            // noise($Prefg*k) is evaluated at the root's position
     float id, u, v, face_seed, c_length, c_width, t;
+    uint32_t prefix, has_prefix;  // rand()'s SeExpr prefix
 };
 
 // Inputs of one program (input_value, xgen_classic_runtime.cpp:503-556).
@@ -98,7 +106,7 @@ __device__ __noinline__ bool fx_eval(const DeviceExpression &e, const float4 *ta
                                      const FxContext &c, float *value) {
     float inputs[kExprMaxInputs];
     fx_bind(e, table, c, inputs);
-    return evaluate(e, inputs, RootContext{c.u, c.v, c.face_seed, c.t}, perm, value);
+    return evaluate(e, inputs, RootContext{c.u, c.v, c.face_seed, c.t, c.prefix, c.has_prefix}, perm, value);
 }
 
 // One strand's curve: positions in local arrays.
@@ -320,6 +328,28 @@ __device__ inline bool fx_noise(FxCurve &k, int P, const DeviceExpression *m, co
     return true;
 }
 
+// The rebuild of both cuts: `source` resampled to P CVs at parameters
+// i * cut / (P - 1), increasing, so the span window moves forward only.
+__device__ inline void fx_resample(FxCurve &k, const FxCurve &source, int P, float cut) {
+    const float step = __fdiv_rn(cut, static_cast<float>(P - 1));
+    FxWindow w;
+    w.start(source, P);
+    k.p[0] = source.p[0];
+    for (int i = 1; i < P; ++i) {
+        const float t = __fmul_rn(step, static_cast<float>(i));
+        if (t < 1.0e-7f) {
+            k.p[i] = source.p[0];
+        } else if (t > 1.0f - 1.0e-7f) {
+            k.p[i] = source.p[P - 1];
+        } else {
+            int span = 0;
+            const float4 weights = fx_weights(t, P, span);
+            w.seek(source, P, span);
+            k.p[i] = w.at(weights);
+        }
+    }
+}
+
 // cut_from_tip_and_rebuild (xgen_classic_runtime.cpp:692-748): walks the
 // curve's spline back from the tip in 2P + 4 steps until `amount` of length
 // is behind, then resamples the remaining span to P CVs.  Returns the cut
@@ -358,26 +388,181 @@ __device__ inline float fx_cut(FxCurve &k, FxCurve &scratch, int P, float amount
     if (collapsed) {
         for (int i = 0; i < P; ++i) { k.p[i] = scratch.p[0]; }
     } else if (cut_parameter > 0.0f) {
-        // Increasing parameters: the span window moves forward only.
-        const float step = __fdiv_rn(cut_parameter, static_cast<float>(P - 1));
-        FxWindow w;
-        w.start(scratch, P);
-        k.p[0] = scratch.p[0];
-        for (int i = 1; i < P; ++i) {
-            const float t = __fmul_rn(step, static_cast<float>(i));
-            if (t < 1.0e-7f) {
-                k.p[i] = scratch.p[0];
-            } else if (t > 1.0f - 1.0e-7f) {
-                k.p[i] = scratch.p[P - 1];
-            } else {
-                int span = 0;
-                const float4 weights = fx_weights(t, P, span);
-                w.seek(scratch, P, span);
-                k.p[i] = w.at(weights);
-            }
-        }
+        fx_resample(k, scratch, P, cut_parameter);
     }
     return cut_parameter;
+}
+
+// rotate_between (xgen_classic_runtime.cpp:1103-1116): `value` turned about
+// from x to by `fraction` of the angle between them.
+__device__ inline F3 fx_rotate_between(F3 value, F3 from, F3 to, float fraction) {
+    F3 axis = xcross(from, to);
+    const float axis_l2 = xdot(axis, axis);
+    if (!(axis_l2 >= 1.0e-12f)) { return value; }
+    axis = xmul(axis, __fdiv_rn(1.0f, __fsqrt_rn(axis_l2)));
+    const float angle = __fmul_rn(acosf(std_clamp(xdot(from, to), -1.0f, 1.0f)), fraction);
+    const float cosine = cosf(angle);
+    const float sine = sinf(angle);
+    return xadd(xadd(xmul(value, cosine), xmul(xcross(axis, value), sine)),
+                xmul(axis, __fmul_rn(xdot(axis, value), __fsub_rn(1.0f, cosine))));
+}
+
+// cut_to_length_and_rebuild (xgen_classic_runtime.cpp:749-800): keeps the
+// curve up to `target` of its length measured from the root, searching the
+// 2P + 4 spline samples of the length measure, then rebuilds P CVs on
+// [0, cut].  The curve is rebuilt even when the whole of it is kept.
+__device__ inline void fx_cut_to_length(FxCurve &k, FxCurve &scratch, int P, float target, const FxTables &tb) {
+    for (int i = 0; i < P; ++i) { scratch.p[i] = k.p[i]; }
+    if (target <= 1.0e-10f) {
+        for (int i = 1; i < P; ++i) { k.p[i] = scratch.p[0]; }
+        return;
+    }
+    const int intervals = 2 * P + 4;
+    const float step = __fdiv_rn(1.0f, static_cast<float>(intervals));
+    float previous_parameter = 0.0f, accumulated = 0.0f, cut = 1.0f;
+    F3 previous = scratch.p[0];
+    FxWindow w;
+    w.start(scratch, P);
+    for (int sample = 1; sample <= intervals; ++sample) {
+        const bool last = sample == intervals;
+        const float parameter = last ? 1.0f : __fmul_rn(step, static_cast<float>(sample));
+        F3 current = scratch.p[P - 1];
+        if (!last) {
+            w.seek(scratch, P, tb.length_span[sample]);
+            current = w.at(tb.length_weights[sample]);
+        }
+        const F3 d = xsub(current, previous);
+        const float segment = __fsqrt_rn(xdot(d, d));
+        accumulated = __fadd_rn(accumulated, segment);
+        if (accumulated >= target && segment > 0.0f) {
+            cut = __fsub_rn(parameter, __fmul_rn(__fdiv_rn(__fsub_rn(accumulated, target), segment),
+                                                 __fsub_rn(parameter, previous_parameter)));
+            break;
+        }
+        previous_parameter = parameter;
+        previous = current;
+    }
+    fx_resample(k, scratch, P, cut);
+}
+
+// The ClumpingFX step for one strand (xgen_classic_runtime.cpp:1680-1788),
+// with world-space guides: the mask; the guide-noise axis of
+// build_clump_noise_axis (:1041-1181) in the guide's context (its uv and
+// SeExpr prefix); the cut to the guide's length; the pull of every CV after
+// the root toward the guide's rebuilt CV by mask * clump * (1 - 2 clumpScale);
+// the guide noise added on top.  The noise axis depends only on the guide's
+// CVs, so it is computed in the same pass over the CVs as the pull.
+// `clumped` reports whether the curve changed (the reference recomputes
+// cLength only then).  False where the reference throws; *code says why.
+__device__ __noinline__ bool fx_clump(FxCurve &k, FxCurve &scratch, int P, const DeviceExpression *m,
+                                const nxg_classic_clump_guides &cg, uint32_t strand, const float4 *table,
+                                const uint8_t *perm, const FxTables &tb, FxContext &c, uint32_t *code,
+                                bool *clumped) {
+    *clumped = false;
+    const uint32_t g = cg.strand_guides[strand];
+    if (g == kInvalid) { return true; }
+    if (g >= cg.guide_count) {
+        *code = NXG_ERROR_INVALID_ARGUMENT;
+        return false;
+    }
+    const float *axis = cg.render_axes + 3u * static_cast<uint64_t>(g) * static_cast<uint32_t>(P);
+    const float *source = cg.axes + 3u * static_cast<uint64_t>(g) * static_cast<uint32_t>(P);
+    c.t = 0.0f;
+    float raw = 0.0f;
+    if (!fx_eval(m[kClumpMask], table, perm, c, &raw)) { return false; }
+    const float mask = std_clamp(raw, 0.0f, 1.0f);
+    if (mask <= 0.0f) { return true; }
+    FxContext gc = c;
+    gc.u = cg.uvs[2u * g];
+    gc.v = cg.uvs[2u * g + 1u];
+    gc.prefix = cg.random_prefixes[g];
+    gc.has_prefix = 1u;
+    if (!fx_eval(m[kClumpNoise], table, perm, gc, &raw)) { return false; }
+    const float noise = std_max(raw, 0.0f);
+    const bool noisy = noise > 1.0e-5f && mask > 1.0e-4f;
+    float effective_frequency = 0.0f;
+    F3 domain{}, tu{}, tv{}, ct{};
+    if (noisy) {
+        float raw_frequency = 0.0f, raw_correlation = 0.0f;
+        if (!fx_eval(m[kClumpNoiseFrequency], table, perm, gc, &raw_frequency) ||
+            !fx_eval(m[kClumpNoiseCorrelation], table, perm, gc, &raw_correlation)) {
+            return false;
+        }
+        const float frequency = std_max(raw_frequency, 0.0f);
+        const float correlation = std_clamp(__fmul_rn(raw_correlation, 0.01f), 0.0f, 1.0f);
+        float polyline = 0.0f;
+        for (int cv = 1; cv < P; ++cv) {
+            const F3 d = xsub(ld3(source, cv), ld3(source, cv - 1));
+            polyline = __fadd_rn(polyline, __fsqrt_rn(xdot(d, d)));
+        }
+        effective_frequency = polyline > 0.0f ? std_max(__fdiv_rn(0.5f, polyline), frequency) : frequency;
+        const float decorrelation = __fsub_rn(1.0f, correlation);
+        const float domain_scale = __fmul_rn(__fmul_rn(100.0f, decorrelation), decorrelation);
+        const F3 position = cg.reference_positions ? ld3(cg.reference_positions, g) : ld3(source, 0);
+        domain = xmul(xadd(position, F3{0.419276f, 0.184247f, 0.805721f}), domain_scale);
+        F3 normal = ld3(cg.normals, g), tangent = ld3(cg.tangents, g);
+        normal = xdot(normal, normal) > 1.0e-20f ? xnormalize(normal) : F3{0.0f, 1.0f, 0.0f};
+        tangent = xdot(tangent, tangent) > 1.0e-20f ? xnormalize(tangent) : fx_fallback_surface_u(normal);
+        tu = tangent;
+        tv = xcross(normal, tangent);
+        ct = normal;
+        const F3 first_segment = xsub(ld3(axis, 1), ld3(axis, 0));
+        if (xdot(first_segment, first_segment) > 1.0e-20f) { ct = xnormalize(first_segment); }
+        if (xdot(normal, ct) < 0.99999f) {
+            tu = fx_rotate_between(tu, normal, ct, 1.0f);
+            tv = fx_rotate_between(tv, normal, ct, 1.0f);
+        }
+    }
+    fx_cut_to_length(k, scratch, P, cg.spline_lengths[g], tb);
+    c.c_length = fx_spline_length(k, P, tb);
+    if (!fx_eval(m[kClumpAmount], table, perm, c, &raw)) { return false; }
+    const float pull = __fmul_rn(mask, std_clamp(raw, 0.0f, 1.0f));
+    float travelled = 0.0f;
+    for (int cv = 1; cv < P; ++cv) {
+        F3 displacement{0.0f, 0.0f, 0.0f};
+        if (noisy) {
+            const F3 d = xsub(ld3(source, cv), ld3(source, cv - 1));
+            travelled = __fadd_rn(travelled, __fsqrt_rn(xdot(d, d)));
+            F3 su = tu, sv = tv, nt = ct;
+            bool advance = false;
+            if (cv + 1 < P) {
+                const F3 segment = xsub(ld3(axis, cv + 1), ld3(axis, cv));
+                if (xdot(segment, segment) > 1.0e-20f) {
+                    nt = xnormalize(segment);
+                    if (fabsf(xdot(ct, nt)) < 0.99999f) {
+                        su = fx_rotate_between(tu, ct, nt, 0.5f);
+                        sv = fx_rotate_between(tv, ct, nt, 0.5f);
+                        advance = true;
+                    } else {
+                        ct = nt;
+                    }
+                }
+            }
+            gc.t = tb.t[cv];
+            float raw_scale = 0.0f;
+            if (!fx_eval(m[kClumpNoiseScale], table, perm, gc, &raw_scale)) { return false; }
+            const float magnitude = __fmul_rn(__fmul_rn(mask, noise), std_max(raw_scale, 0.0f));
+            if (!isfinite(magnitude)) { return false; }
+            const float distance = __fmul_rn(travelled, effective_frequency);
+            const float first = __fsub_rn(classic_noise(table, __fadd_rn(domain.x, distance), domain.y, domain.z), 0.5f);
+            const float second = __fsub_rn(classic_noise(table, domain.x, domain.y, __fadd_rn(domain.z, distance)), 0.5f);
+            displacement = xmul(xadd(xmul(su, first), xmul(sv, second)), magnitude);
+            if (advance) {
+                tu = fx_rotate_between(tu, ct, nt, 1.0f);
+                tv = fx_rotate_between(tv, ct, nt, 1.0f);
+                ct = nt;
+            }
+        }
+        c.t = tb.t[cv];
+        float scale = 0.0f;
+        if (!fx_eval(m[kClumpScale], table, perm, c, &scale)) { return false; }
+        const F3 current = k.p[cv];
+        const F3 pulled = xadd(current, xmul(xsub(ld3(axis, cv), current),
+                                             __fmul_rn(pull, __fsub_rn(1.0f, __fmul_rn(2.0f, scale)))));
+        k.p[cv] = xadd(pulled, displacement);
+    }
+    *clumped = true;
+    return true;
 }
 
 __device__ inline void fx_fail(uint32_t *status, uint32_t code = NXG_ERROR_EXPRESSION_DOMAIN) {
@@ -413,6 +598,12 @@ __global__ void __launch_bounds__(128, 5) classic_fx_kernel(const FxArgs k) {
         c.c_length = 0.0f;
         c.c_width = 0.0f;
         c.t = 0.0f;
+        c.prefix = k.random_prefixes ? k.random_prefixes[i] : 0u;
+        c.has_prefix = k.random_prefixes != nullptr;
+        if (plan.uses_random && !k.random_prefixes) {  // rand() needs the strands' SeExpr prefixes
+            fx_fail(k.status, NXG_ERROR_INVALID_ARGUMENT);
+            continue;
+        }
         float4 *pts = k.points + static_cast<uint64_t>(i) * k.P;
         FxCurve curve, scratch;
         for (int j = 0; j < P; ++j) { curve.p[j] = xyz(pts[j]); }
@@ -446,10 +637,22 @@ __global__ void __launch_bounds__(128, 5) classic_fx_kernel(const FxArgs k) {
         }
         c.c_width = raw_width;
         bool keep = true;
-        bool tangents = true;
+        uint32_t code = NXG_ERROR_EXPRESSION_DOMAIN;
+        uint32_t clump = 0u;
         for (uint32_t e = 0; ok && e < plan.effect_count; ++e) {
-            if (plan.effect_type[e] == NXG_CLASSIC_FX_NOISE && k.surface_tangents == nullptr) {
-                ok = tangents = false;  // NoiseFX needs the strand's surface tangent
+            bool changed = true;
+            if (plan.effect_type[e] == NXG_CLASSIC_FX_CLUMP) {
+                if (clump >= k.clump_count || P < 3) {  // the module's guides, of at least 3 CVs
+                    ok = false;
+                    code = NXG_ERROR_INVALID_ARGUMENT;
+                } else {
+                    const nxg_classic_clump_guides guides = k.clumps[clump];
+                    ok = fx_clump(curve, scratch, P, plan.effect[e], guides, i, table, perm, tb, c, &code, &changed);
+                }
+                ++clump;
+            } else if (plan.effect_type[e] == NXG_CLASSIC_FX_NOISE && k.surface_tangents == nullptr) {
+                ok = false;  // NoiseFX needs the strand's surface tangent
+                code = NXG_ERROR_INVALID_ARGUMENT;
             } else if (plan.effect_type[e] == NXG_CLASSIC_FX_NOISE) {
                 const F3 domain = k.noise_domains
                     ? F3{k.noise_domains[3u * i], k.noise_domains[3u * i + 1u], k.noise_domains[3u * i + 2u]}
@@ -463,7 +666,7 @@ __global__ void __launch_bounds__(128, 5) classic_fx_kernel(const FxArgs k) {
                 if (ok && fx_cut(curve, scratch, P, std_max(amount, 0.0f)) < 1.0e-4f) { keep = false; }
             }
             // cLength after this effect, where a later program reads it.
-            if (ok && plan.length_after[e]) { c.c_length = fx_spline_length(curve, P, tb); }
+            if (ok && changed && plan.length_after[e]) { c.c_length = fx_spline_length(curve, P, tb); }
         }
         float taper = 0.0f, taper_start = 0.0f;
         if (ok && plan.taper.present) { ok = fx_eval(plan.taper, table, perm, c, &taper); }
@@ -492,12 +695,35 @@ __global__ void __launch_bounds__(128, 5) classic_fx_kernel(const FxArgs k) {
             radii[j] = radius;
         }
         if (!ok) {
-            fx_fail(k.status, tangents ? NXG_ERROR_EXPRESSION_DOMAIN : NXG_ERROR_INVALID_ARGUMENT);
+            fx_fail(k.status, code);
             continue;
         }
         for (int j = 0; j < P; ++j) { pts[j] = make_float4(curve.p[j].x, curve.p[j].y, curve.p[j].z, radii[j]); }
         if (!keep) { k.point_counts[i] = 0u; }
     }
+}
+
+// prepare_xgen_classic_clump_runtime_data (xgen_classic_runtime.cpp:839-892)
+// for world-space guides: one thread per guide.
+__global__ void __launch_bounds__(128) clump_prepare_kernel(const float *axes, uint32_t guides, uint32_t P,
+                                                            float *render_axes, float *lengths) {
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= guides) { return; }
+    const float *src = axes + 3u * static_cast<uint64_t>(g) * P;
+    float *out = render_axes + 3u * static_cast<uint64_t>(g) * P;
+    const auto source = [src](int i) { return ld3(src, static_cast<uint32_t>(i)); };
+    const int n = static_cast<int>(P);
+    const auto put = [out](int i, F3 v) {
+        out[3 * i] = v.x;
+        out[3 * i + 1] = v.y;
+        out[3 * i + 2] = v.z;
+    };
+    put(0, source(0));
+    for (int cv = 1; cv + 1 < n; ++cv) {
+        put(cv, classic_curve_eval_by(source, n, __fdiv_rn(static_cast<float>(cv), static_cast<float>(n - 1))));
+    }
+    put(n - 1, source(n - 1));
+    lengths[g] = classic_spline_length_by(source, n);
 }
 
 } // namespace dev
@@ -549,15 +775,23 @@ uint32_t nxg_classic_fx_plan_upload(const nxg_classic_fx_plan *plan, void *devic
         const nxg_classic_fx &fx = plan->effects[e];
         host.effect_type[e] = fx.type;
         if (fx.type == NXG_CLASSIC_FX_NOISE) {
-            const nxg_expression *programs[nxg::dev::kFxSlots] = {fx.mask, fx.magnitude, fx.magnitude_scale,
-                                                                 fx.frequency, fx.correlation, fx.preserve_length};
-            for (int k = 0; k < nxg::dev::kFxSlots; ++k) {
+            const nxg_expression *programs[] = {fx.mask, fx.magnitude, fx.magnitude_scale,
+                                                fx.frequency, fx.correlation, fx.preserve_length};
+            for (int k = 0; k < 6; ++k) {
                 if (!programs[k]) { return NXG_ERROR_INVALID_ARGUMENT; }
                 if ((error = nxg::pack_optional(programs[k], host.effect[e][k]))) { return error; }
             }
         } else if (fx.type == NXG_CLASSIC_FX_CUT) {
             if (!fx.amount) { return NXG_ERROR_INVALID_ARGUMENT; }
             if ((error = nxg::pack_optional(fx.amount, host.effect[e][0]))) { return error; }
+        } else if (fx.type == NXG_CLASSIC_FX_CLUMP) {
+            const nxg_expression *programs[nxg::dev::kFxSlots] = {fx.mask, fx.clump, fx.clump_scale, fx.noise,
+                                                                 fx.noise_scale, fx.noise_frequency,
+                                                                 fx.noise_correlation};
+            for (int k = 0; k < nxg::dev::kFxSlots; ++k) {
+                if (!programs[k]) { return NXG_ERROR_INVALID_ARGUMENT; }
+                if ((error = nxg::pack_optional(programs[k], host.effect[e][k]))) { return error; }
+            }
         } else {
             return NXG_ERROR_INVALID_ARGUMENT;
         }
@@ -597,8 +831,22 @@ uint32_t nxg_classic_fx_apply(const void *device_plan, const nxg_classic_fx_curv
         reinterpret_cast<std::uintptr_t>(device_plan) % 256u != 0u) {
         return NXG_ERROR_MISALIGNED_OUTPUT;
     }
+    if (curves->clump_count > NXG_CLASSIC_MAX_FX || (curves->clump_count && !curves->clumps)) {
+        return NXG_ERROR_INVALID_ARGUMENT;
+    }
+    for (uint32_t m = 0; m < curves->clump_count; ++m) {
+        const nxg_classic_clump_guides &g = curves->clumps[m];
+        if (!g.strand_guides ||
+            (g.guide_count && (!g.axes || !g.render_axes || !g.spline_lengths || !g.normals || !g.tangents ||
+                               !g.uvs || !g.random_prefixes))) {
+            return NXG_ERROR_INVALID_ARGUMENT;
+        }
+    }
     if (curves->strand_count == 0u) { return NXG_ERROR_NONE; }
     nxg::dev::FxArgs k{};
+    k.random_prefixes = curves->random_prefixes;
+    k.clump_count = curves->clump_count;
+    for (uint32_t m = 0; m < curves->clump_count; ++m) { k.clumps[m] = curves->clumps[m]; }
     k.plan = static_cast<const nxg::dev::FxPlan *>(device_plan);
     k.points = reinterpret_cast<float4 *>(curves->points);
     k.point_counts = curves->point_counts;
@@ -615,6 +863,19 @@ uint32_t nxg_classic_fx_apply(const void *device_plan, const nxg_classic_fx_curv
     const uint32_t blocks = static_cast<uint32_t>(std::min<uint64_t>(
         (uint64_t{k.count} + threads - 1u) / threads, static_cast<uint64_t>(nxg::device_sm_count()) * 16u));
     nxg::dev::classic_fx_kernel<<<blocks, threads, 0, static_cast<cudaStream_t>(stream)>>>(k);
+    return nxg::record_cuda(cudaGetLastError());
+}
+
+uint32_t nxg_classic_clump_prepare(const float *axes, uint32_t guide_count, uint32_t cvs_per_guide,
+                                   float *render_axes, float *spline_lengths, void *stream) {
+    if (cvs_per_guide < 3u || cvs_per_guide > NXG_CLASSIC_MAX_FX_CVS ||
+        (guide_count && (!axes || !render_axes || !spline_lengths))) {
+        return NXG_ERROR_INVALID_ARGUMENT;
+    }
+    if (guide_count == 0u) { return NXG_ERROR_NONE; }
+    nxg::set_last_cuda_error(0);
+    nxg::dev::clump_prepare_kernel<<<(guide_count + 127u) / 128u, 128u, 0, static_cast<cudaStream_t>(stream)>>>(
+        axes, guide_count, cvs_per_guide, render_axes, spline_lengths);
     return nxg::record_cuda(cudaGetLastError());
 }
 

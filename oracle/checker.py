@@ -417,7 +417,8 @@ class Reference:
         SplinePrimitive attributes in `primitive` (length, width, taper,
         taperStart, widthRamp) and FX modules `effects`, each ("noise", {mask,
         magnitude, magnitudeScale, frequency, correlation, preserveLength}) or
-        ("cut", {amount}), in order."""
+        ("cut", {amount}) or ("clump", {mask, clump, clumpScale, noise,
+        noiseScale, noiseFrequency, noiseCorrelation}), in order."""
         lib = self._expression_prototypes()
         if not getattr(self, "_fx_ready", False):
             lib.ref_classic_plan_fx.restype = _P
@@ -426,8 +427,12 @@ class Reference:
             lib.ref_classic_plan_effects.argtypes = [_P, _P]
             lib.ref_classic_apply_fx.restype = ctypes.c_uint32
             lib.ref_classic_apply_fx.argtypes = [_P, _P, _P, _P, _P, ctypes.c_uint32, ctypes.c_uint32,
-                                                 ctypes.c_float, _P, ctypes.c_uint64, _P, ctypes.c_uint32, _P,
+                                                 ctypes.c_float, _P, ctypes.c_uint64, _P, _P, ctypes.c_uint32, _P,
+                                                 _P, _P, _P, _P, _P, _P, _P, ctypes.c_uint32, _P,
                                                  ctypes.c_char_p, ctypes.c_uint64]
+            lib.ref_classic_clump_prepare.restype = ctypes.c_uint32
+            lib.ref_classic_clump_prepare.argtypes = [_P, ctypes.c_uint32, ctypes.c_uint32, _P, _P,
+                                                      ctypes.c_char_p, ctypes.c_uint64]
             self._fx_ready = True
         keep = []
 
@@ -439,12 +444,16 @@ class Reference:
             return b
         prim = (ctypes.c_char_p * 5)(*[text(primitive.get(k)) for k in
                                        ("length", "width", "taper", "taperStart", "widthRamp")])
-        types = np.array([0 if kind == "noise" else 1 for kind, _ in effects] or [0], np.uint32)
-        noise_names = ("mask", "magnitude", "magnitudeScale", "frequency", "correlation", "preserveLength")
+        kinds = {"noise": 0, "cut": 1, "clump": 2}
+        types = np.array([kinds[kind] for kind, _ in effects] or [0], np.uint32)
+        names = {"noise": ("mask", "magnitude", "magnitudeScale", "frequency", "correlation", "preserveLength"),
+                 "cut": ("amount",),
+                 "clump": ("mask", "clump", "clumpScale", "noise", "noiseScale", "noiseFrequency",
+                           "noiseCorrelation")}
         attrs = []
         for kind, values in effects:
-            attrs += [text(values.get(n)) for n in noise_names] if kind == "noise" else \
-                [text(values["amount"])] + [None] * 5
+            row = [text(values.get(n)) for n in names[kind]]
+            attrs += row + [None] * (7 - len(row))
         arr = (ctypes.c_char_p * max(1, len(attrs)))(*attrs)
         msg = ctypes.create_string_buffer(4096)
         ptr = lib.ref_classic_plan_fx(ctypes.cast(prim, _P), len(effects), types.ctypes.data, ctypes.cast(arr, _P),
@@ -452,14 +461,31 @@ class Reference:
         if not ptr:
             raise ValueError(msg.value.decode())
         plan = Reference.Plan(self, ptr, [r for r in msg.value.decode().split("\n") if r])
-        counts = np.zeros(3, np.uint32)
+        counts = np.zeros(4, np.uint32)
         lib.ref_classic_plan_effects(ptr, counts.ctypes.data)
         plan.effect_counts = tuple(int(c) for c in counts)
         return plan
 
+    def classic_clump_prepare(self, axes):
+        """prepare_xgen_classic_clump_runtime_data of world-space guide axes
+        [G, P, 3]: (render axes [G, P, 3], spline lengths [G])."""
+        self.classic_plan_fx({}, [])  # sets the prototypes
+        axes = np.ascontiguousarray(axes, np.float32)
+        G, P = axes.shape[0], axes.shape[1]
+        render = np.zeros_like(axes)
+        lengths = np.zeros(G, np.float32)
+        msg = ctypes.create_string_buffer(512)
+        if self.lib.ref_classic_clump_prepare(axes.ctypes.data, G, P, render.ctypes.data, lengths.ctypes.data,
+                                              msg, 512):
+            raise ValueError(msg.value.decode())
+        return render, lengths
+
     def classic_apply_fx(self, plan, points, counts, roots, uvs, cvs: int, radius_scale: float, runtime_inputs=None,
-                         surface_tangents=None, workers: int = 1):
-        """apply_xgen_classic_float_runtime_plan_cpu with surface tangents;
+                         surface_tangents=None, workers: int = 1, random_prefixes=None, clumps=()):
+        """apply_xgen_classic_float_runtime_plan_cpu with surface tangents,
+        per-strand SeExpr prefixes and ClumpingFX guides (each a dict of
+        axes [G, P, 3], normals, tangents [G, 3], uvs [G, 2], prefixes [G],
+        strand_guides [S] and optionally reference_positions [G, 3]);
         returns the compacted (points, counts, roots, uvs)."""
         lib = self.lib
         points = np.ascontiguousarray(points, np.float32).copy()
@@ -469,14 +495,34 @@ class Reference:
         S = counts.size
         inputs = None if runtime_inputs is None else np.ascontiguousarray(runtime_inputs, np.float32)
         tang = None if surface_tangents is None else np.ascontiguousarray(surface_tangents, np.float32)
+        prefixes = None if random_prefixes is None else np.ascontiguousarray(random_prefixes, np.uint32)
+        keep = []
+
+        def arr(a, dtype):
+            if a is None:
+                return None
+            a = np.ascontiguousarray(a, dtype)
+            keep.append(a)
+            return a.ctypes.data
+        n = max(1, len(clumps))
+        tables = {k: (_P * n)(*[arr(c.get(k), np.uint32 if k in ("prefixes", "strand_guides") else np.float32)
+                                 for c in clumps])
+                  for k in ("axes", "normals", "tangents", "uvs", "prefixes", "reference_positions",
+                            "strand_guides")}
+        guide_counts = np.array([np.asarray(c["axes"]).shape[0] for c in clumps] or [0], np.uint32)
         kept = ctypes.c_uint32()
         msg = ctypes.create_string_buffer(512)
         rc = lib.ref_classic_apply_fx(plan.ptr, points.ctypes.data, counts.ctypes.data, roots.ctypes.data,
                                       uvs.ctypes.data, S, cvs, radius_scale,
                                       None if inputs is None else inputs.ctypes.data,
                                       0 if inputs is None else inputs.size,
-                                      None if tang is None else tang.ctypes.data, workers, ctypes.byref(kept),
-                                      msg, 512)
+                                      None if tang is None else tang.ctypes.data,
+                                      None if prefixes is None else prefixes.ctypes.data, len(clumps),
+                                      guide_counts.ctypes.data,
+                                      *(ctypes.cast(tables[k], _P) for k in ("axes", "normals", "tangents", "uvs",
+                                                                              "prefixes", "reference_positions",
+                                                                              "strand_guides")),
+                                      workers, ctypes.byref(kept), msg, 512)
         if rc != 0:
             raise ValueError(msg.value.decode())
         k = kept.value

@@ -247,14 +247,19 @@ void *ref_classic_plan_fx(const char *const *primitive, std::uint32_t effect_cou
         description.objects.push_back(spline);
         const char *noise_names[6] = {"mask", "magnitude", "magnitudeScale", "frequency", "correlation",
                                       "preserveLength"};
+        const char *clump_names[7] = {"mask", "clump", "clumpScale", "noise", "noiseScale", "noiseFrequency",
+                                      "noiseCorrelation"};
         for (std::uint32_t e = 0; e < effect_count; ++e) {
             ClassicObject fx{};
-            const char *const *a = effect_attributes + 6u * e;
+            const char *const *a = effect_attributes + 7u * e;
             fx.attributes.push_back({"name", "fx" + std::to_string(e), 0u});
             if (types[e] == 0u) {
                 fx.type = "NoiseFXModule";
                 fx.attributes.push_back({"mode", "0", 0u});
                 for (int k = 0; k < 6; ++k) { fx.attributes.push_back({noise_names[k], a[k], 0u}); }
+            } else if (types[e] == 2u) {
+                fx.type = "ClumpingFXModule";
+                for (int k = 0; k < 7; ++k) { fx.attributes.push_back({clump_names[k], a[k], 0u}); }
             } else {
                 fx.type = "CutFXModule";
                 fx.attributes.push_back({"rebuildType", "1", 0u});
@@ -273,23 +278,77 @@ void *ref_classic_plan_fx(const char *const *primitive, std::uint32_t effect_cou
     }
 }
 
-// Effects compiled into a plan: count of NoiseFX, CutFX and of all effects.
+// Effects compiled into a plan: count of NoiseFX, CutFX, of all effects and
+// of ClumpingFX.
 void ref_classic_plan_effects(const void *plan, std::uint32_t *out) {
     const ClassicFloatRuntimePlan &p = *static_cast<const ClassicFloatRuntimePlan *>(plan);
     out[0] = static_cast<std::uint32_t>(p.noises.size());
     out[1] = static_cast<std::uint32_t>(p.cuts.size());
     out[2] = static_cast<std::uint32_t>(p.effects.size());
+    out[3] = static_cast<std::uint32_t>(p.clumps.size());
+}
+
+// prepare_xgen_classic_clump_runtime_data on world-space guides: [G*P] Vec3
+// axes in, [G*P] Vec3 render axes and [G] spline lengths out.
+std::uint32_t ref_classic_clump_prepare(const float *axes, std::uint32_t guides, std::uint32_t cvs,
+                                        float *render_axes, float *lengths, char *msg, std::uint64_t cap) {
+    try {
+        ClassicClumpRuntimeData data{};
+        data.cvs_per_guide = cvs;
+        const auto *a = reinterpret_cast<const Vec3 *>(axes);
+        data.guide_axes.assign(a, a + static_cast<std::size_t>(guides) * cvs);
+        prepare_xgen_classic_clump_runtime_data(data);
+        std::memcpy(render_axes, data.guide_render_axes.data(), data.guide_render_axes.size() * sizeof(Vec3));
+        std::memcpy(lengths, data.guide_spline_lengths.data(), data.guide_spline_lengths.size() * sizeof(float));
+        copy_text("", msg, cap);
+        return 0u;
+    } catch (const std::exception &e) {
+        copy_text(e.what(), msg, cap);
+        return 1u;
+    }
 }
 
 // ref_classic_apply with one surface tangent per strand ([S] Vec3, may be
 // NULL when the plan has no NoiseFX).
+// random_prefixes: [S] or NULL.  Clump module m (in plan order) has
+// guide_counts[m] world-space guides: axes [G*P] Vec3, normals, tangents
+// [G] Vec3, uvs [G] Vec2, SeExpr prefixes [G], reference positions [G] Vec3
+// or NULL, and strand_guides [S]; the reference prepares the render axes.
 std::uint32_t ref_classic_apply_fx(const void *plan, float *points, std::uint32_t *counts, void *roots,
                                    float *root_uvs, std::uint32_t strands, std::uint32_t cvs, float radius_scale,
                                    const float *runtime_inputs, std::uint64_t runtime_input_count,
-                                   const float *surface_tangents, std::uint32_t workers, std::uint32_t *kept,
-                                   char *msg, std::uint64_t cap) {
+                                   const float *surface_tangents, const std::uint32_t *random_prefixes,
+                                   std::uint32_t clump_count, const std::uint32_t *guide_counts,
+                                   const float *const *clump_axes, const float *const *clump_normals,
+                                   const float *const *clump_tangents, const float *const *clump_uvs,
+                                   const std::uint32_t *const *clump_prefixes,
+                                   const float *const *clump_reference_positions,
+                                   const std::uint32_t *const *clump_strand_guides, std::uint32_t workers,
+                                   std::uint32_t *kept, char *msg, std::uint64_t cap) {
     try {
         const ClassicFloatRuntimePlan &p = *static_cast<const ClassicFloatRuntimePlan *>(plan);
+        std::vector<ClassicClumpRuntimeData> clumps(clump_count);
+        for (std::uint32_t m = 0; m < clump_count; ++m) {
+            ClassicClumpRuntimeData &d = clumps[m];
+            const std::size_t G = guide_counts[m];
+            d.module_name = m < p.clumps.size() ? p.clumps[m].name : std::string();
+            d.cvs_per_guide = cvs;
+            const auto *axes = reinterpret_cast<const Vec3 *>(clump_axes[m]);
+            d.guide_axes.assign(axes, axes + G * cvs);
+            const auto *n = reinterpret_cast<const Vec3 *>(clump_normals[m]);
+            d.guide_normals.assign(n, n + G);
+            const auto *t = reinterpret_cast<const Vec3 *>(clump_tangents[m]);
+            d.guide_tangents.assign(t, t + G);
+            const auto *uv = reinterpret_cast<const Vec2 *>(clump_uvs[m]);
+            d.guide_uvs.assign(uv, uv + G);
+            d.guide_face_ids.assign(G, 0u);
+            d.guide_random_prefixes.assign(clump_prefixes[m], clump_prefixes[m] + G);
+            if (clump_reference_positions[m]) {
+                const auto *r = reinterpret_cast<const Vec3 *>(clump_reference_positions[m]);
+                d.guide_reference_positions.assign(r, r + G);
+            }
+            d.strand_guide_indices.assign(clump_strand_guides[m], clump_strand_guides[m] + strands);
+        }
         PackedGeneratedCurves curves{};
         curves.strand_count = strands;
         curves.cvs_per_strand = cvs;
@@ -304,9 +363,11 @@ std::uint32_t ref_classic_apply_fx(const void *plan, float *points, std::uint32_
         }
         std::span<const Vec3> tangents;
         if (surface_tangents) { tangents = std::span<const Vec3>(reinterpret_cast<const Vec3 *>(surface_tangents), strands); }
+        std::span<const std::uint32_t> prefixes;
+        if (random_prefixes) { prefixes = std::span<const std::uint32_t>(random_prefixes, strands); }
         NanoXGenContext context(workers == 0u ? 1u : workers);
         apply_xgen_classic_float_runtime_plan_cpu(
-            curves, p, radius_scale, tangents, {}, {}, {},
+            curves, p, radius_scale, tangents, prefixes, {}, clumps,
             std::span<const float>(runtime_inputs, runtime_inputs ? runtime_input_count : 0u), {}, false,
             &context);
         std::memcpy(points, curves.points.data(), curves.points.size() * sizeof(PackedCurvePoint));
