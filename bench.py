@@ -793,21 +793,55 @@ def run_batched_classic(args):
 
 def _fx_workload():
     """The Classic FX workload's plan: the cfg5 length and width expressions,
-    a NoiseFX pass, a CutFX pass on a share of cLength and a taper."""
+    a NoiseFX pass, a ClumpingFX pass with guide noise, a CutFX pass on a
+    share of cLength and a taper."""
     from nanoxgen_b200 import fixtures
     primitive = {"length": fixtures.CLASSIC_LENGTH.replace("*clamp(1-$v,0.2,1)", ""),
                  "width": fixtures.CLASSIC_WIDTH, "taper": "0.6", "taperStart": "0.3"}
     effects = [("noise", dict(mask="1", magnitude="0.03", magnitudeScale="1", frequency="8", correlation="30",
                               preserveLength="40")),
+               ("clump", dict(mask="1", clump="0.6", clumpScale="0.1", noise="0.02", noiseScale="1",
+                              noiseFrequency="6", noiseCorrelation="40")),
                ("cut", {"amount": "$cLength*0.1"})]
     return primitive, effects
+
+
+def _fx_clump_guides(w, P, roots, device):
+    """ClumpingFX guides of the FX workload: the description's own guides
+    resampled linearly to P CVs, their root normals and uvs, tangents normal x
+    z (y near the poles), seeded SeExpr prefixes; each strand takes the guide
+    whose root is nearest to its root (found on the device)."""
+    import numpy as np
+    import torch
+    gs = w.build_input.guides
+    counts = gs.cv_counts.astype(np.int64)
+    starts = np.concatenate([[0], np.cumsum(counts)[:-1]])
+    u = np.linspace(0.0, 1.0, P)
+    axes = np.empty((counts.size, P, 3), np.float32)
+    for g in range(counts.size):
+        c = gs.cvs[starts[g]:starts[g] + counts[g]].astype(np.float64)
+        x = np.linspace(0.0, 1.0, counts[g])
+        axes[g] = np.stack([np.interp(u, x, c[:, k]) for k in range(3)], 1)
+    n = gs.root_normals.astype(np.float64)
+    ref = np.where(np.abs(n[:, 2:3]) < 0.999, [[0.0, 0.0, 1.0]], [[0.0, 1.0, 0.0]])
+    t = np.cross(n, ref)
+    t /= np.maximum(np.linalg.norm(t, axis=1, keepdims=True), 1e-30)
+    guide_roots = torch.from_numpy(axes[:, 0, :]).to(device)
+    strand_roots = torch.from_numpy(roots["position"].astype(np.float32)).to(device)
+    nearest = torch.cat([torch.cdist(strand_roots[i:i + 65536], guide_roots).argmin(1)
+                         for i in range(0, strand_roots.shape[0], 65536)])
+    return dict(axes=axes, normals=gs.root_normals.astype(np.float32), tangents=t.astype(np.float32),
+                uvs=gs.root_uvs.astype(np.float32),
+                prefixes=np.random.default_rng(77).integers(0, 2**32, counts.size, dtype=np.uint32),
+                strand_guides=nearest.cpu().numpy().astype(np.uint32))
 
 
 def run_classic_fx(args):
     """Classic FX passes over a generated frame: the large description's mesh
     (200,000 triangles, 4,096 guides), 1,000,000 strands x 24 CVs generated
     without generator noise, then nxg_classic_fx_apply with the plan of
-    _fx_workload.  A step is generation plus the FX pass (the pass works in
+    _fx_workload (NoiseFX, ClumpingFX toward the description's guides,
+    CutFX, taper).  A step is generation plus the FX pass (the pass works in
     place, so each step regenerates its input); the FX kernel is also timed
     alone.  The CPU baseline is the reference's
     apply_xgen_classic_float_runtime_plan_cpu on a prefix sample."""
@@ -816,7 +850,7 @@ def run_classic_fx(args):
 
     from nanoxgen_b200 import fixtures
     from nanoxgen_b200.asset import build_asset
-    from nanoxgen_b200.classic import FxPlan, classic_fx_apply
+    from nanoxgen_b200.classic import ClumpGuides, FxPlan, classic_fx_apply
     from nanoxgen_b200.generator import DeviceAsset, allocate_outputs, generate_packed, get_tile
     device = torch.device("cuda", 0)
     torch.cuda.set_device(device)
@@ -839,6 +873,9 @@ def run_classic_fx(args):
     tan = np.cross(rn, axis)
     tan /= np.maximum(np.linalg.norm(tan, axis=1, keepdims=True), 1e-30)
     tangents = torch.from_numpy(tan.astype(np.float32)).to(device)
+    cg = _fx_clump_guides(w, P, out.roots_numpy(), device)
+    guides = [ClumpGuides(cg["axes"], cg["normals"], cg["tangents"], cg["uvs"], cg["prefixes"], cg["strand_guides"],
+                          device=device)]
     status = torch.zeros(2, dtype=torch.int32, device=device)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=device)
     stream = torch.cuda.current_stream(device)
@@ -848,7 +885,7 @@ def run_classic_fx(args):
         generate_packed(d, params, points=points, roots=roots, root_uvs=uvs, point_counts=counts, stream=stream)
         if ev is not None:
             ev.record(stream)
-        classic_fx_apply(plan, out, tangents, status=status, stream=stream)
+        classic_fx_apply(plan, out, tangents, status=status, stream=stream, clumps=guides)
 
     for _ in range(args.warmup):
         flush.fill_(1)
@@ -877,7 +914,7 @@ def run_classic_fx(args):
                        "l2": "flushed between timed steps (256 MiB write)"},
             "fx_pass": {"ms": fx_ms, "points_per_s": S * P / (fx_ms / 1e3), "strands_kept": kept,
                         "status": st},
-            "clocks": clocks, "gpu_launches": (kernels_per_step(get_tile(P, False)) + 1) * args.steps}
+            "clocks": clocks, "gpu_launches": (kernels_per_step(get_tile(P, False)) + 2) * args.steps}
     if not args.no_cpu_baseline:
         from oracle.checker import Reference, reference_available
         if reference_available():
@@ -890,7 +927,7 @@ def run_classic_fx(args):
             in_roots = out.roots_numpy()[:n].copy()
             in_uvs = uvs[:n].cpu().numpy().copy()
             in_counts = counts[:n].cpu().numpy().view(np.uint32).copy()
-            classic_fx_apply(plan, out, tangents, status=status)
+            classic_fx_apply(plan, out, tangents, status=status, clumps=guides)
             torch.cuda.synchronize()
             ref = Reference()
             rplan = ref.classic_plan_fx(primitive, effects, 3, "description")
@@ -898,8 +935,9 @@ def run_classic_fx(args):
             inputs = (np.stack([ref.classic_noise(in_roots["position"], f) for f in freqs], 1)
                       if len(freqs) else None)
             cores = os.cpu_count() or 1
+            sample_guides = [dict(cg, strand_guides=cg["strand_guides"][:n])]
             apply = lambda: ref.classic_apply_fx(rplan, in_pts, in_counts, in_roots, in_uvs, P, 1.0, inputs,
-                                                 tan[:n].astype(np.float32), workers=cores)
+                                                 tan[:n].astype(np.float32), workers=cores, clumps=sample_guides)
             got = apply()
             times = []
             for _ in range(7):
@@ -909,7 +947,7 @@ def run_classic_fx(args):
             med, p90 = statistics.median(times), _percentile(times, 0.9)
             t0 = time.perf_counter()
             ref.classic_apply_fx(rplan, in_pts, in_counts, in_roots, in_uvs, P, 1.0, inputs,
-                                 tan[:n].astype(np.float32), workers=1)
+                                 tan[:n].astype(np.float32), workers=1, clumps=sample_guides)
             single = time.perf_counter() - t0
             mine_pts = points[:n * P].cpu().numpy()
             keep = counts[:n].cpu().numpy() != 0

@@ -202,6 +202,10 @@ typedef struct nxg_classic_clump_guides {
     const float *uvs;                 /* guide_count x 2 */
     const uint32_t *random_prefixes;  /* guide_count SeExpr prefixes (rand() in the guide noise) */
     const uint32_t *strand_guides;    /* strand_count: the strand's guide, or NXG_INVALID_INDEX */
+    float *noise_table;               /* guide_count x P float4 scratch, or NULL: when the module's
+                                         guide-noise programs read no per-strand input ($id, $cLength,
+                                         $cWidth, noise($Prefg)), the apply computes each guide's
+                                         noise axis once into it instead of once per strand */
     uint32_t guide_count;
     uint32_t reserved;
 } nxg_classic_clump_guides;

@@ -197,7 +197,7 @@ class ClassicClumpGuides(ctypes.Structure):
                 ("normals", ctypes.c_void_p), ("tangents", ctypes.c_void_p),
                 ("reference_positions", ctypes.c_void_p), ("uvs", ctypes.c_void_p),
                 ("random_prefixes", ctypes.c_void_p), ("strand_guides", ctypes.c_void_p),
-                ("guide_count", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+                ("noise_table", ctypes.c_void_p), ("guide_count", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
 
 
 class ClassicFxPlan(ctypes.Structure):

@@ -264,10 +264,12 @@ class ClumpGuides:
     the rebuild), normals and tangents [G, 3], uvs [G, 2], SeExpr prefixes
     [G], the guide of every strand [S] (NXG_INVALID_INDEX = none) and,
     optionally, the guide-noise domain positions [G, 3].  The render axes and
-    spline lengths are prepared on the device (nxg_classic_clump_prepare)."""
+    spline lengths are prepared on the device (nxg_classic_clump_prepare);
+    a [G, P, 4] scratch table lets the apply compute the guide noise once
+    per guide where the module's programs allow it."""
 
     def __init__(self, axes, normals, tangents, uvs, random_prefixes, strand_guides, reference_positions=None,
-                 device="cuda", stream: Optional[torch.cuda.Stream] = None):
+                 device="cuda", stream: Optional[torch.cuda.Stream] = None, noise_table: bool = True):
         f32 = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.float32)).to(device)
         u32 = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.uint32).view(np.int32)).to(device)
         self.axes = f32(axes)
@@ -278,6 +280,8 @@ class ClumpGuides:
         self.random_prefixes, self.strand_guides = u32(random_prefixes), u32(strand_guides)
         self.reference_positions = None if reference_positions is None else f32(reference_positions)
         self.render_axes = torch.empty_like(self.axes)
+        self.noise_table = (torch.empty((G, P, 4), dtype=torch.float32, device=self.axes.device)
+                            if noise_table else None)
         self.spline_lengths = torch.empty(G, dtype=torch.float32, device=self.axes.device)
         check(lib().nxg_classic_clump_prepare(self.axes.data_ptr(), G, P, self.render_axes.data_ptr(),
                                               self.spline_lengths.data_ptr(), _stream_handle(stream)),
@@ -290,7 +294,7 @@ class ClumpGuides:
                                        self.spline_lengths.data_ptr(), self.normals.data_ptr(),
                                        self.tangents.data_ptr(), ptr(self.reference_positions), self.uvs.data_ptr(),
                                        self.random_prefixes.data_ptr(), self.strand_guides.data_ptr(),
-                                       self.guide_count, 0)
+                                       ptr(self.noise_table), self.guide_count, 0)
 
 
 def classic_fx_apply(plan: FxPlan, curves: PackedCurves, surface_tangents: Optional[torch.Tensor] = None,

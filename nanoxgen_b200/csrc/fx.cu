@@ -48,6 +48,7 @@ struct FxPlan {
     uint32_t effect_count;
     uint32_t effect_type[kFxMaxEffects];
     uint32_t length_after[kFxMaxEffects];  // a later program binds cLength
+    uint32_t guide_noise_shared[kFxMaxEffects];  // ClumpingFX guide noise reads no per-strand input
     uint32_t uses_random;
     float description_id;   // rand() face seed inputs
     float patch_seed;
@@ -445,57 +446,26 @@ __device__ inline void fx_cut_to_length(FxCurve &k, FxCurve &scratch, int P, flo
     fx_resample(k, scratch, P, cut);
 }
 
-// The ClumpingFX step for one strand (xgen_classic_runtime.cpp:1680-1788),
-// with world-space guides: the mask; the guide-noise axis of
-// build_clump_noise_axis (:1041-1181) in the guide's context (its uv and
-// SeExpr prefix); the cut to the guide's length; the pull of every CV after
-// the root toward the guide's rebuilt CV by mask * clump * (1 - 2 clumpScale);
-// the guide noise added on top.  The noise axis depends only on the guide's
-// CVs, so it is computed in the same pass over the CVs as the pull.
-// `clumped` reports whether the curve changed (the reference recomputes
-// cLength only then).  False where the reference throws; *code says why.
-__device__ __noinline__ bool fx_clump(FxCurve &k, FxCurve &scratch, int P, const DeviceExpression *m,
-                                const nxg_classic_clump_guides &cg, uint32_t strand, const float4 *table,
-                                const uint8_t *perm, const FxTables &tb, FxContext &c, uint32_t *code,
-                                bool *clumped) {
-    *clumped = false;
-    const uint32_t g = cg.strand_guides[strand];
-    if (g == kInvalid) { return true; }
-    if (g >= cg.guide_count) {
-        *code = NXG_ERROR_INVALID_ARGUMENT;
-        return false;
-    }
-    const float *axis = cg.render_axes + 3u * static_cast<uint64_t>(g) * static_cast<uint32_t>(P);
-    const float *source = cg.axes + 3u * static_cast<uint64_t>(g) * static_cast<uint32_t>(P);
-    c.t = 0.0f;
-    float raw = 0.0f;
-    if (!fx_eval(m[kClumpMask], table, perm, c, &raw)) { return false; }
-    const float mask = std_clamp(raw, 0.0f, 1.0f);
-    if (mask <= 0.0f) { return true; }
-    FxContext gc = c;
-    gc.u = cg.uvs[2u * g];
-    gc.v = cg.uvs[2u * g + 1u];
-    gc.prefix = cg.random_prefixes[g];
-    gc.has_prefix = 1u;
-    if (!fx_eval(m[kClumpNoise], table, perm, gc, &raw)) { return false; }
-    const float noise = std_max(raw, 0.0f);
-    const bool noisy = noise > 1.0e-5f && mask > 1.0e-4f;
-    float effective_frequency = 0.0f;
-    F3 domain{}, tu{}, tv{}, ct{};
-    if (noisy) {
-        float raw_frequency = 0.0f, raw_correlation = 0.0f;
-        if (!fx_eval(m[kClumpNoiseFrequency], table, perm, gc, &raw_frequency) ||
-            !fx_eval(m[kClumpNoiseCorrelation], table, perm, gc, &raw_correlation)) {
-            return false;
-        }
-        const float frequency = std_max(raw_frequency, 0.0f);
+// The guide-noise axis of build_clump_noise_axis (xgen_classic_runtime.cpp:
+// 1041-1181) after its early-out, for a guide with render CVs `axis` and
+// source CVs `source`: begin() sets up the domain, the effective frequency
+// and the frame transported from the guide's normal and tangent; step(cv)
+// returns CV cv's displacement before the magnitude,
+// sample_u * first + sample_v * second, and moves the frame on.
+struct FxGuideNoise {
+    F3 domain, tu, tv, ct;
+    float frequency, travelled;
+
+    __device__ void begin(const nxg_classic_clump_guides &cg, uint32_t g, const float *axis, const float *source,
+                          int P, float raw_frequency, float raw_correlation) {
+        const float f = std_max(raw_frequency, 0.0f);
         const float correlation = std_clamp(__fmul_rn(raw_correlation, 0.01f), 0.0f, 1.0f);
         float polyline = 0.0f;
         for (int cv = 1; cv < P; ++cv) {
             const F3 d = xsub(ld3(source, cv), ld3(source, cv - 1));
             polyline = __fadd_rn(polyline, __fsqrt_rn(xdot(d, d)));
         }
-        effective_frequency = polyline > 0.0f ? std_max(__fdiv_rn(0.5f, polyline), frequency) : frequency;
+        frequency = polyline > 0.0f ? std_max(__fdiv_rn(0.5f, polyline), f) : f;
         const float decorrelation = __fsub_rn(1.0f, correlation);
         const float domain_scale = __fmul_rn(__fmul_rn(100.0f, decorrelation), decorrelation);
         const F3 position = cg.reference_positions ? ld3(cg.reference_positions, g) : ld3(source, 0);
@@ -512,54 +482,151 @@ __device__ __noinline__ bool fx_clump(FxCurve &k, FxCurve &scratch, int P, const
             tu = fx_rotate_between(tu, normal, ct, 1.0f);
             tv = fx_rotate_between(tv, normal, ct, 1.0f);
         }
+        travelled = 0.0f;
+    }
+
+    __device__ F3 step(const float *axis, const float *source, int P, int cv, const float4 *table) {
+        const F3 d = xsub(ld3(source, cv), ld3(source, cv - 1));
+        travelled = __fadd_rn(travelled, __fsqrt_rn(xdot(d, d)));
+        F3 su = tu, sv = tv, nt = ct;
+        bool advance = false;
+        if (cv + 1 < P) {
+            const F3 segment = xsub(ld3(axis, cv + 1), ld3(axis, cv));
+            if (xdot(segment, segment) > 1.0e-20f) {
+                nt = xnormalize(segment);
+                if (fabsf(xdot(ct, nt)) < 0.99999f) {
+                    su = fx_rotate_between(tu, ct, nt, 0.5f);
+                    sv = fx_rotate_between(tv, ct, nt, 0.5f);
+                    advance = true;
+                } else {
+                    ct = nt;
+                }
+            }
+        }
+        const float distance = __fmul_rn(travelled, frequency);
+        const float first = __fsub_rn(classic_noise(table, __fadd_rn(domain.x, distance), domain.y, domain.z), 0.5f);
+        const float second = __fsub_rn(classic_noise(table, domain.x, domain.y, __fadd_rn(domain.z, distance)), 0.5f);
+        const F3 unit = xadd(xmul(su, first), xmul(sv, second));
+        if (advance) {
+            tu = fx_rotate_between(tu, ct, nt, 1.0f);
+            tv = fx_rotate_between(tv, ct, nt, 1.0f);
+            ct = nt;
+        }
+        return unit;
+    }
+};
+
+// Guide-noise table entries: CV 0 of each guide holds (noise, flags), CVs
+// 1.. hold (the unit displacement, the raw noiseScale).
+enum : uint32_t { kGuideNoiseFailed = 1u, kGuideRestFailed = 2u };
+
+// The guide's context for its noise programs: its uv and SeExpr prefix.
+__device__ inline void fx_guide_context(FxContext &gc, const nxg_classic_clump_guides &cg, uint32_t g) {
+    gc.u = cg.uvs[2u * g];
+    gc.v = cg.uvs[2u * g + 1u];
+    gc.prefix = cg.random_prefixes[g];
+    gc.has_prefix = 1u;
+}
+
+// The ClumpingFX step for one strand (xgen_classic_runtime.cpp:1680-1788),
+// with world-space guides: the mask; the guide-noise axis (from the
+// module's per-guide table when `shared`, else evaluated here in the guide's
+// context); the cut to the guide's length; the pull of every CV after the
+// root toward the guide's rebuilt CV by mask * clump * (1 - 2 clumpScale);
+// the guide noise, times (mask * noise) * max(noiseScale, 0), added on top.
+// The noise axis depends only on the guide, so it is taken in the same pass
+// over the CVs as the pull.  `clumped` reports whether the curve changed
+// (the reference recomputes cLength only then).  False where the reference
+// throws; *code says why.
+__device__ __noinline__ bool fx_clump(FxCurve &k, FxCurve &scratch, int P, const DeviceExpression *m,
+                                      const nxg_classic_clump_guides &cg, bool shared, uint32_t strand,
+                                      const float4 *table, const uint8_t *perm, const FxTables &tb, FxContext &c,
+                                      uint32_t *code, bool *clumped) {
+    *clumped = false;
+    const uint32_t g = cg.strand_guides[strand];
+    if (g == kInvalid) { return true; }
+    if (g >= cg.guide_count) {
+        *code = NXG_ERROR_INVALID_ARGUMENT;
+        return false;
+    }
+    const float *axis = cg.render_axes + 3u * static_cast<uint64_t>(g) * static_cast<uint32_t>(P);
+    const float *source = cg.axes + 3u * static_cast<uint64_t>(g) * static_cast<uint32_t>(P);
+    const float4 *entries = shared ? reinterpret_cast<const float4 *>(cg.noise_table) +
+                                         static_cast<uint64_t>(g) * static_cast<uint32_t>(P)
+                                   : nullptr;
+    c.t = 0.0f;
+    float raw = 0.0f;
+    if (!fx_eval(m[kClumpMask], table, perm, c, &raw)) { return false; }
+    const float mask = std_clamp(raw, 0.0f, 1.0f);
+    if (mask <= 0.0f) { return true; }
+    FxContext gc = c;
+    fx_guide_context(gc, cg, g);
+    float noise = 0.0f;
+    uint32_t flags = 0u;
+    if (shared) {
+        const float4 head = entries[0];
+        noise = head.x;
+        flags = __float_as_uint(head.y);
+        if (flags & kGuideNoiseFailed) { return false; }
+    } else {
+        if (!fx_eval(m[kClumpNoise], table, perm, gc, &raw)) { return false; }
+        noise = std_max(raw, 0.0f);
+    }
+    const bool noisy = noise > 1.0e-5f && mask > 1.0e-4f;
+    FxGuideNoise gn;
+    if (noisy) {
+        if (shared) {
+            if (flags & kGuideRestFailed) { return false; }
+        } else {
+            float raw_frequency = 0.0f, raw_correlation = 0.0f;
+            if (!fx_eval(m[kClumpNoiseFrequency], table, perm, gc, &raw_frequency) ||
+                !fx_eval(m[kClumpNoiseCorrelation], table, perm, gc, &raw_correlation)) {
+                return false;
+            }
+            gn.begin(cg, g, axis, source, P, raw_frequency, raw_correlation);
+        }
     }
     fx_cut_to_length(k, scratch, P, cg.spline_lengths[g], tb);
     c.c_length = fx_spline_length(k, P, tb);
     if (!fx_eval(m[kClumpAmount], table, perm, c, &raw)) { return false; }
     const float pull = __fmul_rn(mask, std_clamp(raw, 0.0f, 1.0f));
-    float travelled = 0.0f;
+    const float strength = __fmul_rn(mask, noise);
+    // clumpScale depends on the CV only through a ramp of t; without one it
+    // is taken once.
+    const bool scale_per_cv = m[kClumpScale].ramp_count != 0u;
+    float factor = 0.0f;
+    if (!scale_per_cv) {
+        float scale = 0.0f;
+        c.t = tb.t[1];
+        if (!fx_eval(m[kClumpScale], table, perm, c, &scale)) { return false; }
+        factor = __fmul_rn(pull, __fsub_rn(1.0f, __fmul_rn(2.0f, scale)));
+    }
     for (int cv = 1; cv < P; ++cv) {
         F3 displacement{0.0f, 0.0f, 0.0f};
         if (noisy) {
-            const F3 d = xsub(ld3(source, cv), ld3(source, cv - 1));
-            travelled = __fadd_rn(travelled, __fsqrt_rn(xdot(d, d)));
-            F3 su = tu, sv = tv, nt = ct;
-            bool advance = false;
-            if (cv + 1 < P) {
-                const F3 segment = xsub(ld3(axis, cv + 1), ld3(axis, cv));
-                if (xdot(segment, segment) > 1.0e-20f) {
-                    nt = xnormalize(segment);
-                    if (fabsf(xdot(ct, nt)) < 0.99999f) {
-                        su = fx_rotate_between(tu, ct, nt, 0.5f);
-                        sv = fx_rotate_between(tv, ct, nt, 0.5f);
-                        advance = true;
-                    } else {
-                        ct = nt;
-                    }
-                }
-            }
-            gc.t = tb.t[cv];
+            F3 unit;
             float raw_scale = 0.0f;
-            if (!fx_eval(m[kClumpNoiseScale], table, perm, gc, &raw_scale)) { return false; }
-            const float magnitude = __fmul_rn(__fmul_rn(mask, noise), std_max(raw_scale, 0.0f));
-            if (!isfinite(magnitude)) { return false; }
-            const float distance = __fmul_rn(travelled, effective_frequency);
-            const float first = __fsub_rn(classic_noise(table, __fadd_rn(domain.x, distance), domain.y, domain.z), 0.5f);
-            const float second = __fsub_rn(classic_noise(table, domain.x, domain.y, __fadd_rn(domain.z, distance)), 0.5f);
-            displacement = xmul(xadd(xmul(su, first), xmul(sv, second)), magnitude);
-            if (advance) {
-                tu = fx_rotate_between(tu, ct, nt, 1.0f);
-                tv = fx_rotate_between(tv, ct, nt, 1.0f);
-                ct = nt;
+            if (shared) {
+                const float4 e = entries[cv];
+                unit = F3{e.x, e.y, e.z};
+                raw_scale = e.w;
+            } else {
+                gc.t = tb.t[cv];
+                if (!fx_eval(m[kClumpNoiseScale], table, perm, gc, &raw_scale)) { return false; }
+                unit = gn.step(axis, source, P, cv, table);
             }
+            const float magnitude = __fmul_rn(strength, std_max(raw_scale, 0.0f));
+            if (!isfinite(magnitude)) { return false; }
+            displacement = xmul(unit, magnitude);
         }
         c.t = tb.t[cv];
-        float scale = 0.0f;
-        if (!fx_eval(m[kClumpScale], table, perm, c, &scale)) { return false; }
+        if (scale_per_cv) {
+            float scale = 0.0f;
+            if (!fx_eval(m[kClumpScale], table, perm, c, &scale)) { return false; }
+            factor = __fmul_rn(pull, __fsub_rn(1.0f, __fmul_rn(2.0f, scale)));
+        }
         const F3 current = k.p[cv];
-        const F3 pulled = xadd(current, xmul(xsub(ld3(axis, cv), current),
-                                             __fmul_rn(pull, __fsub_rn(1.0f, __fmul_rn(2.0f, scale)))));
-        k.p[cv] = xadd(pulled, displacement);
+        k.p[cv] = xadd(xadd(current, xmul(xsub(ld3(axis, cv), current), factor)), displacement);
     }
     *clumped = true;
     return true;
@@ -647,7 +714,9 @@ __global__ void __launch_bounds__(128, 5) classic_fx_kernel(const FxArgs k) {
                     code = NXG_ERROR_INVALID_ARGUMENT;
                 } else {
                     const nxg_classic_clump_guides guides = k.clumps[clump];
-                    ok = fx_clump(curve, scratch, P, plan.effect[e], guides, i, table, perm, tb, c, &code, &changed);
+                    const bool shared = guides.noise_table != nullptr && plan.guide_noise_shared[e] != 0u;
+                    ok = fx_clump(curve, scratch, P, plan.effect[e], guides, shared, i, table, perm, tb, c, &code,
+                                  &changed);
                 }
                 ++clump;
             } else if (plan.effect_type[e] == NXG_CLASSIC_FX_NOISE && k.surface_tangents == nullptr) {
@@ -701,6 +770,65 @@ __global__ void __launch_bounds__(128, 5) classic_fx_kernel(const FxArgs k) {
         for (int j = 0; j < P; ++j) { pts[j] = make_float4(curve.p[j].x, curve.p[j].y, curve.p[j].z, radii[j]); }
         if (!keep) { k.point_counts[i] = 0u; }
     }
+}
+
+// The guide-noise table of the plan's ClumpingFX module number `module`,
+// one thread per guide: the guide noise evaluated once per guide instead of
+// once per strand, when the module's guide-noise programs read no per-strand
+// input.  Entry 0 holds (noise, failure flags); entries 1.. the unit
+// displacement and the raw noiseScale.  The early-outs and failures of
+// build_clump_noise_axis are kept as flags, for the strands to apply with
+// their own mask.
+__global__ void __launch_bounds__(128) clump_guide_noise_kernel(const FxPlan *plan_ptr, uint32_t module,
+                                                                const nxg_classic_clump_guides cg, uint32_t P) {
+    __shared__ float4 table[256];
+    __shared__ uint8_t perm[256];
+    __shared__ FxTables tb;
+    stage_classic_tables(table, perm);
+    fx_fill_tables(tb, static_cast<int>(P));
+    __syncthreads();
+    const FxPlan &plan = *plan_ptr;
+    int effect = -1;
+    for (uint32_t e = 0, seen = 0; e < plan.effect_count; ++e) {
+        if (plan.effect_type[e] == NXG_CLASSIC_FX_CLUMP && seen++ == module) { effect = static_cast<int>(e); }
+    }
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (effect < 0 || !plan.guide_noise_shared[effect] || g >= cg.guide_count) { return; }
+    const DeviceExpression *m = plan.effect[effect];
+    const int n = static_cast<int>(P);
+    const float *axis = cg.render_axes + 3u * static_cast<uint64_t>(g) * P;
+    const float *source = cg.axes + 3u * static_cast<uint64_t>(g) * P;
+    float4 *out = reinterpret_cast<float4 *>(cg.noise_table) + static_cast<uint64_t>(g) * P;
+    FxContext gc{};
+    fx_guide_context(gc, cg, g);
+    uint32_t flags = 0u;
+    float raw = 0.0f, noise = 0.0f;
+    if (!fx_eval(m[kClumpNoise], table, perm, gc, &raw)) {
+        flags = kGuideNoiseFailed;
+    } else {
+        noise = std_max(raw, 0.0f);
+    }
+    if (flags == 0u && noise > 1.0e-5f) {
+        float raw_frequency = 0.0f, raw_correlation = 0.0f;
+        if (!fx_eval(m[kClumpNoiseFrequency], table, perm, gc, &raw_frequency) ||
+            !fx_eval(m[kClumpNoiseCorrelation], table, perm, gc, &raw_correlation)) {
+            flags = kGuideRestFailed;
+        } else {
+            FxGuideNoise gn;
+            gn.begin(cg, g, axis, source, n, raw_frequency, raw_correlation);
+            for (int cv = 1; cv < n; ++cv) {
+                gc.t = tb.t[cv];
+                float raw_scale = 0.0f;
+                if (!fx_eval(m[kClumpNoiseScale], table, perm, gc, &raw_scale)) {
+                    flags = kGuideRestFailed;
+                    break;
+                }
+                const F3 unit = gn.step(axis, source, n, cv, table);
+                out[cv] = make_float4(unit.x, unit.y, unit.z, raw_scale);
+            }
+        }
+    }
+    out[0] = make_float4(noise, __uint_as_float(flags), 0.0f, 0.0f);
 }
 
 // prepare_xgen_classic_clump_runtime_data (xgen_classic_runtime.cpp:839-892)
@@ -796,6 +924,22 @@ uint32_t nxg_classic_fx_plan_upload(const nxg_classic_fx_plan *plan, void *devic
             return NXG_ERROR_INVALID_ARGUMENT;
         }
     }
+    // A ClumpingFX module's guide noise is shared by the strands of a guide
+    // when its programs bind none of $id, $cLength, $cWidth, noise($Prefg).
+    for (uint32_t e = 0; e < plan->effect_count; ++e) {
+        if (host.effect_type[e] != NXG_CLASSIC_FX_CLUMP) { continue; }
+        bool shared = true;
+        for (int slot : {nxg::dev::kClumpNoise, nxg::dev::kClumpNoiseScale, nxg::dev::kClumpNoiseFrequency,
+                         nxg::dev::kClumpNoiseCorrelation}) {
+            const nxg::DeviceExpression &d = host.effect[e][slot];
+            for (uint32_t i = 0; i < d.input_count; ++i) {
+                const uint8_t b = d.input_binding[i];
+                shared = shared && b != nxg::kBindPrefNoise && b != nxg::kBindId && b != nxg::kBindCLength &&
+                         b != nxg::kBindCWidth;
+            }
+        }
+        host.guide_noise_shared[e] = shared ? 1u : 0u;
+    }
     // cLength is recomputed after an effect only for a program that follows
     // it: a later effect's, or the width profile's.
     uint32_t later = host.taper.uses_clength | host.taper_start.uses_clength | host.width_ramp.uses_clength;
@@ -862,6 +1006,12 @@ uint32_t nxg_classic_fx_apply(const void *device_plan, const nxg_classic_fx_curv
     const uint32_t threads = 128u;
     const uint32_t blocks = static_cast<uint32_t>(std::min<uint64_t>(
         (uint64_t{k.count} + threads - 1u) / threads, static_cast<uint64_t>(nxg::device_sm_count()) * 16u));
+    for (uint32_t m = 0; m < curves->clump_count; ++m) {
+        const nxg_classic_clump_guides &g = curves->clumps[m];
+        if (!g.noise_table || g.guide_count == 0u) { continue; }
+        nxg::dev::clump_guide_noise_kernel<<<(g.guide_count + 127u) / 128u, 128u, 0,
+                                             static_cast<cudaStream_t>(stream)>>>(k.plan, m, g, k.P);
+    }
     nxg::dev::classic_fx_kernel<<<blocks, threads, 0, static_cast<cudaStream_t>(stream)>>>(k);
     return nxg::record_cuda(cudaGetLastError());
 }

@@ -76,7 +76,7 @@ def _run(curves, reference, primitive, effects, radius_scale=1.0, description_id
                         roots=dev(roots.view(np.int32).reshape(-1, 12)), root_uvs=dev(uvs),
                         point_counts=dev(counts.view(np.int32)))
     guides = [ClumpGuides(c["axes"], c["normals"], c["tangents"], c["uvs"], c["prefixes"], c["strand_guides"],
-                          c.get("reference_positions")) for c in clumps]
+                          c.get("reference_positions"), noise_table=c.get("noise_table", True)) for c in clumps]
     status = classic_fx_apply(plan, mine, dev(tangents) if plan.has_noise else None, radius_scale,
                               random_prefixes=None if prefixes is None else dev(prefixes.view(np.int32)),
                               clumps=guides)
@@ -87,7 +87,7 @@ def _run(curves, reference, primitive, effects, radius_scale=1.0, description_id
     inputs = np.stack([reference.classic_noise(roots["position"], f) for f in freqs], 1) if len(freqs) else None
     theirs = reference.classic_apply_fx(rplan, pts, counts, roots, uvs, P, radius_scale, inputs,
                                         tangents if plan.has_noise else None, workers=8, random_prefixes=prefixes,
-                                        clumps=clumps)
+                                        clumps=[{k: v for k, v in c.items() if k != "noise_table"} for c in clumps])
     return (status.cpu().tolist(), mine.points.cpu().numpy(), mine.point_counts.cpu().numpy().view(np.uint32)), theirs
 
 
@@ -197,11 +197,15 @@ def test_clump_prepare_matches_reference(curves, reference):
     np.testing.assert_array_equal(mine.spline_lengths.cpu().numpy().view(np.uint32), lengths.view(np.uint32))
 
 
-def test_clump_fx(curves, reference):
-    g = _clump_guides(curves)
-    mine, theirs = _run(curves, reference, {"width": "0.01"}, [("clump", CLUMP)], clumps=[g])
+@pytest.mark.parametrize("path", ["per guide", "per strand", "strand input"])
+def test_clump_fx(curves, reference, path):
+    # The guide noise from the per-guide table, evaluated per strand (no
+    # table), and per strand because a guide-noise program reads $id.
+    g = dict(_clump_guides(curves), noise_table=path != "per strand")
+    clump = dict(CLUMP, noiseScale="0.5 + hash($id)") if path == "strand input" else CLUMP
+    mine, theirs = _run(curves, reference, {"width": "0.01"}, [("clump", clump)], clumps=[g])
     err, kept = _check(curves, mine, theirs)
-    print("ClumpingFX: max error %.3g x diag, %d strands" % (err, kept))
+    print("ClumpingFX (%s): max error %.3g x diag, %d strands" % (path, err, kept))
 
 
 def test_clump_without_noise_is_exact(curves, reference):
