@@ -394,7 +394,7 @@ __device__ inline float fx_cut(FxCurve &k, FxCurve &scratch, int P, float amount
     return cut_parameter;
 }
 
-// rotate_between (xgen_classic_runtime.cpp:1103-1116): `value` turned about
+// rotate_between (xgen_classic_runtime.cpp:1106-1118): `value` turned about
 // from x to by `fraction` of the angle between them.
 __device__ inline F3 fx_rotate_between(F3 value, F3 from, F3 to, float fraction) {
     F3 axis = xcross(from, to);
