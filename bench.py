@@ -46,7 +46,7 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["nxg", "reference"], default="nxg")
     ap.add_argument("--workload", choices=["large", "batched", "motion", "classic", "batched_classic",
-                                           "asset_build", "classic_fx"],
+                                           "asset_build", "classic_fx", "curve_cache"],
                     default="large",
                     help="large: the single large description (headline); batched: nine descriptions in one "
                          "persistent launch vs. one launch per description; motion: five shutter samples of the "
@@ -970,6 +970,117 @@ def run_classic_fx(args):
     print(json.dumps(line), flush=True)
 
 
+def run_curve_cache(args):
+    """Curve-cache (.nxc) ingest on the device: a cache of the large
+    description's generated frame (1,000,000 strands x 32 CVs of float4,
+    point counts, root uvs as patch uvs, triangles as face ids; 530 MB),
+    uploaded once; a step is one nxg_curve_cache_validate_device pass over
+    the device copy (every element check of validate_curve_cache, the
+    point-count sum and the bit checksum), timed with CUDA events; the blob
+    exceeds L2, which is also flushed between steps.  `e2e` adds the upload
+    of the blob from pinned host memory and the read-back of the result.
+    The CPU baseline is the reference's validate_curve_cache on the same
+    blob (serial: its content hash is a dependent chain over 64-bit words),
+    with this library's host hash of the same bytes beside it."""
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    from nanoxgen_b200.asset import build_asset
+    from nanoxgen_b200.curve_cache import (DeviceCurveCache, build_curve_cache, content_hash, header,
+                                           point_checksum)
+    from nanoxgen_b200.generator import DeviceAsset, generate_packed
+    device = torch.device("cuda", 0)
+    torch.cuda.set_device(device)
+    w = workload(args.strands)
+    asset = build_asset(w.build_input, w.stencil_slots)
+    out = generate_packed(DeviceAsset(asset, device), w.params)
+    torch.cuda.synchronize()
+    S, P = int(w.params.strand_count), int(w.params.cvs_per_strand)
+    roots = out.roots_numpy()
+    blob = build_curve_cache(np.full(S, P, np.uint32), out.points.cpu().numpy(),
+                             patch_uvs=out.root_uvs.cpu().numpy(), face_ids=roots["triangle_index"])
+    del out
+    h = header(blob)
+    cache = DeviceCurveCache(blob, device)
+    pinned = torch.empty(blob.size, dtype=torch.uint8, pin_memory=True)
+    pinned.numpy()[:] = blob
+    result_host = torch.empty(cache.result.numel(), dtype=torch.uint8, pin_memory=True)
+    stream = torch.cuda.current_stream(device)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=device)
+    algorithmic = 4 * S + 16 * h.point_count + 8 * S  # counts, points, patch uvs
+    for _ in range(args.warmup):
+        flush.fill_(1)
+        cache.validate(stream)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(0)
+    sampler.start()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for k in range(args.steps):
+        flush.fill_(k & 0xFF)
+        ev[k][0].record(stream)
+        cache.validate(stream)
+        ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    ms = statistics.mean(a.elapsed_time(b) for a, b in ev)
+    message, point_sum, checksum = cache.outcome()
+    host_checksum = point_checksum(blob)
+    if message or point_sum != h.point_count or checksum != host_checksum:
+        raise SystemExit("device check disagrees with the host: %r %d %d" % (message, point_sum, checksum))
+    # e2e: upload + check + result read-back per step
+    e2e = []
+    for k in range(max(3, args.steps // 2)):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        cache.blob.copy_(pinned, non_blocking=True)
+        cache.validate(stream)
+        result_host.copy_(cache.result, non_blocking=True)
+        b.record(stream)
+        b.synchronize()
+        e2e.append(a.elapsed_time(b))
+    e2e_ms = statistics.median(e2e)
+    peak, peak_kind = measured_peak()
+    achieved = algorithmic / (ms / 1e3) / 1e9
+    line = {"metric": "points/sec", "value": h.point_count / (ms / 1e3), "unit": "points/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32/f32", "data": "synthetic",
+            "config": {"workload": "curve-cache/displaced-sphere-200k-tris/%d-strands-x%d" % (S, P),
+                       "blob_bytes": int(blob.size), "sections": "point counts, points, patch uvs, face ids",
+                       "l2": "blob larger than L2; flushed between steps (256 MiB write)",
+                       "reference_doc": "the reference's own GPU traversal of 47.4 M cached points: 1.24 ms "
+                                        "(docs/xgen-research.md:266-268, other hardware)"},
+            "roofline": {"bound": "hbm", "kernel": "check_kernel", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                         "traffic": None, "algorithmic_bytes": algorithmic},
+            "device_check": {"message": message, "point_sum": point_sum, "checksum": "%016x" % checksum},
+            "e2e": {"value": h.point_count / (e2e_ms / 1e3), "unit": "points/s",
+                    "h2d_bytes_per_step": int(blob.size), "d2h_bytes_per_step": int(cache.result.numel())},
+            "clocks": clocks, "gpu_launches": 3 * args.steps}
+    if not args.no_cpu_baseline:
+        from oracle.checker import Reference, reference_available
+        t0 = time.perf_counter()
+        ours = content_hash(blob[128:])
+        hash_s = time.perf_counter() - t0
+        base = {"cores": 1, "cpu_model": cpu_model(), "host_content_hash_s": hash_s,
+                "host_content_hash_matches": ours == h.content_hash}
+        if reference_available():
+            ref = Reference()
+            times = []
+            for _ in range(3):
+                t0 = time.perf_counter()
+                msg = ref.curve_cache_validate(blob)
+                times.append(time.perf_counter() - t0)
+            med = statistics.median(times)
+            base.update({"value": h.point_count / med, "unit": "points/s", "kind": "reference",
+                         "median_s": med, "message": msg,
+                         "sample": "the reference's validate_curve_cache on the whole %d-byte blob "
+                                   "(median of 3 calls)" % blob.size})
+        line["cpu_baseline"] = base
+    print(json.dumps(line), flush=True)
+
+
 def run_asset_build(args):
     """The asset build of the large description's mesh (200,000 triangles,
     4,096 guides): the per-triangle stencil search (stencil.cu) timed alone
@@ -1056,6 +1167,8 @@ def main():
         run_asset_build(args)
     elif args.workload == "classic_fx":
         run_classic_fx(args)
+    elif args.workload == "curve_cache":
+        run_curve_cache(args)
     else:
         run_gpu_arm(args)
 

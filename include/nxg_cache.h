@@ -111,9 +111,10 @@ uint32_t nxg_curve_cache_validate(const void *blob, uint64_t size);
 /* content_hash over `size` bytes (the blob's bytes after the header). */
 uint64_t nxg_curve_cache_content_hash(const void *bytes, uint64_t size);
 
-/* The bit checksum of the device check, on the host: the sum modulo 2^64 of
- * mix64(word ^ (index << 32)) over the points section's 32-bit words, with
- * mix64 the SplitMix64 finaliser (Steele, Lea and Flood, 2014). */
+/* The bit checksum of the device check, on the host: over the points, the
+ * sum modulo 2^64 of mix64((xy ^ i * 0x9e3779b97f4a7c15) + zw *
+ * 0xd6e8feb86659fd93), with xy and zw point i's two little-endian 64-bit
+ * words and mix64 the SplitMix64 finaliser (Steele, Lea and Flood, 2014). */
 uint64_t nxg_curve_cache_point_checksum(const void *blob, uint64_t size);
 
 typedef struct nxg_curve_cache_check {

@@ -218,6 +218,35 @@ class ClassicFxCurves(ctypes.Structure):
                 ("clump_count", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
 
 
+class CurveCacheInput(ctypes.Structure):
+    """nxg_curve_cache_input (nxg_cache.h)."""
+    _fields_ = [(name, t) for pair in (("point_counts", "strand_count"), ("points", "point_count"),
+                                        ("texcoords", "texcoord_count"), ("patch_uvs", "patch_uv_count"),
+                                        ("face_uvs", "face_uv_count"), ("face_ids", "face_id_count"),
+                                        ("motion_times", "motion_sample_count"),
+                                        ("motion_points", "motion_point_count"))
+                for name, t in ((pair[0], ctypes.c_void_p), (pair[1], ctypes.c_uint64))]
+
+
+class CurveCacheHeader(ctypes.Structure):
+    """nxg_curve_cache_header (nxg_cache.h): CurveCacheHeader, 128 bytes."""
+    _fields_ = [("magic", ctypes.c_uint64), ("version_major", ctypes.c_uint16), ("version_minor", ctypes.c_uint16),
+                ("flags", ctypes.c_uint32), ("byte_size", ctypes.c_uint64), ("content_hash", ctypes.c_uint64),
+                ("strand_count", ctypes.c_uint32), ("point_count", ctypes.c_uint32),
+                ("motion_sample_count", ctypes.c_uint32), ("reserved", ctypes.c_uint32),
+                ("point_counts_offset", ctypes.c_uint64), ("points_offset", ctypes.c_uint64),
+                ("motion_times_offset", ctypes.c_uint64), ("motion_points_offset", ctypes.c_uint64),
+                ("texcoords_offset", ctypes.c_uint64), ("patch_uvs_offset", ctypes.c_uint64),
+                ("face_uvs_offset", ctypes.c_uint64), ("face_ids_offset", ctypes.c_uint64),
+                ("padding", ctypes.c_uint8 * 16)]
+
+
+class CurveCacheCheck(ctypes.Structure):
+    """nxg_curve_cache_check (nxg_cache.h)."""
+    _fields_ = [("error", ctypes.c_uint32), ("reserved", ctypes.c_uint32), ("point_sum", ctypes.c_uint64),
+                ("checksum", ctypes.c_uint64), ("first_bad", ctypes.c_uint64 * 8)]
+
+
 CLASSIC_FX_NOISE = 0
 CLASSIC_FX_CUT = 1
 CLASSIC_FX_CLUMP = 2
@@ -401,6 +430,14 @@ _SIGNATURES = {
     "nxg_classic_fx_plan_upload": (ctypes.c_uint32, [ctypes.POINTER(ClassicFxPlan), _P, ctypes.c_uint64, _P]),
     "nxg_classic_fx_apply": (ctypes.c_uint32, [_P, ctypes.POINTER(ClassicFxCurves), _P, _P]),
     "nxg_classic_clump_prepare": (ctypes.c_uint32, [_P, ctypes.c_uint32, ctypes.c_uint32, _P, _P, _P]),
+    "nxg_curve_cache_error_message": (ctypes.c_char_p, [ctypes.c_uint32]),
+    "nxg_curve_cache_build": (ctypes.c_uint32, [ctypes.POINTER(CurveCacheInput), ctypes.POINTER(ctypes.c_void_p),
+                                                ctypes.POINTER(ctypes.c_uint64), ctypes.c_char_p, ctypes.c_uint64]),
+    "nxg_curve_cache_validate": (ctypes.c_uint32, [_P, ctypes.c_uint64]),
+    "nxg_curve_cache_content_hash": (ctypes.c_uint64, [_P, ctypes.c_uint64]),
+    "nxg_curve_cache_point_checksum": (ctypes.c_uint64, [_P, ctypes.c_uint64]),
+    "nxg_curve_cache_validate_device": (ctypes.c_uint32, [_P, _P, ctypes.c_uint64, _P,
+                                                          ctypes.POINTER(ctypes.c_uint32), _P]),
     "nxg_classic_root_scalars": (ctypes.c_uint32, [ctypes.POINTER(DeviceAssetDesc), ctypes.POINTER(GenerationParams),
                                                    ctypes.POINTER(ClassicScalarPlan), ctypes.c_uint32,
                                                    ctypes.c_uint32, _P, _P, _P]),

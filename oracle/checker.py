@@ -466,6 +466,43 @@ class Reference:
         plan.effect_counts = tuple(int(c) for c in counts)
         return plan
 
+    def curve_cache_build(self, point_counts, points, texcoords=None, patch_uvs=None, face_uvs=None,
+                          face_ids=None, motion_times=None, motion_points=None) -> np.ndarray:
+        """build_curve_cache: the blob as uint8 (raises ValueError with the
+        reference's message)."""
+        lib = self.lib
+        if not getattr(self, "_cache_ready", False):
+            lib.ref_curve_cache_build.restype = ctypes.c_uint64
+            lib.ref_curve_cache_build.argtypes = [_P, ctypes.c_uint64] * 8 + [_P, ctypes.c_uint64, ctypes.c_char_p,
+                                                                             ctypes.c_uint64]
+            lib.ref_curve_cache_validate.argtypes = [_P, ctypes.c_uint64, ctypes.c_char_p, ctypes.c_uint64]
+            self._cache_ready = True
+        keep, args = [], []
+        for value, dtype, width in ((point_counts, np.uint32, 1), (points, np.float32, 4), (texcoords, np.float32, 2),
+                                    (patch_uvs, np.float32, 2), (face_uvs, np.float32, 2), (face_ids, np.uint32, 1),
+                                    (motion_times, np.float32, 1), (motion_points, np.float32, 3)):
+            if value is None:
+                args += [None, 0]
+                continue
+            a = np.ascontiguousarray(value, dtype)
+            keep.append(a)
+            args += [a.ctypes.data, a.size // width]
+        msg = ctypes.create_string_buffer(512)
+        size = lib.ref_curve_cache_build(*args, None, 0, msg, 512)
+        if size == 0:
+            raise ValueError(msg.value.decode())
+        out = np.zeros(size, np.uint8)
+        lib.ref_curve_cache_build(*args, out.ctypes.data, size, msg, 512)
+        return out
+
+    def curve_cache_validate(self, blob: np.ndarray) -> str:
+        """validate_curve_cache's message ("" when valid); `blob` must be
+        64-byte aligned for the reference's alignment check to pass."""
+        self.curve_cache_build([2], [[0, 0, 0, 0.1], [0, 1, 0, 0.1]])  # sets the prototypes
+        msg = ctypes.create_string_buffer(512)
+        self.lib.ref_curve_cache_validate(blob.ctypes.data, blob.size, msg, 512)
+        return msg.value.decode()
+
     def classic_clump_prepare(self, axes):
         """prepare_xgen_classic_clump_runtime_data of world-space guide axes
         [G, P, 3]: (render axes [G, P, 3], spline lengths [G])."""
