@@ -46,7 +46,7 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["nxg", "reference"], default="nxg")
     ap.add_argument("--workload", choices=["large", "batched", "motion", "classic", "batched_classic",
-                                           "asset_build", "classic_fx", "curve_cache"],
+                                           "asset_build", "classic_fx", "curve_cache", "payload"],
                     default="large",
                     help="large: the single large description (headline); batched: nine descriptions in one "
                          "persistent launch vs. one launch per description; motion: five shutter samples of the "
@@ -1081,6 +1081,95 @@ def run_curve_cache(args):
     print(json.dumps(line), flush=True)
 
 
+def run_payload(args):
+    """Renderer payload batches: the large description's generated frame
+    (1,000,000 strands x 32 CVs) as the base curve set (positions, widths =
+    2 x radius, root uvs) with one motion sample (the positions moved by
+    0.01), cut into 65,536-strand batches through an affine transform -- one
+    nxg_build_curve_batches per step over resident inputs, timed with CUDA
+    events (inputs and outputs exceed L2; L2 is also flushed between steps).
+    The CPU baseline is the reference's build_curve_batches on a 100,000-strand
+    prefix of the same set (single-threaded, as the reference is)."""
+    import numpy as np
+    import torch
+
+    from nanoxgen_b200.asset import build_asset
+    from nanoxgen_b200.generator import DeviceAsset, generate_packed
+    from nanoxgen_b200.payload import Curves, build_curve_batches
+    device = torch.device("cuda", 0)
+    torch.cuda.set_device(device)
+    w = workload(args.strands)
+    out = generate_packed(DeviceAsset(build_asset(w.build_input, w.stencil_slots), device), w.params)
+    torch.cuda.synchronize()
+    S, P = int(w.params.strand_count), int(w.params.cvs_per_strand)
+    xyz = out.points[:, :3].contiguous()
+    widths = (2.0 * out.points[:, 3]).contiguous()
+    uvs = out.root_uvs.contiguous()
+    moved = (xyz + 0.01).contiguous()
+    del out
+    transform = (0.98, -0.17, 0.0, 0.5, 0.17, 0.98, 0.0, -0.25, 0.0, 0.0, 1.0, 2.0)
+    base = Curves(points=xyz, strand_count=S, fixed_cvs_per_strand=P, widths=widths, root_uvs=uvs)
+    sample = Curves(points=moved, strand_count=S, fixed_cvs_per_strand=P, constant_width=0.0)
+    kw = dict(max_strands_per_batch=65536, transform=transform)
+    stream = torch.cuda.current_stream(device)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=device)
+    result = None
+    for _ in range(args.warmup):
+        flush.fill_(1)
+        result = build_curve_batches(base, [(0.5, sample)], **kw)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(0)
+    sampler.start()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for k in range(args.steps):
+        flush.fill_(k & 0xFF)
+        ev[k][0].record(stream)
+        result = build_curve_batches(base, [(0.5, sample)], **kw)
+        ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    ms = statistics.mean(a.elapsed_time(b) for a, b in ev)
+    points = S * P
+    # reads: base xyz + widths, sample xyz, root uvs; writes: float4 points,
+    # motion xyz, counts, root uvs
+    algorithmic = points * (12 + 4 + 12) + S * 8 + points * (16 + 12) + S * (4 + 8)
+    peak, peak_kind = measured_peak()
+    achieved = algorithmic / (ms / 1e3) / 1e9
+    line = {"metric": "points/sec", "value": points / (ms / 1e3), "unit": "points/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "payload/displaced-sphere-200k-tris/%d-strands-x%d/1-motion-sample" % (S, P),
+                       "batches": int(result.batch_first_point.numel() - 1), "max_strands_per_batch": 65536,
+                       "transform": transform, "l2": "inputs and outputs larger than L2; flushed between steps"},
+            "roofline": {"bound": "hbm", "kernel": "batches_kernel", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                         "algorithmic_bytes": algorithmic},
+            "clocks": clocks, "gpu_launches": args.steps}
+    if not args.no_cpu_baseline:
+        from oracle.checker import Reference, reference_available
+        if reference_available():
+            n = 100_000
+            host = lambda t: t[:n * P].cpu().numpy()
+            rbase = dict(points=host(xyz), strands=n, fixed=P, widths=host(widths), root_uvs=uvs[:n].cpu().numpy())
+            rsample = dict(points=host(moved), strands=n, fixed=P)
+            ref = Reference()
+            times = []
+            for _ in range(3):
+                t0 = time.perf_counter()
+                theirs = ref.build_curve_batches(rbase, [(0.5, rsample)], per_batch=65536, transform=transform)
+                times.append(time.perf_counter() - t0)
+            med = statistics.median(times)
+            mine = result.points[:n * P].cpu().numpy()
+            same = bool(np.array_equal(mine.view(np.uint32), theirs["points"].view(np.uint32)))
+            line["cpu_baseline"] = {"value": n * P / med, "unit": "points/s", "cores": 1, "kind": "reference",
+                                    "cpu_model": cpu_model(), "median_s": med,
+                                    "sample": "the reference's build_curve_batches on the first %d strands "
+                                              "(median of 3 calls, including the test shim's copy of its batches "
+                                              "into flat arrays)" % n,
+                                    "parity": {"strands_checked": n, "points_bit_identical": same}}
+    print(json.dumps(line), flush=True)
+
+
 def run_asset_build(args):
     """The asset build of the large description's mesh (200,000 triangles,
     4,096 guides): the per-triangle stencil search (stencil.cu) timed alone
@@ -1169,6 +1258,8 @@ def main():
         run_classic_fx(args)
     elif args.workload == "curve_cache":
         run_curve_cache(args)
+    elif args.workload == "payload":
+        run_payload(args)
     else:
         run_gpu_arm(args)
 

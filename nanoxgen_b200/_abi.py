@@ -247,6 +247,33 @@ class CurveCacheCheck(ctypes.Structure):
                 ("checksum", ctypes.c_uint64), ("first_bad", ctypes.c_uint64 * 8)]
 
 
+class CurveSet(ctypes.Structure):
+    """nxg_curve_set (nxg_payload.h): the reference's CurveSetView on the device."""
+    _fields_ = [("strand_count", ctypes.c_uint32), ("fixed_cvs_per_strand", ctypes.c_uint32),
+                ("point_counts", ctypes.c_void_p), ("points", ctypes.c_void_p), ("point_count", ctypes.c_uint64),
+                ("widths", ctypes.c_void_p), ("root_uvs", ctypes.c_void_p), ("roots", ctypes.c_void_p),
+                ("constant_width", ctypes.c_float), ("reserved", ctypes.c_uint32)]
+
+
+class MotionSet(ctypes.Structure):
+    """nxg_motion_set (nxg_payload.h)."""
+    _fields_ = [("time", ctypes.c_float), ("reserved", ctypes.c_uint32), ("curves", CurveSet)]
+
+
+class PayloadOptions(ctypes.Structure):
+    """nxg_payload_options (nxg_payload.h)."""
+    _fields_ = [("max_strands_per_batch", ctypes.c_uint32), ("resample_cv_count", ctypes.c_uint32),
+                ("radius_scale", ctypes.c_float), ("transform", ctypes.c_float * 12)]
+
+
+class PayloadOutput(ctypes.Structure):
+    """nxg_payload_output (nxg_payload.h)."""
+    _fields_ = [("point_counts", ctypes.c_void_p), ("points", ctypes.c_void_p), ("root_uvs", ctypes.c_void_p),
+                ("motion_points", ctypes.c_void_p), ("batch_first_point", ctypes.c_void_p)]
+
+
+PAYLOAD_MAX_SAMPLES = 32
+
 CLASSIC_FX_NOISE = 0
 CLASSIC_FX_CUT = 1
 CLASSIC_FX_CLUMP = 2
@@ -431,6 +458,13 @@ _SIGNATURES = {
     "nxg_classic_fx_apply": (ctypes.c_uint32, [_P, ctypes.POINTER(ClassicFxCurves), _P, _P]),
     "nxg_classic_clump_prepare": (ctypes.c_uint32, [_P, ctypes.c_uint32, ctypes.c_uint32, _P, _P, _P]),
     "nxg_curve_cache_error_message": (ctypes.c_char_p, [ctypes.c_uint32]),
+    "nxg_payload_error_message": (ctypes.c_char_p, [ctypes.c_uint32]),
+    "nxg_payload_point_count": (ctypes.c_uint64, [ctypes.POINTER(CurveSet), ctypes.POINTER(PayloadOptions)]),
+    "nxg_payload_batch_count": (ctypes.c_uint32, [ctypes.POINTER(CurveSet), ctypes.POINTER(PayloadOptions)]),
+    "nxg_payload_workspace_size": (ctypes.c_uint64, [ctypes.POINTER(CurveSet), _P, ctypes.c_uint32]),
+    "nxg_build_curve_batches": (ctypes.c_uint32, [ctypes.POINTER(CurveSet), _P, ctypes.c_uint32,
+                                                  ctypes.POINTER(PayloadOptions), ctypes.POINTER(PayloadOutput),
+                                                  _P, ctypes.c_uint64, _P, ctypes.POINTER(ctypes.c_uint32), _P]),
     "nxg_curve_cache_build": (ctypes.c_uint32, [ctypes.POINTER(CurveCacheInput), ctypes.POINTER(ctypes.c_void_p),
                                                 ctypes.POINTER(ctypes.c_uint64), ctypes.c_char_p, ctypes.c_uint64]),
     "nxg_curve_cache_validate": (ctypes.c_uint32, [_P, ctypes.c_uint64]),

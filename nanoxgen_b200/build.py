@@ -29,7 +29,7 @@ NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-
                      "-Xptxas", "-warn-spills"]
 CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-ffp-contract=off", "-Wall", "-Wextra", "-I" + INCLUDE]
 
-CUDA_SOURCES = ["generate.cu", "batched.cu", "classic.cu", "surrogate.cu", "stencil.cu", "fx.cu", "curve_cache.cu"]
+CUDA_SOURCES = ["generate.cu", "batched.cu", "classic.cu", "surrogate.cu", "stencil.cu", "fx.cu", "curve_cache.cu", "payload.cu"]
 HOST_SOURCES = ["host.cpp", "expression.cpp"]
 
 

@@ -503,6 +503,67 @@ class Reference:
         self.lib.ref_curve_cache_validate(blob.ctypes.data, blob.size, msg, 512)
         return msg.value.decode()
 
+    class _RefCurveSet(ctypes.Structure):
+        _fields_ = [("strands", ctypes.c_uint32), ("fixed", ctypes.c_uint32), ("counts", ctypes.c_void_p),
+                    ("points", ctypes.c_void_p), ("point_count", ctypes.c_uint64), ("widths", ctypes.c_void_p),
+                    ("root_uvs", ctypes.c_void_p), ("roots", ctypes.c_void_p), ("constant_width", ctypes.c_float)]
+
+    def build_curve_batches(self, base: dict, samples=(), per_batch: int = 65536, resample: int = 0,
+                            radius_scale: float = 1.0, transform=(1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0)):
+        """build_curve_batches with the batches concatenated.  A curve set is
+        a dict: points [N, 3], strands, and optionally counts [S], fixed,
+        widths [N], root_uvs [S, 2], roots (RootSample records),
+        constant_width; samples are (time, set) pairs.  Returns point counts,
+        points [total, 4], root uvs (or None), motion points and batch first
+        points; raises ValueError with the reference's message."""
+        lib = self.lib
+        if not getattr(self, "_payload_ready", False):
+            lib.ref_build_curve_batches.restype = ctypes.c_uint64
+            lib.ref_build_curve_batches.argtypes = [_P, _P, _P, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                                    ctypes.c_float, _P, _P, _P, _P, _P, _P, _P, ctypes.c_uint64,
+                                                    ctypes.c_char_p, ctypes.c_uint64]
+            self._payload_ready = True
+        keep = []
+
+        def arr(a, dtype):
+            if a is None:
+                return None
+            a = np.ascontiguousarray(a, dtype)
+            keep.append(a)
+            return a.ctypes.data
+
+        def make(d):
+            pts = np.ascontiguousarray(d["points"], np.float32).reshape(-1, 3)
+            keep.append(pts)
+            return Reference._RefCurveSet(d["strands"], d.get("fixed", 0), arr(d.get("counts"), np.uint32),
+                                          pts.ctypes.data, pts.shape[0], arr(d.get("widths"), np.float32),
+                                          arr(d.get("root_uvs"), np.float32),
+                                          None if d.get("roots") is None else arr(d["roots"], np.uint8),
+                                          d.get("constant_width", 0.0))
+        b = make(base)
+        sets = (Reference._RefCurveSet * max(1, len(samples)))(*[make(c) for _, c in samples])
+        times = np.array([t for t, _ in samples] or [0.0], np.float32)
+        n_points = np.asarray(base["points"]).size // 3
+        S = int(base["strands"])
+        cap = max(1, S * resample if resample else n_points)
+        counts = np.zeros(max(S, 1), np.uint32)
+        points = np.zeros((cap, 4), np.float32)
+        uvs = np.zeros((max(S, 1), 2), np.float32)
+        has = ctypes.c_uint32()
+        motion = np.zeros((max(1, len(samples)) * cap, 3), np.float32)
+        first = np.zeros(max(S, 1) + 2, np.uint64)
+        tr = np.asarray(transform, np.float32)
+        msg = ctypes.create_string_buffer(512)
+        total = lib.ref_build_curve_batches(ctypes.byref(b), sets, times.ctypes.data, len(samples), per_batch,
+                                            resample, radius_scale, tr.ctypes.data, counts.ctypes.data,
+                                            points.ctypes.data, uvs.ctypes.data, ctypes.byref(has), motion.ctypes.data,
+                                            first.ctypes.data, cap, msg, 512)
+        if total == 0 and msg.value:
+            raise ValueError(msg.value.decode())
+        batches = (S + per_batch - 1) // per_batch
+        return dict(point_counts=counts[:S], points=points[:total], root_uvs=uvs[:S] if has.value else None,
+                    motion_points=motion[:len(samples) * total], batch_first_point=first[:batches + 1])
+
     def classic_clump_prepare(self, axes):
         """prepare_xgen_classic_clump_runtime_data of world-space guide axes
         [G, P, 3]: (render axes [G, P, 3], spline lengths [G])."""

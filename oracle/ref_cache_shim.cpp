@@ -6,7 +6,9 @@
 #include "nanoxgen/curve_cache.h"
 #include "nanoxgen/curve_payload.h"
 
+#include <algorithm>
 #include <cstdint>
+#include <stdexcept>
 #include <cstring>
 #include <exception>
 #include <span>
@@ -66,6 +68,81 @@ void ref_curve_cache_validate(const void *bytes, std::uint64_t size, char *msg, 
     put_text(validate_curve_cache(std::span<const std::byte>(static_cast<const std::byte *>(bytes),
                                                              static_cast<std::size_t>(size))),
              msg, cap);
+}
+
+// build_curve_batches over host arrays, with the batches concatenated.
+// A curve set is (strands, fixed CVs, counts or NULL, points [N x 3],
+// point count, widths or NULL, root uvs [S x 2] or NULL, roots or NULL,
+// constant width); samples are `sample_count` such sets with their times.
+// Outputs (capacities in elements): point counts [S], points [total x 4],
+// root uvs [S x 2] (written when the batches carry them; *has_uvs says),
+// motion points [samples * total x 3], batch first points [batches + 1].
+// Returns the total points (0 on error, with the exception text in msg).
+struct RefCurveSet {
+    std::uint32_t strands, fixed;
+    const std::uint32_t *counts;
+    const float *points;
+    std::uint64_t point_count;
+    const float *widths;
+    const float *root_uvs;
+    const void *roots;
+    float constant_width;
+};
+
+std::uint64_t ref_build_curve_batches(const RefCurveSet *base, const RefCurveSet *samples, const float *times,
+                                      std::uint32_t sample_count, std::uint32_t per_batch, std::uint32_t resample,
+                                      float radius_scale, const float *transform, std::uint32_t *out_counts,
+                                      float *out_points, float *out_uvs, std::uint32_t *has_uvs, float *out_motion,
+                                      std::uint64_t *out_first, std::uint64_t capacity, char *msg,
+                                      std::uint64_t cap) {
+    try {
+        const auto view = [](const RefCurveSet &v) {
+            CurveSetView out{};
+            out.strand_count = v.strands;
+            out.fixed_cvs_per_strand = v.fixed;
+            out.point_counts = v.counts ? std::span<const std::uint32_t>(v.counts, v.strands)
+                                        : std::span<const std::uint32_t>{};
+            out.points = std::span<const Vec3>(reinterpret_cast<const Vec3 *>(v.points), v.point_count);
+            out.widths = v.widths ? std::span<const float>(v.widths, v.point_count) : std::span<const float>{};
+            out.root_uvs = v.root_uvs ? std::span<const Vec2>(reinterpret_cast<const Vec2 *>(v.root_uvs), v.strands)
+                                      : std::span<const Vec2>{};
+            out.roots = v.roots ? std::span<const RootSample>(static_cast<const RootSample *>(v.roots), v.strands)
+                                : std::span<const RootSample>{};
+            out.constant_width = v.constant_width;
+            return out;
+        };
+        std::vector<MotionSampleView> motion;
+        for (std::uint32_t k = 0; k < sample_count; ++k) { motion.push_back({times[k], view(samples[k])}); }
+        CurvePayloadOptions options{};
+        options.max_strands_per_batch = per_batch;
+        options.resample_cv_count = resample;
+        options.radius_scale = radius_scale;
+        std::copy(transform, transform + 12, options.transform.values.begin());
+        const std::vector<CurveBatch> batches = build_curve_batches(view(*base), motion, {}, {}, options);
+        std::uint64_t strand = 0u, point = 0u, motion_at = 0u;
+        *has_uvs = 0u;
+        for (std::size_t b = 0; b < batches.size(); ++b) {
+            const CurveBatch &batch = batches[b];
+            out_first[b] = point;
+            if (point + batch.points.size() > capacity) { throw std::runtime_error("shim capacity"); }
+            std::memcpy(out_counts + strand, batch.point_counts.data(), batch.point_counts.size() * 4u);
+            std::memcpy(out_points + 4u * point, batch.points.data(), batch.points.size() * 16u);
+            if (!batch.root_uvs.empty()) {
+                *has_uvs = 1u;
+                std::memcpy(out_uvs + 2u * strand, batch.root_uvs.data(), batch.root_uvs.size() * 8u);
+            }
+            std::memcpy(out_motion + 3u * motion_at, batch.motion_points.data(), batch.motion_points.size() * 12u);
+            strand += batch.point_counts.size();
+            point += batch.points.size();
+            motion_at += batch.motion_points.size();
+        }
+        out_first[batches.size()] = point;
+        put_text("", msg, cap);
+        return point;
+    } catch (const std::exception &e) {
+        put_text(e.what(), msg, cap);
+        return 0u;
+    }
 }
 
 } // extern "C"
