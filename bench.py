@@ -455,13 +455,20 @@ def run_gpu_arm(args):
                              "profile shows limiting the kernel"},
         "clocks": clocks, "gpu_launches": kernels_per_step(tile) * args.steps,
     }
+    parity_ok = True
     if cpu and "parity" in cpu:
-        line["max_error_rel_diag"] = cpu["parity"]["max_error_rel_diag"]
+        par = cpu["parity"]
+        line["max_error_rel_diag"] = par["max_error_rel_diag"]
+        parity_ok = (par["max_error_rel_diag"] <= par["tolerance_rel_diag"] and
+                     par["max_radius_error_rel_diag"] <= par["tolerance_rel_diag"] and par["root_triangles_equal"])
+        line["parity_ok"] = parity_ok
     if e2e:
         line["e2e"] = e2e
     if cpu:
         line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)
+    if not parity_ok:  # a fast wrong answer is not a result
+        raise SystemExit("the generated points differ from the reference's beyond the tolerance")
 
 
 def _graph_time(device, fn, steps: int, warmup: int, flush) -> list:
