@@ -344,6 +344,126 @@ __global__ void __launch_bounds__(256) batches_kernel(const BatchArgs a) {
     }
 }
 
+// The per-strand outputs alone (point counts, root uvs, batch boundaries),
+// for the flat path.
+__global__ void __launch_bounds__(256) strand_outputs_kernel(const BatchArgs a) {
+    const uint32_t S = a.strands, M = a.per_batch, P = a.base.fixed;
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < S; s += gridDim.x * blockDim.x) {
+        a.out.point_counts[s] = P;
+        if (a.out.root_uvs && (a.root_uvs || a.roots)) {
+            float2 uv;
+            if (a.root_uvs) {
+                uv = make_float2(a.root_uvs[2u * uint64_t{s}], a.root_uvs[2u * uint64_t{s} + 1u]);
+            } else {
+                uv = make_float2(__uint_as_float(a.roots[12u * uint64_t{s} + 6u]),
+                                 __uint_as_float(a.roots[12u * uint64_t{s} + 7u]));
+            }
+            reinterpret_cast<float2 *>(a.out.root_uvs)[s] = uv;
+        }
+        const uint32_t b = s / M;
+        if (s == b * M) { a.out.batch_first_point[b] = uint64_t{s} * P; }
+        if (s + 1u == S) { a.out.batch_first_point[b + 1u] = a.total; }
+    }
+}
+
+// Flat path: every set has the same fixed CV count P and nothing is
+// resampled, so output point i is input point i of each set, and its motion
+// position goes to K * first + k * bp + (i - first) of its batch (first
+// point `first`, bp points).  A thread takes four consecutive points: three
+// 16-byte loads of their xyz (48 bytes), one of their widths, four float4
+// stores, and per motion sample three loads and three stores when the four
+// share a batch and the addresses are 16-byte aligned; otherwise point by
+// point.
+__global__ void __launch_bounds__(256) flat_points_kernel(const BatchArgs a) {
+    const uint64_t total = a.total;
+    const uint64_t batch_points = uint64_t{a.per_batch} * a.base.fixed;
+    const uint32_t K = a.sample_count;
+    float4 *points = reinterpret_cast<float4 *>(a.out.points);
+    const bool vector_widths = a.base.widths && (reinterpret_cast<uintptr_t>(a.base.widths) & 15u) == 0u;
+    const bool vector_xyz = (reinterpret_cast<uintptr_t>(a.base.points) & 15u) == 0u;
+    for (uint64_t i0 = (uint64_t{blockIdx.x} * blockDim.x + threadIdx.x) * 4u; i0 < total;
+         i0 += uint64_t{gridDim.x} * blockDim.x * 4u) {
+        const bool four = i0 + 4u <= total;
+        float3 p[4];
+        float w[4];
+        if (four && vector_xyz) {
+            const float4 *src = reinterpret_cast<const float4 *>(a.base.points + 3u * i0);
+            const float4 q0 = __ldcs(src), q1 = __ldcs(src + 1), q2 = __ldcs(src + 2);
+            p[0] = make_float3(q0.x, q0.y, q0.z);
+            p[1] = make_float3(q0.w, q1.x, q1.y);
+            p[2] = make_float3(q1.z, q1.w, q2.x);
+            p[3] = make_float3(q2.y, q2.z, q2.w);
+        } else {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                p[u] = i0 + u < total ? load3(a.base.points, i0 + u) : make_float3(0.0f, 0.0f, 0.0f);
+            }
+        }
+        if (four && vector_widths) {
+            const float4 q = __ldcs(reinterpret_cast<const float4 *>(a.base.widths + i0));
+            w[0] = q.x;
+            w[1] = q.y;
+            w[2] = q.z;
+            w[3] = q.w;
+        } else {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                w[u] = a.base.widths ? (i0 + u < total ? a.base.widths[i0 + u] : 0.0f) : a.base.constant_width;
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (i0 + u >= total) { break; }
+            float3 q = p[u];
+            if (!a.identity) { q = transform_point(a.transform, q); }
+            __stcs(points + i0 + u, make_float4(q.x, q.y, q.z, __fmul_rn(w[u], a.radius_factor)));
+        }
+        if (K == 0u) { continue; }
+        const uint64_t b = i0 / batch_points;
+        const bool one_batch = four && (i0 + 3u) / batch_points == b;
+        for (uint32_t k = 0; k < K; ++k) {
+            const float *sp = a.samples[k].points;
+            if (one_batch) {
+                const uint64_t first = b * batch_points;
+                const uint64_t bp = min(first + batch_points, total) - first;
+                float *mo = a.out.motion_points + 3u * (uint64_t{K} * first + uint64_t{k} * bp + (i0 - first));
+                const float *in = sp + 3u * i0;
+                if ((reinterpret_cast<uintptr_t>(in) & 15u) == 0u && (reinterpret_cast<uintptr_t>(mo) & 15u) == 0u) {
+                    const float4 *src = reinterpret_cast<const float4 *>(in);
+                    float4 q0 = __ldcs(src), q1 = __ldcs(src + 1), q2 = __ldcs(src + 2);
+                    if (!a.identity) {
+                        const float3 r0 = transform_point(a.transform, make_float3(q0.x, q0.y, q0.z));
+                        const float3 r1 = transform_point(a.transform, make_float3(q0.w, q1.x, q1.y));
+                        const float3 r2 = transform_point(a.transform, make_float3(q1.z, q1.w, q2.x));
+                        const float3 r3 = transform_point(a.transform, make_float3(q2.y, q2.z, q2.w));
+                        q0 = make_float4(r0.x, r0.y, r0.z, r1.x);
+                        q1 = make_float4(r1.y, r1.z, r2.x, r2.y);
+                        q2 = make_float4(r2.z, r3.x, r3.y, r3.z);
+                    }
+                    float4 *d = reinterpret_cast<float4 *>(mo);
+                    __stcs(d, q0);
+                    __stcs(d + 1, q1);
+                    __stcs(d + 2, q2);
+                    continue;
+                }
+            }
+            for (int u = 0; u < 4; ++u) {
+                const uint64_t i = i0 + u;
+                if (i >= total) { break; }
+                const uint64_t bu = i / batch_points;
+                const uint64_t first = bu * batch_points;
+                const uint64_t bp = min(first + batch_points, total) - first;
+                float3 q = load3(sp, i);
+                if (!a.identity) { q = transform_point(a.transform, q); }
+                float *mo = a.out.motion_points + 3u * (uint64_t{K} * first + uint64_t{k} * bp + (i - first));
+                mo[0] = q.x;
+                mo[1] = q.y;
+                mo[2] = q.z;
+            }
+        }
+    }
+}
+
 } // namespace payload
 } // namespace nxg
 
@@ -522,6 +642,22 @@ uint32_t nxg_build_curve_batches(const nxg_curve_set *base, const nxg_motion_set
     a.total = total;
     a.status = variable_sets ? device_status : nullptr;
     a.out = *output;
+    // Flat path: one fixed CV count everywhere and no resampling.
+    bool flat = !base->point_counts && options->resample_cv_count == 0u;
+    for (uint32_t k = 0; flat && k < sample_count; ++k) {
+        flat = !samples[k].curves.point_counts &&
+               samples[k].curves.fixed_cvs_per_strand == base->fixed_cvs_per_strand;
+    }
+    if (flat) {
+        const uint64_t quads = (total + 3u) / 4u;
+        const uint32_t sgrid = static_cast<uint32_t>(std::max<uint64_t>(
+            1u, std::min<uint64_t>((uint64_t{base->strand_count} + 255u) / 256u, uint64_t(nxg::device_sm_count()) * 8u)));
+        strand_outputs_kernel<<<sgrid, 256, 0, st>>>(a);
+        const uint32_t pgrid = static_cast<uint32_t>(std::max<uint64_t>(
+            1u, std::min<uint64_t>((quads + 255u) / 256u, uint64_t(nxg::device_sm_count()) * 8u)));
+        flat_points_kernel<<<pgrid, 256, 0, st>>>(a);
+        return nxg::record_cuda(cudaGetLastError());
+    }
     int per_sm = 0;
     if (const uint32_t e = nxg::record_cuda(
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batches_kernel, 256, 0))) {

@@ -73,6 +73,19 @@ def test_fixed_copy_with_motion(cuda, nxg_lib, reference):
     _compare(reference, base, samples, max_strands_per_batch=1024, radius_scale=0.7)
 
 
+@pytest.mark.parametrize("transform", [None, AFFINE])
+def test_fixed_copy_batches_straddle_quads(cuda, nxg_lib, reference, transform):
+    # The flat path with 35-point batches (7 strands x 5 CVs) and an odd
+    # total: four-point groups cross batch boundaries and the end.
+    rng = np.random.default_rng(6)
+    base = _curves(rng, 1001, fixed=5, widths=False, roots=True, constant_width=0.02)
+    samples = [(0.1, _curves(rng, 1001, fixed=5)), (0.9, _curves(rng, 1001, fixed=5))]
+    kw = dict(max_strands_per_batch=7)
+    if transform:
+        kw["transform"] = transform
+    _compare(reference, base, samples, **kw)
+
+
 def test_variable_resample_transform(cuda, nxg_lib, reference):
     rng = np.random.default_rng(2)
     counts = rng.integers(2, 70, 20000)
