@@ -239,3 +239,59 @@ def test_classic_judged_path_full_size(classic_full):
     tiles = (int(params.strand_count) + 127) // 128
     print("judged surrogate, 4M roots all checked: max rel length error %.3g, width %.3g; %d of %d batches "
           "re-run exactly" % (rel[:, 0].max(), rel[:, 1].max(), st[2], tiles))
+
+
+def test_classic_fx_full_size(cuda, nxg_lib, reference):
+    """The FX bench workload at its size: 1,000,000 strands x 24 CVs of the
+    large description through NoiseFX, ClumpingFX (the description's guides,
+    per-guide noise table) and CutFX with a taper.  Every strand passes; the
+    first 20,000 strands match the reference's runtime on the same input
+    curves (same survivors, positions and radii within 1e-5 of the
+    diagonal)."""
+    import sys
+
+    import torch
+
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+    from nanoxgen_b200 import fixtures
+    from nanoxgen_b200.asset import build_asset
+    from nanoxgen_b200.classic import ClumpGuides, FxPlan, classic_fx_apply
+    from nanoxgen_b200.generator import DeviceAsset, generate_packed
+    w = fixtures.large_sphere(strands=1_000_000, cvs=24)
+    params = w.params.copy(noise_amplitude=0.0)
+    P = int(params.cvs_per_strand)
+    asset = build_asset(w.build_input, w.stencil_slots)
+    out = generate_packed(DeviceAsset(asset, cuda), params)
+    torch.cuda.synchronize()
+    n = 20_000
+    in_pts = out.points[:n * P].cpu().numpy().copy()
+    roots = out.roots_numpy()
+    in_roots = roots[:n].copy()
+    in_uvs = out.root_uvs[:n].cpu().numpy().copy()
+    in_counts = out.point_counts[:n].cpu().numpy().view(np.uint32).copy()
+    rn = roots["normal"].astype(np.float64)
+    axis = np.where(np.abs(rn[:, 2:3]) < 0.999, [[0.0, 0.0, 1.0]], [[0.0, 1.0, 0.0]])
+    tan = np.cross(rn, axis)
+    tan = (tan / np.maximum(np.linalg.norm(tan, axis=1, keepdims=True), 1e-30)).astype(np.float32)
+    primitive, effects = bench._fx_workload()
+    cg = bench._fx_clump_guides(w, P, roots, cuda)
+    plan = FxPlan(primitive, effects, 3, "description")
+    guides = [ClumpGuides(cg["axes"], cg["normals"], cg["tangents"], cg["uvs"], cg["prefixes"], cg["strand_guides"])]
+    status = classic_fx_apply(plan, out, torch.from_numpy(tan).cuda(), clumps=guides)
+    torch.cuda.synchronize()
+    assert status.cpu().tolist() == [0, 0]
+    rplan = reference.classic_plan_fx(primitive, effects, 3, "description")
+    freqs = rplan.info()["pref_noise"]
+    inputs = np.stack([reference.classic_noise(in_roots["position"], f) for f in freqs], 1)
+    theirs = reference.classic_apply_fx(rplan, in_pts, in_counts, in_roots, in_uvs, P, 1.0, inputs, tan[:n],
+                                        workers=THREADS, clumps=[dict(cg, strand_guides=cg["strand_guides"][:n])])
+    keep = out.point_counts[:n].cpu().numpy() != 0
+    assert keep.sum() == theirs[1].size
+    sel = np.repeat(keep, P)
+    mine = out.points[:n * P].cpu().numpy()[sel]
+    diag = asset.bbox_diagonal()
+    err = max_position_error(mine, theirs[0]) / diag
+    radius_err = float(np.abs(mine[:, 3].astype(np.float64) - theirs[0][:, 3]).max()) / diag
+    print("Classic FX, 1M x 24: max error on the first %d strands %.3g x diag" % (n, err))
+    assert err <= TOL and radius_err <= TOL
