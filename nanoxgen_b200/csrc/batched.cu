@@ -318,7 +318,8 @@ __device__ __noinline__ void batched_noise_walk_item(const BatchDesc &d, uint32_
     __syncwarp();
     walk_base<false>(d.g, records, stage, locals, tvals, rvals, d.offsets, lane, in_batch, P, inv_p);
     __syncwarp();
-    walk_frame(d.g.p, wr, lane < in_batch, stage + lane * kWalkRowFloats, lattice + lane, tvals, table, P);
+    walk_frame(d.g.p, wr, lane < in_batch, stage + lane * kWalkRowFloats, lattice + lane, tvals, table, P,
+               kWalkAxisColumns);
     __syncwarp();
     if (CLASSIC && d.g.scalars != nullptr) {
         walk_store<true>(d.g, stage, locals, rvals, lane, in_batch, P, inv_p);

@@ -104,9 +104,10 @@ __global__ void generate_kernel(LaunchArgs g, const float4 *offsets) {
 // writes the roots, root UVs and point counts), base, frame (with noise) and
 // store.  Without noise the base step writes the output directly (no
 // stage), applying Classic scalars itself when given.  Register budgets:
-// the noise variant runs one CTA of up to twelve warps per SM (its shared
-// memory allows no more); the plain one three CTAs of eight warps (at most 80
-// registers), the plain Classic one two.
+// the noise variant runs one CTA of up to eleven warps per SM (its shared
+// memory allows no more: eleven-warp CTAs hold ten lattice columns per axis
+// and strand, smaller ones twelve); the plain one three CTAs of eight warps
+// (at most 80 registers), the plain Classic one two.
 template <bool NOISE, bool CLASSIC>
 __global__ void __launch_bounds__(NOISE ? 384 : 256, NOISE ? 1 : (CLASSIC ? 2 : 3))
     generate_walk_kernel(LaunchArgs g, const float4 *offsets) {
@@ -133,7 +134,8 @@ __global__ void __launch_bounds__(NOISE ? 384 : 256, NOISE ? 1 : (CLASSIC ? 2 : 
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    constexpr size_t kWarpBytes = walk_warp_bytes(kWalk, kStaged);
+    const int columns = walk_lattice_columns(warps);
+    const size_t kWarpBytes = walk_warp_bytes(kWalk, kStaged, columns);
     unsigned char *mine = warp_base + kWarpBytes * warp;
     float *stage = reinterpret_cast<float *>(mine);  // staged variants only
     float4 *records = reinterpret_cast<float4 *>(kStaged ? mine + kWalkStageBytes : mine);
@@ -158,17 +160,22 @@ __global__ void __launch_bounds__(NOISE ? 384 : 256, NOISE ? 1 : (CLASSIC ? 2 : 
             __syncwarp();
         }
         if constexpr (kStaged) {
-            walk_base<false>(g, records, stage, locals, tvals, rvals, offsets, lane, in_batch, P, inv_p);
+            walk_base_direct<false, true>(g, records, locals, tvals, rvals, offsets, lane, in_batch, P, stage);
         } else {
             walk_base_direct<CLASSIC>(g, records, locals, tvals, rvals, offsets, lane, in_batch, P);
         }
         __syncwarp();
         if constexpr (kWalk) {
-            walk_frame(g.p, wr, lane < in_batch, stage + lane * kWalkRowFloats, lattice + lane, tvals, table, P);
+            walk_frame(g.p, wr, lane < in_batch, stage + lane * kWalkRowFloats, lattice + lane, tvals, table, P,
+                       columns);
             __syncwarp();
         }
         if constexpr (kStaged) {
-            walk_store<CLASSIC>(g, stage, locals, rvals, lane, in_batch, P, inv_p);
+            if constexpr (CLASSIC) {
+                walk_store<true>(g, stage, locals, rvals, lane, in_batch, P, inv_p);
+            } else {
+                walk_store8(g, stage, locals, rvals, lane, in_batch, P);
+            }
             __syncwarp();
         }
     }
@@ -251,7 +258,8 @@ __global__ void __launch_bounds__(64, 1) generate_pipe_kernel(LaunchArgs g, cons
             wr.normal = F3{fr[3 * 32 + lane], fr[4 * 32 + lane], fr[5 * 32 + lane]};
             wr.surface_u = F3{fr[6 * 32 + lane], fr[7 * 32 + lane], fr[8 * 32 + lane]};
             wr.domain = F3{fr[9 * 32 + lane], fr[10 * 32 + lane], fr[11 * 32 + lane]};
-            walk_frame(g.p, wr, lane < in_batch, stage + lane * kWalkRowFloats, lattice + lane, tvals, table, P);
+            walk_frame(g.p, wr, lane < in_batch, stage + lane * kWalkRowFloats, lattice + lane, tvals, table, P,
+                       kWalkAxisColumns);
             __syncwarp();
             walk_store<false>(g, stage, locals, rvals, lane, in_batch, P, inv_p);
             if (it + 2u < iterations) { named_arrive(3u + b); }
@@ -818,7 +826,7 @@ bool valid_tile(uint32_t P, uint32_t lanes, uint32_t ppt) {
 }
 
 // Tile shape for P CVs: the registered one, else the lane-walk generator for
-// 2..32 CVs (lanes_per_strand 1; CTAs of 320 threads with noise, 256
+// 2..32 CVs (lanes_per_strand 1; CTAs of 352 threads with noise, 256
 // without), else four CVs per lane on the narrowest power-of-two group that
 // holds the strand.
 void default_tile(uint32_t P, bool noise, int *lanes, int *ppt, uint32_t *block) {
@@ -832,7 +840,7 @@ void default_tile(uint32_t P, bool noise, int *lanes, int *ppt, uint32_t *block)
     if (P >= 2u && P <= static_cast<uint32_t>(dev::kWalkMaxCvs)) {  // the lane-walk generator
         *lanes = 1;
         *ppt = 1;
-        *block = noise ? 320u : 256u;  // with noise: ten 22 KB warps fill the SM's shared memory
+        *block = noise ? 352u : 256u;  // with noise: eleven 20 KB warps fill the SM's shared memory
         return;
     }
     *ppt = 4;
@@ -867,7 +875,8 @@ uint32_t launch_kernel(void (*fn)(LaunchArgs, const float4 *), uint32_t grid, ui
 size_t generate_smem_bytes(uint32_t P, int lanes, int ppt, bool noise, bool staged, uint32_t warps) {
     if (lanes == 1) {
         const bool walk = noise && staged;
-        return dev::walk_head_bytes(walk) + dev::walk_warp_bytes(walk, staged) * warps;
+        return dev::walk_head_bytes(walk) +
+               dev::walk_warp_bytes(walk, staged, dev::walk_lattice_columns(static_cast<int>(warps))) * warps;
     }
     const size_t per_warp = sizeof(uint32_t) * dev::kRecFields * 32u + sizeof(float4) * 32u / lanes * lanes * ppt +
                             (noise ? sizeof(float2) * 384u : 0u);
@@ -1283,7 +1292,7 @@ uint32_t nxg_autotune_packed(const nxg_device_asset_desc *asset, const nxg_defor
     nxg_tile winner{0u, 0u, 0u};
     float winner_ms = 0.0f;
     const uint32_t reps = std::max(1u, repeats);
-    const uint32_t blocks[4] = {64u, 128u, 256u, 320u};
+    const uint32_t blocks[5] = {64u, 128u, 256u, 320u, 352u};
     for (uint32_t lanes = 1u; lanes <= 32u && !error; lanes *= 2u) {
         for (uint32_t ppt = 1u; ppt <= 4u && !error; ppt *= 2u) {
             // tiles that hold the strand without idling half of their lanes

@@ -7,7 +7,7 @@
 //   base   (lane = CV)      the base curve from the guide-offset table, read
 //                           as coalesced rows (consecutive lanes on
 //                           consecutive CVs of one guide), into a stage in
-//                           shared memory, one row of 33 xyz slots per strand;
+//                           shared memory, one row of 32 xyz slots per strand;
 //   frame  (lane = strand)  with noise: the arc-length prefix, the strand's
 //                           noise lattice, then the reference's cursor walk
 //                           (generate.h:445-502) over the staged row -- the
@@ -19,9 +19,11 @@
 //                           stores, with the Classic application when
 //                           per-root scalars are given.
 //
-// Stage rows are 99 words apart and a CV takes 3 words; both strides are odd,
+// Stage rows are 97 words apart and a CV takes 3 words; both strides are odd,
 // so a warp reading column c of 32 rows (frame step) and a warp reading one
-// row (base/store steps) are both free of shared-memory bank conflicts.
+// row are free of shared-memory bank conflicts, and the eight-lane base and
+// store steps (four strands of eight CVs per access) meet at most two lanes
+// to a bank (97 = 1 mod 32 shifts each strand's banks by one).
 #pragma once
 
 #include "generator_core.cuh"
@@ -30,9 +32,8 @@ namespace nxg {
 namespace dev {
 
 constexpr int kWalkMaxCvs = 32;
-constexpr int kWalkStride = kWalkMaxCvs + 1;   // CV slots per staged strand row
-constexpr int kWalkRowFloats = 3 * kWalkStride; // a row holds x, y, z per CV (99 words: an odd stride)
-constexpr int kWalkAxisColumns = 12;           // noise lattice columns per axis and strand
+constexpr int kWalkRowFloats = 3 * kWalkMaxCvs + 1; // a row holds x, y, z per CV (97 words: an odd stride)
+constexpr int kWalkAxisColumns = 12;           // noise lattice columns per axis and strand, at most
 constexpr int kWalkRecords = 8;                // float4 setup records per strand
 
 // Shared-memory bytes per warp.  Staged variants (noise or Classic scalars):
@@ -43,11 +44,22 @@ constexpr int kWalkRecords = 8;                // float4 setup records per stran
 constexpr size_t kWalkStageBytes = sizeof(float) * 32u * kWalkRowFloats;
 constexpr size_t kWalkRecordBytes = sizeof(float4) * kWalkRecords * 32u;
 constexpr size_t kWalkLatticeBytes = sizeof(float2) * 3u * kWalkAxisColumns * 32u;
+// Lattice columns per axis and strand for a CTA of `warps` noise warps:
+// twelve up to ten warps; ten for eleven-warp CTAs, whose shared memory holds
+// no more.  A strand needs floor(d + span) - floor(d) + 2 columns on an axis
+// whose noise coordinate starts at d and advances by span over the strand
+// (at most ceil(span) + 2); a warp with a strand that needs more takes direct
+// noise.
+__host__ __device__ constexpr int walk_lattice_columns(int warps) { return warps > 10 ? 10 : kWalkAxisColumns; }
+__host__ __device__ constexpr size_t walk_lattice_bytes(int columns) {
+    return sizeof(float2) * 3u * static_cast<size_t>(columns) * 32u;
+}
 constexpr size_t kWalkRootWordBytes = sizeof(uint32_t) * 12u * 32u;
 constexpr size_t kWalkLocalBytes = sizeof(uint32_t) * 32u;
-__host__ __device__ constexpr size_t walk_warp_bytes(bool noise, bool staged) {
-    return staged ? kWalkStageBytes + (noise && kWalkLatticeBytes > kWalkRecordBytes ? kWalkLatticeBytes
-                                                                                     : kWalkRecordBytes) +
+__host__ __device__ constexpr size_t walk_warp_bytes(bool noise, bool staged, int columns = kWalkAxisColumns) {
+    return staged ? kWalkStageBytes +
+                        (noise && walk_lattice_bytes(columns) > kWalkRecordBytes ? walk_lattice_bytes(columns)
+                                                                                 : kWalkRecordBytes) +
                         kWalkLocalBytes
                   : kWalkRecordBytes + kWalkRootWordBytes + kWalkLocalBytes;
 }
@@ -487,12 +499,16 @@ __device__ __forceinline__ void walk_base(const LaunchArgs &g, const float4 *rec
 // pass runs as many slot pairs as its strands' largest count; a strand's
 // loads past its own count are predicated off (no memory request), and its
 // records there hold the zero row with weight 0, so the accumulation needs
-// no predicate.  CLASSIC applies records 6 and 7 as walk_base does.  Every
-// lane of the warp calls it.
-template <bool CLASSIC>
+// no predicate.  CLASSIC applies records 6 and 7 as walk_base does.  STAGED
+// writes the base points into the strands' stage rows instead of the output
+// (the noise walk reads them there); a stage row of 97 words keeps the
+// four strands of a pass at most two lanes to a bank.  Every lane of the
+// warp calls it.
+template <bool CLASSIC, bool STAGED = false>
 __device__ __forceinline__ void walk_base_direct(const LaunchArgs &g, const float4 *records, const uint32_t *locals,
                                                  const float *tvals, const float *rvals, const float4 *offsets,
-                                                 int lane, int in_batch, int P) {
+                                                 int lane, int in_batch, int P, float *stage = nullptr) {
+    static_assert(!(CLASSIC && STAGED), "staged strands take the Classic application at the store");
     constexpr int kPerLane = kWalkMaxCvs / 8;
     const int c = lane & 7;
     const int cpl = (P + 7) >> 3;
@@ -534,6 +550,18 @@ __device__ __forceinline__ void walk_base_direct(const LaunchArgs &g, const floa
                 if (m < cpl) { acc[m] = acc[m] + xyz(da[m]) * gw.y + xyz(db[m]) * gw.w; }
             }
         }
+        if constexpr (STAGED) {
+            float *row = stage + s * kWalkRowFloats;
+#pragma unroll
+            for (int m = 0; m < kPerLane; ++m) {
+                const int cm = c + 8 * m;
+                if (live && m < cpl && cm < P) {
+                    stage_put(row, cm,
+                              F3{head.x, head.y, head.z} + (acc[m] * head.w + F3{tail.x, tail.y, tail.z} * tv[m]) * ls);
+                }
+            }
+            continue;
+        }
         const uint32_t word = live ? locals[s] : 0x80000000u;
         float4 front = {0.0f, 0.0f, 0.0f, 1.0f}, width = {0.0f, 0.0f, 0.0f, 0.0f};
         if constexpr (CLASSIC) {
@@ -556,46 +584,73 @@ __device__ __forceinline__ void walk_base_direct(const LaunchArgs &g, const floa
     }
 }
 
-// noise - 0.5 along one axis from the strand's lattice columns (the
-// regrouped blend of lattice_noise).
-__device__ __forceinline__ float walk_lattice_delta(const float2 *lat, int axis, int lo, int n, float x) {
-    const float fx = floorf(x);
-    const float w = x - fx;
-    int k = static_cast<int>(fx) - lo;
-    k = max(0, min(k, n - 2));
-    const float2 c0 = lat[(axis * kWalkAxisColumns + k) * 32];
-    const float2 c1 = lat[(axis * kWalkAxisColumns + k + 1) * 32];
+// Floor by a round-down add: for |x| < 2^22, x + 1.5 * 2^23 lies in
+// [2^23, 2^24), where consecutive floats are consecutive integers, so the
+// sum rounded toward minus infinity is 1.5 * 2^23 + floor(x) exactly.  Its
+// bit pattern minus that of 1.5 * 2^23 is floor(x) as an integer, and the
+// sum minus 1.5 * 2^23 is floor(x) as a float (an exact difference).  Two
+// adds on the FMA pipe replace the rounding and conversion instructions.
+constexpr float kFloorMagic = 12582912.0f;      // 1.5 * 2^23
+constexpr uint32_t kFloorMagicBits = 0x4b400000u;
+constexpr float kFloorMagicLimit = 4194304.0f;  // 2^22
+
+// 2 (noise - 0.5) along one axis from the strand's lattice columns (the
+// regrouped blend of lattice_noise); the caller folds the 1/2 into the
+// magnitude, a product by an exact power of two.  The axis' columns start at
+// column axis * columns of the strand's lattice; `bias` is the bit pattern
+// of 1.5 * 2^23 plus the axis' first lattice coordinate minus that start, so
+// the sum's bits minus `bias` index the lattice directly, and `kmax` (the
+// axis' last pair) bounds the index (x never lies below the first column:
+// the walk's distances are non-negative; lanes with no strand read some
+// column of their own lattice).
+__device__ __forceinline__ float walk_lattice_delta(const float2 *lat, uint32_t bias, uint32_t kmax, float x) {
+    const float t = __fadd_rd(x, kFloorMagic);
+    const float w = x - (t - kFloorMagic);
+    const uint32_t k = min(__float_as_uint(t) - bias, kmax);
+    const float2 *col = lat + static_cast<int>(k) * 32;
+    const float2 c0 = col[0];
+    const float2 c1 = col[32];
     const float s = s_curve(w);
     const float v0 = c0.x * w + c0.y;
     const float v1 = c1.x * (w - 1.0f) + c1.y;
-    return 0.5f * (v0 + s * (v1 - v0));
+    return v0 + s * (v1 - v0);
 }
 
 // Lattice columns (A, B) of the three noise axes for one strand (see
-// lattice_noise): columns lo .. floor(d0 + span) + 2 cover every CV's X and
-// X + 1 with one column of margin for rounding in the arc-length prefix.
-// `lat` is this lane's column 0 of axis 0; column k of axis a is at
-// lat[(a * kWalkAxisColumns + k) * 32].  fits is false when a strand needs
-// more columns than the lattice holds (it then takes direct noise).
+// lattice_noise): columns lo .. floor(d0 + span) + 1 cover every CV's X and
+// X + 1 (the walk's noise coordinates d0 + arc * f are computed in the same
+// IEEE operations as d0 + span, so none passes it).  `lat` is this lane's
+// column 0 of axis 0; column k of axis a is at lat[(a * columns + k) * 32].
+// fits is false when a strand needs
+// more columns than the lattice holds, or coordinates beyond the round-down
+// floor's range (it then takes direct noise).  bias and kmax are the
+// per-axis arguments of walk_lattice_delta.
 struct WalkLattice {
     int lo[3], n[3];
+    uint32_t bias[3], kmax[3];
     bool fits;
 };
 
-__device__ __forceinline__ WalkLattice walk_fill_lattice(F3 dom, float span, float2 *lat, const float4 *table) {
+__device__ __forceinline__ WalkLattice walk_fill_lattice(F3 dom, float span, float2 *lat, const float4 *table,
+                                                       int columns) {
     WalkLattice wl;
     wl.fits = true;
 #pragma unroll
     for (int ax = 0; ax < 3; ++ax) {
         const float d0 = component(dom, ax);
         wl.lo[ax] = static_cast<int>(floorf(d0));
-        wl.n[ax] = static_cast<int>(floorf(d0 + span)) + 3 - wl.lo[ax];
-        wl.fits = wl.fits && wl.n[ax] >= 2 && wl.n[ax] <= kWalkAxisColumns;
+        wl.n[ax] = static_cast<int>(floorf(__fadd_rn(d0, span))) + 2 - wl.lo[ax];
+        wl.fits = wl.fits && wl.n[ax] >= 2 && wl.n[ax] <= columns && fabsf(d0) + span < kFloorMagicLimit;
     }
     if (!wl.fits) {  // lattice reads stay in bounds (column 0 and 1) whatever the strand
         wl.n[0] = wl.n[1] = wl.n[2] = 2;
-        return wl;
     }
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+        wl.bias[ax] = kFloorMagicBits + static_cast<uint32_t>(wl.lo[ax]) - static_cast<uint32_t>(ax * columns);
+        wl.kmax[ax] = static_cast<uint32_t>(ax * columns + wl.n[ax] - 2);
+    }
+    if (!wl.fits) { return wl; }
 #pragma unroll
     for (int ax = 0; ax < 3; ++ax) {
         const int ib = ax == 0 ? 1 : 0;  // the fixed axes, ascending
@@ -632,7 +687,7 @@ __device__ __forceinline__ WalkLattice walk_fill_lattice(F3 dom, float span, flo
                 A += wgt[corner] * component4(gr, ax);
                 B += component4(gr, ib) * wdb[corner] + component4(gr, ic) * wdc[corner];
             }
-            lat[(ax * kWalkAxisColumns + k) * 32] = make_float2(A, B);
+            lat[(ax * columns + k) * 32] = make_float2(A, B);
         }
     }
     return wl;
@@ -640,6 +695,13 @@ __device__ __forceinline__ WalkLattice walk_fill_lattice(F3 dom, float span, flo
 
 __device__ __forceinline__ float walk_effective_frequency(const ParamArgs &p, float original_length) {
     return original_length > 0.0f ? fmaxf(0.5f / original_length, p.noise_frequency) : p.noise_frequency;
+}
+
+// |b - a| in fixed IEEE operations (no contraction left to the compiler), so
+// the length pass and the cursor walk's arc-length prefix agree bit for bit.
+__device__ __forceinline__ float walk_segment_length(F3 b, F3 a) {
+    const F3 d = b - a;
+    return sqrt_approx(__fmaf_rn(d.z, d.z, __fmaf_rn(d.y, d.y, __fmul_rn(d.x, d.x))));
 }
 
 // The cursor walk (generate.h:465-502) over base points base(0..P-1),
@@ -662,7 +724,9 @@ template <bool LATTICE, bool PRESERVE, class Base, class Emit>
 __device__ __forceinline__ float walk_cursor(const ParamArgs &p, const WalkRoot &wr, float f_eff,
                                              const WalkLattice &wl, const float2 *lat, const float *tvals,
                                              const float4 *table, int P, Base base, Emit emit) {
-    const float mscale = p.noise_mask * p.noise_amplitude;
+    // Lattice deltas come doubled (walk_lattice_delta): their magnitude takes
+    // the 1/2, which leaves every product bit-identical.
+    const float mscale = LATTICE ? 0.5f * (p.noise_mask * p.noise_amplitude) : p.noise_mask * p.noise_amplitude;
     const F3 dom = wr.domain;
     F3 tan = wr.normal;
     F3 v = wr.surface_u;
@@ -676,10 +740,12 @@ __device__ __forceinline__ float walk_cursor(const ParamArgs &p, const WalkRoot 
 #pragma unroll 2
     for (int c = 0; c < P; ++c) {
         const F3 further = c + 3 < P ? base(c + 3) : ahead;
-        const F3 d = cur - previous_base;
-        arc += sqrt_approx(dot(d, d));
-        const F3 seg = xsub(nxt, cur);
-        const F3 ntan = (c + 1 < P && xdot(seg, seg) > 0.0f) ? normalize(seg) : tan;
+        arc = __fadd_rn(arc, walk_segment_length(cur, previous_base));
+        // The reference's length_squared(segment) > 0 holds exactly when some
+        // component's square does not round to zero: the same test on the
+        // fused sum (no flush to zero here).
+        const F3 seg = nxt - cur;
+        const F3 ntan = (c + 1 < P && dot(seg, seg) > 0.0f) ? normalize(seg) : tan;
         const F3 axis = cross(tan, ntan);
         const float cs = fminf(fmaxf(dot(tan, ntan), -1.0f), 1.0f);
         const float sn = sqrt_approx(fmaf(-cs, cs, 1.0f));
@@ -690,17 +756,17 @@ __device__ __forceinline__ float walk_cursor(const ParamArgs &p, const WalkRoot 
         v = dot(axis, axis) > 0.0f ? rotated : v;
         const F3 bn = cross(v, ntan);
         const F3 tt = cross(bn, v);
-        const float distance = arc * f_eff;
+        const float distance = __fmul_rn(arc, f_eff);
         const float magnitude = mscale * tvals[c];
         float gx, gy, gz;
         if constexpr (LATTICE) {
-            gx = walk_lattice_delta(lat, 0, wl.lo[0], wl.n[0], dom.x + distance);
-            gy = walk_lattice_delta(lat, 1, wl.lo[1], wl.n[1], dom.y + distance);
-            gz = walk_lattice_delta(lat, 2, wl.lo[2], wl.n[2], dom.z + distance);
+            gx = walk_lattice_delta(lat, wl.bias[0], wl.kmax[0], __fadd_rn(dom.x, distance));
+            gy = walk_lattice_delta(lat, wl.bias[1], wl.kmax[1], __fadd_rn(dom.y, distance));
+            gz = walk_lattice_delta(lat, wl.bias[2], wl.kmax[2], __fadd_rn(dom.z, distance));
         } else {
-            gx = gradient_noise(table, dom.x + distance, dom.y, dom.z) - 0.5f;
-            gy = gradient_noise(table, dom.x, dom.y + distance, dom.z) - 0.5f;
-            gz = gradient_noise(table, dom.x, dom.y, dom.z + distance) - 0.5f;
+            gx = gradient_noise(table, __fadd_rn(dom.x, distance), dom.y, dom.z) - 0.5f;
+            gy = gradient_noise(table, dom.x, __fadd_rn(dom.y, distance), dom.z) - 0.5f;
+            gz = gradient_noise(table, dom.x, dom.y, __fadd_rn(dom.z, distance)) - 0.5f;
         }
         const F3 q = cur + v * (gx * magnitude) + bn * (gy * magnitude) + tt * (gz * magnitude);
         if constexpr (PRESERVE) {
@@ -750,22 +816,22 @@ __device__ __forceinline__ float walk_preserve_scale(const ParamArgs &p, float o
 // warp calls it; lanes whose strand does not count (past the batch) work on
 // whatever their row holds and are ignored.
 __device__ __forceinline__ void walk_frame(const ParamArgs &p, const WalkRoot &wr, bool counts, float *row,
-                                           float2 *lat, const float *tvals, const float4 *table, int P) {
+                                           float2 *lat, const float *tvals, const float4 *table, int P,
+                                           int columns) {
     // Length of the base curve (generate.h:420-433); the walk accumulates the
-    // same prefix again as its arc length.
+    // same prefix again as its arc length, in the same operations.
     float original_length = 0.0f;
     {
         F3 prev = stage_get(row, 0);
 #pragma unroll 8
         for (int c = 1; c < P; ++c) {
             const F3 cur = stage_get(row, c);
-            const F3 d = cur - prev;
-            original_length += sqrt_approx(dot(d, d));
+            original_length = __fadd_rn(original_length, walk_segment_length(cur, prev));
             prev = cur;
         }
     }
     const float f_eff = walk_effective_frequency(p, original_length);
-    const WalkLattice wl = walk_fill_lattice(wr.domain, original_length * f_eff, lat, table);
+    const WalkLattice wl = walk_fill_lattice(wr.domain, __fmul_rn(original_length, f_eff), lat, table, columns);
     const float noisy = walk_cursor_any(
         p, wr, f_eff, wl, counts, lat, tvals, table, P, [&](int c) { return stage_get(row, c); },
         [&](int c, F3 q) { stage_put(row, c, q); });
@@ -824,6 +890,34 @@ __device__ __forceinline__ void walk_store(const LaunchArgs &g, const float *sta
             if (!keep && c == 0 && g.point_counts != nullptr) { g.point_counts[word] = 0u; }
         }
         walk_emit(g, word, P, c, q);
+    }
+}
+
+// Store step without Classic scalars, eight lanes per strand as in
+// walk_base_direct: lane (s = pass * 4 + lane / 8, c = lane % 8) stores CVs
+// c + 8m of its strand's staged row, so each store instruction writes four
+// strands' runs of eight consecutive float4s, and a lane's radii are fixed
+// for the whole kernel.  Every lane of the warp calls it.
+__device__ __forceinline__ void walk_store8(const LaunchArgs &g, const float *stage, const uint32_t *locals,
+                                            const float *rvals, int lane, int in_batch, int P) {
+    constexpr int kPerLane = kWalkMaxCvs / 8;
+    const int c = lane & 7;
+    const int cpl = (P + 7) >> 3;
+    float rv[kPerLane];
+#pragma unroll
+    for (int m = 0; m < kPerLane; ++m) { rv[m] = rvals[min(c + 8 * m, P - 1)]; }
+    for (int first = 0; first < in_batch; first += 4) {
+        const int s = first + (lane >> 3);  // at most 31
+        const uint32_t word = s < in_batch ? locals[s] : 0x80000000u;
+        const float *row = stage + s * kWalkRowFloats;
+#pragma unroll
+        for (int m = 0; m < kPerLane; ++m) {
+            const int cm = c + 8 * m;
+            if (m < cpl && cm < P) {
+                const F3 q = stage_get(row, cm);
+                walk_emit(g, word, P, cm, make_float4(q.x, q.y, q.z, rv[m]));
+            }
+        }
     }
 }
 

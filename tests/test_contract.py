@@ -259,7 +259,7 @@ def test_tile_registry(nxg_lib):
     t = Tile()
     # built-in choice for 2..32 CVs: the lane-walk generator (one lane per strand)
     assert L.nxg_get_tile(32, 1, ctypes.byref(t)) == 0
-    assert (t.lanes_per_strand, t.cvs_per_lane, t.block_size) == (1, 1, 320)
+    assert (t.lanes_per_strand, t.cvs_per_lane, t.block_size) == (1, 1, 352)
     assert L.nxg_get_tile(64, 1, ctypes.byref(t)) == 0 and t.lanes_per_strand * t.cvs_per_lane >= 64
     assert L.nxg_set_tile(32, 1, ctypes.byref(Tile(1, 1, 256))) == 0
     assert L.nxg_set_tile(33, 1, ctypes.byref(Tile(1, 1, 256))) == ERRORS["InvalidArgument"]

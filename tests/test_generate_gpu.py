@@ -354,10 +354,11 @@ def test_launch_block_sizes(torch_cuda, sphere, block):
     assert all(np.array_equal(x, y) for x, y in zip(ref, out))
 
 
-@pytest.mark.parametrize("block", [64, 96, 320])
+@pytest.mark.parametrize("block", [64, 96, 320, 352])
 def test_lane_walk_ctas_match_oracle(torch_cuda, oracle, sphere, block):
     """The lane-walk generator with noise as producer/consumer warp pairs
-    (64 threads) and as three- and ten-warp CTAs, over CV counts that do and
+    (64 threads) and as three-, ten- and eleven-warp CTAs (the last with ten
+    lattice columns per axis instead of twelve), over CV counts that do and
     do not fill a warp, with and without preserveLength."""
     from nanoxgen_b200.generator import set_tile
     w, asset = sphere
@@ -370,14 +371,21 @@ def test_lane_walk_ctas_match_oracle(torch_cuda, oracle, sphere, block):
             set_tile(cvs, True)
 
 
-def test_lane_walk_direct_noise_when_the_lattice_overflows(torch_cuda, oracle, sphere):
+@pytest.mark.parametrize("block", [320, 352])
+def test_lane_walk_direct_noise_when_the_lattice_overflows(torch_cuda, oracle, sphere, block):
     """At a high noise frequency a strand spans more lattice columns than the
-    lane walk keeps (12 per axis); its warp then evaluates gradient noise
-    directly.  Also a frequency just inside the limit."""
+    lane walk keeps (12 per axis in ten-warp CTAs, 10 in eleven-warp ones);
+    its warp then evaluates gradient noise directly.  Also frequencies near
+    either limit, where some warps fit and others do not."""
+    from nanoxgen_b200.generator import set_tile
     w, asset = sphere
-    for frequency in (60.0, 14.0):
-        params = w.params.copy(strand_count=3000, cvs_per_strand=32, noise_frequency=frequency)
-        _compare(asset, params, _gen(torch_cuda, asset, params), oracle.generate(asset.buffer, params, threads=8))
+    try:
+        set_tile(32, True, 1, 1, block)
+        for frequency in (60.0, 14.0, 11.0):
+            params = w.params.copy(strand_count=3000, cvs_per_strand=32, noise_frequency=frequency)
+            _compare(asset, params, _gen(torch_cuda, asset, params), oracle.generate(asset.buffer, params, threads=8))
+    finally:
+        set_tile(32, True)
 
 
 def test_every_tile_matches_oracle_and_autotuner(torch_cuda, oracle, sphere):
@@ -394,8 +402,8 @@ def test_every_tile_matches_oracle_and_autotuner(torch_cuda, oracle, sphere):
             set_tile(P, True, lanes, ppt, 128)
             _compare(asset, w.params, _gen(torch_cuda, d, w.params), theirs)
         # the lane walk as producer/consumer warp pairs (64-thread CTAs) and
-        # as ten-warp CTAs
-        for block in (64, 320):
+        # as ten- and eleven-warp CTAs
+        for block in (64, 320, 352):
             set_tile(P, True, 1, 1, block)
             _compare(asset, w.params, _gen(torch_cuda, d, w.params), theirs)
         pts, *_ = allocate_outputs(w.params.strand_count, P, "cuda")
