@@ -291,23 +291,27 @@ static_assert(kBatchStageBytes >= sizeof(float4) * kWalkMaxCvs, "spline scratch 
 static_assert(kBatchStageBytes >= kWalkRootWordBytes, "RootSample words fit the stage area");
 static_assert(kBatchLatticeBytes >= kWalkLocalBytes, "output words fit the lattice area");
 
-// Per-warp shared memory when some description takes noisy lane-walk items:
-// stage | records aliased by the lattice | output words.
-constexpr size_t kBatchWalkWarpBytes = kWalkStageBytes + kWalkLatticeBytes + kWalkLocalBytes;
-static_assert(kWalkLatticeBytes >= kWalkRecordBytes, "records fit the lattice area");
+// Per-warp shared memory of the noisy lane-walk class in a CTA of `warps`
+// warps: stage | records aliased by the lattice (walk_lattice_columns) |
+// output words.
+__host__ __device__ constexpr size_t batch_walk_warp_bytes(int warps) {
+    return kWalkStageBytes + walk_lattice_bytes(walk_lattice_columns(warps)) + kWalkLocalBytes;
+}
+static_assert(walk_lattice_bytes(walk_lattice_columns(11)) >= kWalkRecordBytes, "records fit the lattice area");
 
 // A noisy description on the lane-walk tile (2..32 CVs): setup (with the
 // root outputs), base into the stage, the frame walk and the store step
 // (walk.cuh), with the Classic application when the description has scalars.
 template <bool CLASSIC>
 __device__ __noinline__ void batched_noise_walk_item(const BatchDesc &d, uint32_t batch, uint32_t end, int lane,
-                                                     unsigned char *mine, const float4 *table, const float *tvals) {
+                                                     unsigned char *mine, const float4 *table, const float *tvals,
+                                                     int columns) {
     const float *rvals = tvals + 2 * kWalkMaxCvs;
     float *stage = reinterpret_cast<float *>(mine);
     unsigned char *after_stage = mine + kWalkStageBytes;
     float4 *records = reinterpret_cast<float4 *>(after_stage);
     float2 *lattice = reinterpret_cast<float2 *>(after_stage);
-    uint32_t *locals = reinterpret_cast<uint32_t *>(after_stage + kWalkLatticeBytes);
+    uint32_t *locals = reinterpret_cast<uint32_t *>(after_stage + walk_lattice_bytes(columns));
     const int P = static_cast<int>(d.g.p.cvs_per_strand);
     const uint32_t item = batch + static_cast<uint32_t>(lane);
     const bool valid = item < end;
@@ -316,15 +320,15 @@ __device__ __noinline__ void batched_noise_walk_item(const BatchDesc &d, uint32_
     const WalkRoot wr = walk_setup<true>(d.g, records, locals, lane, valid ? item : batch, valid,
                                          static_cast<uint32_t>(P));
     __syncwarp();
-    walk_base<false>(d.g, records, stage, locals, tvals, rvals, d.offsets, lane, in_batch, P, inv_p);
+    walk_base_direct<false, true>(d.g, records, locals, tvals, rvals, d.offsets, lane, in_batch, P, stage);
     __syncwarp();
     walk_frame(d.g.p, wr, lane < in_batch, stage + lane * kWalkRowFloats, lattice + lane, tvals, table, P,
-               kWalkAxisColumns);
+               columns);
     __syncwarp();
     if (CLASSIC && d.g.scalars != nullptr) {
         walk_store<true>(d.g, stage, locals, rvals, lane, in_batch, P, inv_p);
     } else {
-        walk_store<false>(d.g, stage, locals, rvals, lane, in_batch, P, inv_p);
+        walk_store8(d.g, stage, locals, rvals, lane, in_batch, P);
     }
     __syncwarp();
 }
@@ -397,7 +401,7 @@ __device__ __forceinline__ void batched_dispatch_lanes(const BatchDesc &d, uint3
 // lane-group items), so each launch holds only its variants' code and runs
 // at their register and shared-memory footprint.
 template <int PPT, bool CLASSIC, int CLS>
-__global__ void __launch_bounds__(CLS == 1 ? 256 : 320, CLS == 1 ? 3 : 1)
+__global__ void __launch_bounds__(CLS == 1 ? 256 : 352, CLS == 1 ? 3 : 1)
     batched_generate_kernel(const __grid_constant__ BatchArgs b) {
     extern __shared__ float4 smem[];
     __shared__ uint32_t claimed;
@@ -454,7 +458,8 @@ __global__ void __launch_bounds__(CLS == 1 ? 256 : 320, CLS == 1 ? 3 : 1)
         if (batch >= d.g.count) { break; }
         const uint32_t end = min(batch + 32u, d.g.count);
         if constexpr (CLS == 0) {
-            batched_noise_walk_item<CLASSIC>(d, batch, end, lane, mine, table, tvals);
+            batched_noise_walk_item<CLASSIC>(d, batch, end, lane, mine, table, tvals,
+                                             walk_lattice_columns(static_cast<int>(warps)));
         } else if constexpr (CLS == 1) {
             if (d.lanes == 1u) {
                 batched_walk_item<CLASSIC>(d, batch, end, lane, mine, tvals);
@@ -578,7 +583,7 @@ uint32_t generate_batched(const nxg_device_asset_desc *assets, const nxg_deforme
     const uint32_t ppt = max_cvs <= 64u ? 2u : 4u;
     // Work-item class of each description, one generate launch per class at
     // its own occupancy: 0 for noisy descriptions on the lane-walk tile, whose
-    // warps need the walk's stage and lattice (ten-warp CTAs fill the SM's
+    // warps need the walk's stage and lattice (eleven-warp CTAs fill the SM's
     // shared memory); 1 for noise-free descriptions; 2 for noisy descriptions
     // on lane-group tiles.
     constexpr uint32_t kClasses = 3u;
@@ -613,19 +618,22 @@ uint32_t generate_batched(const nxg_device_asset_desc *assets, const nxg_deforme
         cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
     }
     // CTA size per class (work items are one 32-strand batch per warp).
-    const size_t class_warp_bytes[kClasses] = {dev::kBatchWalkWarpBytes, dev::kBatchWarpBytes,
-                                               dev::kBatchWarpBytes};
+    auto warp_bytes_of = [](uint32_t c, uint32_t warps) {
+        return c == 0u ? dev::batch_walk_warp_bytes(static_cast<int>(warps)) : dev::kBatchWarpBytes;
+    };
+    size_t class_warp_bytes[kClasses] = {0u, 0u, 0u};
     uint32_t class_block[kClasses] = {0u, 0u, 0u};
     for (uint32_t c = 0; c < kClasses; ++c) {
         cudaFuncAttributes attr{};
         if ((status = record_cuda(cudaFuncGetAttributes(&attr, kernel(c))))) { return status; }
         uint32_t block = std::min(static_cast<uint32_t>(attr.maxThreadsPerBlock) / 32u * 32u,
-                                  c == 0u ? 320u : std::max<uint32_t>(32u, (cfg.block_size + 31u) / 32u * 32u));
-        while (block > 32u &&
-               dev::kBatchHeadBytes + class_warp_bytes[c] * (block / 32u) + 64u > static_cast<size_t>(smem_optin)) {
+                                  c == 0u ? 352u : std::max<uint32_t>(32u, (cfg.block_size + 31u) / 32u * 32u));
+        while (block > 32u && dev::kBatchHeadBytes + warp_bytes_of(c, block / 32u) * (block / 32u) + 64u >
+                                  static_cast<size_t>(smem_optin)) {
             block -= 32u;
         }
         class_block[c] = block;
+        class_warp_bytes[c] = warp_bytes_of(c, block / 32u);
     }
 
     auto *w = static_cast<unsigned char *>(workspace);

@@ -747,15 +747,24 @@ __device__ __forceinline__ float walk_cursor(const ParamArgs &p, const WalkRoot 
         const F3 seg = nxt - cur;
         const F3 ntan = (c + 1 < P && dot(seg, seg) > 0.0f) ? normalize(seg) : tan;
         const F3 axis = cross(tan, ntan);
-        const float cs = fminf(fmaxf(dot(tan, ntan), -1.0f), 1.0f);
-        const float sn = sqrt_approx(fmaf(-cs, cs, 1.0f));
+        // A zero axis leaves the normal as it is: cos 1, sin 0 (then k = 0
+        // and the update below is v itself, exactly).
+        const bool turn = dot(axis, axis) > 0.0f;
+        const float d = fminf(fmaxf(dot(tan, ntan), -1.0f), 1.0f);
+        const float cs = turn ? d : 1.0f;
+        const float sn = turn ? sqrt_approx(fmaf(-d, d, 1.0f)) : 0.0f;
         const float k = (1.0f - cs) * dot(axis, v);
         const F3 axv = cross(axis, v);
-        const F3 rotated = normalize(F3{v.x * cs + axis.x * k + axv.x * sn, v.y * cs + axis.y * k + axv.y * sn,
-                                        v.z * cs + axis.z * k + axv.z * sn});
-        v = dot(axis, axis) > 0.0f ? rotated : v;
-        const F3 bn = cross(v, ntan);
-        const F3 tt = cross(bn, v);
+        v = F3{v.x * cs + axis.x * k + axv.x * sn, v.y * cs + axis.y * k + axv.y * sn,
+               v.z * cs + axis.z * k + axv.z * sn};
+        // The update is linear in v and the reference renormalises after
+        // every step, a positive factor each time: so the transported normal
+        // is the direction of this unnormalised v, which is carried as it is
+        // (each step keeps at least 0.86 of its length, so 32 steps neither
+        // underflow nor overflow) and normalised here for the frame only.
+        const F3 vu = v * rsqrtf(dot(v, v));
+        const F3 bn = cross(vu, ntan);
+        const F3 tt = cross(bn, vu);
         const float distance = __fmul_rn(arc, f_eff);
         const float magnitude = mscale * tvals[c];
         float gx, gy, gz;
@@ -768,7 +777,7 @@ __device__ __forceinline__ float walk_cursor(const ParamArgs &p, const WalkRoot 
             gy = gradient_noise(table, dom.x, __fadd_rn(dom.y, distance), dom.z) - 0.5f;
             gz = gradient_noise(table, dom.x, dom.y, __fadd_rn(dom.z, distance)) - 0.5f;
         }
-        const F3 q = cur + v * (gx * magnitude) + bn * (gy * magnitude) + tt * (gz * magnitude);
+        const F3 q = cur + vu * (gx * magnitude) + bn * (gy * magnitude) + tt * (gz * magnitude);
         if constexpr (PRESERVE) {
             const F3 e = q - previous_point;
             noisy += sqrt_approx(dot(e, e));
