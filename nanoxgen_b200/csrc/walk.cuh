@@ -651,6 +651,19 @@ __device__ __forceinline__ WalkLattice walk_fill_lattice(F3 dom, float span, flo
         wl.kmax[ax] = static_cast<uint32_t>(ax * columns + wl.n[ax] - 2);
     }
     if (!wl.fits) { return wl; }
+    // Columns 0 and 1 of every axis are faces of the unit lattice cube at
+    // floor(dom): its eight corner gradients (corner o = ox + 2 oy + 4 oz)
+    // serve all three axes, the gradients of columns 2.. are looked up.
+    float4 cube[8];
+    {
+        const uint32_t base = static_cast<uint32_t>(wl.lo[0]) * kLcgA2 + static_cast<uint32_t>(wl.lo[1]) * kLcgA +
+                              static_cast<uint32_t>(wl.lo[2]) + kLcgK;
+#pragma unroll
+        for (int o = 0; o < 8; ++o) {
+            cube[o] = table[temper_index(base + ((o & 1) ? kLcgA2 : 0u) + ((o & 2) ? kLcgA : 0u) +
+                                         ((o & 4) ? 1u : 0u))];
+        }
+    }
 #pragma unroll
     for (int ax = 0; ax < 3; ++ax) {
         const int ib = ax == 0 ? 1 : 0;  // the fixed axes, ascending
@@ -678,8 +691,19 @@ __device__ __forceinline__ WalkLattice walk_fill_lattice(F3 dom, float span, flo
             wdb[corner] = wgt[corner] * (wb - static_cast<float>(ob));
             wdc[corner] = wgt[corner] * (wc - static_cast<float>(oc));
         }
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            float A = 0.0f, B = 0.0f;
+#pragma unroll
+            for (int corner = 0; corner < 4; ++corner) {
+                const float4 gr = cube[(k << ax) | ((corner & 1) << ib) | ((corner >> 1) << ic)];
+                A += wgt[corner] * component4(gr, ax);
+                B += component4(gr, ib) * wdb[corner] + component4(gr, ic) * wdc[corner];
+            }
+            lat[(ax * columns + k) * 32] = make_float2(A, B);
+        }
 #pragma unroll 2
-        for (int k = 0; k < wl.n[ax]; ++k) {
+        for (int k = 2; k < wl.n[ax]; ++k) {
             float A = 0.0f, B = 0.0f;
 #pragma unroll
             for (int corner = 0; corner < 4; ++corner) {
@@ -764,7 +788,9 @@ __device__ __forceinline__ float walk_cursor(const ParamArgs &p, const WalkRoot 
         // underflow nor overflow) and normalised here for the frame only.
         const F3 vu = v * rsqrtf(dot(v, v));
         const F3 bn = cross(vu, ntan);
-        const F3 tt = cross(bn, vu);
+        // The frame's third vector cross(bn, vu) is ntan - vu (vu . ntan) for
+        // a unit vu; its part along vu joins vu's coefficient below.
+        const float vn = dot(vu, ntan);
         const float distance = __fmul_rn(arc, f_eff);
         const float magnitude = mscale * tvals[c];
         float gx, gy, gz;
@@ -777,7 +803,8 @@ __device__ __forceinline__ float walk_cursor(const ParamArgs &p, const WalkRoot 
             gy = gradient_noise(table, dom.x, __fadd_rn(dom.y, distance), dom.z) - 0.5f;
             gz = gradient_noise(table, dom.x, dom.y, __fadd_rn(dom.z, distance)) - 0.5f;
         }
-        const F3 q = cur + vu * (gx * magnitude) + bn * (gy * magnitude) + tt * (gz * magnitude);
+        const float gzm = gz * magnitude;
+        const F3 q = cur + vu * fmaf(-gzm, vn, gx * magnitude) + bn * (gy * magnitude) + ntan * gzm;
         if constexpr (PRESERVE) {
             const F3 e = q - previous_point;
             noisy += sqrt_approx(dot(e, e));
