@@ -418,8 +418,11 @@ uint32_t nxg_generate_packed_ordered(const nxg_device_asset_desc *asset,
  * lanes_per_strand 1 (with cvs_per_lane 1, strands of 2..32 CVs) selects the
  * lane-walk generator: base curve and stores lane-parallel, one lane walking
  * each strand's noise frame; with noise and block_size 64 (or below) its
- * CTAs are producer/consumer warp pairs.  It is the built-in choice for
- * 2..32 CVs (320-thread CTAs with noise, 256 without). */
+ * CTAs are producer/consumer warp pairs; with noise, CTAs of eleven warps
+ * keep ten noise-lattice columns per axis and strand, smaller CTAs twelve (a
+ * warp holding a strand whose noise needs more evaluates gradient noise
+ * directly).  It is the built-in choice for 2..32 CVs (352-thread CTAs with
+ * noise, 256 without). */
 typedef struct nxg_tile {
     uint32_t lanes_per_strand;
     uint32_t cvs_per_lane;
@@ -435,8 +438,8 @@ uint32_t nxg_set_tile(uint32_t cvs_per_strand, uint32_t noise, const nxg_tile *t
 uint32_t nxg_get_tile(uint32_t cvs_per_strand, uint32_t noise, nxg_tile *tile);
 
 /* Autotuner: prepares the strand order, then times every admissible tile
- * (lane groups and CVs per lane that hold the strand, CTAs of 64/128/256/320
- * threads) over `repeats` launches of nxg_generate_packed_ordered with CUDA
+ * (lane groups and CVs per lane that hold the strand, CTAs of
+ * 64/128/256/320/352 threads) over `repeats` launches of nxg_generate_packed_ordered with CUDA
  * events on `stream`, registers the fastest with nxg_set_tile and returns
  * it.  It writes the outputs and synchronises the stream, so it is a
  * set-up call, not part of the enqueue-only path. */
