@@ -165,10 +165,12 @@ __device__ __forceinline__ Root walk_root(const AssetArgs &a, const FrameArgs &f
 // takes the fast power; it calls this only for strands whose sum may lie on
 // the other side of the 1e-12 threshold that chooses between blending and the
 // nearest-guide fallback (generate.h:261), so that choice is the reference's
-// (to the last-bit agreement of CUDA's powf with the host's).  Not inlined:
-// the hot path rarely takes it.
-static __device__ __noinline__ float walk_exact_weights(const LaunchArgs &g, uint32_t triangle, F3 position,
-                                                        F3 normal, float *slot_words, int lane) {
+// (to the last-bit agreement of CUDA's powf with the host's).  The hot path
+// rarely takes it: the noise walk calls the out-of-line copy below (inlined
+// it costs that kernel more registers than the call), the noise-free walk
+// this inlined one (the call's saved registers cost it more).
+__device__ __forceinline__ float walk_exact_weights_inline(const LaunchArgs &g, uint32_t triangle, F3 position,
+                                                          F3 normal, float *slot_words, int lane) {
     const AssetArgs &a = g.a;
     const ParamArgs &p = g.p;
     float wsum = 0.0f;
@@ -191,6 +193,11 @@ static __device__ __noinline__ float walk_exact_weights(const LaunchArgs &g, uin
         wsum = __fadd_rn(wsum, w);
     }
     return wsum;
+}
+
+static __device__ __noinline__ float walk_exact_weights(const LaunchArgs &g, uint32_t triangle, F3 position,
+                                                        F3 normal, float *slot_words, int lane) {
+    return walk_exact_weights_inline(g, triangle, position, normal, slot_words, lane);
 }
 
 // Whether a weight sum from the fast power (__powf, within p * 4e-7 + 1e-5
@@ -327,7 +334,11 @@ __device__ __forceinline__ WalkRoot walk_setup(const LaunchArgs &g, float4 *reco
         wsum = __fadd_rn(wsum, w);
     }
     if (!square && blended != 0u && walk_blend_uncertain(wsum, p.weight_power)) {
-        wsum = walk_exact_weights(g, root.triangle, root.position, root.normal, slot_words, lane);
+        if constexpr (NOISE) {
+            wsum = walk_exact_weights(g, root.triangle, root.position, root.normal, slot_words, lane);
+        } else {
+            wsum = walk_exact_weights_inline(g, root.triangle, root.position, root.normal, slot_words, lane);
+        }
     }
     float inv = 0.0f;
     F3 normal_term = {0.0f, 0.0f, 0.0f};
