@@ -410,6 +410,11 @@ __global__ void __launch_bounds__(CLS == 1 ? 256 : 352, CLS == 1 ? 3 : 1)
     const int warp = threadIdx.x >> 5;
     const uint32_t warps = blockDim.x >> 5;
     const uint32_t per_item = warps * batches_per_warp(CLS);
+    // The next class's launch reads nothing this one writes (its own
+    // descriptions' outputs; the strand order and offset tables were done
+    // before this launch began), so it may start as soon as this launch's
+    // CTAs leave SMs free.
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     float4 *table = smem;
     float *tvals = reinterpret_cast<float *>(reinterpret_cast<unsigned char *>(smem) + kBatchTableBytes);
     unsigned char *mine = reinterpret_cast<unsigned char *>(smem) + kBatchHeadBytes + b.warp_bytes[CLS] * warp;
@@ -730,6 +735,7 @@ uint32_t generate_batched(const nxg_device_asset_desc *assets, const nxg_deforme
 
     // One generate launch per class with work, in stream order; each runs
     // persistent CTAs at its own occupancy.
+    bool launched = false;
     for (uint32_t c = 0; c < kClasses; ++c) {
         if (items[c] == 0u) { continue; }
         const void *fn = kernel(c);
@@ -747,7 +753,23 @@ uint32_t generate_batched(const nxg_device_asset_desc *assets, const nxg_deforme
         const uint32_t grid = static_cast<uint32_t>(
             std::min<uint64_t>(items[c], static_cast<uint64_t>(std::max(1, sms * std::max(per_sm, 1)))));
         void *args[] = {&b};
-        if ((status = record_cuda(cudaLaunchKernel(fn, dim3(grid), dim3(block), args, shm, s)))) { return status; }
+        // Every class launch after the first of the frame is a programmatic
+        // dependent of the one before: its CTAs take the SMs that the earlier
+        // class's tail leaves idle.  That is safe because the classes share
+        // no output, and the strand order and offset tables they read were
+        // complete before the first class started.
+        cudaLaunchConfig_t lc{};
+        lc.gridDim = dim3(grid);
+        lc.blockDim = dim3(block);
+        lc.dynamicSmemBytes = shm;
+        lc.stream = s;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = launched ? 1 : 0;
+        lc.attrs = attr;
+        lc.numAttrs = 1;
+        if ((status = record_cuda(cudaLaunchKernelExC(&lc, fn, args)))) { return status; }
+        launched = true;
     }
     return record_cuda(cudaGetLastError());
 }
