@@ -478,13 +478,18 @@ uint64_t nxg_batched_workspace_size(const nxg_device_asset_desc *assets, const n
                                     uint32_t count);
 
 /* Several descriptions -- each its own asset, strand count, CV count (<= 128),
- * stencil and noise settings -- in one persistent generate launch: warps pull
- * (description, 32-strand batch) work items from an atomic counter, costliest
- * descriptions first, and run each with its description's registered tile
- * (nxg_set_tile / nxg_autotune_packed).  Every description is validated as by
- * nxg_validate_packed_request and written as by nxg_generate_packed;
- * `deformed` is NULL or an array of `count`.  Seven launches per call, all
- * enqueue-only (capturable as one graph). */
+ * stencil and noise settings -- in one persistent generate launch per work
+ * class (noisy descriptions on the lane walk, noise-free descriptions, noisy
+ * descriptions on lane-group tiles): CTAs pull (description, strand range)
+ * work items from an atomic counter, costliest descriptions first, and run
+ * each with its description's registered tile (nxg_set_tile /
+ * nxg_autotune_packed).  Each class launch after the first is a programmatic
+ * dependent launch of the one before (the classes share no output), so its
+ * CTAs start on the SMs the earlier class leaves idle.  Every description is
+ * validated as by nxg_validate_packed_request and written as by
+ * nxg_generate_packed; `deformed` is NULL or an array of `count`.  Five
+ * set-up launches plus one per class with work, all enqueue-only (capturable
+ * as one graph, where the chaining becomes programmatic edges). */
 uint32_t nxg_generate_batched(const nxg_device_asset_desc *assets, const nxg_deformed_desc *deformed,
                               const nxg_generation_params *params, const nxg_packed_output_desc *outputs,
                               uint32_t count, const nxg_launch_config *config, void *workspace,
