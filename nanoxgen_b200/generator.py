@@ -274,9 +274,14 @@ class HostPipeline:
     """The reference API's contract -- host asset in, host arrays out
     (generate_packed_cpu, asset.cpp:412-419) -- served by the GPU.
 
-    Each run() uploads the asset from pinned memory, generates the strands
-    in `chunks` ranges on a compute stream and copies every finished range to
-    pinned host arrays on a copy stream, so readback overlaps generation."""
+    Each run() uploads the asset from pinned memory on an upload stream,
+    generates the strands in `chunks` ranges on a compute stream and copies
+    every finished range to pinned host arrays on a copy stream.  Readback
+    overlaps generation, and a run's upload and generation overlap the
+    previous run's readback: a range is regenerated once its previous
+    readback is done, and the asset is replaced once the previous run's
+    generation no longer reads it.  The readback (device to host) and the
+    upload (host to device) use the two directions of the link."""
 
     def __init__(self, asset: Asset, params: GenerationParams, radius_scale: float = 1.0, chunks: int = 8,
                  device: str | torch.device = "cuda", first_strand: int = 0, count: Optional[int] = None):
@@ -294,9 +299,11 @@ class HostPipeline:
         self.host_counts = torch.empty(self.point_counts.shape, dtype=torch.int32, pin_memory=True)
         self.compute = torch.cuda.Stream(device)
         self.copy = torch.cuda.Stream(device)
+        self.upload = torch.cuda.Stream(device)
         bounds = np.linspace(0, self.count, max(1, chunks) + 1).astype(np.int64)
         self.ranges = [(int(a), int(b)) for a, b in zip(bounds[:-1], bounds[1:]) if b > a]
-        self.events = [torch.cuda.Event() for _ in self.ranges]
+        self.events = [torch.cuda.Event() for _ in self.ranges]      # range generated
+        self.read_back = [None for _ in self.ranges]                 # range copied out (previous run)
         for a, b in self.ranges:
             self.dasset.workspace(params, b - a)
 
@@ -312,10 +319,14 @@ class HostPipeline:
         """Enqueue one full upload -> generate -> readback; returns without
         synchronising (wait on `self.copy`)."""
         P = int(self.params.cvs_per_strand)
-        with torch.cuda.stream(self.compute):
-            self.compute.wait_stream(self.copy)  # previous readback done with the outputs
+        with torch.cuda.stream(self.upload):
+            self.upload.wait_stream(self.compute)  # the previous run's generation is done with the asset
             self.dasset.tensor.copy_(self.pinned_asset, non_blocking=True)
-            for (a, b), ev in zip(self.ranges, self.events):
+        with torch.cuda.stream(self.compute):
+            self.compute.wait_stream(self.upload)
+            for i, ((a, b), ev) in enumerate(zip(self.ranges, self.events)):
+                if self.read_back[i] is not None:
+                    self.compute.wait_event(self.read_back[i])  # previous readback done with this range
                 n = b - a
                 generate_packed(self.dasset, self.params, self.radius_scale, first_strand=self.first + a,
                                 count=n, points=self.points[a * P:b * P], roots=self.roots[a:b],
@@ -323,12 +334,15 @@ class HostPipeline:
                                 stream=self.compute)
                 ev.record(self.compute)
         with torch.cuda.stream(self.copy):
-            for (a, b), ev in zip(self.ranges, self.events):
+            for i, ((a, b), ev) in enumerate(zip(self.ranges, self.events)):
                 self.copy.wait_event(ev)
                 self.host_points[a * P:b * P].copy_(self.points[a * P:b * P], non_blocking=True)
                 self.host_roots[a:b].copy_(self.roots[a:b], non_blocking=True)
                 self.host_uvs[a:b].copy_(self.root_uvs[a:b], non_blocking=True)
                 self.host_counts[a:b].copy_(self.point_counts[a:b], non_blocking=True)
+                done = torch.cuda.Event()
+                done.record(self.copy)
+                self.read_back[i] = done
 
 
 def set_tile(cvs_per_strand: int, noise: bool, lanes: int = 0, cvs_per_lane: int = 0, block_size: int = 0) -> None:

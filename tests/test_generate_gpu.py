@@ -413,3 +413,23 @@ def test_every_tile_matches_oracle_and_autotuner(torch_cuda, oracle, sphere):
         _compare(asset, w.params, _gen(torch_cuda, d, w.params), theirs)
     finally:
         set_tile(P, True)
+
+
+def test_host_pipeline_runs_match_direct_generation(torch_cuda, sphere):
+    """HostPipeline (host asset in, host arrays out, ranges read back while
+    later ranges generate, a run's upload and generation under the previous
+    run's readback): two consecutive runs leave exactly the arrays that one
+    direct generation of the whole request produces."""
+    from nanoxgen_b200.generator import HostPipeline
+    w, asset = sphere
+    params = w.params.copy(strand_count=20000)
+    pts, roots, uvs, counts = _gen(torch_cuda, asset, params)
+    pipe = HostPipeline(asset, params, 1.0, chunks=5, device="cuda")
+    for _ in range(2):
+        pipe.run()
+    torch_cuda.cuda.synchronize()
+    assert np.array_equal(pipe.host_points.numpy(), pts)
+    assert np.array_equal(pipe.host_roots.numpy().reshape(-1).view(np.uint8),
+                          np.ascontiguousarray(roots).reshape(-1).view(np.uint8))
+    assert np.array_equal(pipe.host_uvs.numpy(), uvs)
+    assert np.array_equal(pipe.host_counts.numpy().view(np.uint32), counts)
