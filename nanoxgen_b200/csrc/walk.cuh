@@ -774,7 +774,10 @@ __device__ __forceinline__ float walk_cursor(const ParamArgs &p, const WalkRoot 
     float arc = 0.0f;
 #pragma unroll 2
     for (int c = 0; c < P; ++c) {
-        const F3 further = c + 3 < P ? base(c + 3) : ahead;
+        // Past the strand's end the look-ahead repeats the last CV, which is
+        // what `ahead` and `nxt` already hold there (the tip's tangent does
+        // not read it).
+        const F3 further = base(min(c + 3, P - 1));
         arc = __fadd_rn(arc, walk_segment_length(cur, previous_base));
         // The reference's length_squared(segment) > 0 holds exactly when some
         // component's square does not round to zero: the same test on the
