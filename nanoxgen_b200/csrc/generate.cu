@@ -135,13 +135,13 @@ __global__ void __launch_bounds__(NOISE ? 384 : 256, NOISE ? 1 : (CLASSIC ? 2 : 
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const int columns = walk_lattice_columns(warps);
-    const size_t kWarpBytes = walk_warp_bytes(kWalk, kStaged, columns);
-    unsigned char *mine = warp_base + kWarpBytes * warp;
+    const size_t warp_bytes = walk_warp_bytes(kWalk, kStaged, columns);
+    unsigned char *mine = warp_base + warp_bytes * warp;
     float *stage = reinterpret_cast<float *>(mine);  // staged variants only
     float4 *records = reinterpret_cast<float4 *>(kStaged ? mine + kWalkStageBytes : mine);
     float2 *lattice = reinterpret_cast<float2 *>(mine + kWalkStageBytes);
     float4 *scratch = reinterpret_cast<float4 *>(mine + kWalkRecordBytes);  // plain Classic variant only
-    uint32_t *locals = reinterpret_cast<uint32_t *>(mine + kWarpBytes - kWalkLocalBytes);
+    uint32_t *locals = reinterpret_cast<uint32_t *>(mine + warp_bytes - kWalkLocalBytes);
     const float inv_p = 1.0f / static_cast<float>(P);
     const uint32_t span = g.range_end - g.range_begin;
     const uint32_t begin = g.range_begin + static_cast<uint32_t>(static_cast<uint64_t>(blockIdx.x) * span / gridDim.x);

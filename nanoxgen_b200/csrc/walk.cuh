@@ -632,10 +632,9 @@ __device__ __forceinline__ float walk_lattice_delta(const float2 *lat, uint32_t 
 // X + 1 (the walk's noise coordinates d0 + arc * f are computed in the same
 // IEEE operations as d0 + span, so none passes it).  `lat` is this lane's
 // column 0 of axis 0; column k of axis a is at lat[(a * columns + k) * 32].
-// fits is false when a strand needs
-// more columns than the lattice holds, or coordinates beyond the round-down
-// floor's range (it then takes direct noise).  bias and kmax are the
-// per-axis arguments of walk_lattice_delta.
+// fits is false when a strand needs more columns than the lattice holds, or
+// has coordinates beyond the round-down floor's range (it then takes direct
+// noise).  bias and kmax are the per-axis arguments of walk_lattice_delta.
 struct WalkLattice {
     int lo[3], n[3];
     uint32_t bias[3], kmax[3];
