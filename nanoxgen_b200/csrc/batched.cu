@@ -316,7 +316,6 @@ __device__ __noinline__ void batched_noise_walk_item(const BatchDesc &d, uint32_
     const uint32_t item = batch + static_cast<uint32_t>(lane);
     const bool valid = item < end;
     const int in_batch = static_cast<int>(end - batch);
-    const float inv_p = 1.0f / static_cast<float>(P);
     const WalkRoot wr = walk_setup<true>(d.g, records, locals, lane, valid ? item : batch, valid,
                                          static_cast<uint32_t>(P));
     __syncwarp();
@@ -326,7 +325,9 @@ __device__ __noinline__ void batched_noise_walk_item(const BatchDesc &d, uint32_
                columns);
     __syncwarp();
     if (CLASSIC && d.g.scalars != nullptr) {
-        walk_store<true>(d.g, stage, locals, rvals, lane, in_batch, P, inv_p);
+        walk_classic_strand(d.g, records, stage, locals, lane, in_batch, P);
+        __syncwarp();
+        walk_store8_classic(d.g, records, stage, locals, rvals, lane, in_batch, P);
     } else {
         walk_store8(d.g, stage, locals, rvals, lane, in_batch, P);
     }

@@ -142,7 +142,6 @@ __global__ void __launch_bounds__(NOISE ? 384 : 256, NOISE ? 1 : (CLASSIC ? 2 : 
     float2 *lattice = reinterpret_cast<float2 *>(mine + kWalkStageBytes);
     float4 *scratch = reinterpret_cast<float4 *>(mine + kWalkRecordBytes);  // plain Classic variant only
     uint32_t *locals = reinterpret_cast<uint32_t *>(mine + warp_bytes - kWalkLocalBytes);
-    const float inv_p = 1.0f / static_cast<float>(P);
     const uint32_t span = g.range_end - g.range_begin;
     const uint32_t begin = g.range_begin + static_cast<uint32_t>(static_cast<uint64_t>(blockIdx.x) * span / gridDim.x);
     const uint32_t end =
@@ -172,7 +171,9 @@ __global__ void __launch_bounds__(NOISE ? 384 : 256, NOISE ? 1 : (CLASSIC ? 2 : 
         }
         if constexpr (kStaged) {
             if constexpr (CLASSIC) {
-                walk_store<true>(g, stage, locals, rvals, lane, in_batch, P, inv_p);
+                walk_classic_strand(g, records, stage, locals, lane, in_batch, P);
+                __syncwarp();
+                walk_store8_classic(g, records, stage, locals, rvals, lane, in_batch, P);
             } else {
                 walk_store8(g, stage, locals, rvals, lane, in_batch, P);
             }
@@ -261,7 +262,7 @@ __global__ void __launch_bounds__(64, 1) generate_pipe_kernel(LaunchArgs g, cons
             walk_frame(g.p, wr, lane < in_batch, stage + lane * kWalkRowFloats, lattice + lane, tvals, table, P,
                        kWalkAxisColumns);
             __syncwarp();
-            walk_store<false>(g, stage, locals, rvals, lane, in_batch, P, inv_p);
+            walk_store8(g, stage, locals, rvals, lane, in_batch, P);
             if (it + 2u < iterations) { named_arrive(3u + b); }
         }
     }

@@ -15,9 +15,10 @@
 //                           lane carries it CV by CV with the reference's
 //                           rotation applied as a vector update, and no
 //                           matrix products or cross-lane scans are needed;
-//   store  (lane = CV)      the strand's float4s as coalesced streaming
-//                           stores, with the Classic application when
-//                           per-root scalars are given.
+//   store  (8 lanes/strand) the strands' float4s as coalesced streaming
+//                           stores; with per-root Classic scalars, a step
+//                           with lane = strand first takes each strand's
+//                           Classic values (scale, width, drop rule) once.
 //
 // Stage rows are 97 words apart and a CV takes 3 words; both strides are odd,
 // so a warp reading column c of 32 rows (frame step) and a warp reading one
@@ -899,49 +900,6 @@ constexpr size_t kPipeBufferBytes = kWalkStageBytes + kPipeFrameBytes + kWalkLoc
 constexpr size_t kPipeSmemBytes = sizeof(float4) * kTableFloat4 + 2u * sizeof(float) * kWalkMaxCvs +
                                   2u * kPipeBufferBytes + kWalkRecordBytes + kWalkLatticeBytes;
 
-// Store step: item = s * P + c; the Classic application (scale about the
-// first point, width override, drop rule) as in emit_strand.
-template <bool CLASSIC>
-__device__ __forceinline__ void walk_store(const LaunchArgs &g, const float *stage, const uint32_t *locals,
-                                           const float *rvals, int lane, int in_batch, int P, float inv_p) {
-    const ParamArgs &p = g.p;
-    const int items = in_batch * P;
-    for (int item = lane; item < items; item += 32) {
-        const int s = walk_strand(item, inv_p);
-        const int c = item - s * P;
-        const uint32_t word = locals[s];
-        if (word >> 31) { continue; }
-        const float *row = stage + s * kWalkRowFloats;
-        const F3 point = stage_get(row, c);
-        float4 q = make_float4(point.x, point.y, point.z, rvals[c]);
-        if constexpr (CLASSIC) {
-            const float2 sc = __ldg(g.scalars + word);
-            const F3 front = stage_get(row, 0);
-            const F3 back = stage_get(row, P - 1);
-            const float scale = g.classic_length ? sc.x : 1.0f;
-            const float raw_width = g.classic_width ? sc.y
-                : (p.radius_scale > 0.0f ? __fdiv_rn(__fmul_rn(2.0f, strand_radius(p, 0.0f)), p.radius_scale) : 0.0f);
-            bool keep = !(raw_width < 1.0e-4f);
-            const F3 chord = back - front;
-            if (keep && !(sqrtf(dot(chord, chord)) * scale > 1.01e-4f)) {
-                keep = !(__fmul_rn(classic_spline_length_by([row](int i) { return stage_get(row, i); }, P), scale) <
-                         1.0e-4f);
-            }
-            if (g.classic_length) {
-                const F3 v = xadd(front, xmul(xsub(xyz(q), front), scale));
-                q.x = v.x;
-                q.y = v.y;
-                q.z = v.z;
-            }
-            if (g.classic_width) {
-                q.w = __fmul_rn(__fmul_rn(0.5f, raw_width < 0.0f ? 0.0f : raw_width), p.radius_scale);
-            }
-            if (!keep && c == 0 && g.point_counts != nullptr) { g.point_counts[word] = 0u; }
-        }
-        walk_emit(g, word, P, c, q);
-    }
-}
-
 // Store step without Classic scalars, eight lanes per strand as in
 // walk_base_direct: lane (s = pass * 4 + lane / 8, c = lane % 8) stores CVs
 // c + 8m of its strand's staged row, so each store instruction writes four
@@ -965,6 +923,67 @@ __device__ __forceinline__ void walk_store8(const LaunchArgs &g, const float *st
             if (m < cpl && cm < P) {
                 const F3 q = stage_get(row, cm);
                 walk_emit(g, word, P, cm, make_float4(q.x, q.y, q.z, rv[m]));
+            }
+        }
+    }
+}
+
+// The Classic application's per-strand values for the noisy walk, once per
+// strand after the walk (lane = strand; the rules of emit_strand: scale about
+// the first point, width override, the drop rule with its chord bound and
+// sampled-spline measure): records 6 and 7 take (first point, length scale)
+// and (width radius); a dropped strand's point count becomes 0.  The records
+// are free again once the walk is done (the lattice aliased them).  Every
+// lane of the warp calls it.
+__device__ __forceinline__ void walk_classic_strand(const LaunchArgs &g, float4 *records, const float *stage,
+                                                    const uint32_t *locals, int lane, int in_batch, int P) {
+    const ParamArgs &p = g.p;
+    const uint32_t word = locals[lane];
+    if (lane >= in_batch || (word >> 31)) { return; }
+    const float *row = stage + lane * kWalkRowFloats;
+    const float2 sc = __ldg(g.scalars + word);
+    const F3 front = stage_get(row, 0);
+    const F3 back = stage_get(row, P - 1);
+    const float scale = g.classic_length ? sc.x : 1.0f;
+    const float raw_width = g.classic_width ? sc.y
+        : (p.radius_scale > 0.0f ? __fdiv_rn(__fmul_rn(2.0f, strand_radius(p, 0.0f)), p.radius_scale) : 0.0f);
+    bool keep = !(raw_width < 1.0e-4f);
+    const F3 chord = back - front;
+    if (keep && !(sqrtf(dot(chord, chord)) * scale > 1.01e-4f)) {
+        keep = !(__fmul_rn(classic_spline_length_by([row](int i) { return stage_get(row, i); }, P), scale) <
+                 1.0e-4f);
+    }
+    records[6 * 32 + lane] = make_float4(front.x, front.y, front.z, scale);
+    records[7 * 32 + lane] =
+        make_float4(__fmul_rn(__fmul_rn(0.5f, raw_width < 0.0f ? 0.0f : raw_width), p.radius_scale), 0.0f, 0.0f, 0.0f);
+    if (!keep && g.point_counts != nullptr) { g.point_counts[word] = 0u; }
+}
+
+// Store step with the Classic application of records 6 and 7
+// (walk_classic_strand), eight lanes per strand as in walk_store8.  Every
+// lane of the warp calls it.
+__device__ __forceinline__ void walk_store8_classic(const LaunchArgs &g, const float4 *records, const float *stage,
+                                                    const uint32_t *locals, const float *rvals, int lane,
+                                                    int in_batch, int P) {
+    constexpr int kPerLane = kWalkMaxCvs / 8;
+    const int c = lane & 7;
+    const int cpl = (P + 7) >> 3;
+    float rv[kPerLane];
+#pragma unroll
+    for (int m = 0; m < kPerLane; ++m) { rv[m] = rvals[min(c + 8 * m, P - 1)]; }
+    for (int first = 0; first < in_batch; first += 4) {
+        const int s = first + (lane >> 3);  // at most 31
+        const uint32_t word = s < in_batch ? locals[s] : 0x80000000u;
+        const float *row = stage + s * kWalkRowFloats;
+        const float4 front = records[6 * 32 + s];
+        const float width = records[7 * 32 + s].x;
+#pragma unroll
+        for (int m = 0; m < kPerLane; ++m) {
+            const int cm = c + 8 * m;
+            if (m < cpl && cm < P) {
+                F3 q = stage_get(row, cm);
+                if (g.classic_length) { q = xadd(xyz(front), xmul(xsub(q, xyz(front)), front.w)); }
+                walk_emit(g, word, P, cm, make_float4(q.x, q.y, q.z, g.classic_width ? width : rv[m]));
             }
         }
     }
